@@ -1,0 +1,155 @@
+"""cress_b200: B200 (sm_100a) implementation of CReSS's solver time integration.
+
+This module is the host-side mirror of the reference's call interface
+(the Fortran module procedures s_smalldrv, s_hevi, ... of SrcOrig/), bound
+through ctypes to the C-ABI library built from cress_b200/csrc
+(declarations: include/cress_b200.h).  Arrays cross the boundary as
+float32 numpy arrays in the reference layout a(0:ni+1, 0:nj+1, 1:nk), i.e.
+numpy shape (nk, nj+2, ni+2) in C order (x fastest).
+
+There is no CPU fallback: if the shared library is missing or cannot be
+loaded, every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libcress_b200.so")
+
+# Field and level ids (include/cress_b200.h: enum cress_field / cress_level).
+FIELDS = ["u", "v", "w", "pp", "ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+PAST, NOW, FUTURE, FORCING = 0, 1, 2, 3
+# enum cress_base order
+BASE_NAMES = ["jcb", "jcb8u", "jcb8v", "jcb8w", "rbr", "ptbr", "rst", "rst8u", "rst8v",
+              "rst8w", "rcsq"]
+
+ERRORS = {1: "CRESS_E_ARG", 2: "CRESS_E_UNSUPPORTED", 3: "CRESS_E_CUDA",
+          4: "CRESS_E_NONUNIFORM", 5: "CRESS_E_NONFINITE", 6: "CRESS_E_TIMEOUT",
+          7: "CRESS_E_STATE"}
+
+
+class CressError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Cfg(ctypes.Structure):
+    """cress_cfg: resolved namelist values."""
+    _fields_ = [("ni", ctypes.c_int), ("nj", ctypes.c_int), ("nk", ctypes.c_int),
+                ("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float),
+                ("sthopt", ctypes.c_int), ("impopt", ctypes.c_int), ("divopt", ctypes.c_int),
+                ("buyopt", ctypes.c_int), ("gwmopt", ctypes.c_int), ("weicoe", ctypes.c_float),
+                ("wbc", ctypes.c_int), ("ebc", ctypes.c_int), ("sbc", ctypes.c_int),
+                ("nbc", ctypes.c_int), ("bbc", ctypes.c_int), ("tbc", ctypes.c_int),
+                ("tile", ctypes.c_int), ("reserved", ctypes.c_int * 16)]
+
+
+_lib = None
+_FP = ctypes.POINTER(ctypes.c_float)
+
+
+def lib():
+    """Load the C-ABI library (raises if it is absent: no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing; run `python -m cress_b200.build` "
+                           "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.cress_last_error.restype = ctypes.c_char_p
+    L.cress_abi_version.restype = ctypes.c_int
+    L.cress_create.argtypes = [ctypes.POINTER(Cfg), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.cress_destroy.argtypes = [ctypes.c_void_p]
+    L.cress_destroy.restype = None
+    L.cress_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.cress_sync.argtypes = [ctypes.c_void_p]
+    L.cress_set_base3d.argtypes = [ctypes.c_void_p, ctypes.POINTER(_FP)]
+    L.cress_put_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _FP]
+    L.cress_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _FP]
+    L.cress_small_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]
+    L.cress_smalldrv.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float] + [_FP] * 12
+    L.cress_launch_count.argtypes = [ctypes.c_void_p]
+    L.cress_launch_count.restype = ctypes.c_longlong
+    _lib = L
+    return L
+
+
+def _check(code):
+    if code != 0:
+        raise CressError(code, lib().cress_last_error().decode())
+
+
+def fptr(a):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_FP)
+
+
+class Solver:
+    """One domain on one GPU (a cress_ctx)."""
+
+    def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6,
+                 tile=0, device=0):
+        L = lib()
+        c = Cfg()
+        c.ni, c.nj, c.nk = ni, nj, nk
+        c.dx, c.dy, c.dz = dx, dy, dz
+        c.sthopt, c.impopt, c.divopt, c.buyopt, c.gwmopt = sthopt, 1, divopt, buyopt, 0
+        c.weicoe = weicoe
+        c.wbc = c.ebc = c.sbc = c.nbc = -1
+        c.bbc = c.tbc = 2
+        c.tile = tile
+        self.cfg = c
+        self.shape = (nk, nj + 2, ni + 2)
+        h = ctypes.c_void_p()
+        _check(L.cress_create(ctypes.byref(c), device, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cress_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_stream(self, stream_ptr):
+        _check(lib().cress_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def sync(self):
+        _check(lib().cress_sync(self._h))
+
+    def set_base3d(self, base):
+        arrs = [np.ascontiguousarray(base[n], dtype=np.float32) for n in BASE_NAMES]
+        for a in arrs:
+            assert a.shape == self.shape, (a.shape, self.shape)
+        ptrs = (_FP * len(arrs))(*[fptr(a) for a in arrs])
+        _check(lib().cress_set_base3d(self._h, ptrs))
+
+    def put_field(self, name, level, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        assert a.shape == self.shape
+        _check(lib().cress_put_field(self._h, FIELD_ID[name], level, fptr(a)))
+
+    def get_field(self, name, level):
+        a = np.empty(self.shape, np.float32)
+        _check(lib().cress_get_field(self._h, FIELD_ID[name], level, fptr(a)))
+        return a
+
+    def small_steps(self, nsstp, dts):
+        _check(lib().cress_small_steps(self._h, int(nsstp), float(dts)))
+
+    def smalldrv(self, nsstp, dts, up, vp, wp, ppp, ufrc, vfrc, wfrc, pfrc, out=None):
+        """s_smalldrv with host arrays (SrcOrig/smalldrv.f90:343-398)."""
+        ins = [np.ascontiguousarray(a, dtype=np.float32) for a in
+               (up, vp, wp, ppp, ufrc, vfrc, wfrc, pfrc)]
+        outs = out if out is not None else [np.empty(self.shape, np.float32) for _ in range(4)]
+        _check(lib().cress_smalldrv(self._h, int(nsstp), float(dts),
+                                    *[fptr(a) for a in ins], *[fptr(a) for a in outs]))
+        return outs
+
+    def launch_count(self):
+        return lib().cress_launch_count(self._h)

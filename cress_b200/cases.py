@@ -1,0 +1,143 @@
+"""Synthetic idealized cases: base state columns and initial perturbations.
+
+The reference builds its base state on the host during s_inivar
+(SrcOrig/inivar.f90:611-850): sounding -> hydrostatic 1-D profile (set1d)
+-> 3-D base arrays (setbase, baserho, sndwave) and passes them to the
+solver.  The C-ABI receives those arrays; this module produces them for
+standalone runs and benchmarks, horizontally uniform (flat terrain), in the
+reference layout a(0:ni+1, 0:nj+1, 1:nk) = numpy (nk, nj+2, ni+2).
+
+Rules followed:
+  rst = |jcb| * rbr                       SrcOrig/baserho.f90:160
+  rst8w(k) = .5*(rst(k-1)+rst(k)), bc8w   SrcOrig/var8uvw.f90:190-196, SrcOrig/bc8w.f90:130-184
+  rcsq = cp/cv * pbr                      SrcOrig/sndwave.f90:119
+  rbr = pbr / (rd * ptvbr * pibr)         SrcOrig/setbase.f90:177-182
+"""
+import numpy as np
+
+G, CP, CV, RD, RV, P0 = 9.8, 1004.0, 717.0, 287.0, 461.0, 1.0e5
+BASE_NAMES = ["jcb", "jcb8u", "jcb8v", "jcb8w", "rbr", "ptbr", "rst", "rst8u", "rst8v",
+              "rst8w", "rcsq"]
+
+
+def dims(nx, ny, nz):
+    """Array dims of an nx x ny x nz interior (SrcOrig/setdim.f90:196-199)."""
+    return nx + 3, ny + 3, nz + 3
+
+
+def stretched_jcb(nk, dz, dzmin):
+    """Jacobian jcb(k) = dz_k/dz of a tanh-stretched grid with the lowest
+    layer dzmin and mean spacing dz (top = dz*(nk-3))."""
+    k = np.arange(nk + 1, dtype=np.float64)
+    n = nk - 3
+    s = np.linspace(0.0, 1.0, n)
+    w = dzmin / dz + (2.0 - 2.0 * dzmin / dz) * s  # linear ramp, mean 1
+    jcb = np.ones(nk + 1)
+    jcb[2:2 + n] = w
+    jcb[1] = jcb[2]
+    jcb[nk - 1:] = jcb[nk - 2]
+    return jcb
+
+
+def base_columns(nk, dz, sthopt=0, dzmin=None, theta_sfc=300.0, dthdz=0.0, qv_sfc=0.0):
+    """1-D base columns (index k = 1..nk) of a hydrostatic profile integrated
+    in FP64 (Exner form) with theta(z) = theta_sfc + dthdz*z."""
+    if sthopt:
+        jcb = stretched_jcb(nk, dz, dzmin if dzmin else 0.4 * dz)
+    else:
+        jcb = np.ones(nk + 1)
+    zw = np.zeros(nk + 1)
+    for k in range(3, nk + 1):
+        zw[k] = zw[k - 1] + jcb[k - 1] * dz
+    zw[2] = 0.0
+    zs = np.zeros(nk + 1)
+    zs[1:nk] = 0.5 * (zw[1:nk] + zw[2:nk + 1])
+    zs[1] = -zs[2]
+    zs[nk] = zs[nk - 1] + jcb[nk - 1] * dz
+    theta = theta_sfc + dthdz * zs
+    # Exner integration d(pi)/dz = -g/(cp*theta), FP64 trapezoid from the surface
+    pi = np.ones(nk + 1)
+    pi_s = 1.0
+    for k in range(1, nk + 1):
+        pi[k] = pi_s - G * zs[k] / (CP * 0.5 * (theta_sfc + theta[k])) if dthdz else \
+            pi_s - G * zs[k] / (CP * theta_sfc)
+    pbr = P0 * pi ** (CP / RD)
+    ptv = theta
+    rbr = pbr / (RD * ptv * pi)
+    f32 = lambda a: np.asarray(a, np.float32)
+    c = {"jcb": f32(jcb), "ptbr": f32(theta), "pbr": f32(pbr), "rbr": f32(rbr),
+         "zs": zs}
+    c["rst"] = (np.abs(c["jcb"]) * c["rbr"]).astype(np.float32)
+    c["rcsq"] = (np.float32(CP / CV) * c["pbr"]).astype(np.float32)
+    for name in ("jcb", "rst"):
+        v8w = np.zeros(nk + 1, np.float32)
+        for k in range(2, nk):
+            v8w[k] = np.float32(0.5) * (c[name][k - 1] + c[name][k])
+        v8w[1] = v8w[3]
+        v8w[nk] = v8w[nk - 2]
+        c[name + "8w"] = v8w
+        c[name + "8u"] = (np.float32(0.5) * (c[name] + c[name])).astype(np.float32)
+        c[name + "8v"] = c[name + "8u"].copy()
+    return c
+
+
+def expand(colk, ni, nj, nk):
+    a = np.empty((nk, nj + 2, ni + 2), np.float32)
+    a[:] = np.asarray(colk, np.float32)[1:nk + 1, None, None]
+    return a
+
+
+def base3d(ni, nj, nk, dz, **kw):
+    c = base_columns(nk, dz, **kw)
+    return {n: expand(c[n], ni, nj, nk) for n in BASE_NAMES + ["pbr"]}, c
+
+
+def bcycle(a, stag):
+    """Periodic wrap of SrcOrig/bcycle.f90:159-225 (plus the identity of the
+    duplicated face u(ni-1)=u(2), v(nj-1)=v(2) of a periodic domain)."""
+    nk, nj2, ni2 = a.shape
+    ni, nj = ni2 - 2, nj2 - 2
+    if stag == "u":
+        a[:, :, ni - 1] = a[:, :, 2]
+        a[:, :, 1] = a[:, :, ni - 2]
+        a[:, :, ni] = a[:, :, 3]
+    else:
+        a[:, :, 1] = a[:, :, ni - 2]
+        a[:, :, ni - 1] = a[:, :, 2]
+    if stag == "v":
+        a[:, nj - 1, :] = a[:, 2, :]
+        a[:, 1, :] = a[:, nj - 2, :]
+        a[:, nj, :] = a[:, 3, :]
+    else:
+        a[:, 1, :] = a[:, nj - 2, :]
+        a[:, nj - 1, :] = a[:, 2, :]
+    return a
+
+
+def _noise(rng, shape, amp):
+    x = rng.standard_normal(shape)
+    for ax in (1, 2):
+        x = (x + np.roll(x, 1, ax) + np.roll(x, -1, ax)) / 3.0
+    return (amp * x / (np.abs(x).max() + 1e-30)).astype(np.float32)
+
+
+def acoustic_case(nx, ny, nz, dx, dz, seed=0, sthopt=1):
+    """A perturbed dry state for the small step: past-level u, v, w, p' and
+    the large-step forcings ufrc, vfrc, wfrc, pfrc (seeded, periodic)."""
+    ni, nj, nk = dims(nx, ny, nz)
+    base, cols = base3d(ni, nj, nk, dz, sthopt=sthopt, dthdz=0.003)
+    rng = np.random.default_rng(seed)
+    shp = (nk, nj + 2, ni + 2)
+    u = _noise(rng, shp, 6.0) + np.float32(8.0)
+    v = _noise(rng, shp, 6.0) - np.float32(2.0)
+    w = _noise(rng, shp, 1.5)
+    pp = _noise(rng, shp, 40.0)
+    w[1] = 0.0
+    w[nk - 2] = 0.0
+    rst = base["rst"]
+    frc = [_noise(rng, shp, 2e-3) * rst, _noise(rng, shp, 2e-3) * rst,
+           _noise(rng, shp, 4e-3) * rst, _noise(rng, shp, 0.3)]
+    st = [u, v, w, pp]
+    for a, t in zip(st + frc, ["u", "v", "s", "s", "u", "v", "s", "s"]):
+        bcycle(a, t)
+    return (ni, nj, nk), base, st, frc

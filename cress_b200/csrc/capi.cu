@@ -1,0 +1,359 @@
+// C-ABI implementation: contexts, device-resident state, host syncs and the
+// small-step driver.  Declarations and the reference interface each entry
+// point replaces are in include/cress_b200.h.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+#include "../../include/cress_b200.h"
+#include "common.cuh"
+#include "ctx.h"
+#include "hevi.cuh"
+
+namespace cress {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return CRESS_OK;
+  return set_error(CRESS_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Physical constants used on the host side (SrcOrig/comphy.f90:49,61,64,459).
+static const float kG = 9.8f, kCp = 1004.f, kCv = 717.f, kDivndc = 0.05f;
+
+float* Ctx::alloc_field() {
+  float* p = nullptr;
+  if (cudaMalloc(&p, sizeof(float) * (size_t)g.count()) != cudaSuccess) return nullptr;
+  cudaMemsetAsync(p, 0, sizeof(float) * (size_t)g.count(), stream);
+  owned.push_back(p);
+  return p;
+}
+
+Ctx::~Ctx() {
+  cudaSetDevice(device);
+  for (void* p : owned) cudaFree(p);
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+int Ctx::put_host(float* dst, const float* host) {
+  const size_t wbytes = sizeof(float) * (size_t)(g.ni + 2);
+  const size_t rows = (size_t)(g.nj + 2) * (size_t)g.nk;
+  return cuda_check(cudaMemcpy2DAsync(dst, sizeof(float) * g.px, host, wbytes, wbytes, rows,
+                                      cudaMemcpyHostToDevice, stream),
+                    "host->device copy");
+}
+
+int Ctx::get_host(float* host, const float* src) {
+  const size_t wbytes = sizeof(float) * (size_t)(g.ni + 2);
+  const size_t rows = (size_t)(g.nj + 2) * (size_t)g.nk;
+  return cuda_check(cudaMemcpy2DAsync(host, wbytes, src, sizeof(float) * g.px, wbytes, rows,
+                                      cudaMemcpyDeviceToHost, stream),
+                    "device->host copy");
+}
+
+// Coefficients of the w tridiagonal system of s_stepwi for buyopt=0/1
+// (SrcOrig/stepwi.f90:308-416), formed in float exactly as the reference
+// does for a horizontally uniform base state, followed by the
+// elimination factors of s_gaussel impopt=1 (SrcOrig/gaussel.f90:189-240)
+// in double.  They depend on dts only through sbsqzi/sbsqg5.
+int Ctx::thomas_for(float dts, const ThomasSet** out) {
+  uint32_t key;
+  std::memcpy(&key, &dts, 4);
+  auto it = thomas.find(key);
+  if (it != thomas.end()) { *out = &it->second; return CRESS_OK; }
+  const int nk = g.nk;
+  auto C = [&](int f, int k) { return col_h[(size_t)f * (nk + 1) + k]; };
+  const float dziv = 1.f / cfg.dz, weicoe = cfg.weicoe;
+  const float g05 = .5f * kG;
+  const float sbsqzi = dts * dts * weicoe * weicoe * dziv;
+  const float sbsqg5 = .5f * kG * dts * dts * weicoe * weicoe;
+  std::vector<float> fwc(nk + 2, 0.f), wcc(nk + 2, 0.f), rr(nk + 2, 0.f), ss(nk + 2, 0.f),
+      tt(nk + 2, 0.f);
+  for (int k = 2; k <= nk - 2; ++k) {
+    float t1 = g05 * C(C_RBR, k) / C(C_RCSQ, k);
+    float t2 = dziv / C(C_JCB, k);
+    fwc[k] = t1 + t2;
+    wcc[k] = t1 - t2;
+  }
+  for (int k = 3; k <= nk - 2; ++k) {
+    if (cfg.buyopt == 0) {
+      float a = sbsqzi / C(C_RST8W, k);
+      float mm = a * C(C_RCSQ, k - 1);
+      float nn = a * C(C_RCSQ, k);
+      rr[k] = -mm * fwc[k - 1];
+      ss[k] = 1.f + (nn * fwc[k] - mm * wcc[k - 1]);
+      tt[k] = nn * wcc[k];
+    } else {
+      float rstiv = 1.f / C(C_RST8W, k);
+      float a = rstiv * sbsqzi;
+      float b = rstiv * sbsqg5;
+      float mm = b * C(C_RST, k - 1) - a * C(C_RCSQ, k - 1);
+      float nn = b * C(C_RST, k) + a * C(C_RCSQ, k);
+      rr[k] = mm * fwc[k - 1];
+      ss[k] = 1.f + (mm * wcc[k - 1] + nn * fwc[k]);
+      tt[k] = nn * wcc[k];
+    }
+  }
+  const int ks = 3, ke = nk - 2;
+  std::vector<double> cp(nk + 2, 0.0), aa(nk + 2, 0.0);
+  aa[ks] = 1.0 / (double)ss[ks];
+  cp[ks] = (double)tt[ks] * aa[ks];
+  for (int k = ks + 1; k <= ke - 1; ++k) {
+    aa[k] = 1.0 / ((double)ss[k] - (double)rr[k] * cp[k - 1]);
+    cp[k] = (double)tt[k] * aa[k];
+  }
+  aa[ke] = 1.0 / ((double)ss[ke] - (double)rr[ke] * cp[ke - 1]);
+  ThomasSet t;
+  if (cudaMalloc(&t.rr, sizeof(float) * (nk + 2)) != cudaSuccess ||
+      cudaMalloc(&t.aa, sizeof(double) * (nk + 2)) != cudaSuccess ||
+      cudaMalloc(&t.cp, sizeof(double) * (nk + 2)) != cudaSuccess)
+    return set_error(CRESS_E_CUDA, "cudaMalloc (tridiagonal factors) failed");
+  owned.push_back(t.rr); owned.push_back(t.aa); owned.push_back(t.cp);
+  int rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(t.rr, rr.data(), sizeof(float) * (nk + 2), cudaMemcpyHostToDevice, stream), "copy rr")) ||
+      (rc = cuda_check(cudaMemcpyAsync(t.aa, aa.data(), sizeof(double) * (nk + 2), cudaMemcpyHostToDevice, stream), "copy aa")) ||
+      (rc = cuda_check(cudaMemcpyAsync(t.cp, cp.data(), sizeof(double) * (nk + 2), cudaMemcpyHostToDevice, stream), "copy cp")))
+    return rc;
+  // The host vectors above are freed on return; make the copies complete.
+  if ((rc = cuda_check(cudaStreamSynchronize(stream), "sync after factor upload"))) return rc;
+  auto res = thomas.emplace(key, t);
+  *out = &res.first->second;
+  return CRESS_OK;
+}
+
+int Ctx::small_steps(int nsstp, float dts) {
+  if (!base_set) return set_error(CRESS_E_STATE, "cress_small_steps: base state not set");
+  if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_small_steps: nsstp=%d", nsstp);
+  const ThomasSet* th = nullptr;
+  int rc = thomas_for(dts, &th);
+  if (rc) return rc;
+  HeviArgs a{};
+  a.g = g;
+  a.ufrc = lev[CRESS_U][CRESS_FORCING]; a.vfrc = lev[CRESS_V][CRESS_FORCING];
+  a.wfrc = lev[CRESS_W][CRESS_FORCING]; a.pfrc = lev[CRESS_PP][CRESS_FORCING];
+  a.col = col_d;
+  a.thom_rr = th->rr; a.thom_aa = th->aa; a.thom_cp = th->cp;
+  a.dts = dts;
+  a.dxiv = 1.f / cfg.dx; a.dyiv = 1.f / cfg.dy; a.dziv = 1.f / cfg.dz;
+  a.divch = kDivndc / dts * cfg.dx * cfg.dy;     // pgrad.f90:253
+  a.divcv = kDivndc / dts * cfg.dz * cfg.dz;     // pgrad.f90:254
+  a.weicoe = cfg.weicoe;
+  a.dtdzw = dts * a.dziv * cfg.weicoe;           // pgradiv.f90:135
+  a.dtw = dts * cfg.weicoe;                      // buoywsi.f90:153
+  a.g05 = .5f * kG;
+  a.g05n = -.5f * kG;
+  a.divopt = cfg.divopt; a.buyopt = cfg.buyopt; a.sthopt = cfg.sthopt; a.bbc = cfg.bbc;
+  const int F[4] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP};
+  // Substep 1 reads the past level directly (smalldrv.f90:343-346 copies it
+  // into the future arrays first); later substeps ping-pong between the
+  // future buffer and a spare, so halo reads see old values only.
+  float* olds[4];
+  float* news[4];
+  for (int n = 0; n < 4; ++n) { olds[n] = lev[F[n]][CRESS_PAST]; news[n] = lev[F[n]][CRESS_FUTURE]; }
+  for (int s = 0; s < nsstp; ++s) {
+    a.u_old = olds[0]; a.v_old = olds[1]; a.w_old = olds[2]; a.p_old = olds[3];
+    a.u_new = news[0]; a.v_new = news[1]; a.w_new = news[2]; a.p_new = news[3];
+    rc = launch_hevi_substep(a, cfg.tile, stream);
+    ++launches;
+    if (rc) return set_error(rc, "HE-VI substep launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    for (int n = 0; n < 4; ++n) {
+      float* t = news[n];
+      news[n] = (s == 0) ? spare[F[n]] : olds[n];
+      olds[n] = t;
+    }
+  }
+  // olds[] now hold the result; make it the future level.
+  for (int n = 0; n < 4; ++n) {
+    if (olds[n] != lev[F[n]][CRESS_FUTURE]) {
+      spare[F[n]] = lev[F[n]][CRESS_FUTURE];
+      lev[F[n]][CRESS_FUTURE] = olds[n];
+    }
+  }
+  return CRESS_OK;
+}
+
+}  // namespace cress
+
+using namespace cress;
+
+extern "C" {
+
+const char* cress_last_error(void) { return g_last_error.c_str(); }
+int cress_abi_version(void) { return 1; }
+
+int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
+  if (!cfg || !out) return set_error(CRESS_E_ARG, "cress_create: null argument");
+  *out = nullptr;
+  if (cfg->ni < 8 || cfg->nj < 8 || cfg->nk < 8)
+    return set_error(CRESS_E_ARG, "cress_create: dims too small (%d,%d,%d)", cfg->ni, cfg->nj, cfg->nk);
+  if (cfg->impopt != 1 || cfg->gwmopt != 0)
+    return set_error(CRESS_E_UNSUPPORTED, "only impopt=1, gwmopt=0 run on the GPU");
+  if (!(cfg->wbc == -1 && cfg->ebc == -1 && cfg->sbc == -1 && cfg->nbc == -1))
+    return set_error(CRESS_E_UNSUPPORTED, "only periodic lateral boundaries (-1) run on the GPU");
+  if (cfg->bbc != 2 || cfg->tbc != 2)
+    return set_error(CRESS_E_UNSUPPORTED, "only rigid bottom/top (bbc=tbc=2) run on the GPU");
+  if (cfg->dx <= 0.f || cfg->dy <= 0.f || cfg->dz <= 0.f)
+    return set_error(CRESS_E_ARG, "cress_create: non-positive grid spacing");
+  int rc = cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  if (rc) return rc;
+  Ctx* c = new Ctx();
+  c->device = device;
+  c->cfg = *cfg;
+  c->g = make_grid(cfg->ni, cfg->nj, cfg->nk);
+  if ((rc = cuda_check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate"))) {
+    delete c;
+    return rc;
+  }
+  c->own_stream = c->stream;
+  for (int f = 0; f < CRESS_NFIELD; ++f) {
+    for (int l = 0; l < 4; ++l) c->lev[f][l] = nullptr;
+    c->spare[f] = nullptr;
+  }
+  const int dyn[4] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP};
+  for (int f : dyn) {
+    for (int l = 0; l < 4; ++l) c->lev[f][l] = c->alloc_field();
+    c->spare[f] = c->alloc_field();
+    for (int l = 0; l < 4; ++l)
+      if (!c->lev[f][l]) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the state failed"); }
+    if (!c->spare[f]) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the state failed"); }
+  }
+  c->col_h.assign((size_t)C_NFIELDS * (cfg->nk + 1), 0.f);
+  if ((rc = cuda_check(cudaMalloc(&c->col_d, sizeof(float) * c->col_h.size()), "cudaMalloc cols"))) {
+    delete c;
+    return rc;
+  }
+  c->owned.push_back(c->col_d);
+  *out = reinterpret_cast<cress_ctx*>(c);
+  return CRESS_OK;
+}
+
+void cress_destroy(cress_ctx* ctx) { delete reinterpret_cast<Ctx*>(ctx); }
+
+int cress_set_stream(cress_ctx* ctx, void* stream) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  cudaSetDevice(c->device);
+  c->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : c->own_stream;
+  return CRESS_OK;
+}
+
+int cress_sync(cress_ctx* ctx) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  cudaSetDevice(c->device);
+  return cuda_check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+}
+
+int cress_set_base3d(cress_ctx* ctx, const float* const* b3) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !b3) return set_error(CRESS_E_ARG, "cress_set_base3d: null argument");
+  for (int n = 0; n < CRESS_B_N; ++n)
+    if (!b3[n]) return set_error(CRESS_E_ARG, "cress_set_base3d: array %d is null", n);
+  cudaSetDevice(c->device);
+  const int ni = c->cfg.ni, nj = c->cfg.nj, nk = c->cfg.nk;
+  auto at = [&](const float* a, int i, int j, int k) {
+    return a[(size_t)i + (size_t)(ni + 2) * ((size_t)j + (size_t)(nj + 2) * (size_t)(k - 1))];
+  };
+  // Map from the C-ABI list to the kernels' column ids.
+  const int map[CRESS_B_N] = {C_JCB, C_JCB8U, C_JCB8V, C_JCB8W, C_RBR, C_PTBR,
+                              C_RST, C_RST8U, C_RST8V, C_RST8W, C_RCSQ};
+  // The columns are taken at the domain centre; every point the small step
+  // reads (i in 1..ni, j in 1..nj) must carry the same value.
+  const int ic = ni / 2, jc = nj / 2;
+  for (int n = 0; n < CRESS_B_N; ++n) {
+    const float* a = b3[n];
+    for (int k = 1; k <= nk; ++k) {
+      const float v = at(a, ic, jc, k);
+      c->col_h[(size_t)map[n] * (nk + 1) + k] = v;
+      for (int j = 1; j <= nj; ++j)
+        for (int i = 1; i <= ni; ++i) {
+          const float x = at(a, i, j, k);
+          if (x != v && !(std::isnan(x) && std::isnan(v)))
+            return set_error(CRESS_E_NONUNIFORM,
+                             "base array %d varies horizontally at (%d,%d,%d): %g vs %g", n, i, j, k,
+                             (double)x, (double)v);
+        }
+    }
+  }
+  int rc = cuda_check(cudaMemcpyAsync(c->col_d, c->col_h.data(), sizeof(float) * c->col_h.size(),
+                                      cudaMemcpyHostToDevice, c->stream),
+                      "copy base columns");
+  if (rc) return rc;
+  rc = cuda_check(cudaStreamSynchronize(c->stream), "sync base columns");
+  if (rc) return rc;
+  c->thomas.clear();
+  c->base_set = true;
+  return CRESS_OK;
+}
+
+int cress_put_field(cress_ctx* ctx, int field, int level, const float* host) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !host) return set_error(CRESS_E_ARG, "cress_put_field: null argument");
+  if (field < 0 || field >= CRESS_NFIELD || level < 0 || level > 3 || !c->lev[field][level])
+    return set_error(CRESS_E_ARG, "cress_put_field: field %d level %d not held", field, level);
+  cudaSetDevice(c->device);
+  return c->put_host(c->lev[field][level], host);
+}
+
+int cress_get_field(cress_ctx* ctx, int field, int level, float* host) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !host) return set_error(CRESS_E_ARG, "cress_get_field: null argument");
+  if (field < 0 || field >= CRESS_NFIELD || level < 0 || level > 3 || !c->lev[field][level])
+    return set_error(CRESS_E_ARG, "cress_get_field: field %d level %d not held", field, level);
+  cudaSetDevice(c->device);
+  int rc = c->get_host(host, c->lev[field][level]);
+  if (rc) return rc;
+  return cuda_check(cudaStreamSynchronize(c->stream), "sync after device->host copy");
+}
+
+int cress_small_steps(cress_ctx* ctx, int nsstp, float dts) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  cudaSetDevice(c->device);
+  return c->small_steps(nsstp, dts);
+}
+
+int cress_smalldrv(cress_ctx* ctx, int nsstp, float dts, const float* up, const float* vp,
+                   const float* wp, const float* ppp, const float* ufrc, const float* vfrc,
+                   const float* wfrc, const float* pfrc, float* uf, float* vf, float* wf,
+                   float* ppf) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  const float* in[8] = {up, vp, wp, ppp, ufrc, vfrc, wfrc, pfrc};
+  float* out[4] = {uf, vf, wf, ppf};
+  for (auto p : in) if (!p) return set_error(CRESS_E_ARG, "cress_smalldrv: null input");
+  for (auto p : out) if (!p) return set_error(CRESS_E_ARG, "cress_smalldrv: null output");
+  cudaSetDevice(c->device);
+  const int F[4] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP};
+  int rc;
+  for (int n = 0; n < 4; ++n) {
+    if ((rc = c->put_host(c->lev[F[n]][CRESS_PAST], in[n]))) return rc;
+    if ((rc = c->put_host(c->lev[F[n]][CRESS_FORCING], in[4 + n]))) return rc;
+  }
+  if ((rc = c->small_steps(nsstp, dts))) return rc;
+  for (int n = 0; n < 4; ++n)
+    if ((rc = c->get_host(out[n], c->lev[F[n]][CRESS_FUTURE]))) return rc;
+  return cuda_check(cudaStreamSynchronize(c->stream), "cress_smalldrv sync");
+}
+
+long long cress_launch_count(const cress_ctx* ctx) {
+  const Ctx* c = reinterpret_cast<const Ctx*>(ctx);
+  return c ? c->launches : -1;
+}
+
+}  // extern "C"

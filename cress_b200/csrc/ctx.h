@@ -1,0 +1,48 @@
+// Context object behind the opaque cress_ctx handle (internal).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+#include "../../include/cress_b200.h"
+#include "common.cuh"
+
+namespace cress {
+
+int set_error(int code, const char* fmt, ...);
+int cuda_check(cudaError_t e, const char* what);
+
+// Elimination factors of the w system for one dts (device arrays indexed by k).
+struct ThomasSet {
+  float* rr = nullptr;
+  double* aa = nullptr;
+  double* cp = nullptr;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream all work is ordered on
+  cudaStream_t own_stream = nullptr;  // the context's own stream (destroyed with it)
+  cress_cfg cfg{};
+  Grid g{};
+  // Device state: lev[field][CRESS_PAST/NOW/FUTURE/FORCING]; spare[] is the
+  // ping-pong partner of the future level during the small-step loop.
+  float* lev[CRESS_NFIELD][4];
+  float* spare[CRESS_NFIELD];
+  std::vector<float> col_h;   // 1-D base columns on the host
+  float* col_d = nullptr;
+  bool base_set = false;
+  std::map<uint32_t, ThomasSet> thomas;
+  std::vector<void*> owned;
+  long long launches = 0;
+
+  float* alloc_field();
+  int put_host(float* dst, const float* host);
+  int get_host(float* host, const float* src);
+  int thomas_for(float dts, const ThomasSet** out);
+  int small_steps(int nsstp, float dts);
+  ~Ctx();
+};
+
+}  // namespace cress

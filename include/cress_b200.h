@@ -1,0 +1,123 @@
+/*
+ * cress_b200 — C-ABI of the B200 (sm_100a) implementation of CReSS's solver
+ * time integration.
+ *
+ * Boundary.  In the reference every hot-path routine is a Fortran module
+ * procedure s_xxx(ids..., ni,nj,nk, arrays...) that resolves its options
+ * from integer name-table ids (SrcOrig/getiname.f90) and works on
+ * explicit-shape arrays a(0:ni+1, 0:nj+1, 1:nk) (e.g. SrcOrig/hevi.f90:106-160).
+ * A Fortran shim (cress_b200/fortran/m_cress_gpu.f90, bind(C)) resolves the
+ * ids once, then calls the entry points below with the VALUES and with the
+ * Fortran arrays as plain float pointers in exactly that layout (x fastest,
+ * halo 0..ni+1, 0..nj+1, k = 1..nk).  Nothing in these signatures is a
+ * torch or C++ type.
+ *
+ * Ownership.  The library owns the device copy of the prognostic state
+ * between calls; host arrays are only read or written inside the call that
+ * receives them.  One context = one domain on one device, driven by one
+ * host thread; contexts are not re-entrant.
+ *
+ * Errors.  Every entry point returns 0 on success or a CRESS_E_* code (the
+ * reference has no return codes: it calls destroy(...,'stop') after a
+ * collective chkerr, SrcOrig/chkerr_multi.f90; the shim maps nonzero to
+ * that path).  cress_last_error() gives a one-line message.
+ */
+#ifndef CRESS_B200_H
+#define CRESS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRESS_OK 0
+#define CRESS_E_ARG 1
+#define CRESS_E_UNSUPPORTED 2
+#define CRESS_E_CUDA 3
+#define CRESS_E_NONUNIFORM 4
+#define CRESS_E_NONFINITE 5
+#define CRESS_E_TIMEOUT 6
+#define CRESS_E_STATE 7
+
+/* Resolved namelist values (the reference reads them through
+ * getiname/getrname; SrcOrig/rdconf.f90:88-146 lists the namelists). */
+typedef struct cress_cfg {
+  int ni, nj, nk;       /* array dims: ni = xdim = nx+3, nk = zdim (SrcOrig/setdim.f90:196-199) */
+  float dx, dy, dz;     /* grid spacing; dz is the mean spacing when sthopt=1 */
+  int sthopt;           /* 0 uniform, >=1 stretched vertical grid (jcb varies in k) */
+  int impopt;           /* 1 = HE-VI with Thomas solve (the only small-step scheme on the GPU) */
+  int divopt;           /* divergence damping 0/1/2 (SrcOrig/pgrad.f90:260-349) */
+  int buyopt;           /* 1 = buoyancy in the small step (SrcOrig/hevi.f90:377) */
+  int gwmopt;           /* 0 only */
+  float weicoe;         /* implicit weight beta (SrcOrig/advbspi.f90:140) */
+  int wbc, ebc, sbc, nbc;  /* lateral BCs after chknlslv: -1 = periodic */
+  int bbc, tbc;         /* 2 = rigid (SrcOrig/vbcw.f90:201) */
+  int tile;             /* HE-VI tile shape id (0 = autotuned default) */
+  int reserved[16];
+} cress_cfg;
+
+typedef struct cress_ctx cress_ctx;
+
+/* Fields addressed by the sync calls. */
+enum cress_field {
+  CRESS_U = 0, CRESS_V, CRESS_W, CRESS_PP, CRESS_PTP, CRESS_QV,
+  CRESS_QC, CRESS_QR, CRESS_QI, CRESS_QS, CRESS_QG, CRESS_NI, CRESS_NS, CRESS_NG,
+  CRESS_NFIELD
+};
+/* Time levels: t-dt ("p" arrays: up, vp, ...), t (u, v, ...), t+dt ("f"). */
+enum cress_level { CRESS_PAST = 0, CRESS_NOW = 1, CRESS_FUTURE = 2, CRESS_FORCING = 3 };
+
+/* Base-state arrays in cress_set_base3d's list, in this order. */
+enum cress_base {
+  CRESS_B_JCB = 0, CRESS_B_JCB8U, CRESS_B_JCB8V, CRESS_B_JCB8W, CRESS_B_RBR, CRESS_B_PTBR,
+  CRESS_B_RST, CRESS_B_RST8U, CRESS_B_RST8V, CRESS_B_RST8W, CRESS_B_RCSQ, CRESS_B_N
+};
+
+const char* cress_last_error(void);
+int cress_abi_version(void);
+
+/* Create a context on CUDA device `device` (the caller's rank's GPU).
+ * Replaces the allocation of the solver arrays in SrcOrig/allocslv.f90:388
+ * for the device side; the host arrays stay Fortran-owned. */
+int cress_create(const cress_cfg* cfg, int device, cress_ctx** out);
+void cress_destroy(cress_ctx* ctx);
+
+/* Use an external CUDA stream (cudaStream_t passed as void*); 0 = the
+ * context's own stream.  All work of the context is ordered on it. */
+int cress_set_stream(cress_ctx* ctx, void* stream);
+int cress_sync(cress_ctx* ctx);
+
+/* Base state and metrics, as the reference holds them after s_inivar
+ * (SrcOrig/inivar.f90:674-850: setbase, baserho, sndwave): CRESS_B_N host
+ * arrays in reference layout.  They must be horizontally uniform (flat
+ * terrain, no map factors); otherwise CRESS_E_NONUNIFORM. */
+int cress_set_base3d(cress_ctx* ctx, const float* const* base3d);
+
+/* Host <-> device copy of one prognostic field at one time level
+ * (reference layout).  Used at restart read / dump / restart write times
+ * (SrcOrig/outres.f90:868-900 reads the same arrays). */
+int cress_put_field(cress_ctx* ctx, int field, int level, const float* host);
+int cress_get_field(cress_ctx* ctx, int field, int level, float* host);
+
+/* Acoustic small-step loop on the device-resident state: replaces the body
+ * of s_smalldrv (SrcOrig/smalldrv.f90:343-398) for impopt=1: future u, v,
+ * w, p' start from the past level, then nsstp HE-VI substeps of dts
+ * (SrcOrig/hevi.f90:339-426) run with the forcing level's u, v, w, p'
+ * forcings (ufrc, vfrc, wfrc, pfrc).  The result is the FUTURE level. */
+int cress_small_steps(cress_ctx* ctx, int nsstp, float dts);
+
+/* Same call with host arrays, as s_smalldrv receives them: copies
+ * up, vp, wp, ppp and the four forcings to the device, runs the loop,
+ * copies uf, vf, wf, ppf back. */
+int cress_smalldrv(cress_ctx* ctx, int nsstp, float dts,
+                   const float* up, const float* vp, const float* wp, const float* ppp,
+                   const float* ufrc, const float* vfrc, const float* wfrc, const float* pfrc,
+                   float* uf, float* vf, float* wf, float* ppf);
+
+/* Number of kernel launches the library issued since the context was
+ * created (instrumentation for benchmarks). */
+long long cress_launch_count(const cress_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRESS_B200_H */

@@ -1,0 +1,94 @@
+"""CPU oracle for the CReSS hot path — TEST INFRASTRUCTURE ONLY.
+
+A C++ restatement of the reference's Fortran routines (each function in
+oracle/*.h cites the SrcOrig file:line it follows), compiled with g++
+(-O2 -ffp-contract=off, no fast-math) into oracle/_build/liboracle_cress.so.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use
+it, always as the checker or the timed CPU baseline; the product library
+(cress_b200) never imports, links or calls anything here.
+
+Parity status: the reference is Fortran with no compiler in this image and
+ships no golden outputs, so this restatement is pinned by the reference's
+own formulas and by self-consistency checks (tests/test_oracle.py), not by
+reference-produced vectors: parity unpinned.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(BUILD, "liboracle_cress.so")
+LIB_OMP = os.path.join(BUILD, "liboracle_cress_omp.so")
+SOURCES = ["oracle_capi.cpp"]
+HEADERS = [f for f in os.listdir(HERE) if f.endswith(".h")]
+
+_FP = ctypes.POINTER(ctypes.c_float)
+
+
+def build(force=False):
+    """Compile the oracle (plain and OpenMP builds) if sources changed."""
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = [os.path.join(HERE, s) for s in SOURCES]
+    newest = max(os.path.getmtime(os.path.join(HERE, f)) for f in SOURCES + HEADERS)
+    for out, extra in ((LIB, []), (LIB_OMP, ["-fopenmp", "-DORACLE_OMP=1"])):
+        if not force and os.path.exists(out) and os.path.getmtime(out) >= newest:
+            continue
+        cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC",
+               "-shared", "-o", out + ".tmp"] + extra + srcs
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("oracle build failed:\n" + r.stderr)
+        os.replace(out + ".tmp", out)
+    return LIB
+
+
+_libs = {}
+
+
+def lib(omp=False):
+    path = LIB_OMP if omp else LIB
+    if path not in _libs:
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.oracle_small_steps.argtypes = [
+            ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+            ctypes.c_double, ctypes.c_int, ctypes.POINTER(_FP), ctypes.POINTER(_FP),
+            ctypes.POINTER(_FP)]
+        _libs[path] = L
+    return _libs[path]
+
+
+BASE_NAMES = ["jcb", "jcb8u", "jcb8v", "jcb8w", "rbr", "ptbr", "rst", "rst8u", "rst8v",
+              "rst8w", "rcsq"]
+
+
+def _fp(a):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_FP)
+
+
+def small_steps(cfg, base, frc, state, nsstp, dts, prec=32, fp64_solve=1, omp=False):
+    """Run s_smalldrv's loop (phy2cnt + nsstp x s_hevi) on the CPU.
+
+    cfg: dict with ni,nj,nk,dx,dy,dz,sthopt,divopt,buyopt,weicoe.
+    base: dict of 3-D float32 arrays (BASE_NAMES); frc: [ufrc,vfrc,wfrc,pfrc];
+    state: [uf,vf,wf,ppf] (updated in place).
+    """
+    io = (ctypes.c_int * 10)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
+                             cfg.get("buyopt", 1), 0, 1, 2, 2, int(fp64_solve))
+    ro = (ctypes.c_double * 4)(cfg["dx"], cfg["dy"], cfg["dz"], cfg.get("weicoe", 0.6))
+    b = [np.ascontiguousarray(base[n], np.float32) for n in BASE_NAMES]
+    f = [np.ascontiguousarray(x, np.float32) for x in frc]
+    for s in state:
+        assert s.dtype == np.float32 and s.flags.c_contiguous
+    rc = lib(omp).oracle_small_steps(prec, cfg.get("sthopt", 0), io, ro, float(dts), int(nsstp),
+                                     (_FP * len(b))(*[_fp(x) for x in b]),
+                                     (_FP * 4)(*[_fp(x) for x in f]),
+                                     (_FP * 4)(*[_fp(x) for x in state]))
+    if rc != 0:
+        raise RuntimeError(f"oracle_small_steps failed ({rc})")
+    return state

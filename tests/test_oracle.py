@@ -1,0 +1,82 @@
+"""CPU checks of the oracle itself (no GPU).
+
+The reference ships no tests or golden outputs, so the oracle is pinned by
+properties the reference's equations must satisfy:
+  * a hydrostatic rest state with zero forcing stays exactly at rest;
+  * a periodic shift of the inputs shifts the outputs (bcycle wrap);
+  * the FP32 and FP64 builds agree to float rounding;
+  * the FP32 Thomas solve and the FP64 solve agree to float rounding.
+"""
+import numpy as np
+
+import helpers as H
+
+
+def cfg_for(ni, nj, nk, dx=500.0, dz=300.0, sthopt=0):
+    return dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=sthopt, divopt=2, buyopt=1,
+                weicoe=0.6)
+
+
+def test_rest_state(oracle_lib):
+    ni, nj, nk = H.dims(16, 12, 10)
+    base = H.base3d(ni, nj, nk, 300.0)
+    z = [np.zeros((nk, nj + 2, ni + 2), np.float32) for _ in range(4)]
+    st = [a.copy() for a in z]
+    oracle_lib.small_steps(cfg_for(ni, nj, nk), base, z, st, 4, 0.25)
+    for a in st:
+        assert np.all(a == 0.0)
+
+
+def test_periodic_shift_equivariance(oracle_lib):
+    nx, ny, nz = 16, 12, 10
+    ni, nj, nk = H.dims(nx, ny, nz)
+    base = H.base3d(ni, nj, nk, 300.0)
+    st, frc = H.small_state(ni, nj, nk, 3, base)
+    cfg = cfg_for(ni, nj, nk)
+    a = [x.copy() for x in st]
+    oracle_lib.small_steps(cfg, base, frc, a, 3, 0.25)
+
+    def shift(x, stag, s):
+        y = x.copy()
+        # interior x-range of the periodic domain: i = 2..ni-2 (period nx)
+        y[:, :, 2:ni - 1] = np.roll(x[:, :, 2:ni - 1], s, axis=2)
+        if stag == "u":
+            y[:, :, ni - 1] = y[:, :, 2]
+        return H.bcycle(y, stag)
+
+    stags = ["u", "v", "s", "s"]
+    st2 = [shift(x, t, 5) for x, t in zip(st, stags)]
+    frc2 = [shift(x, t, 5) for x, t in zip(frc, stags)]
+    b = [x.copy() for x in st2]
+    oracle_lib.small_steps(cfg, base, frc2, b, 3, 0.25)
+    for x, y, t in zip(a, b, stags):
+        m = H.interior_mask(ni, nj, nk, t)
+        xs = shift(x, t, 5)
+        assert np.array_equal(xs[m], y[m])
+
+
+def test_fp32_vs_fp64_spread(oracle_lib):
+    ni, nj, nk = H.dims(20, 16, 12)
+    base = H.base3d(ni, nj, nk, 250.0, sthopt=1)
+    st, frc = H.small_state(ni, nj, nk, 4, base)
+    cfg = cfg_for(ni, nj, nk, dx=1000.0, dz=250.0, sthopt=1)
+    a = [x.copy() for x in st]
+    b = [x.copy() for x in st]
+    oracle_lib.small_steps(cfg, base, frc, a, 6, 0.5, prec=32, fp64_solve=0)
+    oracle_lib.small_steps(cfg, base, frc, b, 6, 0.5, prec=64)
+    for x, y in zip(a, b):
+        scale = np.abs(y).max()
+        assert np.abs(x - y).max() <= 1e-4 * scale
+
+
+def test_fp64_solve_close_to_fp32_solve(oracle_lib):
+    ni, nj, nk = H.dims(20, 16, 30)
+    base = H.base3d(ni, nj, nk, 250.0, sthopt=1)
+    st, frc = H.small_state(ni, nj, nk, 8, base)
+    cfg = cfg_for(ni, nj, nk, dx=1000.0, dz=250.0, sthopt=1)
+    a = [x.copy() for x in st]
+    b = [x.copy() for x in st]
+    oracle_lib.small_steps(cfg, base, frc, a, 2, 0.5, prec=32, fp64_solve=0)
+    oracle_lib.small_steps(cfg, base, frc, b, 2, 0.5, prec=32, fp64_solve=1)
+    w32, w64 = a[2], b[2]
+    assert np.abs(w32 - w64).max() <= 1e-5 * np.abs(w64).max()
