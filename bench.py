@@ -161,7 +161,11 @@ def main():
                                                       seed=100 + rank, sthopt=1)
     s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, args.dz, sthopt=1, tile=args.tile,
                           device=local)
-    stream = torch.cuda.current_stream()
+    # A dedicated (non-default) stream shared by the library and torch's
+    # events, so the events bracket exactly the library's kernels.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
     s.set_stream(stream.cuda_stream)
     s.set_base3d(base)
     for name, a in zip(("u", "v", "w", "pp"), st):

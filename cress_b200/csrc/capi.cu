@@ -33,8 +33,8 @@ int cuda_check(cudaError_t e, const char* what) {
   return set_error(CRESS_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-// Physical constants used on the host side (SrcOrig/comphy.f90:49,61,64,459).
-static const float kG = 9.8f, kCp = 1004.f, kCv = 717.f, kDivndc = 0.05f;
+// Physical constants used on the host side (SrcOrig/comphy.f90:49,459).
+static const float kG = 9.8f, kDivndc = 0.05f;
 
 float* Ctx::alloc_field() {
   float* p = nullptr;
@@ -136,6 +136,47 @@ int Ctx::thomas_for(float dts, const ThomasSet** out) {
   return CRESS_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 3-D tensor map (x = i, y = j, z = k-1) over one field buffer with a box
+// of kHeviBoxX x rows x 1, cached per (buffer, rows).
+int Ctx::tmap(const float* buf, int rows, CUtensorMap* out) {
+  auto key = std::make_pair(reinterpret_cast<const void*>(buf), rows);
+  auto it = tmaps.find(key);
+  if (it != tmaps.end()) { *out = it->second; return CRESS_OK; }
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return set_error(CRESS_E_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+  CUtensorMap m;
+  cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.nk};
+  cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.plane * 4};
+  cuuint32_t box[3] = {(cuuint32_t)kHeviBoxX, (cuuint32_t)rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(buf), dims, strides, box,
+                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(CRESS_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  tmaps.emplace(key, m);
+  *out = m;
+  return CRESS_OK;
+}
+
 int Ctx::small_steps(int nsstp, float dts) {
   if (!base_set) return set_error(CRESS_E_STATE, "cress_small_steps: base state not set");
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_small_steps: nsstp=%d", nsstp);
@@ -144,10 +185,9 @@ int Ctx::small_steps(int nsstp, float dts) {
   if (rc) return rc;
   HeviArgs a{};
   a.g = g;
-  a.ufrc = lev[CRESS_U][CRESS_FORCING]; a.vfrc = lev[CRESS_V][CRESS_FORCING];
-  a.wfrc = lev[CRESS_W][CRESS_FORCING]; a.pfrc = lev[CRESS_PP][CRESS_FORCING];
   a.col = col_d;
   a.thom_rr = th->rr; a.thom_aa = th->aa; a.thom_cp = th->cp;
+  a.err = err_d;
   a.dts = dts;
   a.dxiv = 1.f / cfg.dx; a.dyiv = 1.f / cfg.dy; a.dziv = 1.f / cfg.dz;
   a.divch = kDivndc / dts * cfg.dx * cfg.dy;     // pgrad.f90:253
@@ -158,6 +198,13 @@ int Ctx::small_steps(int nsstp, float dts) {
   a.g05 = .5f * kG;
   a.g05n = -.5f * kG;
   a.divopt = cfg.divopt; a.buyopt = cfg.buyopt; a.sthopt = cfg.sthopt; a.bbc = cfg.bbc;
+  const int TY = hevi_tile_rows(cfg.tile);
+  HeviMaps maps;
+  if ((rc = tmap(lev[CRESS_U][CRESS_FORCING], TY, &maps.uf)) ||
+      (rc = tmap(lev[CRESS_V][CRESS_FORCING], TY + 1, &maps.vf)) ||
+      (rc = tmap(lev[CRESS_W][CRESS_FORCING], TY, &maps.wf)) ||
+      (rc = tmap(lev[CRESS_PP][CRESS_FORCING], TY, &maps.pf)))
+    return rc;
   const int F[4] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP};
   // Substep 1 reads the past level directly (smalldrv.f90:343-346 copies it
   // into the future arrays first); later substeps ping-pong between the
@@ -166,9 +213,12 @@ int Ctx::small_steps(int nsstp, float dts) {
   float* news[4];
   for (int n = 0; n < 4; ++n) { olds[n] = lev[F[n]][CRESS_PAST]; news[n] = lev[F[n]][CRESS_FUTURE]; }
   for (int s = 0; s < nsstp; ++s) {
-    a.u_old = olds[0]; a.v_old = olds[1]; a.w_old = olds[2]; a.p_old = olds[3];
+    a.u_old = olds[0]; a.v_old = olds[1]; a.p_old = olds[3];
     a.u_new = news[0]; a.v_new = news[1]; a.w_new = news[2]; a.p_new = news[3];
-    rc = launch_hevi_substep(a, cfg.tile, stream);
+    if ((rc = tmap(olds[0], TY + 2, &maps.u)) || (rc = tmap(olds[1], TY + 3, &maps.v)) ||
+        (rc = tmap(olds[2], TY + 2, &maps.w)) || (rc = tmap(olds[3], TY + 2, &maps.p)))
+      return rc;
+    rc = launch_hevi_substep(a, maps, cfg.tile, stream);
     ++launches;
     if (rc) return set_error(rc, "HE-VI substep launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     for (int n = 0; n < 4; ++n) {
@@ -183,6 +233,19 @@ int Ctx::small_steps(int nsstp, float dts) {
       spare[F[n]] = lev[F[n]][CRESS_FUTURE];
       lev[F[n]][CRESS_FUTURE] = olds[n];
     }
+  }
+  return CRESS_OK;
+}
+
+// Read and clear the device error word (bounded-wait failures).
+int Ctx::check_device_error() {
+  int h = 0;
+  int rc = cuda_check(cudaMemcpyAsync(&h, err_d, sizeof(int), cudaMemcpyDeviceToHost, stream), "read error word");
+  if (rc) return rc;
+  if ((rc = cuda_check(cudaStreamSynchronize(stream), "sync"))) return rc;
+  if (h) {
+    cudaMemsetAsync(err_d, 0, sizeof(int), stream);
+    return set_error(CRESS_E_TIMEOUT, "a bounded device-side wait gave up (TMA staging did not complete)");
   }
   return CRESS_OK;
 }
@@ -238,6 +301,12 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
     return rc;
   }
   c->owned.push_back(c->col_d);
+  if ((rc = cuda_check(cudaMalloc(&c->err_d, sizeof(int)), "cudaMalloc error word"))) {
+    delete c;
+    return rc;
+  }
+  c->owned.push_back(c->err_d);
+  cudaMemsetAsync(c->err_d, 0, sizeof(int), c->stream);
   *out = reinterpret_cast<cress_ctx*>(c);
   return CRESS_OK;
 }
@@ -256,7 +325,8 @@ int cress_sync(cress_ctx* ctx) {
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (!c) return set_error(CRESS_E_ARG, "null context");
   cudaSetDevice(c->device);
-  return cuda_check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  int rc = cuda_check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  return rc ? rc : c->check_device_error();
 }
 
 int cress_set_base3d(cress_ctx* ctx, const float* const* b3) {
@@ -290,6 +360,14 @@ int cress_set_base3d(cress_ctx* ctx, const float* const* b3) {
         }
     }
   }
+  // Reciprocals of the per-level divisors (the kernels multiply by them).
+  const int inv_src[6] = {C_RST8U, C_RST8V, C_JCB, C_RCSQ, C_RST8W, C_JCB8W};
+  const int inv_dst[6] = {C_IRST8U, C_IRST8V, C_IJCB, C_IRCSQ, C_IRST8W, C_IJCB8W};
+  for (int n = 0; n < 6; ++n)
+    for (int k = 1; k <= nk; ++k) {
+      const float v = c->col_h[(size_t)inv_src[n] * (nk + 1) + k];
+      c->col_h[(size_t)inv_dst[n] * (nk + 1) + k] = (v != 0.f) ? 1.f / v : 0.f;
+    }
   int rc = cuda_check(cudaMemcpyAsync(c->col_d, c->col_h.data(), sizeof(float) * c->col_h.size(),
                                       cudaMemcpyHostToDevice, c->stream),
                       "copy base columns");
@@ -318,7 +396,8 @@ int cress_get_field(cress_ctx* ctx, int field, int level, float* host) {
   cudaSetDevice(c->device);
   int rc = c->get_host(host, c->lev[field][level]);
   if (rc) return rc;
-  return cuda_check(cudaStreamSynchronize(c->stream), "sync after device->host copy");
+  rc = cuda_check(cudaStreamSynchronize(c->stream), "sync after device->host copy");
+  return rc ? rc : c->check_device_error();
 }
 
 int cress_small_steps(cress_ctx* ctx, int nsstp, float dts) {
@@ -348,7 +427,8 @@ int cress_smalldrv(cress_ctx* ctx, int nsstp, float dts, const float* up, const 
   if ((rc = c->small_steps(nsstp, dts))) return rc;
   for (int n = 0; n < 4; ++n)
     if ((rc = c->get_host(out[n], c->lev[F[n]][CRESS_FUTURE]))) return rc;
-  return cuda_check(cudaStreamSynchronize(c->stream), "cress_smalldrv sync");
+  rc = cuda_check(cudaStreamSynchronize(c->stream), "cress_smalldrv sync");
+  return rc ? rc : c->check_device_error();
 }
 
 long long cress_launch_count(const cress_ctx* ctx) {

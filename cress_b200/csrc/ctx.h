@@ -1,5 +1,6 @@
 // Context object behind the opaque cress_ctx handle (internal).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <map>
@@ -34,6 +35,8 @@ struct Ctx {
   float* col_d = nullptr;
   bool base_set = false;
   std::map<uint32_t, ThomasSet> thomas;
+  std::map<std::pair<const void*, int>, CUtensorMap> tmaps;  // (buffer, box rows) -> map
+  int* err_d = nullptr;                                       // device error word
   std::vector<void*> owned;
   long long launches = 0;
 
@@ -42,6 +45,8 @@ struct Ctx {
   int get_host(float* host, const float* src);
   int thomas_for(float dts, const ThomasSet** out);
   int small_steps(int nsstp, float dts);
+  int tmap(const float* buf, int rows, CUtensorMap* out);
+  int check_device_error();
   ~Ctx();
 };
 

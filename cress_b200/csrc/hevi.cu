@@ -5,7 +5,7 @@
 // boundaries on one GPU, rigid bottom/top (bbc=tbc=2):
 //   pgrad + diver3d (divergence damping)   pgrad.f90:251-395, diver3d.f90:182-326
 //   stepuv + bcycle + vbcu/vbcv            stepuv.f90:288-424
-//   diverpih + diver2d                     diverpih.f90:188-214
+//   diverpih + diver2d                     diverpih.f90:188-214, diver2d.f90:280-295
 //   diverpiv, advbspi('back')              diverpiv.f90:118-130, advbspi.f90:150-165
 //   pgradiv, buoywsi                       pgradiv.f90:135-170, buoywsi.f90:153-211
 //   stepwi (predictor, tridiagonal, gaussel Thomas in FP64, bcycle, vbcw)
@@ -13,202 +13,229 @@
 //   diverpiv, advbspi('fore'), steppi + bcycle + vbcp
 //                                          advbspi.f90:167-182, steppi.f90:211-316
 //
-// Design: one thread owns one (i,j) column of a TX x TY tile and the block
-// marches k upward.  Each level's old u, v, w, p' planes (tile + 1-2 halo)
-// are staged in shared memory; the divergence-damped pressure, the new u
-// and v, the horizontal and vertical divergences, the w right-hand side
-// and the forward Thomas elimination are formed on the way up.  The
-// modified right-hand side (double) and the backward pressure tendency
-// (float) of every level are kept in shared memory; the way down does the
-// back substitution and the p' update.  Old and new time levels are
-// separate buffers (ping-pong across substeps), so halo reads never see a
-// neighbour tile's new values.  Each field is read once and written once
-// per substep from HBM, apart from tile-halo re-reads that L1/L2 serve.
+// Design.  A block owns a 32 x TY tile of (i,j) columns, one thread per
+// column, and marches k upward (2.5-D).  For every level one elected thread
+// issues eight TMA box loads (old u, v, w, p' with their halos and the four
+// forcings) into an S-stage shared-memory ring guarded by mbarriers, so S-2
+// levels are in flight while the block computes.  Per level each thread
+// forms the divergence-damped pressure of its own column (plus one halo
+// point), then, after one barrier, the new u on its west and east faces, the
+// new v on its south and north faces, the horizontal divergence of the new
+// winds, the backward pressure tendency, the w right-hand side and one step
+// of the forward Thomas elimination.  The eliminated right-hand sides stay
+// in shared memory as doubles; the backward pressure tendency is parked in
+// the new p' array (an L2 round trip that its final value overwrites).  The
+// way down does the back substitution, the p' update and the boundary
+// rows.  Old and new time levels are separate buffers (ping-pong across
+// substeps), so halo reads never see a neighbour tile's new values.
 //
-// With a horizontally uniform base state (idealized, flat terrain) the
-// tridiagonal coefficients depend on k only, so the elimination factors
-// c'_k and 1/(b_k - a_k c'_{k-1}) are formed once per dts on the host and
-// read as 1-D columns.
+// With a horizontally uniform base state the tridiagonal coefficients
+// depend on k only: the elimination factors c'_k and 1/(b_k - a_k c'_{k-1})
+// come precomputed (double) from the host.
+#include <cuda.h>
 #include <cuda_runtime.h>
-#include <cstdio>
+#include <cstdint>
 #include "common.cuh"
 #include "hevi.cuh"
+#include "tma.cuh"
 
 namespace cress {
 
 namespace {
 
-template <int TX, int TY>
-struct HeviSmem {
-  float u[TY + 2][TX + 3];   // old u  at i in [i0-1, i0+TX+1], j in [j0-1, j0+TY]
-  float v[TY + 3][TX + 2];   // old v  at i in [i0-1, i0+TX],   j in [j0-1, j0+TY+1]
-  float w[2][TY + 2][TX + 2];// old w  at levels k (slot k&1) and k+1
-  float p[TY + 2][TX + 2];   // old p' at level k
-  float t3h[TY + 2][TX + 2]; // jcb*(p' + divch*div3d/jcb)  (pgrad.f90:341,363)
-  float un[TY][TX + 1];      // new u on the tile's x faces
-  float vn[TY + 1][TX];      // new v on the tile's y faces
+constexpr int r128(int n) { return (n + 31) / 32 * 32; }  // floats -> multiple of 128 B
+
+template <int TY, int S>
+struct HeviLayout {
+  using R = HeviRows<TY>;
+  static constexpr int BX = kHeviBoxX;
+  static constexpr int oU = 0;
+  static constexpr int oV = oU + r128(BX * R::u);
+  static constexpr int oW = oV + r128(BX * R::v);
+  static constexpr int oP = oW + r128(BX * R::w);
+  static constexpr int oUF = oP + r128(BX * R::p);
+  static constexpr int oVF = oUF + r128(BX * R::uf);
+  static constexpr int oWF = oVF + r128(BX * R::vf);
+  static constexpr int oPF = oWF + r128(BX * R::wf);
+  static constexpr int stage = oPF + r128(BX * R::pf);  // floats per ring stage
+  static constexpr uint32_t tx_bytes =
+      4u * BX * (R::u + R::v + R::w + R::p + R::uf + R::vf + R::wf + R::pf);
+  static constexpr int t3h_floats = r128((TY + 2) * BX);
+  __host__ __device__ static size_t cols_floats(int nk) { return (size_t)((C_NFIELDS * (nk + 1) + 31) / 32 * 32); }
+  __host__ __device__ static size_t bytes(int nk) {
+    return 4 * ((size_t)S * stage + t3h_floats + cols_floats(nk)) + 8 * (size_t)S +
+           8 * (size_t)(nk - 4) * (kHeviTX * TY);
+  }
 };
 
-template <int TX, int TY>
-__global__ void __launch_bounds__(TX * TY)
-k_hevi_substep(const HeviArgs a) {
+template <int TY, int S>
+__global__ void __launch_bounds__(kHeviTX * TY)
+k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
+  using L = HeviLayout<TY, S>;
+  constexpr int TX = kHeviTX, BX = kHeviBoxX, NT = TX * TY;
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = ty * TX + tx;
-  const int NT = TX * TY;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = 2 + blockIdx.x * TX, j0 = 2 + blockIdx.y * TY;
+  const int xb = i0 - 2;  // box x origin (multiple of 32)
   const int ilast = min(i0 + TX - 1, ni - 2), jlast = min(j0 + TY - 1, nj - 2);
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= ilast) && (j <= jlast);
-
-  __shared__ HeviSmem<TX, TY> s;
-  extern __shared__ __align__(16) unsigned char dsm[];
-  // Column store: forward-eliminated RHS (double, levels 3..nk-2) and the
-  // backward pressure tendency fp (float, levels 2..nk-2).
-  double* fcol = reinterpret_cast<double*>(dsm);
-  float* fpcol = reinterpret_cast<float*>(dsm + sizeof(double) * (size_t)(nk - 4) * NT);
-
-  const float* __restrict__ col = a.col;   // 1-D base columns, [field*(nk+1) + k]
-  const float* __restrict__ uo = a.u_old;
-  const float* __restrict__ vo = a.v_old;
-  const float* __restrict__ wo = a.w_old;
-  const float* __restrict__ po = a.p_old;
   const int ncol = nk + 1;
-#define COL(f, k) __ldg(col + (f) * ncol + (k))
+  // Columns whose values the periodic wrap also copies into ghost cells.
+  const bool edge = (i <= 3) || (i >= ni - 2) || (j <= 3) || (j >= nj - 2);
 
-  // Extents of the staged planes (clipped for partial edge tiles).
-  const int ux = ilast - i0 + 4, uy = jlast - j0 + 3;   // u plane
-  const int vx = ilast - i0 + 3, vy = jlast - j0 + 4;   // v plane
-  const int sx = ilast - i0 + 3, sy = jlast - j0 + 3;   // w, p planes and the div3d region
+  extern __shared__ __align__(1024) float smem[];
+  float* ring = smem;
+  float* t3h = ring + S * L::stage;                // [(TY+2)][BX], rows from j0-1, x from i0-2
+  float* cols = t3h + L::t3h_floats;               // [C_NFIELDS][nk+1]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
+  double* fcol = reinterpret_cast<double*>(bars + S);  // [(nk-4)][NT]
 
-  auto load_w = [&](int k, int slot) {
-    for (int n = tid; n < sx * sy; n += NT) {
-      int x = n % sx, y = n / sx;
-      s.w[slot][y][x] = wo[g.at(i0 - 1 + x, j0 - 1 + y, k)];
-    }
+  for (int n = tid; n < C_NFIELDS * ncol; n += NT) cols[n] = __ldg(a.col + n);
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  // Levels 2..nk-1 are staged (w is needed one level above the top update).
+  const int klast = nk - 1;
+  auto issue = [&](int k) {
+    const int s = (k - 2) % S;
+    float* st = ring + s * L::stage;
+    uint64_t* bar = &bars[s];
+    const int z = k - 1;
+    mbar_arrive_expect_tx(bar, L::tx_bytes);
+    tma_load_3d(st + L::oU, &m.u, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oV, &m.v, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oW, &m.w, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oP, &m.p, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oUF, &m.uf, xb, j0, z, bar);
+    tma_load_3d(st + L::oVF, &m.vf, xb, j0, z, bar);
+    tma_load_3d(st + L::oWF, &m.wf, xb, j0, z, bar);
+    tma_load_3d(st + L::oPF, &m.pf, xb, j0, z, bar);
   };
+  if (tid == 0)
+    for (int k = 2; k <= min(S, klast); ++k) issue(k);
 
-  load_w(2, 0);
-
+  // Halo points of the damped-pressure plane: the rows south/north of the
+  // tile and the columns west/east of it (2*TX + 2*TY points, spread over
+  // the threads; box coordinates).
+  constexpr int NH = 2 * TX + 2 * TY;
+  auto halo_xy = [&](int n, int& hx, int& hy) {
+    if (n < TX) { hx = n + 2; hy = 0; }
+    else if ((n -= TX) < TX) { hx = n + 2; hy = TY + 1; }
+    else if ((n -= TX) < TY) { hx = 1; hy = n + 1; }
+    else { n -= TY; hx = TX + 2; hy = n + 1; }
+  };
+  const int ox = tx + 2, oy = ty + 1;  // own column in the boxes that start at j0-1
+  const float dts = a.dts, dxiv = a.dxiv, dyiv = a.dyiv, dziv = a.dziv;
+  const float weic1m = 1.f - a.weicoe;
   float t3v_prev = 0.f, fpdvj_prev = 0.f, wb8s_prev = 0.f;
   double fprev = 0.0;
-  const float dts = a.dts;
-  const float weic1m = 1.f - a.weicoe;
+  bool fail = false;
+  const long long plane = g.plane;
+  long long id = g.at(i, j, 2);
 
-  for (int k = 2; k <= nk - 2; ++k) {
-    const int sk = k & 1, sk1 = (k + 1) & 1;
-    // --- stage old planes at level k (w at k+1) --------------------------
-    for (int n = tid; n < ux * uy; n += NT) {
-      int x = n % ux, y = n / ux;
-      s.u[y][x] = uo[g.at(i0 - 1 + x, j0 - 1 + y, k)];
+  for (int k = 2; k <= nk - 2; ++k, id += plane) {
+    __syncthreads();  // the previous level's stage and t3h are no longer read
+    if (tid == 0 && k + S - 1 <= klast) {
+      fence_proxy_async_smem();
+      issue(k + S - 1);
     }
-    for (int n = tid; n < vx * vy; n += NT) {
-      int x = n % vx, y = n / vx;
-      s.v[y][x] = vo[g.at(i0 - 1 + x, j0 - 1 + y, k)];
-    }
-    for (int n = tid; n < sx * sy; n += NT) {
-      int x = n % sx, y = n / sx;
-      s.p[y][x] = po[g.at(i0 - 1 + x, j0 - 1 + y, k)];
-      s.w[sk1][y][x] = wo[g.at(i0 - 1 + x, j0 - 1 + y, k + 1)];
+    const int s0 = (k - 2) % S, s1 = (k - 1) % S;
+    if (!fail) fail = !mbar_wait(&bars[s0], ((k - 2) / S) & 1);
+    if (!fail) fail = !mbar_wait(&bars[s1], ((k - 1) / S) & 1);
+    const float* U = ring + s0 * L::stage + L::oU;
+    const float* V = ring + s0 * L::stage + L::oV;
+    const float* W0 = ring + s0 * L::stage + L::oW;
+    const float* W1 = ring + s1 * L::stage + L::oW;
+    const float* P = ring + s0 * L::stage + L::oP;
+    const float* UF = ring + s0 * L::stage + L::oUF;
+    const float* VF = ring + s0 * L::stage + L::oVF;
+    const float* WF = ring + s0 * L::stage + L::oWF;
+    const float* PF = ring + s0 * L::stage + L::oPF;
+    const float rst8u = cols[C_RST8U * ncol + k], rst8v = cols[C_RST8V * ncol + k];
+    const float rst8wk = cols[C_RST8W * ncol + k], rst8wk1 = cols[C_RST8W * ncol + k + 1];
+    const float jcbk = cols[C_JCB * ncol + k], ijcbk = cols[C_IJCB * ncol + k];
+    const float irst8u = cols[C_IRST8U * ncol + k], irst8v = cols[C_IRST8V * ncol + k];
+    const float ij8wk = cols[C_IJCB8W * ncol + k], ij8wk1 = cols[C_IJCB8W * ncol + k + 1];
+
+    // diver3d.f90:318 (with phy2cnt.f90:219 for the contravariant w)
+    auto div3d_at = [&](int x, int y) {
+      float wck = W0[y * BX + x], wck1 = W1[y * BX + x];
+      if (a.sthopt) { wck = wck * ij8wk; wck1 = wck1 * ij8wk1; }
+      return (rst8wk * wck - rst8wk1 * wck1) * dziv +
+             ((rst8u * U[y * BX + x] - rst8u * U[y * BX + x + 1]) * dxiv +
+              (rst8v * V[y * BX + x] - rst8v * V[(y + 1) * BX + x]) * dyiv);
+    };
+    // pgrad.f90:300,341,363
+    auto t3h_of = [&](float div, float pp) {
+      float th = (a.divopt == 2) ? pp + a.divch * div * ijcbk
+               : (a.divopt >= 1) ? pp + a.divcv * jcbk * div : pp;
+      return jcbk * th;
+    };
+    const float divo = div3d_at(ox, oy);
+    const float ppo = P[oy * BX + ox];
+    t3h[oy * BX + ox] = t3h_of(divo, ppo);
+    const float t3v = (a.divopt >= 1) ? ppo + a.divcv * jcbk * divo : ppo;  // pgrad.f90:300
+    for (int n = tid; n < NH; n += NT) {
+      int hx, hy;
+      halo_xy(n, hx, hy);
+      t3h[hy * BX + hx] = t3h_of(div3d_at(hx, hy), P[hy * BX + hx]);
     }
     __syncthreads();
 
-    // --- diver3d + divergence damping on the tile + 1 halo ---------------
-    const float rst8u = COL(C_RST8U, k), rst8v = COL(C_RST8V, k);
-    const float rst8wk = COL(C_RST8W, k), rst8wk1 = COL(C_RST8W, k + 1);
-    const float jcbk = COL(C_JCB, k);
-    const float j8wk = COL(C_JCB8W, k), j8wk1 = COL(C_JCB8W, k + 1);
-    for (int n = tid; n < sx * sy; n += NT) {
-      int x = n % sx, y = n / sx;
-      float wck = s.w[sk][y][x], wck1 = s.w[sk1][y][x];
-      if (a.sthopt) { wck = wck / j8wk; wck1 = wck1 / j8wk1; }                     // phy2cnt.f90:219
-      float div = (rst8wk * wck - rst8wk1 * wck1) * a.dziv +
-                  ((rst8u * s.u[y][x] - rst8u * s.u[y][x + 1]) * a.dxiv +
-                   (rst8v * s.v[y][x] - rst8v * s.v[y + 1][x]) * a.dyiv);         // diver3d.f90:318
-      float pp = s.p[y][x];
-      float th = (a.divopt == 2) ? pp + a.divch * div / jcbk                        // pgrad.f90:341
-               : (a.divopt >= 1) ? pp + a.divcv * jcbk * div : pp;                 // pgrad.f90:300
-      s.t3h[y][x] = jcbk * th;                                                      // pgrad.f90:363
-    }
-    // The own column's vertically damped pressure (pgrad.f90:300), kept in
-    // a register for wpg at this level and the next.
-    float t3v = 0.f;
-    if (own) {
-      const int x = tx + 1, y = ty + 1;
-      float wck = s.w[sk][y][x], wck1 = s.w[sk1][y][x];
-      if (a.sthopt) { wck = wck / j8wk; wck1 = wck1 / j8wk1; }
-      float div = (rst8wk * wck - rst8wk1 * wck1) * a.dziv +
-                  ((rst8u * s.u[y][x] - rst8u * s.u[y][x + 1]) * a.dxiv +
-                   (rst8v * s.v[y][x] - rst8v * s.v[y + 1][x]) * a.dyiv);
-      float pp = s.p[y][x];
-      t3v = (a.divopt >= 1) ? pp + a.divcv * jcbk * div : pp;
-    }
-    __syncthreads();
+    // stepuv.f90:294,304 with pgrad.f90:379,389 on the four faces of the column
+    const float tc = t3h[oy * BX + ox];
+    const float un0 = U[oy * BX + ox] + dts * (UF[ty * BX + ox] + (t3h[oy * BX + ox - 1] - tc) * dxiv) * irst8u;
+    const float un1 = U[oy * BX + ox + 1] + dts * (UF[ty * BX + ox + 1] + (tc - t3h[oy * BX + ox + 1]) * dxiv) * irst8u;
+    const float vn0 = V[oy * BX + ox] + dts * (VF[ty * BX + ox] + (t3h[(oy - 1) * BX + ox] - tc) * dyiv) * irst8v;
+    const float vn1 = V[(oy + 1) * BX + ox] + dts * (VF[(ty + 1) * BX + ox] + (tc - t3h[(oy + 1) * BX + ox]) * dyiv) * irst8v;
 
-    // --- stepuv: new u on faces i0..ilast+1, new v on faces j0..jlast+1 ---
     if (own) {
-      const long long id = g.at(i, j, k);
-      float upg = (s.t3h[ty + 1][tx] - s.t3h[ty + 1][tx + 1]) * a.dxiv;            // pgrad.f90:379
-      float un = s.u[ty + 1][tx + 1] + dts * (__ldg(a.ufrc + id) + upg) / rst8u;  // stepuv.f90:294
-      float vpg = (s.t3h[ty][tx + 1] - s.t3h[ty + 1][tx + 1]) * a.dyiv;            // pgrad.f90:389
-      float vn = s.v[ty + 1][tx + 1] + dts * (__ldg(a.vfrc + id) + vpg) / rst8v;  // stepuv.f90:304
-      s.un[ty][tx] = un;
-      s.vn[ty][tx] = vn;
-      store_periodic(a.u_new, g, STAG_U, i, j, k, un);
-      store_periodic(a.v_new, g, STAG_V, i, j, k, vn);
-      if (k == 2) { store_periodic(a.u_new, g, STAG_U, i, j, 1, un);            // vbcu.f90:120
-                    store_periodic(a.v_new, g, STAG_V, i, j, 1, vn); }
-      if (k == nk - 2) { store_periodic(a.u_new, g, STAG_U, i, j, nk - 1, un);  // vbcu.f90:134
-                         store_periodic(a.v_new, g, STAG_V, i, j, nk - 1, vn); }
-      if (i == ilast) {  // east face of the tile
-        const int xe = tx + 2;
-        float upg2 = (s.t3h[ty + 1][xe - 1] - s.t3h[ty + 1][xe]) * a.dxiv;
-        float un2 = s.u[ty + 1][xe] + dts * (__ldg(a.ufrc + id + 1) + upg2) / rst8u;
-        s.un[ty][tx + 1] = un2;
-        if (i + 1 == ni - 1) {   // the reference also updates u(ni-1) (stepuv.f90:293)
-          store_periodic(a.u_new, g, STAG_U, i + 1, j, k, un2);
-          if (k == 2) store_periodic(a.u_new, g, STAG_U, i + 1, j, 1, un2);
-          if (k == nk - 2) store_periodic(a.u_new, g, STAG_U, i + 1, j, nk - 1, un2);
-        }
+      if (edge) {
+        store_periodic(a.u_new, g, STAG_U, i, j, k, un0);
+        store_periodic(a.v_new, g, STAG_V, i, j, k, vn0);
+      } else {
+        a.u_new[id] = un0;
+        a.v_new[id] = vn0;
       }
-      if (j == jlast) {  // north face of the tile
-        const int yn = ty + 2;
-        float vpg2 = (s.t3h[yn - 1][tx + 1] - s.t3h[yn][tx + 1]) * a.dyiv;
-        float vn2 = s.v[yn][tx + 1] + dts * (__ldg(a.vfrc + id + g.px) + vpg2) / rst8v;
-        s.vn[ty + 1][tx] = vn2;
-        if (j + 1 == nj - 1) {
-          store_periodic(a.v_new, g, STAG_V, i, j + 1, k, vn2);
-          if (k == 2) store_periodic(a.v_new, g, STAG_V, i, j + 1, 1, vn2);
-          if (k == nk - 2) store_periodic(a.v_new, g, STAG_V, i, j + 1, nk - 1, vn2);
-        }
+      if (k == 2) { store_periodic(a.u_new, g, STAG_U, i, j, 1, un0);          // vbcu.f90:120
+                    store_periodic(a.v_new, g, STAG_V, i, j, 1, vn0); }
+      if (k == nk - 2) { store_periodic(a.u_new, g, STAG_U, i, j, nk - 1, un0); // vbcu.f90:134
+                         store_periodic(a.v_new, g, STAG_V, i, j, nk - 1, vn0); }
+      if (i == ilast && i + 1 == ni - 1) {  // stepuv.f90:293 updates u(ni-1) too
+        store_periodic(a.u_new, g, STAG_U, i + 1, j, k, un1);
+        if (k == 2) store_periodic(a.u_new, g, STAG_U, i + 1, j, 1, un1);
+        if (k == nk - 2) store_periodic(a.u_new, g, STAG_U, i + 1, j, nk - 1, un1);
       }
-    }
-    __syncthreads();
+      if (j == jlast && j + 1 == nj - 1) {  // stepuv.f90:302 updates v(nj-1) too
+        store_periodic(a.v_new, g, STAG_V, i, j + 1, k, vn1);
+        if (k == 2) store_periodic(a.v_new, g, STAG_V, i, j + 1, 1, vn1);
+        if (k == nk - 2) store_periodic(a.v_new, g, STAG_V, i, j + 1, nk - 1, vn1);
+      }
 
-    // --- column work: fp (back), fw, w predictor, forward elimination -----
-    if (own) {
-      const long long id = g.at(i, j, k);
-      const float jcb8u = COL(C_JCB8U, k), jcb8v = COL(C_JCB8V, k);
-      const float rcsq = COL(C_RCSQ, k), rst = COL(C_RST, k), rbr = COL(C_RBR, k);
-      float phd = (jcb8u * s.un[ty][tx] - jcb8u * s.un[ty][tx + 1]) * a.dxiv +
-                  (jcb8v * s.vn[ty][tx] - jcb8v * s.vn[ty + 1][tx]) * a.dyiv;     // diver2d.f90:288
-      phd = rcsq * phd;                                                              // diverpih.f90:208
-      const float wk = s.w[sk][ty + 1][tx + 1], wk1 = s.w[sk1][ty + 1][tx + 1];
-      const float pvd = rcsq * (wk - wk1) * a.dziv;                                  // diverpiv.f90:124
-      const float fp = __ldg(a.pfrc + id) + phd +
-                       weic1m * (a.g05 * (wk + wk1) * rst + pvd);                    // advbspi.f90:158
-      fpcol[(k - 2) * NT + tid] = fp;
-      const float fpdvj = fp / jcbk;                                                 // pgradiv.f90:149
-      const float wb8s = (s.p[ty + 1][tx + 1] * rst + fp * rbr * a.dtw) / rcsq * a.g05n;  // buoywsi.f90:171
+      const float jcb8u = cols[C_JCB8U * ncol + k], jcb8v = cols[C_JCB8V * ncol + k];
+      const float rcsq = cols[C_RCSQ * ncol + k], rst = cols[C_RST * ncol + k];
+      const float rbr = cols[C_RBR * ncol + k];
+      float phd = (jcb8u * un0 - jcb8u * un1) * dxiv + (jcb8v * vn0 - jcb8v * vn1) * dyiv;  // diver2d.f90:288
+      phd = rcsq * phd;                                                                       // diverpih.f90:208
+      const float wk = W0[oy * BX + ox], wk1 = W1[oy * BX + ox];
+      const float pvd = rcsq * (wk - wk1) * dziv;                                             // diverpiv.f90:124
+      const float fp = PF[ty * BX + ox] + phd + weic1m * (a.g05 * (wk + wk1) * rst + pvd);    // advbspi.f90:158
+      a.p_new[id] = fp;  // parked until the way down
+      const float fpdvj = fp * ijcbk;                                                          // pgradiv.f90:149
+      const float wb8s = (ppo * rst + fp * rbr * a.dtw) * cols[C_IRCSQ * ncol + k] * a.g05n;                      // buoywsi.f90:171
       if (k >= 3) {
-        const float wpg = (t3v_prev - t3v) * a.dziv;                                 // pgrad.f90:320
-        float fw = __ldg(a.wfrc + id) + wpg + (fpdvj_prev - fpdvj) * a.dtdzw;        // pgradiv.f90:163
-        if (a.buyopt == 1) fw = fw + (wb8s_prev + wb8s);                             // buoywsi.f90:205
-        const float wrhs = wk + dts * fw / COL(C_RST8W, k);                          // stepwi.f90:325
-        // gaussel.f90:189-240 in double with precomputed 1-D factors
+        const float wpg = (t3v_prev - t3v) * dziv;                                            // pgrad.f90:320
+        float fw = WF[ty * BX + ox] + wpg + (fpdvj_prev - fpdvj) * a.dtdzw;                   // pgradiv.f90:163
+        if (a.buyopt == 1) fw = fw + (wb8s_prev + wb8s);                                      // buoywsi.f90:205
+        const float wrhs = wk + dts * fw * cols[C_IRST8W * ncol + k];                          // stepwi.f90:325
+        // gaussel.f90:189-240 in double with the 1-D factors
         const double rr = (double)__ldg(a.thom_rr + k), aa = __ldg(a.thom_aa + k);
-        double f = (k == 3) ? (double)wrhs * aa : ((double)wrhs - rr * fprev) * aa;
+        const double f = (k == 3) ? (double)wrhs * aa : ((double)wrhs - rr * fprev) * aa;
         fcol[(k - 3) * NT + tid] = f;
         fprev = f;
       }
@@ -216,43 +243,61 @@ k_hevi_substep(const HeviArgs a) {
       fpdvj_prev = fpdvj;
       wb8s_prev = wb8s;
     }
-    // The next iteration's staging overwrites s.u/s.v/s.p; s.un/s.vn are
-    // rewritten only after two more barriers.
-    __syncthreads();
   }
 
-  // --- way down: back substitution, w BCs, p' update ----------------------
+  if (__syncthreads_or(fail)) {
+    // A bounded wait gave up: record it, let the copies still in flight
+    // land (bounded again) so no TMA write outlives the block, and leave.
+    if (tid == 0) {
+      atomicExch(a.err, 1);
+      const int kmax = min(nk - 2 + S - 1, klast);
+      for (int s = 0; s < S; ++s) {
+        int kl = -1;
+        for (int k = 2; k <= kmax; ++k)
+          if ((k - 2) % S == s) kl = k;
+        if (kl >= 0) mbar_wait(&bars[s], ((kl - 2) / S) & 1);
+      }
+    }
+    return;
+  }
+
+  // --- way down: back substitution, w boundary rows, p' update ------------
   if (own) {
-    const float dziv = a.dziv;
-    float wup = 0.f;          // w(k+1) as float; w(nk-1)=0 (vbcw.f90:481)
+    float wup = 0.f;          // w(k+1) as float; w(nk-1) = 0 (vbcw.f90:481)
     double wupd = 0.0;        // w(k+1) as double for the recurrence
     float w3 = 0.f, wkend = 0.f, p2 = 0.f, p3 = 0.f, pkend = 0.f;
-    for (int k = nk - 2; k >= 2; --k) {
+    long long idk = g.at(i, j, nk - 2);
+    float fpn = a.p_new[idk], pon = a.p_old[idk];
+    for (int k = nk - 2; k >= 2; --k, idk -= plane) {
+      const float fpb = fpn, po = pon;
+      if (k > 2) { fpn = a.p_new[idk - plane]; pon = a.p_old[idk - plane]; }
       float wk;
       if (k >= 3) {
-        double f = fcol[(k - 3) * NT + tid];
-        double wd = (k == nk - 2) ? f : f - __ldg(a.thom_cp + k) * wupd;            // gaussel.f90:254
+        const double f = fcol[(k - 3) * NT + tid];
+        const double wd = (k == nk - 2) ? f : f - __ldg(a.thom_cp + k) * wupd;                  // gaussel.f90:254
         wupd = wd;
         wk = (float)wd;
-        store_periodic(a.w_new, g, STAG_S, i, j, k, wk);
+        if (edge) store_periodic(a.w_new, g, STAG_S, i, j, k, wk);
+        else a.w_new[idk] = wk;
         if (k == 3) w3 = wk;
         if (k == nk - 2) wkend = wk;
       } else {
-        wk = 0.f;             // vbcw.f90:317 (flat terrain)
+        wk = 0.f;  // vbcw.f90:317 (flat terrain)
       }
-      const long long id = g.at(i, j, k);
-      const float rcsq = COL(C_RCSQ, k), rst = COL(C_RST, k), jcb = COL(C_JCB, k);
-      const float pvd = rcsq * (wk - wup) * dziv;                                     // diverpiv.f90:124
-      const float fp = fpcol[(k - 2) * NT + tid] + a.weicoe * (a.g05 * (wk + wup) * rst + pvd);  // advbspi.f90:175
-      const float pn = po[id] + dts * fp / jcb;                                      // steppi.f90:217
-      store_periodic(a.p_new, g, STAG_S, i, j, k, pn);
+      const float rcsq = cols[C_RCSQ * ncol + k], rst = cols[C_RST * ncol + k];
+      const float jcb = cols[C_JCB * ncol + k];
+      const float pvd = rcsq * (wk - wup) * dziv;                                              // diverpiv.f90:124
+      const float fp = fpb + a.weicoe * (a.g05 * (wk + wup) * rst + pvd);                        // advbspi.f90:175
+      const float pn = po + dts * fp * cols[C_IJCB * ncol + k];                                                     // steppi.f90:217
+      if (edge) store_periodic(a.p_new, g, STAG_S, i, j, k, pn);
+      else a.p_new[idk] = pn;
       if (k == 2) p2 = pn;
       if (k == 3) p3 = pn;
       if (k == nk - 2) pkend = pn;
       wup = wk;
     }
     // vbcw.f90:285,317,471,481 (flat terrain; wc = w / jcb8w when stretched)
-    const float j8w3 = COL(C_JCB8W, 3), j8wt = COL(C_JCB8W, nk - 2);
+    const float j8w3 = cols[C_JCB8W * ncol + 3], j8wt = cols[C_JCB8W * ncol + nk - 2];
     const float wc3 = a.sthopt ? w3 / j8w3 : w3;
     const float wct = a.sthopt ? wkend / j8wt : wkend;
     store_periodic(a.w_new, g, STAG_S, i, j, 1, -j8w3 * wc3 - 0.f);
@@ -263,42 +308,51 @@ k_hevi_substep(const HeviArgs a) {
     store_periodic(a.p_new, g, STAG_S, i, j, 1, (a.bbc == 2) ? 2.f * p2 - p3 : p2);
     store_periodic(a.p_new, g, STAG_S, i, j, nk - 1, pkend);
     // Level nk of u, v, p' is not touched by the small step: carry it over.
-    store_periodic(a.p_new, g, STAG_S, i, j, nk, po[g.at(i, j, nk)]);
-    store_periodic(a.u_new, g, STAG_U, i, j, nk, uo[g.at(i, j, nk)]);
-    store_periodic(a.v_new, g, STAG_V, i, j, nk, vo[g.at(i, j, nk)]);
+    store_periodic(a.p_new, g, STAG_S, i, j, nk, a.p_old[g.at(i, j, nk)]);
+    store_periodic(a.u_new, g, STAG_U, i, j, nk, a.u_old[g.at(i, j, nk)]);
+    store_periodic(a.v_new, g, STAG_V, i, j, nk, a.v_old[g.at(i, j, nk)]);
     if (i == ilast && i + 1 == ni - 1)
-      store_periodic(a.u_new, g, STAG_U, i + 1, j, nk, uo[g.at(i + 1, j, nk)]);
+      store_periodic(a.u_new, g, STAG_U, i + 1, j, nk, a.u_old[g.at(i + 1, j, nk)]);
     if (j == jlast && j + 1 == nj - 1)
-      store_periodic(a.v_new, g, STAG_V, i, j + 1, nk, vo[g.at(i, j + 1, nk)]);
+      store_periodic(a.v_new, g, STAG_V, i, j + 1, nk, a.v_old[g.at(i, j + 1, nk)]);
   }
-#undef COL
 }
 
-template <int TX, int TY>
-int launch_hevi_t(const HeviArgs& a, cudaStream_t st) {
+template <int TY, int S>
+int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
+  using L = HeviLayout<TY, S>;
   const Grid& g = a.g;
   const int nx = g.ni - 3, ny = g.nj - 3;
-  dim3 block(TX, TY);
-  dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY);
-  size_t dyn = sizeof(double) * (size_t)(g.nk - 4) * TX * TY + sizeof(float) * (size_t)(g.nk - 3) * TX * TY;
+  const size_t bytes = L::bytes(g.nk);
+  if (bytes > 227 * 1024) return CRESS_E_UNSUPPORTED;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_hevi_substep<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (cudaFuncSetAttribute(k_hevi_substep<TY, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024) != cudaSuccess)
+      return CRESS_E_CUDA;
     attr_set = true;
   }
-  if (dyn + sizeof(HeviSmem<TX, TY>) > 220 * 1024) return CRESS_E_UNSUPPORTED;
-  k_hevi_substep<TX, TY><<<grid, block, dyn, st>>>(a);
+  dim3 block(kHeviTX, TY);
+  dim3 grid((nx + kHeviTX - 1) / kHeviTX, (ny + TY - 1) / TY);
+  k_hevi_substep<TY, S><<<grid, block, bytes, st>>>(maps, a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
 }  // namespace
 
-int launch_hevi_substep(const HeviArgs& a, int tile, cudaStream_t st) {
+int hevi_tile_rows(int tile) {
   switch (tile) {
-    case 1: return launch_hevi_t<32, 2>(a, st);
-    case 2: return launch_hevi_t<32, 8>(a, st);
-    case 3: return launch_hevi_t<16, 8>(a, st);
-    default: return launch_hevi_t<32, 4>(a, st);
+    case 1: return 2;
+    case 2: return 8;
+    default: return 4;
+  }
+}
+
+int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st) {
+  switch (tile) {
+    case 1: return launch_t<2, 6>(a, maps, st);
+    case 2: return launch_t<8, 4>(a, maps, st);
+    default: return launch_t<4, 5>(a, maps, st);
   }
 }
 

@@ -1,5 +1,6 @@
 // HE-VI substep kernel interface (internal to the library).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "status.h"
@@ -10,23 +11,45 @@ namespace cress {
 // stored as col[field*(nk+1) + k], k = 1..nk.
 enum ColField {
   C_JCB = 0, C_JCB8U, C_JCB8V, C_JCB8W, C_RBR, C_PTBR, C_RST, C_RST8U, C_RST8V, C_RST8W, C_RCSQ,
-  C_PBR, C_QVBR, C_UBR, C_VBR, C_ZPH8S, C_NFIELDS
+  C_PBR, C_QVBR, C_UBR, C_VBR, C_ZPH8S,
+  // reciprocals (float) of per-level divisors, so the kernels multiply
+  C_IRST8U, C_IRST8V, C_IJCB, C_IRCSQ, C_IRST8W, C_IJCB8W, C_NFIELDS
+};
+
+// Width (floats) of every TMA box of the HE-VI kernel: x from i0-2 (a
+// multiple of 32, so 16-byte aligned) to i0+33, covering the 32-column
+// tile with the x halos the stencils need.
+constexpr int kHeviTX = 32;
+constexpr int kHeviBoxX = 36;
+
+// Rows of the staged boxes (tile height TY): old u, v, w, p' carry y halos.
+template <int TY> struct HeviRows {
+  static constexpr int u = TY + 2, v = TY + 3, w = TY + 2, p = TY + 2;
+  static constexpr int uf = TY, vf = TY + 1, wf = TY, pf = TY;
+};
+
+// Tensor maps of the eight staged fields (3-D: x = i, y = j, z = k-1).
+struct HeviMaps {
+  CUtensorMap u, v, w, p, uf, vf, wf, pf;
 };
 
 struct HeviArgs {
   Grid g;
-  const float* u_old; const float* v_old; const float* w_old; const float* p_old;
+  const float* u_old; const float* v_old; const float* p_old;
   float* u_new; float* v_new; float* w_new; float* p_new;
-  const float* ufrc; const float* vfrc; const float* wfrc; const float* pfrc;
   const float* col;       // 1-D base columns
   const float* thom_rr;   // [k] sub-diagonal a_k of the w system (float, as formed by stepwi)
   const double* thom_aa;  // [k] 1/(b_k - a_k c'_{k-1})
   const double* thom_cp;  // [k] c'_k
+  int* err;               // device error word (nonzero: a bounded wait gave up)
   float dts, dxiv, dyiv, dziv, divch, divcv, weicoe, dtdzw, dtw, g05, g05n;
   int divopt, buyopt, sthopt, bbc;
 };
 
-// tile: 0 = 32x4 (default), 1 = 32x2, 2 = 32x8, 3 = 16x8
-int launch_hevi_substep(const HeviArgs& a, int tile, cudaStream_t st);
+// Tile heights the kernel is instantiated for.
+int hevi_tile_rows(int tile);
+// Launch one substep; `maps` must describe the buffers in `a` with the
+// box rows of HeviRows<hevi_tile_rows(tile)>.
+int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st);
 
 }  // namespace cress

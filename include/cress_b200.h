@@ -81,8 +81,9 @@ int cress_abi_version(void);
 int cress_create(const cress_cfg* cfg, int device, cress_ctx** out);
 void cress_destroy(cress_ctx* ctx);
 
-/* Use an external CUDA stream (cudaStream_t passed as void*); 0 = the
- * context's own stream.  All work of the context is ordered on it. */
+/* Use an external CUDA stream (cudaStream_t passed as void*); NULL returns
+ * to the context's own (non-blocking) stream.  All work of the context is
+ * ordered on it. */
 int cress_set_stream(cress_ctx* ctx, void* stream);
 int cress_sync(cress_ctx* ctx);
 

@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle_cress.so")
 LIB_OMP = os.path.join(BUILD, "liboracle_cress_omp.so")
-SOURCES = ["oracle_capi.cpp"]
+SOURCES = ["oracle_capi.cpp", "oracle_dry.cpp"]
 HEADERS = [f for f in os.listdir(HERE) if f.endswith(".h")]
 
 _FP = ctypes.POINTER(ctypes.c_float)

@@ -1,0 +1,173 @@
+// Oracle: one leapfrog large step of the dry solver (s_intgdrv with
+// s_fdmdrv, SrcOrig/intgdrv.f90:866-1119, SrcOrig/fdmdrv.f90:661-704).
+//
+// TEST INFRASTRUCTURE ONLY (see arr.h).
+#pragma once
+#include <vector>
+#include "large.h"
+
+namespace oracle {
+
+// Prognostic state of one time level.
+template <class R>
+struct Level {
+  F3<R> u, v, w, pp, ptp;
+  void resize(int ni, int nj, int nk) {
+    u.resize(ni, nj, nk); v.resize(ni, nj, nk); w.resize(ni, nj, nk);
+    pp.resize(ni, nj, nk); ptp.resize(ni, nj, nk);
+  }
+};
+
+template <class R>
+struct DryRun {
+  Opts o;
+  LargeOpts lo;
+  int sthopt = 0;
+  Base<R> b;
+  std::vector<R> rbct;   // vspdmp coefficient rbct(k,2)
+  R fc = R(0);           // 0.5*omega*sin(lat)
+  Level<R> p, c, f;      // t-dt, t, t+dt
+  // scratch
+  F3<R> ufrc, vfrc, wfrc, pfrc, ptfrc, wc, rxu, rxv, rxw, t1, t2, t3, t4, t5, jxu, jxv, jxw;
+  SmallScratch<R> ss;
+  void alloc() {
+    const int ni = o.ni, nj = o.nj, nk = o.nk;
+    p.resize(ni, nj, nk); c.resize(ni, nj, nk); f.resize(ni, nj, nk);
+    for (F3<R>* a : {&ufrc, &vfrc, &wfrc, &pfrc, &ptfrc, &wc, &rxu, &rxv, &rxw, &t1, &t2, &t3, &t4,
+                     &t5, &jxu, &jxv, &jxw})
+      a->resize(ni, nj, nk);
+    ss.resize(ni, nj, nk);
+  }
+};
+
+// s_forceuvw (forceuvw.f90:423-626) for tubopt=0, advopt=2: zero forcing,
+// phy2cnt, smoo4uvw on the past level, vspuvw, coriuv, buoywb, rstuvwc,
+// advuvw on the present level.
+template <class R>
+void forceuvw(DryRun<R>& r) {
+  const Opts& o = r.o;
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  r.ufrc.fill(R(0)); r.vfrc.fill(R(0)); r.wfrc.fill(R(0));
+  phy2cnt(o, r.sthopt, r.b, r.c.w, r.wc);                               // forceuvw.f90:446
+  if (r.lo.smtopt % 10 == 2 || r.lo.smtopt % 10 == 3) {                 // forceuvw.f90:469
+    // smoo4uvw.f90:220-233: a = rst8u*(up-ubr)/jcb8u over k=1..nk-1, j=0..nj, i=0..ni+1
+    for (int k = 1; k <= nk - 1; ++k)
+      for (int j = 0; j <= nj; ++j)
+        for (int i = 0; i <= ni + 1; ++i)
+          r.t4(i, j, k) = r.b.rst8u(i, j, k) * (r.p.u(i, j, k) - r.b.ubr(i, j, k)) / r.b.jcb8u(i, j, k);
+    smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 1, 2, nj - 2, 2, nk - 2, false,
+            r.ufrc, r.t1, r.t2, r.t3);
+    for (int k = 1; k <= nk - 1; ++k)                                   // smoo4uvw.f90:338-351
+      for (int j = 0; j <= nj + 1; ++j)
+        for (int i = 0; i <= ni; ++i)
+          r.t4(i, j, k) = r.b.rst8v(i, j, k) * (r.p.v(i, j, k) - r.b.vbr(i, j, k)) / r.b.jcb8v(i, j, k);
+    smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 2, 2, nj - 1, 2, nk - 2, false,
+            r.vfrc, r.t1, r.t2, r.t3);
+    for (int k = 1; k <= nk; ++k)                                       // smoo4uvw.f90:456-469
+      for (int j = 0; j <= nj; ++j)
+        for (int i = 0; i <= ni; ++i)
+          r.t4(i, j, k) = r.b.rst8w(i, j, k) * r.p.w(i, j, k) / r.b.jcb8w(i, j, k);
+    smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 2, 2, nj - 2, 2, nk - 1, true,
+            r.wfrc, r.t1, r.t2, r.t3);
+  }
+  if (r.lo.vspopt >= 1)                                                 // forceuvw.f90:519
+    vspuvw(o, r.lo, r.b, r.rbct, r.p.u, r.p.v, r.p.w, r.ufrc, r.vfrc, r.wfrc, r.t5);
+  if (r.lo.coropt == 1) coriuv(o, r.fc, r.b, r.c.u, r.c.v, r.ufrc, r.vfrc, r.t1);   // :544
+  buoywb(o, false, r.b, r.c.ptp, (const F3<R>*)nullptr, (const F3<R>*)nullptr, r.wfrc, r.t1);  // :596
+  rstuvwc(o, r.b, r.c.u, r.c.v, r.wc, r.rxu, r.rxv, r.rxw);             // :614
+  advuvw(o, r.rxu, r.rxv, r.rxw, r.c.u, r.c.v, r.c.w, r.ufrc, r.vfrc, r.wfrc, r.t1, r.t2, r.t3, r.t4);  // :626
+}
+
+// s_forcep (forcep.f90:254-311): advp (J-weighted fluxes, advp.f90:249-291),
+// smoo4p on the past level, vspp when vspvar(4:4)='o'.
+template <class R>
+void forcep(DryRun<R>& r) {
+  const Opts& o = r.o;
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  for (int k = 1; k <= nk - 1; ++k) {                                   // advp.f90:255-277
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni; ++i) r.jxu(i, j, k) = r.b.jcb8u(i, j, k) * r.c.u(i, j, k);
+    for (int j = 1; j <= nj; ++j)
+      for (int i = 1; i <= ni - 1; ++i) r.jxv(i, j, k) = r.b.jcb8v(i, j, k) * r.c.v(i, j, k);
+  }
+  for (int k = 1; k <= nk; ++k)                                         // advp.f90:279-291
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) r.jxw(i, j, k) = r.b.jcb8w(i, j, k) * r.wc(i, j, k);
+  advs(o, r.jxu, r.jxv, r.jxw, r.c.pp, r.pfrc, r.t1, r.t2, r.t3);
+  if (r.lo.smtopt % 10 == 2 || r.lo.smtopt % 10 == 3)
+    smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.p.pp, 2, ni - 2, 2, nj - 2, 2, nk - 2, false,
+            r.pfrc, r.t1, r.t2, r.t3);
+  if (r.lo.vspopt >= 1 && r.lo.vspvar[3] == 'o') vsp_scalar(o, r.lo.ksp0, r.rbct, r.b.jcb, r.p.pp, r.pfrc);
+}
+
+// s_forcept (forcept.f90:344-446), tubopt=0: advs, smoo4s on rbr*ptpp,
+// vsps (rst-weighted), advbspt.
+template <class R>
+void forcept(DryRun<R>& r) {
+  const Opts& o = r.o;
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  advs(o, r.rxu, r.rxv, r.rxw, r.c.ptp, r.ptfrc, r.t1, r.t2, r.t3);
+  if (r.lo.smtopt % 10 == 2 || r.lo.smtopt % 10 == 3) {
+    for (int k = 1; k <= nk - 1; ++k)                                   // smoo4s.f90:184-197
+      for (int j = 0; j <= nj; ++j)
+        for (int i = 0; i <= ni; ++i) r.t4(i, j, k) = r.b.rbr(i, j, k) * r.p.ptp(i, j, k);
+    smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 2, 2, nj - 2, 2, nk - 2, false,
+            r.ptfrc, r.t1, r.t2, r.t3);
+  }
+  if (r.lo.vspopt >= 1 && r.lo.vspvar[4] == 'o') vsp_scalar(o, r.lo.ksp0, r.rbct, r.b.rst, r.p.ptp, r.ptfrc);
+  advbspt(o, r.b, r.c.w, r.ptfrc, r.t1);
+}
+
+// One large step (leapfrog from t-dt to t+dt with dtb, nsstp substeps of
+// dts): forcing, small steps, s_steps for theta' (steps.f90:506-574, 3979),
+// s_timeflt (timeflt.f90:335-404), shift2nd planes and swp2nxt rotation.
+template <class R>
+void intgdrv_dry(DryRun<R>& r, R dtb, int nsstp, R dts) {
+  const Opts& o = r.o;
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  forceuvw(r);
+  forcep(r);
+  forcept(r);
+  // s_smalldrv (smalldrv.f90:343-398): future = past, then the substeps.
+  r.f.u = r.p.u; r.f.v = r.p.v; r.f.w = r.p.w; r.f.pp = r.p.pp;
+  phy2cnt(o, r.sthopt, r.b, r.f.w, r.wc);
+  for (int n = 0; n < nsstp; ++n)
+    hevi<R>(o, r.sthopt, dts, r.b, r.ufrc, r.vfrc, r.wfrc, r.pfrc, r.f.ptp, r.f.u, r.f.v, r.f.w, r.wc,
+            r.f.pp, r.ss);
+  // s_steps (steps.f90:506-574): ptpf = ptpp + ptfrc * 2 dtb / rst
+  const R dtb2 = R(2) * dtb;
+  for (int k = 2; k <= nk - 2; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i) {
+        const R dtdrst = dtb2 / r.b.rst(i, j, k);
+        r.f.ptp(i, j, k) = r.p.ptp(i, j, k) + r.ptfrc(i, j, k) * dtdrst;
+      }
+  bcycle(o, 2, 1, ni - 2, ni - 1, 2, 1, nj - 2, nj - 1, nk, r.f.ptp);   // steps.f90:3979
+  // s_timeflt (timeflt.f90:335-404)
+  const R fcoe = R(r.lo.filcoe), m1fc2 = R(1) - R(2) * R(r.lo.filcoe);
+  for (int k = 1; k <= nk - 1; ++k) {
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni; ++i) r.c.u(i, j, k) = m1fc2 * r.c.u(i, j, k) + fcoe * (r.f.u(i, j, k) + r.p.u(i, j, k));
+    for (int j = 1; j <= nj; ++j)
+      for (int i = 1; i <= ni - 1; ++i) r.c.v(i, j, k) = m1fc2 * r.c.v(i, j, k) + fcoe * (r.f.v(i, j, k) + r.p.v(i, j, k));
+  }
+  for (int k = 1; k <= nk; ++k)
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) r.c.w(i, j, k) = m1fc2 * r.c.w(i, j, k) + fcoe * (r.f.w(i, j, k) + r.p.w(i, j, k));
+  for (int k = 1; k <= nk - 1; ++k)
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) {
+        r.c.pp(i, j, k) = m1fc2 * r.c.pp(i, j, k) + fcoe * (r.f.pp(i, j, k) + r.p.pp(i, j, k));
+        r.c.ptp(i, j, k) = m1fc2 * r.c.ptp(i, j, k) + fcoe * (r.f.ptp(i, j, k) + r.p.ptp(i, j, k));
+      }
+  // shift2nd on t and t+dt (intgdrv.f90:1005,1013): both periodic planes
+  for (Level<R>* L : {&r.c, &r.f}) {
+    halo_both(o, 'u', L->u); halo_both(o, 'v', L->v); halo_both(o, 's', L->w);
+    halo_both(o, 's', L->pp); halo_both(o, 's', L->ptp);
+  }
+  // swp2nxt (swp2nxt.f90:358-): past <- t, t <- t+dt
+  std::swap(r.p, r.c);
+  std::swap(r.c, r.f);
+}
+
+}  // namespace oracle

@@ -1,0 +1,49 @@
+"""The C-ABI library loads without a GPU and exports every function that
+include/cress_b200.h declares (no compute calls are made here)."""
+import ctypes
+import os
+import re
+import subprocess
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "cress_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b(?:int|void|long long|const char\*)\s+\*?\s*(cress_\w+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for n in ("cress_create", "cress_destroy", "cress_set_base3d", "cress_small_steps",
+              "cress_smalldrv", "cress_put_field", "cress_get_field"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(cress):
+    lib = ctypes.CDLL(cress.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", cress.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    exported = set(re.findall(r"\bT (cress_\w+)", out))
+    assert set(declared_functions()) <= exported
+
+
+def test_abi_version_and_error_string(cress):
+    L = cress.lib()
+    assert L.cress_abi_version() >= 1
+    assert isinstance(L.cress_last_error(), bytes)
+
+
+def test_bad_config_rejected_without_gpu(cress):
+    # Argument checks run before any CUDA call.
+    c = cress.Cfg()
+    c.ni, c.nj, c.nk = 4, 4, 4
+    h = ctypes.c_void_p()
+    assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 1  # CRESS_E_ARG
+    c.ni, c.nj, c.nk = 20, 20, 20
+    c.impopt, c.dx, c.dy, c.dz = 0, 1.0, 1.0, 1.0
+    assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 2  # unsupported
