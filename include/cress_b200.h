@@ -118,6 +118,31 @@ int cress_smalldrv(cress_ctx* ctx, int nsstp, float dts,
  * created (instrumentation for benchmarks). */
 long long cress_launch_count(const cress_ctx* ctx);
 
+/* One HE-VI acoustic substep that allocates no device memory.  No
+ * counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc from inside their time loop, such as a host model that keeps
+ * all of its device arrays in a pool sized at start-up, or a framework
+ * whose caching allocator owns the device.  No context is needed.
+ *
+ * The caller passes device buffers it owns: the old u, v, w, p' and the
+ * four forcings (inputs) and the new u, v, w, p' (outputs), each in the
+ * layout a(0:ni+1, 0:nj+1, 1:nk) with the x pitch padded to
+ * round_up(ni+2, 32) floats, 16-byte aligned; base3d are host arrays as in
+ * cress_set_base3d.  The small per-column data the kernel needs (base-state
+ * columns, the w-system elimination factors, an error word) goes into one
+ * fixed __device__ array of about 28 KB per GPU, resident until the process
+ * exits; hence nk <= 256 (larger grids return CRESS_E_ARG).  Every call
+ * rewrites that array, so calls whose kernels overlap on the GPU race on
+ * it and must be serialized.  The first call on a device looks up the
+ * array's address with that device current; make it before any stream
+ * capture begins.  The call is synchronous on `stream` (NULL = the default
+ * stream) and returns CRESS_E_TIMEOUT if a bounded device-side wait gave up. */
+int cress_hevi_substep_noalloc(const cress_cfg* cfg, float dts, const float* const* base3d,
+                               const float* u_old, const float* v_old, const float* w_old,
+                               const float* p_old, const float* ufrc, const float* vfrc,
+                               const float* wfrc, const float* pfrc, float* u_new, float* v_new,
+                               float* w_new, float* p_new, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
