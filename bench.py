@@ -1,10 +1,17 @@
 """Benchmark: CReSS solver time integration on B200.
 
-Prints ONE JSON line (rank 0).  See the argparse help for the workload
-options.  Timing: CUDA events on the library's stream (shared with torch's
-current stream), barrier + synchronize around the timed region, max over
-ranks.  Multi-GPU runs are independent replicas (one domain per GPU, no
-data-path collective): "scaling": "weak".
+Workload (default): one leapfrog large step of the dry solver (s_intgdrv:
+forcing of u, v, w, p', theta'; 20 HE-VI acoustic substeps; theta' step;
+Asselin filter; periodic ghost planes) on a 512x512x64 grid with the
+moist-supercell geometry (dx = 1 km, stretched dz, 18 km top), a warm
+bubble in a sheared flow.  Metric: cell-updates/s (interior cells x large
+steps / s).
+
+Prints ONE JSON line (rank 0).  Timing: CUDA events on the library's stream
+(a dedicated torch stream that the library is told to use), barrier +
+synchronize around the timed region, max over ranks.  Multi-GPU runs are
+independent replicas (one domain per GPU, no data-path collective):
+"scaling": "weak".
 """
 import argparse
 import json
@@ -19,7 +26,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-HBM_BYTES_PER_CELL_SUBSTEP = 48  # u,v,w,p' read+write, 4 forcings read (float32)
+HEVI_BYTES_PER_CELL = 48  # u,v,w,p' read + write and 4 forcings read, float32
+METRIC = "cell-updates/s on 1 B200: plain vs learned-microphysics form at stated error"
 
 
 def measured_peaks():
@@ -77,25 +85,58 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def cpu_baseline_small(args, cfg, base, st, frc, threads):
-    """Oracle (C++ restatement, OpenMP) on a bounded sample of the workload:
-    the same nz and substep count on a horizontally reduced domain."""
-    import oracle
+def make_case(args, seed):
     from cress_b200 import cases
+    case = cases.dry_case(args.nx, args.ny, args.nz, args.dx, args.dz, sthopt=1, seed=seed,
+                          vspbar=0.005, shear=20.0)
+    ni, nj, nk = case["dims"]
+    zph = case["zph"]
+    case["botbar"] = 0.6 * zph[nk - 1]
+    return case
+
+
+def vspdmp_columns(nk, zph, vspbar, botbar):
+    """rbct(k), ksp0 of s_vspdmp (vspopt=2, vspdmp.f90:222-292), float32."""
+    rbct = np.zeros(nk + 1, np.float32)
+    ksp0 = 2
+    for k in range(3, nk + 1):
+        if np.float32(zph[k]) > np.float32(botbar):
+            ksp0 = k - 1
+            break
+    cc = np.float32(3.141592)
+    for k in range(2, nk):
+        z = np.float32(zph[k])
+        if z > np.float32(botbar):
+            rbct[k] = np.float32(0.5) * np.float32(vspbar) * (
+                np.float32(1) - np.cos(cc * (z - np.float32(botbar)) /
+                                       (np.float32(zph[nk - 1]) - np.float32(botbar))))
+    return rbct, ksp0
+
+
+def nsstp_of(dtbig, dtsml):
+    """slvstep.f90:176."""
+    return 20 * int(1.e2 * (dtbig + .001)) // int(1.e3 * (dtsml + .0001))
+
+
+def cpu_dry(args, threads, nx, ny, nsteps):
+    """Oracle (C++ restatement, OpenMP) on a bounded sample: nx x ny x nz."""
+    import oracle
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    sx, sy = args.cpu_nx, args.cpu_ny
-    (ni, nj, nk), b2, st2, frc2 = cases.acoustic_case(sx, sy, args.nz, args.dx, args.dz, seed=3,
-                                                      sthopt=1)
-    c2 = dict(cfg, ni=ni, nj=nj, nk=nk)
     oracle.build()
-    s = [a.copy() for a in st2]
+    sub = argparse.Namespace(**vars(args))
+    sub.nx, sub.ny = nx, ny
+    case = make_case(sub, 3)
+    ni, nj, nk = case["dims"]
+    cfg = dict(ni=ni, nj=nj, nk=nk, dx=args.dx, dy=args.dx, dz=args.dz, sthopt=1, smtopt=3,
+               vspopt=2, coropt=0, vspbar=0.005, botbar=case["botbar"])
+    past = [a.copy() for a in case["level"]]
+    now = [a.copy() for a in case["level"]]
     t0 = time.perf_counter()
-    oracle.small_steps(c2, b2, frc2, s, args.nsstp, args.dts, prec=32, fp64_solve=1, omp=True)
+    oracle.dry_steps(cfg, case["base"], case["zph"], past, now, nsteps, args.dtbig, args.dtsml,
+                     start=False, omp=True)
     dt = time.perf_counter() - t0
-    cells = sx * sy * args.nz
-    return {"value": cells / dt, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-            "sample": f"{sx}x{sy}x{args.nz} domain, one small-step loop of {args.nsstp} HE-VI "
-                      f"substeps (C++ oracle, OpenMP {threads} threads), {dt:.2f} s"}
+    cells = nx * ny * args.nz * nsteps
+    return cells / dt, dt
 
 
 def main():
@@ -109,8 +150,8 @@ def main():
     ap.add_argument("--nz", type=int, default=64)
     ap.add_argument("--dx", type=float, default=1000.0)
     ap.add_argument("--dz", type=float, default=281.25)
-    ap.add_argument("--nsstp", type=int, default=20)
-    ap.add_argument("--dts", type=float, default=0.5)
+    ap.add_argument("--dtbig", type=float, default=5.0)
+    ap.add_argument("--dtsml", type=float, default=0.5)
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--cpu-nx", type=int, default=128)
     ap.add_argument("--cpu-ny", type=int, default=128)
@@ -121,30 +162,32 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    cfg_json = {"workload": f"hevi small-step loop, {args.nx}x{args.ny}x{args.nz} moist-supercell "
-                            f"grid shape (stretched dz), {args.nsstp} substeps of dts={args.dts}",
-                "nx": args.nx, "ny": args.ny, "nz": args.nz, "nsstp": args.nsstp,
-                "l2": "inputs larger than L2 (8 x 72 MB fields per step)",
+    nsstp = nsstp_of(args.dtbig, args.dtsml)
+    cfg_json = {"workload": f"dry large step (forcing + {nsstp} HE-VI substeps + theta' step + "
+                            f"Asselin filter + periodic halos), {args.nx}x{args.ny}x{args.nz}, "
+                            f"dx={args.dx:g} m, stretched dz, dtbig={args.dtbig:g} s, "
+                            f"dtsml={args.dtsml:g} s; warm bubble in 5-25 m/s shear",
+                "nx": args.nx, "ny": args.ny, "nz": args.nz, "nsstp": nsstp,
+                "l2": "inputs larger than L2 (each field 72 MB)",
                 "parallelism": f"replicas{world}"}
-    metric = "cell-updates/s on 1 B200: plain vs learned-microphysics form at stated error"
+    cells = args.nx * args.ny * args.nz
 
     if args.impl == "reference":
         if rank != 0:
             return
-        from cress_b200 import cases
-        cfg = dict(dx=args.dx, dy=args.dx, dz=args.dz, sthopt=1, divopt=2, buyopt=1, weicoe=0.6)
         threads = os.cpu_count() or 1
-        times = []
-        res = None
-        for _ in range(args.warmup + args.steps):
-            res = cpu_baseline_small(args, cfg, None, None, None, threads)
-            times.append(res["value"])
-        v = float(np.median(times[args.warmup:]))
-        res["value"] = v
-        print(json.dumps({"metric": metric, "value": v, "unit": "cell-updates/s", "n_gpus": 0,
+        vals = []
+        for n in range(args.warmup + args.steps):
+            v, dt = cpu_dry(args, threads, args.cpu_nx, args.cpu_ny, 1)
+            vals.append(v)
+        v = float(np.median(vals[args.warmup:]))
+        cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} domain, one dry large step of "
+                         f"the C++ oracle (OpenMP, {threads} threads) per timed step"}
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": 0,
                           "steps": args.steps, "warmup": args.warmup, "impl": "reference",
                           "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-                          "config": cfg_json, "cpu_baseline": res,
+                          "config": cfg_json, "cpu_baseline": cpu,
                           "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}))
         return
@@ -156,22 +199,22 @@ def main():
 
     torch.cuda.set_device(local)
     if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    (ni, nj, nk), base, st, frc = cases.acoustic_case(args.nx, args.ny, args.nz, args.dx, args.dz,
-                                                      seed=100 + rank, sthopt=1)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    case = make_case(args, 100 + rank)
+    ni, nj, nk = case["dims"]
+    rbct, ksp0 = vspdmp_columns(nk, case["zph"], 0.005, case["botbar"])
     s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, args.dz, sthopt=1, tile=args.tile,
                           device=local)
-    # A dedicated (non-default) stream shared by the library and torch's
-    # events, so the events bracket exactly the library's kernels.
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    assert stream.cuda_stream != 0
     s.set_stream(stream.cuda_stream)
-    s.set_base3d(base)
-    for name, a in zip(("u", "v", "w", "pp"), st):
-        s.put_field(name, cress_b200.PAST, a)
-    for name, a in zip(("u", "v", "w", "pp"), frc):
-        s.put_field(name, cress_b200.FORCING, a)
+    s.set_base3d(case["base"])
+    s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
+    names = ["u", "v", "w", "pp", "ptp"]
+    for n, a in zip(names, case["level"]):
+        s.put_field(n, cress_b200.PAST, a)
+        s.put_field(n, cress_b200.NOW, a)
     s.sync()
 
     def barrier():
@@ -186,60 +229,86 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    s.large_step(0.5 * args.dtbig, nsstp, 0.5 * args.dtsml)   # the first (half) step
     for _ in range(args.warmup):
-        s.small_steps(args.nsstp, args.dts)
+        s.large_step(args.dtbig, nsstp, args.dtsml)
     barrier()
     l0 = s.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         e0.record(stream)
         for _ in range(args.steps):
-            s.small_steps(args.nsstp, args.dts)
+            s.large_step(args.dtbig, nsstp, args.dtsml)
         e1.record(stream)
         barrier()
     launches = s.launch_count() - l0
     ms = max_over_ranks(e0.elapsed_time(e1))
-    cells = args.nx * args.ny * args.nz
     value = world * cells * args.steps / (ms * 1e-3)
-    per_launch_s = ms * 1e-3 / (args.steps * args.nsstp)
-    peak, peak_kind = measured_peaks()
-    achieved = HBM_BYTES_PER_CELL_SUBSTEP * cells / per_launch_s / 1e9
 
-    # End to end through the public host-array entry point (s_smalldrv's
-    # interface): H2D of u,v,w,p' (past) and the 4 forcings from pinned host
-    # memory, the substeps, D2H of the 4 future fields, every step.
-    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
-    ins = [pin(a) for a in st + frc]
-    outs = [pin(np.empty_like(st[0])) for _ in range(4)]
+    # Dominant kernel (HE-VI substep): timed alone on the same state.
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(2, args.steps // 2)
+    s.small_steps(nsstp, args.dtsml)
+    barrier()
+    h0.record(stream)
+    for _ in range(reps):
+        s.small_steps(nsstp, args.dtsml)
+    h1.record(stream)
+    barrier()
+    hevi_ms = max_over_ranks(h0.elapsed_time(h1)) / (reps * nsstp)
+    peak, peak_kind = measured_peaks()
+    achieved = HEVI_BYTES_PER_CELL * cells / (hevi_ms * 1e-3) / 1e9
+
+    # End to end through the public API with host buffers: every step the
+    # past and present levels (10 fields) go host->device from pinned
+    # memory, one large step runs, the new present level (5 fields) comes
+    # back.
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    past_h = [pin(a) for a in case["level"]]
+    now_h = [pin(a) for a in case["level"]]
+    out_h = [pin(np.empty_like(a)) for a in case["level"]]
+
+    def e2e_step():
+        for n, a, b in zip(names, past_h, now_h):
+            s.put_field(n, cress_b200.PAST, a)
+            s.put_field(n, cress_b200.NOW, b)
+        s.large_step(args.dtbig, nsstp, args.dtsml)
+        for n, o in zip(names, out_h):
+            s.get_field(n, cress_b200.NOW, out=o)
+
     for _ in range(args.warmup):
-        s.smalldrv(args.nsstp, args.dts, *ins, out=outs)
+        e2e_step()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        s.smalldrv(args.nsstp, args.dts, *ins, out=outs)
+        e2e_step()
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
-           "h2d_bytes_per_step": int(sum(a.nbytes for a in ins)),
-           "d2h_bytes_per_step": int(sum(a.nbytes for a in outs))}
+           "h2d_bytes_per_step": int(sum(a.nbytes for a in past_h + now_h)),
+           "d2h_bytes_per_step": int(sum(a.nbytes for a in out_h))}
     s.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cfg = dict(dx=args.dx, dy=args.dx, dz=args.dz, sthopt=1, divopt=2, buyopt=1, weicoe=0.6)
-        cpu = cpu_baseline_small(args, cfg, None, None, None, os.cpu_count() or 1)
+        threads = os.cpu_count() or 1
+        v, dt = cpu_dry(args, threads, args.cpu_nx, args.cpu_ny, 1)
+        cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} domain, one dry large step of the "
+                         f"C++ oracle (OpenMP, {threads} threads), {dt:.2f} s"}
 
     if rank == 0:
         print(json.dumps({
-            "metric": metric, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": cfg_json,
+            "sim_s_per_wall_s": args.dtbig / (ms / args.steps * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "peak_source": peak_kind,
-                         "kernel": "k_hevi_substep", "bytes_per_launch": HBM_BYTES_PER_CELL_SUBSTEP * cells,
-                         "ms_per_launch": per_launch_s * 1e3},
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "kernel": "k_hevi_substep",
+                         "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
+                         "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
             "cpu_baseline": cpu}))
     if world > 1:

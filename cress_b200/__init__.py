@@ -45,7 +45,12 @@ class Cfg(ctypes.Structure):
                 ("buyopt", ctypes.c_int), ("gwmopt", ctypes.c_int), ("weicoe", ctypes.c_float),
                 ("wbc", ctypes.c_int), ("ebc", ctypes.c_int), ("sbc", ctypes.c_int),
                 ("nbc", ctypes.c_int), ("bbc", ctypes.c_int), ("tbc", ctypes.c_int),
-                ("tile", ctypes.c_int), ("reserved", ctypes.c_int * 16)]
+                ("tile", ctypes.c_int),
+                ("advopt", ctypes.c_int), ("smtopt", ctypes.c_int), ("vspopt", ctypes.c_int),
+                ("coropt", ctypes.c_int), ("tubopt", ctypes.c_int), ("cphopt", ctypes.c_int),
+                ("smhcoe", ctypes.c_float), ("smvcoe", ctypes.c_float), ("filcoe", ctypes.c_float),
+                ("fc", ctypes.c_float), ("vspvar", ctypes.c_char * 16),
+                ("reserved", ctypes.c_int * 8)]
 
 
 _lib = None
@@ -75,6 +80,8 @@ def lib():
     L.cress_smalldrv.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float] + [_FP] * 12
     L.cress_launch_count.argtypes = [ctypes.c_void_p]
     L.cress_launch_count.restype = ctypes.c_longlong
+    L.cress_set_base_large.argtypes = [ctypes.c_void_p, _FP, _FP, _FP, ctypes.c_int]
+    L.cress_large_step.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c_float]
     _lib = L
     return L
 
@@ -93,7 +100,8 @@ class Solver:
     """One domain on one GPU (a cress_ctx)."""
 
     def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6,
-                 tile=0, device=0):
+                 tile=0, device=0, smtopt=3, smhcoe=0.001, smvcoe=0.0004, vspopt=2,
+                 vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1):
         L = lib()
         c = Cfg()
         c.ni, c.nj, c.nk = ni, nj, nk
@@ -103,6 +111,9 @@ class Solver:
         c.wbc = c.ebc = c.sbc = c.nbc = -1
         c.bbc = c.tbc = 2
         c.tile = tile
+        c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = 2, smtopt, vspopt, coropt, 0, 0
+        c.smhcoe, c.smvcoe, c.filcoe, c.fc = smhcoe, smvcoe, filcoe, fc
+        c.vspvar = vspvar.encode()[:15]
         self.cfg = c
         self.shape = (nk, nj + 2, ni + 2)
         h = ctypes.c_void_p()
@@ -134,8 +145,9 @@ class Solver:
         assert a.shape == self.shape
         _check(lib().cress_put_field(self._h, FIELD_ID[name], level, fptr(a)))
 
-    def get_field(self, name, level):
-        a = np.empty(self.shape, np.float32)
+    def get_field(self, name, level, out=None):
+        a = np.empty(self.shape, np.float32) if out is None else out
+        assert a.shape == self.shape and a.dtype == np.float32 and a.flags.c_contiguous
         _check(lib().cress_get_field(self._h, FIELD_ID[name], level, fptr(a)))
         return a
 
@@ -153,3 +165,14 @@ class Solver:
 
     def launch_count(self):
         return lib().cress_launch_count(self._h)
+
+    def set_base_large(self, ubr, vbr, rbct, ksp0):
+        """Base winds and the Rayleigh coefficient rbct(:,:,:,2) (SrcOrig/vspdmp.f90)."""
+        arrs = [np.ascontiguousarray(x, dtype=np.float32) for x in (ubr, vbr, rbct)]
+        for a in arrs:
+            assert a.shape == self.shape
+        _check(lib().cress_set_base_large(self._h, *[fptr(a) for a in arrs], int(ksp0)))
+
+    def large_step(self, dtb, nsstp, dts):
+        """One s_intgdrv leapfrog step on the device-resident state."""
+        _check(lib().cress_large_step(self._h, float(dtb), int(nsstp), float(dts)))

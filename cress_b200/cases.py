@@ -114,6 +114,70 @@ def bcycle(a, stag):
     return a
 
 
+def _wrap_index(n, stag_axis):
+    """Source index of every position along one axis under the periodic wrap
+    of both ghost layers (bcycle + shift2nd planes): interior 2..n-2, period
+    n-3; the staggered axis also wraps n-1 (the duplicated face) and n+1."""
+    P = n - 3
+    src = np.arange(n + 2)
+    ghosts = [0, 1, n, n + 1, n - 1] if stag_axis else [0, 1, n - 1, n]
+    for g_ in ghosts:
+        src[g_] = 2 + (g_ - 2) % P
+    return src
+
+
+def periodic_fill(a, stag):
+    """Fill both periodic ghost layers of a (nk, nj+2, ni+2) array."""
+    nk, nj2, ni2 = a.shape
+    ni, nj = ni2 - 2, nj2 - 2
+    sx = _wrap_index(ni, stag == "u")
+    sy = _wrap_index(nj, stag == "v")
+    a[:] = a[:, sy][:, :, sx]
+    return a
+
+
+def dry_case(nx, ny, nz, dx, dz, sthopt=1, seed=0, ptp0=2.0, rad=None, u0=5.0, shear=10.0,
+             vspbar=0.0, botbar=1e9, noise=0.01, dthdz=0.003):
+    """Dry warm-bubble state for whole large steps.
+
+    Base wind ubr = u0 + shear * z/ztop (v = 0), theta'(bubble) = ptp0*cos^2 inside
+    the ellipsoid of radius `rad` (m, x/y/z) centred at mid-domain, z = 1.5 km,
+    plus seeded uniform +-noise K.  Returns a dict with dims, base (3-D
+    arrays incl. ubr, vbr), zph (w-level heights, index k), rbct/ksp0 left
+    for the caller (see oracle.vspdmp) and the initial level (past = now)."""
+    ni, nj, nk = dims(nx, ny, nz)
+    base, cols = base3d(ni, nj, nk, dz, sthopt=sthopt, dthdz=dthdz)
+    jcb = cols["jcb"].astype(np.float64)
+    zph = np.zeros(nk + 1)
+    for k in range(3, nk + 1):
+        zph[k] = zph[k - 1] + jcb[k - 1] * dz
+    zph[1] = -zph[3]
+    ztop = zph[nk - 1]
+    zs = cols["zs"]
+    ubr_col = (u0 + shear * np.clip(zs / ztop, 0.0, 1.0)).astype(np.float32)
+    base["ubr"] = expand(ubr_col, ni, nj, nk)
+    base["vbr"] = np.zeros_like(base["ubr"])
+    rng = np.random.default_rng(seed)
+    shp = (nk, nj + 2, ni + 2)
+    if rad is None:
+        rad = (min(nx, ny) * dx / 6.0, min(nx, ny) * dx / 6.0, 1500.0)
+    x = (np.arange(ni + 2) - 0.5 * (ni + 1)) * dx
+    y = (np.arange(nj + 2) - 0.5 * (nj + 1)) * dx
+    z = zs[1:nk + 1]
+    r = np.sqrt((x[None, None, :] / rad[0]) ** 2 + (y[None, :, None] / rad[1]) ** 2 +
+                ((z[:, None, None] - 1500.0) / rad[2]) ** 2)
+    ptp = np.where(r < 1.0, ptp0 * np.cos(0.5 * np.pi * r) ** 2, 0.0)
+    ptp = (ptp + rng.uniform(-noise, noise, shp)).astype(np.float32)
+    u = base["ubr"].copy()
+    v = np.zeros(shp, np.float32)
+    w = np.zeros(shp, np.float32)
+    pp = np.zeros(shp, np.float32)
+    level = [periodic_fill(u, "u"), periodic_fill(v, "v"), periodic_fill(w, "s"),
+             periodic_fill(pp, "s"), periodic_fill(ptp, "s")]
+    return dict(dims=(ni, nj, nk), base=base, cols=cols, zph=zph, level=level,
+                vspbar=vspbar, botbar=botbar)
+
+
 def _noise(rng, shape, amp):
     x = rng.standard_normal(shape)
     for ax in (1, 2):

@@ -13,6 +13,7 @@
 #include "common.cuh"
 #include "ctx.h"
 #include "hevi.cuh"
+#include "forcing.cuh"
 
 namespace cress {
 
@@ -237,6 +238,71 @@ int Ctx::small_steps(int nsstp, float dts) {
   return CRESS_OK;
 }
 
+// One dry large step on the device-resident state (s_intgdrv order,
+// SrcOrig/intgdrv.f90:866-1119).
+int Ctx::large_step(float dtb, int nsstp, float dts) {
+  if (!base_set || !large_set)
+    return set_error(CRESS_E_STATE, "cress_large_step: base state (set_base3d, set_base_large) not set");
+  if (cfg.advopt != 2 || cfg.tubopt != 0 || cfg.cphopt != 0 ||
+      !(cfg.smtopt == 0 || cfg.smtopt % 10 == 2 || cfg.smtopt % 10 == 3) ||
+      !(cfg.vspopt == 0 || cfg.vspopt == 2) || !(cfg.coropt == 0 || cfg.coropt == 1))
+    return set_error(CRESS_E_UNSUPPORTED,
+                     "cress_large_step: needs advopt=2, tubopt=0, cphopt=0, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
+  ForceArgs f{};
+  f.g = g;
+  f.col = col_d;
+  f.u = lev[CRESS_U][CRESS_NOW]; f.v = lev[CRESS_V][CRESS_NOW]; f.w = lev[CRESS_W][CRESS_NOW];
+  f.pp = lev[CRESS_PP][CRESS_NOW]; f.ptp = lev[CRESS_PTP][CRESS_NOW];
+  f.up = lev[CRESS_U][CRESS_PAST]; f.vp = lev[CRESS_V][CRESS_PAST]; f.wp = lev[CRESS_W][CRESS_PAST];
+  f.ppp = lev[CRESS_PP][CRESS_PAST]; f.ptpp = lev[CRESS_PTP][CRESS_PAST];
+  f.ufrc = lev[CRESS_U][CRESS_FORCING]; f.vfrc = lev[CRESS_V][CRESS_FORCING];
+  f.wfrc = lev[CRESS_W][CRESS_FORCING]; f.pfrc = lev[CRESS_PP][CRESS_FORCING];
+  f.ptpf = lev[CRESS_PTP][CRESS_FUTURE];
+  f.dxiv = 1.f / cfg.dx; f.dyiv = 1.f / cfg.dy; f.dziv = 1.f / cfg.dz;
+  f.smhcoe = cfg.smhcoe; f.smvcoe = cfg.smvcoe;
+  f.fc = cfg.fc;
+  f.dtb2 = 2.f * dtb;
+  f.smtopt = cfg.smtopt; f.vspopt = cfg.vspopt; f.coropt = cfg.coropt; f.sthopt = cfg.sthopt;
+  f.ksp0 = ksp0;
+  auto on = [&](int n) { return cfg.vspvar[n] == 'o' ? 1 : 0; };
+  f.vsp_u = on(0); f.vsp_v = on(1); f.vsp_w = on(2); f.vsp_p = on(3); f.vsp_pt = on(4);
+  int rc = launch_force(f, stream);
+  ++launches;
+  if (rc) return set_error(rc, "forcing launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  if ((rc = small_steps(nsstp, dts))) return rc;
+  FilterArgs t{};
+  t.g = g;
+  t.u = lev[CRESS_U][CRESS_NOW]; t.v = lev[CRESS_V][CRESS_NOW]; t.w = lev[CRESS_W][CRESS_NOW];
+  t.pp = lev[CRESS_PP][CRESS_NOW]; t.ptp = lev[CRESS_PTP][CRESS_NOW];
+  t.uf = lev[CRESS_U][CRESS_FUTURE]; t.vf = lev[CRESS_V][CRESS_FUTURE]; t.wf = lev[CRESS_W][CRESS_FUTURE];
+  t.ppf = lev[CRESS_PP][CRESS_FUTURE]; t.ptpf = lev[CRESS_PTP][CRESS_FUTURE];
+  t.up = lev[CRESS_U][CRESS_PAST]; t.vp = lev[CRESS_V][CRESS_PAST]; t.wp = lev[CRESS_W][CRESS_PAST];
+  t.ppp = lev[CRESS_PP][CRESS_PAST]; t.ptpp = lev[CRESS_PTP][CRESS_PAST];
+  t.filcoe = cfg.filcoe;
+  if ((rc = launch_timeflt(t, stream))) return set_error(rc, "timeflt launch failed");
+  ++launches;
+  HaloArgs h{};
+  h.g = g;
+  const int F[5] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP, CRESS_PTP};
+  const int S[5] = {STAG_U, STAG_V, STAG_S, STAG_S, STAG_S};
+  for (int lvl : {CRESS_NOW, CRESS_FUTURE})
+    for (int n = 0; n < 5; ++n) {
+      h.f[h.n] = lev[F[n]][lvl];
+      h.stag[h.n] = S[n];
+      ++h.n;
+    }
+  if ((rc = launch_halo(h, stream))) return set_error(rc, "halo launch failed");
+  ++launches;
+  // swp2nxt: past <- t, t <- t+dt (pointer rotation)
+  for (int n = 0; n < 5; ++n) {
+    float* p = lev[F[n]][CRESS_PAST];
+    lev[F[n]][CRESS_PAST] = lev[F[n]][CRESS_NOW];
+    lev[F[n]][CRESS_NOW] = lev[F[n]][CRESS_FUTURE];
+    lev[F[n]][CRESS_FUTURE] = p;
+  }
+  return CRESS_OK;
+}
+
 // Read and clear the device error word (bounded-wait failures).
 int Ctx::check_device_error() {
   int h = 0;
@@ -295,7 +361,12 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
       if (!c->lev[f][l]) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the state failed"); }
     if (!c->spare[f]) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the state failed"); }
   }
-  c->col_h.assign((size_t)C_NFIELDS * (cfg->nk + 1), 0.f);
+  // theta' has three time levels (its forcing goes straight into s_steps)
+  for (int l = 0; l < 3; ++l) {
+    c->lev[CRESS_PTP][l] = c->alloc_field();
+    if (!c->lev[CRESS_PTP][l]) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the state failed"); }
+  }
+  c->col_h.assign((size_t)C_NFIELDS_ALL * (cfg->nk + 1), 0.f);
   if ((rc = cuda_check(cudaMalloc(&c->col_d, sizeof(float) * c->col_h.size()), "cudaMalloc cols"))) {
     delete c;
     return rc;
@@ -429,6 +500,47 @@ int cress_smalldrv(cress_ctx* ctx, int nsstp, float dts, const float* up, const 
     if ((rc = c->get_host(out[n], c->lev[F[n]][CRESS_FUTURE]))) return rc;
   rc = cuda_check(cudaStreamSynchronize(c->stream), "cress_smalldrv sync");
   return rc ? rc : c->check_device_error();
+}
+
+int cress_set_base_large(cress_ctx* ctx, const float* ubr, const float* vbr, const float* rbct,
+                         int ksp0) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !ubr || !vbr || !rbct) return set_error(CRESS_E_ARG, "cress_set_base_large: null argument");
+  cudaSetDevice(c->device);
+  const int ni = c->cfg.ni, nj = c->cfg.nj, nk = c->cfg.nk;
+  if (ksp0 < 2 || ksp0 > nk) return set_error(CRESS_E_ARG, "cress_set_base_large: ksp0=%d", ksp0);
+  auto at = [&](const float* a, int i, int j, int k) {
+    return a[(size_t)i + (size_t)(ni + 2) * ((size_t)j + (size_t)(nj + 2) * (size_t)(k - 1))];
+  };
+  const float* src[3] = {ubr, vbr, rbct};
+  const int dst[3] = {C_UBR, C_VBR, C_RBCT};
+  const int ic = ni / 2, jc = nj / 2;
+  for (int n = 0; n < 3; ++n)
+    for (int k = 1; k <= nk; ++k) {
+      const float v = at(src[n], ic, jc, k);
+      c->col_h[(size_t)dst[n] * (nk + 1) + k] = v;
+      for (int j = 1; j <= nj - 1; ++j)
+        for (int i = 1; i <= ni - 1; ++i)
+          if (at(src[n], i, j, k) != v)
+            return set_error(CRESS_E_NONUNIFORM, "large-step base array %d varies horizontally at (%d,%d,%d)",
+                             n, i, j, k);
+    }
+  c->ksp0 = ksp0;
+  int rc = cuda_check(cudaMemcpyAsync(c->col_d, c->col_h.data(), sizeof(float) * c->col_h.size(),
+                                      cudaMemcpyHostToDevice, c->stream),
+                      "copy large-step columns");
+  if (rc) return rc;
+  rc = cuda_check(cudaStreamSynchronize(c->stream), "sync large-step columns");
+  if (rc) return rc;
+  c->large_set = true;
+  return CRESS_OK;
+}
+
+int cress_large_step(cress_ctx* ctx, float dtb, int nsstp, float dts) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  cudaSetDevice(c->device);
+  return c->large_step(dtb, nsstp, dts);
 }
 
 long long cress_launch_count(const cress_ctx* ctx) {

@@ -45,6 +45,9 @@ struct Ctx {
   int get_host(float* host, const float* src);
   int thomas_for(float dts, const ThomasSet** out);
   int small_steps(int nsstp, float dts);
+  int large_step(float dtb, int nsstp, float dts);
+  int ksp0 = 2;            // first Rayleigh-damped level
+  bool large_set = false;  // cress_set_base_large was called
   int tmap(const float* buf, int rows, CUtensorMap* out);
   int check_device_error();
   ~Ctx();

@@ -51,8 +51,19 @@ typedef struct cress_cfg {
   float weicoe;         /* implicit weight beta (SrcOrig/advbspi.f90:140) */
   int wbc, ebc, sbc, nbc;  /* lateral BCs after chknlslv: -1 = periodic */
   int bbc, tbc;         /* 2 = rigid (SrcOrig/vbcw.f90:201) */
-  int tile;             /* HE-VI tile shape id (0 = autotuned default) */
-  int reserved[16];
+  int tile;             /* HE-VI tile shape id (0 = default 32x4) */
+  /* large step (SrcOrig/forcedrv.f90:548-608, SrcOrig/timeflt.f90:335) */
+  int advopt;           /* 2 only: 4th-order horizontal advection */
+  int smtopt;           /* 0 none, 2 horizontal, 3 horizontal + vertical 4th-order smoothing */
+  int vspopt;           /* 0 none, 2 Rayleigh damping above botbar toward the base state */
+  int coropt;           /* 0 none, 1 f-plane Coriolis on u, v */
+  int tubopt;           /* 0 only (turbulence is not implemented on the GPU) */
+  int cphopt;           /* 0 only (dry) */
+  float smhcoe, smvcoe; /* smoothing coefficients */
+  float filcoe;         /* Asselin filter coefficient */
+  float fc;             /* 0.5*omega*sin(lat) (SrcOrig/trilat.f90:118-134) */
+  char vspvar[16];      /* sponge switches u v w p pt ... ('o' on / 'x' off) */
+  int reserved[8];
 } cress_cfg;
 
 typedef struct cress_ctx cress_ctx;
@@ -113,6 +124,22 @@ int cress_smalldrv(cress_ctx* ctx, int nsstp, float dts,
                    const float* up, const float* vp, const float* wp, const float* ppp,
                    const float* ufrc, const float* vfrc, const float* wfrc, const float* pfrc,
                    float* uf, float* vf, float* wf, float* ppf);
+
+/* Large-step base data beyond cress_set_base3d: the base winds ubr, vbr and
+ * the Rayleigh coefficient rbct(:,:,:,2) of s_vspdmp (SrcOrig/vspdmp.f90:
+ * 269-292), host arrays in reference layout (horizontally uniform), and
+ * ksp0(2), the first damped level (SrcOrig/vspdmp.f90:222-232). */
+int cress_set_base_large(cress_ctx* ctx, const float* ubr, const float* vbr, const float* rbct,
+                         int ksp0);
+
+/* One leapfrog large step on the device-resident state, replacing the body
+ * of s_intgdrv for a dry run (SrcOrig/intgdrv.f90:866-1119 with s_fdmdrv,
+ * SrcOrig/fdmdrv.f90:661-704): forcing of u, v, w, p', theta'
+ * (s_forcedrv), nsstp HE-VI substeps of dts (s_smalldrv), the theta' step
+ * (s_steps), the Asselin filter (s_timeflt), both periodic ghost planes
+ * (bcycle, s_shift2nd) and the time-level rotation (s_swp2nxt).  dtb is
+ * s_timeint's large step (half of dtbig on the first step). */
+int cress_large_step(cress_ctx* ctx, float dtb, int nsstp, float dts);
 
 /* Number of kernel launches the library issued since the context was
  * created (instrumentation for benchmarks). */

@@ -64,6 +64,49 @@ def lib(omp=False):
 
 BASE_NAMES = ["jcb", "jcb8u", "jcb8v", "jcb8w", "rbr", "ptbr", "rst", "rst8u", "rst8v",
               "rst8w", "rcsq"]
+DRY_BASE_NAMES = BASE_NAMES + ["ubr", "vbr"]
+STATE_NAMES = ["u", "v", "w", "pp", "ptp"]
+
+
+def vspdmp(nk, zph, vspbar, botbar):
+    """Rayleigh coefficient rbct(k) (index k) and ksp0 of s_vspdmp, vspopt=2."""
+    L = lib()
+    L.oracle_vspdmp.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                ctypes.c_double, _FP]
+    z = np.ascontiguousarray(zph, np.float64)
+    r = np.zeros(nk + 1, np.float32)
+    ksp0 = L.oracle_vspdmp(nk, z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), vspbar, botbar,
+                           r.ctypes.data_as(_FP))
+    return r, ksp0
+
+
+def dry_steps(cfg, base, zph, past, now, nsteps, dtbig, dtsml, start=True, prec=32, fp64_solve=1,
+              omp=False):
+    """Run nsteps dry large steps (s_intgdrv) on the CPU; past/now are lists of
+    u, v, w, pp, ptp arrays, updated in place.  omp=True uses the OpenMP build."""
+    L = lib(omp)
+    L.oracle_dry_steps.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(_FP), ctypes.POINTER(_FP), ctypes.c_int,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    io = (ctypes.c_int * 10)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
+                             cfg.get("buyopt", 1), int(fp64_solve), cfg.get("sthopt", 0),
+                             cfg.get("smtopt", 3), cfg.get("vspopt", 2), cfg.get("coropt", 0))
+    ro = (ctypes.c_double * 10)(cfg["dx"], cfg["dy"], cfg["dz"], cfg.get("weicoe", 0.6),
+                                cfg.get("smhcoe", 0.001), cfg.get("smvcoe", 0.0004),
+                                cfg.get("filcoe", 0.1), cfg.get("vspbar", 0.0),
+                                cfg.get("botbar", 1e9), cfg.get("fc", 0.0))
+    z = np.ascontiguousarray(zph, np.float64)
+    b = [np.ascontiguousarray(base[n], np.float32) for n in DRY_BASE_NAMES]
+    st = past + now
+    for s in st:
+        assert s.dtype == np.float32 and s.flags.c_contiguous
+    rc = L.oracle_dry_steps(prec, io, ro, z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            (_FP * len(b))(*[_fp(x) for x in b]),
+                            (_FP * len(st))(*[_fp(x) for x in st]), int(nsteps), float(dtbig),
+                            float(dtsml), int(bool(start)))
+    if rc != 0:
+        raise RuntimeError(f"oracle_dry_steps failed ({rc})")
 
 
 def _fp(a):

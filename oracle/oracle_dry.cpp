@@ -66,4 +66,16 @@ int oracle_dry_steps(int prec, const int* io, const double* ro, const double* zp
   return run_dry<float>(io, ro, zph, base, st, nsteps, dtbig, dtsml, start);
 }
 
+// s_vspdmp for vspopt=2 (vspdmp.f90:222-292) in float: rbct(k), k=1..nk
+// into rbct[k]; returns ksp0(2).
+int oracle_vspdmp(int nk, const double* zph, double vspbar, double botbar, float* rbct) {
+  Opts o;
+  o.nk = nk;
+  std::vector<double> z(zph, zph + nk + 1);
+  std::vector<float> r;
+  const int ksp0 = vspdmp<float>(o, z, vspbar, botbar, r);
+  for (int k = 0; k <= nk; ++k) rbct[k] = r[k];
+  return ksp0;
+}
+
 }  // extern "C"
