@@ -45,7 +45,10 @@ namespace {
 
 constexpr int r128(int n) { return (n + 31) / 32 * 32; }  // floats -> multiple of 128 B
 
-template <int TY, int S>
+// FT: element type of the column store of eliminated right-hand sides
+// (double by default; float halves the store and doubles resident blocks,
+// with the elimination recurrence itself still in double).
+template <int TY, int S, typename FT = double>
 struct HeviLayout {
   using R = HeviRows<TY>;
   static constexpr int BX = kHeviBoxX;
@@ -64,14 +67,14 @@ struct HeviLayout {
   __host__ __device__ static size_t cols_floats(int nk) { return (size_t)((C_NFIELDS * (nk + 1) + 31) / 32 * 32); }
   __host__ __device__ static size_t bytes(int nk) {
     return 4 * ((size_t)S * stage + t3h_floats + cols_floats(nk)) + 8 * (size_t)S +
-           8 * (size_t)(nk - 4) * (kHeviTX * TY);
+           sizeof(FT) * (size_t)(nk - 4) * (kHeviTX * TY);
   }
 };
 
-template <int TY, int S>
+template <int TY, int S, typename FT>
 __global__ void __launch_bounds__(kHeviTX * TY)
 k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
-  using L = HeviLayout<TY, S>;
+  using L = HeviLayout<TY, S, FT>;
   constexpr int TX = kHeviTX, BX = kHeviBoxX, NT = TX * TY;
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
@@ -90,7 +93,7 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   float* t3h = ring + S * L::stage;                // [(TY+2)][BX], rows from j0-1, x from i0-2
   float* cols = t3h + L::t3h_floats;               // [C_NFIELDS][nk+1]
   uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
-  double* fcol = reinterpret_cast<double*>(bars + S);  // [(nk-4)][NT]
+  FT* fcol = reinterpret_cast<FT*>(bars + S);  // [(nk-4)][NT]
 
   for (int n = tid; n < C_NFIELDS * ncol; n += NT) cols[n] = __ldg(a.col + n);
   if (tid == 0) {
@@ -236,7 +239,7 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
         // gaussel.f90:189-240 in double with the 1-D factors
         const double rr = (double)__ldg(a.thom_rr + k), aa = __ldg(a.thom_aa + k);
         const double f = (k == 3) ? (double)wrhs * aa : ((double)wrhs - rr * fprev) * aa;
-        fcol[(k - 3) * NT + tid] = f;
+        fcol[(k - 3) * NT + tid] = (FT)f;
         fprev = f;
       }
       t3v_prev = t3v;
@@ -273,7 +276,7 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       if (k > 2) { fpn = a.p_new[idk - plane]; pon = a.p_old[idk - plane]; }
       float wk;
       if (k >= 3) {
-        const double f = fcol[(k - 3) * NT + tid];
+        const double f = (double)fcol[(k - 3) * NT + tid];
         const double wd = (k == nk - 2) ? f : f - __ldg(a.thom_cp + k) * wupd;                  // gaussel.f90:254
         wupd = wd;
         wk = (float)wd;
@@ -318,41 +321,46 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   }
 }
 
-template <int TY, int S>
+template <int TY, int S, typename FT>
 int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
-  using L = HeviLayout<TY, S>;
+  using L = HeviLayout<TY, S, FT>;
   const Grid& g = a.g;
   const int nx = g.ni - 3, ny = g.nj - 3;
   const size_t bytes = L::bytes(g.nk);
   if (bytes > 227 * 1024) return CRESS_E_UNSUPPORTED;
   static bool attr_set = false;
   if (!attr_set) {
-    if (cudaFuncSetAttribute(k_hevi_substep<TY, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_hevi_substep<TY, S, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              227 * 1024) != cudaSuccess)
       return CRESS_E_CUDA;
     attr_set = true;
   }
   dim3 block(kHeviTX, TY);
   dim3 grid((nx + kHeviTX - 1) / kHeviTX, (ny + TY - 1) / TY);
-  k_hevi_substep<TY, S><<<grid, block, bytes, st>>>(maps, a);
+  k_hevi_substep<TY, S, FT><<<grid, block, bytes, st>>>(maps, a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
 }  // namespace
 
+// Tile ids: 0-2 keep the eliminated right-hand sides in double (the
+// product setting); 3-5 are the same tiles with a float column store.
 int hevi_tile_rows(int tile) {
   switch (tile) {
-    case 1: return 2;
-    case 2: return 8;
+    case 1: case 4: return 2;
+    case 2: case 5: return 8;
     default: return 4;
   }
 }
 
 int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st) {
   switch (tile) {
-    case 1: return launch_t<2, 6>(a, maps, st);
-    case 2: return launch_t<8, 4>(a, maps, st);
-    default: return launch_t<4, 5>(a, maps, st);
+    case 1: return launch_t<2, 6, double>(a, maps, st);
+    case 2: return launch_t<8, 4, double>(a, maps, st);
+    case 3: return launch_t<4, 4, float>(a, maps, st);
+    case 4: return launch_t<2, 5, float>(a, maps, st);
+    case 5: return launch_t<8, 4, float>(a, maps, st);
+    default: return launch_t<4, 5, double>(a, maps, st);
   }
 }
 
