@@ -81,7 +81,13 @@ def lib():
     L.cress_launch_count.argtypes = [ctypes.c_void_p]
     L.cress_launch_count.restype = ctypes.c_longlong
     L.cress_set_base_large.argtypes = [ctypes.c_void_p, _FP, _FP, _FP, ctypes.c_int]
-    L.cress_large_step.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c_float]
+    L.cress_large_step.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_float, ctypes.c_int,
+                                   ctypes.c_float]
+    L.cress_set_base_moist.argtypes = [ctypes.c_void_p, _FP, _FP]
+    L.cress_cloudphy.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_float]
+    L.cress_satadjst.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]
+    L.cress_get_precip.argtypes = [ctypes.c_void_p, _FP]
+    L.cress_put_precip.argtypes = [ctypes.c_void_p, _FP]
     _lib = L
     return L
 
@@ -101,7 +107,7 @@ class Solver:
 
     def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6,
                  tile=0, device=0, smtopt=3, smhcoe=0.001, smvcoe=0.0004, vspopt=2,
-                 vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1):
+                 vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1, cphopt=0):
         L = lib()
         c = Cfg()
         c.ni, c.nj, c.nk = ni, nj, nk
@@ -111,7 +117,7 @@ class Solver:
         c.wbc = c.ebc = c.sbc = c.nbc = -1
         c.bbc = c.tbc = 2
         c.tile = tile
-        c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = 2, smtopt, vspopt, coropt, 0, 0
+        c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = 2, smtopt, vspopt, coropt, 0, cphopt
         c.smhcoe, c.smvcoe, c.filcoe, c.fc = smhcoe, smvcoe, filcoe, fc
         c.vspvar = vspvar.encode()[:15]
         self.cfg = c
@@ -173,6 +179,29 @@ class Solver:
             assert a.shape == self.shape
         _check(lib().cress_set_base_large(self._h, *[fptr(a) for a in arrs], int(ksp0)))
 
-    def large_step(self, dtb, nsstp, dts):
-        """One s_intgdrv leapfrog step on the device-resident state."""
-        _check(lib().cress_large_step(self._h, float(dtb), int(nsstp), float(dts)))
+    def large_step(self, ctime, dtb, nsstp, dts):
+        """One s_intgdrv leapfrog step on the device-resident state.  ctime is
+        the model time of the present level in ms (0: first step, no
+        Asselin filter); dtb, dts are that step's large and small steps."""
+        _check(lib().cress_large_step(self._h, int(ctime), float(dtb), int(nsstp), float(dts)))
+
+    def set_base_moist(self, pbr, qvbr):
+        arrs = [np.ascontiguousarray(x, dtype=np.float32) for x in (pbr, qvbr)]
+        _check(lib().cress_set_base_moist(self._h, *[fptr(a) for a in arrs]))
+
+    def cloudphy(self, dtb, thresq=1e-12):
+        """s_cloudphy (cphopt=3) on the device-resident past and future levels."""
+        _check(lib().cress_cloudphy(self._h, float(dtb), float(thresq)))
+
+    def satadjst(self, level, thresq=1e-12):
+        _check(lib().cress_satadjst(self._h, int(level), float(thresq)))
+
+    def get_precip(self):
+        ni, nj = self.shape[2] - 2, self.shape[1] - 2
+        a = np.empty((5, 2, nj + 2, ni + 2), np.float32)
+        _check(lib().cress_get_precip(self._h, fptr(a)))
+        return a
+
+    def put_precip(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        _check(lib().cress_put_precip(self._h, fptr(a)))

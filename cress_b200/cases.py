@@ -178,6 +178,62 @@ def dry_case(nx, ny, nz, dx, dz, sthopt=1, seed=0, ptp0=2.0, rad=None, u0=5.0, s
                 vspbar=vspbar, botbar=botbar)
 
 
+def qvs_water(t, p):
+    """Saturation mixing ratio over water, Tetens form of SrcOrig/setblk.f90:333,338."""
+    esw = 610.78 * np.exp(17.269 * (t - 273.16) / (t - 35.86))
+    return 0.622 * esw / (p - esw)
+
+
+def micro_case(nx, ny, nz, dz, seed=0, sthopt=1):
+    """A moist, cloudy state for the cold-rain microphysics: past and future
+    levels of theta', qv, qc, qr, qi, qs, qg, ni, ns, ng (plus the past p')
+    spanning warm rain below the melting level, mixed phase above it and
+    cold ice aloft, sub- and super-saturated air.  Seeded; fields are
+    periodic-consistent.  Returns dims, base (ptbr, rbr, pbr, jcb, rst),
+    past, fut dicts."""
+    ni, nj, nk = dims(nx, ny, nz)
+    b3, cols = base3d(ni, nj, nk, dz, sthopt=sthopt, dthdz=0.004)
+    rng = np.random.default_rng(seed)
+    shp = (nk, nj + 2, ni + 2)
+    zs = cols["zs"][1:nk + 1][:, None, None]
+    pbr = b3["pbr"].astype(np.float64)
+    pi = (pbr / 1.0e5) ** (287.0 / 1004.0)
+    t = b3["ptbr"] * pi
+
+    def field(lo, hi, zlo, zhi, amp):
+        x = _noise(rng, shp, 1.0)
+        blob = np.clip((x - lo) / (hi - lo), 0.0, 1.0)
+        band = ((zs > zlo) & (zs < zhi)).astype(np.float64)
+        return amp * blob * band
+
+    rh = 0.75 + 0.35 * _noise(rng, shp, 1.0)
+    qv = np.minimum(rh * qvs_water(t, pbr), 0.02)
+    qc = field(0.0, 0.6, 500.0, 9000.0, 2.0e-3)
+    qr = field(0.1, 0.8, 0.0, 6000.0, 3.0e-3)
+    qi = field(0.0, 0.7, 6000.0, 14000.0, 5.0e-4)
+    qs = field(0.0, 0.7, 4500.0, 12000.0, 1.5e-3)
+    qg = field(0.1, 0.8, 3000.0, 10000.0, 2.5e-3)
+    rbr = b3["rbr"].astype(np.float64)
+    ni_ = qi / 1.0e-11 * (0.5 + rng.random(shp))
+    ns_ = qs / 5.0e-9 * (0.5 + rng.random(shp))
+    ng_ = qg / 5.0e-8 * (0.5 + rng.random(shp))
+    ptp = 0.5 * _noise(rng, shp, 1.0)
+    pp = 30.0 * _noise(rng, shp, 1.0)
+    past = dict(ptp=ptp, qv=qv, qc=qc, qr=qr, qi=qi, qs=qs, qg=qg, ni=ni_, ns=ns_, ng=ng_, pp=pp)
+    past = {k: periodic_fill(np.asarray(v, np.float32), "s") for k, v in past.items()}
+    fut = {}
+    for k in ("ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"):
+        v = past[k].astype(np.float64)
+        if k == "ptp":
+            v = v + 0.1 * _noise(rng, shp, 1.0)
+        else:
+            v = np.maximum(v * (1.0 + 0.1 * _noise(rng, shp, 1.0)), 0.0)
+        fut[k] = periodic_fill(np.asarray(v, np.float32), "s")
+    base = dict(b3)
+    base["qvbr"] = np.zeros_like(b3["pbr"])
+    return (ni, nj, nk), base, past, fut, cols
+
+
 def _noise(rng, shape, amp):
     x = rng.standard_normal(shape)
     for ax in (1, 2):

@@ -14,6 +14,7 @@
 #include "ctx.h"
 #include "hevi.cuh"
 #include "forcing.cuh"
+#include "micro.cuh"
 
 namespace cress {
 
@@ -240,7 +241,7 @@ int Ctx::small_steps(int nsstp, float dts) {
 
 // One dry large step on the device-resident state (s_intgdrv order,
 // SrcOrig/intgdrv.f90:866-1119).
-int Ctx::large_step(float dtb, int nsstp, float dts) {
+int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
   if (!base_set || !large_set)
     return set_error(CRESS_E_STATE, "cress_large_step: base state (set_base3d, set_base_large) not set");
   if (cfg.advopt != 2 || cfg.tubopt != 0 || cfg.cphopt != 0 ||
@@ -279,8 +280,10 @@ int Ctx::large_step(float dtb, int nsstp, float dts) {
   t.up = lev[CRESS_U][CRESS_PAST]; t.vp = lev[CRESS_V][CRESS_PAST]; t.wp = lev[CRESS_W][CRESS_PAST];
   t.ppp = lev[CRESS_PP][CRESS_PAST]; t.ptpp = lev[CRESS_PTP][CRESS_PAST];
   t.filcoe = cfg.filcoe;
-  if ((rc = launch_timeflt(t, stream))) return set_error(rc, "timeflt launch failed");
-  ++launches;
+  if (filter) {
+    if ((rc = launch_timeflt(t, stream))) return set_error(rc, "timeflt launch failed");
+    ++launches;
+  }
   HaloArgs h{};
   h.g = g;
   const int F[5] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP, CRESS_PTP};
@@ -300,6 +303,47 @@ int Ctx::large_step(float dtb, int nsstp, float dts) {
     lev[F[n]][CRESS_NOW] = lev[F[n]][CRESS_FUTURE];
     lev[F[n]][CRESS_FUTURE] = p;
   }
+  return CRESS_OK;
+}
+
+// s_cloudphy for cphopt=3 on the device-resident past and future levels.
+int Ctx::cloudphy(float dtb, float thresq) {
+  if (cfg.cphopt != 3 || !prec_d) return set_error(CRESS_E_STATE, "cress_cloudphy: context is not cphopt=3");
+  if (!base_set || !moist_set) return set_error(CRESS_E_STATE, "cress_cloudphy: base state not set");
+  MicroArgs m{};
+  m.g = g;
+  m.col = col_d;
+  const int P = CRESS_PAST, F = CRESS_FUTURE;
+  m.ptpp = lev[CRESS_PTP][P]; m.qvp = lev[CRESS_QV][P]; m.qcp = lev[CRESS_QC][P]; m.qrp = lev[CRESS_QR][P];
+  m.qip = lev[CRESS_QI][P]; m.qsp = lev[CRESS_QS][P]; m.qgp = lev[CRESS_QG][P]; m.nip = lev[CRESS_NI][P];
+  m.nsp = lev[CRESS_NS][P]; m.ngp = lev[CRESS_NG][P]; m.ppp = lev[CRESS_PP][P];
+  m.ptpf = lev[CRESS_PTP][F]; m.qvf = lev[CRESS_QV][F]; m.qcf = lev[CRESS_QC][F]; m.qrf = lev[CRESS_QR][F];
+  m.qif = lev[CRESS_QI][F]; m.qsf = lev[CRESS_QS][F]; m.qgf = lev[CRESS_QG][F]; m.nif = lev[CRESS_NI][F];
+  m.nsf = lev[CRESS_NS][F]; m.ngf = lev[CRESS_NG][F];
+  m.prec = prec_d;
+  m.dtp_bits = dtp_d;
+  m.dtb = 2.f * dtb;        // cloudphy.f90:282
+  m.dz = cfg.dz;
+  m.thresq = thresq;
+  int rc = launch_cloudphy(m, stream);
+  launches += 3;
+  if (rc) return set_error(rc, "cloudphy launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return CRESS_OK;
+}
+
+int Ctx::satadjst(int level, float thresq) {
+  if (cfg.cphopt != 3) return set_error(CRESS_E_STATE, "cress_satadjst: context is not cphopt=3");
+  if (!base_set || !moist_set) return set_error(CRESS_E_STATE, "cress_satadjst: base state not set");
+  SatArgs s{};
+  s.g = g;
+  s.col = col_d;
+  s.pp = lev[CRESS_PP][level];
+  s.ptp = lev[CRESS_PTP][level]; s.qv = lev[CRESS_QV][level]; s.qc = lev[CRESS_QC][level];
+  s.qi = lev[CRESS_QI][level]; s.ni = lev[CRESS_NI][level];
+  s.thresq = thresq;
+  int rc = launch_satadjst(s, stream);
+  ++launches;
+  if (rc) return set_error(rc, "satadjst launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   return CRESS_OK;
 }
 
@@ -365,6 +409,29 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   for (int l = 0; l < 3; ++l) {
     c->lev[CRESS_PTP][l] = c->alloc_field();
     if (!c->lev[CRESS_PTP][l]) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the state failed"); }
+  }
+  if (cfg->cphopt == 3) {
+    // moist species: three time levels each (their forcings go straight
+    // into s_steps), plus the surface precipitation planes and the
+    // sedimentation minimum word
+    for (int f = CRESS_QV; f <= CRESS_NG; ++f)
+      for (int l = 0; l < 3; ++l) {
+        c->lev[f][l] = c->alloc_field();
+        if (!c->lev[f][l]) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the moist state failed"); }
+      }
+    const size_t pb = sizeof(float) * 10 * (size_t)c->g.px * c->g.py;
+    if ((rc = cuda_check(cudaMalloc(&c->prec_d, pb), "cudaMalloc precip")) ||
+        (rc = cuda_check(cudaMalloc(&c->dtp_d, sizeof(int)), "cudaMalloc dtp"))) {
+      delete c;
+      return rc;
+    }
+    c->owned.push_back(c->prec_d);
+    c->owned.push_back(c->dtp_d);
+    cudaMemsetAsync(c->prec_d, 0, pb, c->stream);
+    if ((rc = micro_init_tables())) { delete c; return set_error(rc, "Koenig table upload failed"); }
+  } else if (cfg->cphopt != 0) {
+    delete c;
+    return set_error(CRESS_E_UNSUPPORTED, "cphopt=%d: only 0 (dry) and 3 (cold rain) run on the GPU", cfg->cphopt);
   }
   c->col_h.assign((size_t)C_NFIELDS_ALL * (cfg->nk + 1), 0.f);
   if ((rc = cuda_check(cudaMalloc(&c->col_d, sizeof(float) * c->col_h.size()), "cudaMalloc cols"))) {
@@ -536,11 +603,77 @@ int cress_set_base_large(cress_ctx* ctx, const float* ubr, const float* vbr, con
   return CRESS_OK;
 }
 
-int cress_large_step(cress_ctx* ctx, float dtb, int nsstp, float dts) {
+int cress_set_base_moist(cress_ctx* ctx, const float* pbr, const float* qvbr) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !pbr || !qvbr) return set_error(CRESS_E_ARG, "cress_set_base_moist: null argument");
+  cudaSetDevice(c->device);
+  const int ni = c->cfg.ni, nj = c->cfg.nj, nk = c->cfg.nk;
+  auto at = [&](const float* a, int i, int j, int k) {
+    return a[(size_t)i + (size_t)(ni + 2) * ((size_t)j + (size_t)(nj + 2) * (size_t)(k - 1))];
+  };
+  const float* src[2] = {pbr, qvbr};
+  const int dst[2] = {C_PBR, C_QVBR};
+  for (int n = 0; n < 2; ++n)
+    for (int k = 1; k <= nk; ++k) {
+      const float v = at(src[n], ni / 2, nj / 2, k);
+      c->col_h[(size_t)dst[n] * (nk + 1) + k] = v;
+      for (int j = 1; j <= nj - 1; ++j)
+        for (int i = 1; i <= ni - 1; ++i)
+          if (at(src[n], i, j, k) != v)
+            return set_error(CRESS_E_NONUNIFORM, "moist base array %d varies horizontally at (%d,%d,%d)", n, i, j, k);
+    }
+  int rc = cuda_check(cudaMemcpyAsync(c->col_d, c->col_h.data(), sizeof(float) * c->col_h.size(),
+                                      cudaMemcpyHostToDevice, c->stream), "copy moist columns");
+  if (rc) return rc;
+  if ((rc = cuda_check(cudaStreamSynchronize(c->stream), "sync moist columns"))) return rc;
+  c->moist_set = true;
+  return CRESS_OK;
+}
+
+int cress_cloudphy(cress_ctx* ctx, float dtb, float thresq) {
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (!c) return set_error(CRESS_E_ARG, "null context");
   cudaSetDevice(c->device);
-  return c->large_step(dtb, nsstp, dts);
+  return c->cloudphy(dtb, thresq);
+}
+
+int cress_satadjst(cress_ctx* ctx, int level, float thresq) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  if (level != CRESS_NOW && level != CRESS_FUTURE) return set_error(CRESS_E_ARG, "cress_satadjst: level %d", level);
+  cudaSetDevice(c->device);
+  return c->satadjst(level, thresq);
+}
+
+int cress_get_precip(cress_ctx* ctx, float* host) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !host) return set_error(CRESS_E_ARG, "cress_get_precip: null argument");
+  if (!c->prec_d) return set_error(CRESS_E_STATE, "cress_get_precip: context has no microphysics");
+  cudaSetDevice(c->device);
+  const size_t wb = sizeof(float) * (c->g.ni + 2);
+  int rc = cuda_check(cudaMemcpy2DAsync(host, wb, c->prec_d, sizeof(float) * c->g.px, wb,
+                                        (size_t)10 * c->g.py, cudaMemcpyDeviceToHost, c->stream), "precip copy");
+  if (rc) return rc;
+  return cuda_check(cudaStreamSynchronize(c->stream), "precip sync");
+}
+
+int cress_put_precip(cress_ctx* ctx, const float* host) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !host) return set_error(CRESS_E_ARG, "cress_put_precip: null argument");
+  if (!c->prec_d) return set_error(CRESS_E_STATE, "cress_put_precip: context has no microphysics");
+  cudaSetDevice(c->device);
+  const size_t wb = sizeof(float) * (c->g.ni + 2);
+  int rc = cuda_check(cudaMemcpy2DAsync(c->prec_d, sizeof(float) * c->g.px, host, wb, wb,
+                                        (size_t)10 * c->g.py, cudaMemcpyHostToDevice, c->stream), "precip copy");
+  if (rc) return rc;
+  return cuda_check(cudaStreamSynchronize(c->stream), "precip sync");
+}
+
+int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, float dts) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  cudaSetDevice(c->device);
+  return c->large_step(ctime != 0, dtb, nsstp, dts);
 }
 
 long long cress_launch_count(const cress_ctx* ctx) {

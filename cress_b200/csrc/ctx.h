@@ -45,9 +45,14 @@ struct Ctx {
   int get_host(float* host, const float* src);
   int thomas_for(float dts, const ThomasSet** out);
   int small_steps(int nsstp, float dts);
-  int large_step(float dtb, int nsstp, float dts);
+  int large_step(bool filter, float dtb, int nsstp, float dts);
   int ksp0 = 2;            // first Rayleigh-damped level
   bool large_set = false;  // cress_set_base_large was called
+  bool moist_set = false;  // cress_set_base_moist was called
+  float* prec_d = nullptr; // surface precipitation planes (10 x px*py)
+  int* dtp_d = nullptr;    // sedimentation sub-step minimum (float bits)
+  int cloudphy(float dtb, float thresq);
+  int satadjst(int level, float thresq);
   int tmap(const float* buf, int rows, CUtensorMap* out);
   int check_device_error();
   ~Ctx();

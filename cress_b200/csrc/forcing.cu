@@ -236,7 +236,10 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
       };
       f = f + (pta8w(id, k) + pta8w(id + pl, k + 1));
       const float dtdrst = a.dtb2 / C(C_RST, k);                     // steps.f90:528
-      a.ptpf[id] = ld(a.ptpp, id) + f * dtdrst;                       // steps.f90:568
+      const float ptpf = ld(a.ptpp, id) + f * dtdrst;                 // steps.f90:568
+      a.ptpf[id] = ptpf;
+      if (k == 2) a.ptpf[id - pl] = ptpf;                             // vbcs.f90:118
+      if (k == nk - 2) a.ptpf[id + pl] = ptpf;                        // vbcs.f90:132
     }
   }
 }

@@ -343,8 +343,9 @@ int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
 
 }  // namespace
 
-// Tile ids: 0-2 keep the eliminated right-hand sides in double (the
-// product setting); 3-5 are the same tiles with a float column store.
+// Tile ids.  0-2 keep the eliminated right-hand sides as float between the
+// two sweeps (both recurrences still run in double): 3 blocks of 4 warps
+// fit per SM, the default.  3-5 store them as double (2 blocks per SM).
 int hevi_tile_rows(int tile) {
   switch (tile) {
     case 1: case 4: return 2;
@@ -355,12 +356,12 @@ int hevi_tile_rows(int tile) {
 
 int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st) {
   switch (tile) {
-    case 1: return launch_t<2, 6, double>(a, maps, st);
-    case 2: return launch_t<8, 4, double>(a, maps, st);
-    case 3: return launch_t<4, 4, float>(a, maps, st);
-    case 4: return launch_t<2, 5, float>(a, maps, st);
-    case 5: return launch_t<8, 4, float>(a, maps, st);
-    default: return launch_t<4, 5, double>(a, maps, st);
+    case 1: return launch_t<2, 5, float>(a, maps, st);
+    case 2: return launch_t<8, 4, float>(a, maps, st);
+    case 3: return launch_t<4, 5, double>(a, maps, st);
+    case 4: return launch_t<2, 6, double>(a, maps, st);
+    case 5: return launch_t<8, 4, double>(a, maps, st);
+    default: return launch_t<4, 4, float>(a, maps, st);
   }
 }
 

@@ -1,0 +1,221 @@
+// Cold-rain bulk microphysics (s_cloudphy -> s_coldblk, cphopt=3,
+// haiopt=0) and saturation adjustment (s_satadjst) for sm_100a.
+//
+// k_micro_src (one thread per cell, interior columns, k = 1..nk-1, the
+// reference's range): getvdens/getexner/diagnw, adjstni on the future
+// level, termblk on the past level, every process rate of srcblk held in
+// registers (the reference keeps 77 scratch 3-D arrays, SrcOrig/comblk.f90),
+// adjstni again; it writes the ten future fields and folds each cell's
+// sedimentation CFL limit dz*jcb/(u+eps) into one domain minimum
+// (the chkfall allreduce of SrcOrig/fallblk.f90:439) with a warp reduction
+// and one atomicMin per warp.
+// k_micro_fall (one thread per column): recovers npstp and dtp from that
+// minimum (fallblk.f90:441-449), recomputes the past-level fall speeds,
+// runs the upwind sedimentation sub-steps of every species column
+// (upwqp.f90:160-225, upwnp.f90:140-176) with the surface precipitation
+// rate and accumulation, and the final adjstni (coldblk.f90:469).
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "hevi.cuh"
+#include "micro.cuh"
+#include "coldrain.cuh"
+
+namespace cress {
+
+namespace {
+
+constexpr int kMaxNkFall = 160;   // column length the sedimentation kernel holds
+
+__device__ inline void load_cell(const MicroArgs& a, long long id, int k, MCell& c) {
+  const int nc = a.g.nk + 1;
+  const float rddvcp = 287.f / 1004.f, p0iv = 1.f / 1.e5f;
+  c.ptbr = __ldg(a.col + C_PTBR * nc + k);
+  c.rbr = __ldg(a.col + C_RBR * nc + k);
+  c.rbv = 1.f / c.rbr;                                                  // getvdens.f90:106
+  c.p = __ldg(a.col + C_PBR * nc + k) + __ldg(a.ppp + id);              // getexner.f90:129
+  c.pi = expf(rddvcp * logf(p0iv * c.p));                               // getexner.f90:131
+  c.ptpp = __ldg(a.ptpp + id); c.qvp = __ldg(a.qvp + id); c.qcp = __ldg(a.qcp + id);
+  c.qrp = __ldg(a.qrp + id); c.qip = __ldg(a.qip + id); c.qsp = __ldg(a.qsp + id);
+  c.qgp = __ldg(a.qgp + id); c.ncip = __ldg(a.nip + id); c.ncsp = __ldg(a.nsp + id);
+  c.ncgp = __ldg(a.ngp + id);
+  diagnw_cell(c.rbr, c.qrp, c.nccp, c.ncrp);                           // cloudphy.f90:366
+}
+
+__global__ void __launch_bounds__(256) k_micro_src(const MicroArgs a) {
+  const Grid g = a.g;
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  const bool in = i <= g.ni - 2 && j <= g.nj - 2 && k <= g.nk - 1;
+  float lim = 3.0e38f;
+  if (in) {
+    const long long id = g.at(i, j, k);
+    MCell c;
+    load_cell(a, id, k, c);
+    c.ptpf = a.ptpf[id]; c.qvf = a.qvf[id]; c.qcf = a.qcf[id]; c.qrf = a.qrf[id];
+    c.qif = a.qif[id]; c.qsf = a.qsf[id]; c.qgf = a.qgf[id]; c.ncif = a.nif[id];
+    c.ncsf = a.nsf[id]; c.ncgf = a.ngf[id];
+    adjstni_cell(c.rbr, c.rbv, c.qif, c.qsf, c.qgf, c.ncif, c.ncsf, c.ncgf);   // coldblk.f90:327
+    termblk_cell(a.thresq, c);                                                // coldblk.f90:344
+    srcblk_cell(a.dtb, a.thresq, c);                                          // coldblk.f90:356
+    adjstni_cell(c.rbr, c.rbv, c.qif, c.qsf, c.qgf, c.ncif, c.ncsf, c.ncgf);   // coldblk.f90:425
+    a.ptpf[id] = c.ptpf; a.qvf[id] = c.qvf; a.qcf[id] = c.qcf; a.qrf[id] = c.qrf;
+    a.qif[id] = c.qif; a.qsf[id] = c.qsf; a.qgf[id] = c.qgf; a.nif[id] = c.ncif;
+    a.nsf[id] = c.ncsf; a.ngf[id] = c.ncgf;
+    // fallblk.f90:362-377 (flqcqi_opt=1: cloud water and ice fall too)
+    const float eps = 1.e-20f;
+    const float dzjcb = a.dz * __ldg(a.col + C_JCB * (g.nk + 1) + k);
+    lim = fminf(lim, dzjcb / (c.ucq + eps));
+    lim = fminf(lim, dzjcb / (c.urq + eps));
+    lim = fminf(lim, dzjcb / (c.uiq + eps));
+    lim = fminf(lim, dzjcb / (c.usq + eps));
+    lim = fminf(lim, dzjcb / (c.ugq + eps));
+  }
+  for (int o = 16; o > 0; o >>= 1) lim = fminf(lim, __shfl_xor_sync(0xffffffffu, lim, o));
+  if ((threadIdx.x & 31) == 0 && lim < 3.0e38f) atomicMin(a.dtp_bits, __float_as_int(lim));
+}
+
+// s_upwqp / s_upwnp on one column held in registers/local memory.
+__device__ inline void upw_column(int nk, float dziv, float dtp, const float* rbr, const float* rst,
+                                  const float* u, float* q, float* pr_rate, float* pr_acc) {
+  float flx[kMaxNkFall];
+  const float dzvdt = dziv * dtp;
+  for (int k = 1; k <= nk - 1; ++k) flx[k] = rbr[k] * u[k] * q[k];
+  for (int k = 1; k <= nk - 2; ++k) q[k] = fmaxf(q[k] + (flx[k + 1] - flx[k]) / rst[k] * dzvdt, 0.f);
+  q[nk - 1] = q[nk - 2];
+  if (pr_rate) {
+    const float rwiv05 = .5f / 1.e3f, dtp05 = .5f * dtp;
+    *pr_rate = (flx[1] + flx[2]) * rwiv05;
+    *pr_acc = *pr_acc + *pr_rate * dtp05;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_micro_fall(const MicroArgs a) {
+  const Grid g = a.g;
+  const int nk = g.nk;
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > g.ni - 2 || j > g.nj - 2) return;
+  // fallblk.f90:421-449
+  const float dtb = a.dtb;
+  float dtp = fminf(__int_as_float(*a.dtp_bits), dtb);
+  int npstp;
+  if (dtp < dtb) {
+    npstp = (int)((dtb + .001f) / dtp) + 1;
+    dtp = dtb / (float)npstp;
+  } else {
+    npstp = 1;
+    dtp = dtb;
+  }
+  const float dziv = 1.f / a.dz;
+  float rbr[kMaxNkFall], rst[kMaxNkFall], u[kMaxNkFall], q[kMaxNkFall];
+  const int nc = nk + 1;
+  for (int k = 1; k <= nk - 1; ++k) {
+    rbr[k] = __ldg(a.col + C_RBR * nc + k);
+    rst[k] = __ldg(a.col + C_RST * nc + k);
+  }
+  const long long id1 = g.at(i, j, 1);
+  const long long pl = g.plane;
+  const long long pp2 = (long long)g.px * g.py;
+  const long long pid = (long long)j * g.px + i;
+  // Fall speeds of the past level (termblk, as in k_micro_src).
+  auto speeds = [&](int which) {
+    for (int k = 1; k <= nk - 1; ++k) {
+      MCell c;
+      load_cell(a, id1 + (k - 1) * pl, k, c);
+      termblk_cell(a.thresq, c);
+      float v = 0.f;
+      switch (which) {
+        case 0: v = c.ucq; break; case 1: v = c.uiq; break; case 2: v = c.uin; break;
+        case 3: v = c.urq; break; case 4: v = c.usq; break; case 5: v = c.ugq; break;
+        case 6: v = c.usn; break; default: v = c.ugn; break;
+      }
+      u[k] = v;
+    }
+  };
+  float* const fields[8] = {a.qcf, a.qif, a.nif, a.qrf, a.qsf, a.qgf, a.nsf, a.ngf};
+  const int pslot[8] = {0, 2, -1, 1, 3, 4, -1, -1};   // prc, pri, -, prr, prs, prg
+  for (int f = 0; f < 8; ++f) {
+    speeds(f);
+    float* fld = fields[f];
+    for (int k = 1; k <= nk - 1; ++k) q[k] = fld[id1 + (k - 1) * pl];
+    float rate = 0.f, acc = 0.f;
+    const int s = pslot[f];
+    if (s >= 0) { rate = a.prec[(2 * s) * pp2 + pid]; acc = a.prec[(2 * s + 1) * pp2 + pid]; }
+    for (int n = 0; n < npstp; ++n)
+      upw_column(nk, dziv, dtp, rbr, rst, u, q, s >= 0 ? &rate : nullptr, s >= 0 ? &acc : nullptr);
+    for (int k = 1; k <= nk - 1; ++k) fld[id1 + (k - 1) * pl] = q[k];
+    if (s >= 0) { a.prec[(2 * s) * pp2 + pid] = rate; a.prec[(2 * s + 1) * pp2 + pid] = acc; }
+  }
+  // coldblk.f90:467-470: adjstni once more (flqcqi_opt=1)
+  for (int k = 1; k <= nk - 1; ++k) {
+    const long long id = id1 + (k - 1) * pl;
+    const float rb = rbr[k], rbv = 1.f / rb;
+    float nci = a.nif[id], ncs = a.nsf[id], ncg = a.ngf[id];
+    adjstni_cell(rb, rbv, a.qif[id], a.qsf[id], a.qgf[id], nci, ncs, ncg);
+    a.nif[id] = nci; a.nsf[id] = ncs; a.ngf[id] = ncg;
+  }
+}
+
+__global__ void k_init_dtp(int* dtp_bits, float v) { *dtp_bits = __float_as_int(v); }
+
+// s_satadjst (cphopt=3): siadjst then swadjst on one level.
+__global__ void __launch_bounds__(256) k_satadjst(const SatArgs a) {
+  const Grid g = a.g;
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (i > g.ni - 2 || j > g.nj - 2 || k > g.nk - 1) return;
+  const long long id = g.at(i, j, k);
+  const int nc = g.nk + 1;
+  const float rddvcp = 287.f / 1004.f, p0iv = 1.f / 1.e5f;
+  const float p = __ldg(a.col + C_PBR * nc + k) + __ldg(a.pp + id);     // getexner.f90:129
+  const float pi = expf(rddvcp * logf(p0iv * p));
+  float ptp = a.ptp[id], qv = a.qv[id], qc = a.qc[id], qi = a.qi[id], ni = a.ni[id];
+  satadjst_cell(a.thresq, __ldg(a.col + C_PTBR * nc + k), pi, p, ptp, qv, qc, qi, ni);
+  a.ptp[id] = ptp; a.qv[id] = qv; a.qc[id] = qc; a.qi[id] = qi; a.ni[id] = ni;
+}
+
+}  // namespace
+
+int micro_init_tables() {
+  // SrcOrig/setref.f90:473-601
+  static const float c[41] = {0.f, .7939e-10f, .7841e-9f, .3369e-8f, .4336e-8f, .5285e-8f, .3728e-8f,
+                              .1852e-8f, .2991e-9f, .4248e-9f, .7434e-9f, .1812e-8f, .4394e-8f,
+                              .9145e-8f, .1725e-7f, .3348e-7f, .1725e-7f, .9175e-8f, .4412e-8f,
+                              .2252e-8f, .9115e-9f, .4876e-9f, .3473e-9f, .4758e-9f, .6306e-9f,
+                              .8573e-9f, .7868e-9f, .7192e-9f, .6513e-9f, .5956e-9f, .5333e-9f,
+                              .4834e-9f, .4335e-9f, .3836e-9f, .3337e-9f, .2838e-9f, .2339e-9f,
+                              .1840e-9f, .1341e-9f, .8420e-10f, .3430e-10f};
+  static const float p[41] = {0.f, .4006f, .4831f, .5320f, .5307f, .5319f, .5249f, .4888f, .3894f,
+                              .4047f, .4318f, .4771f, .5183f, .5463f, .5651f, .5813f, .5655f, .5478f,
+                              .5203f, .4906f, .4447f, .4126f, .3960f, .4149f, .4320f, .4506f, .4483f,
+                              .4460f, .4433f, .4413f, .4382f, .4361f, .4340f, .4319f, .4298f, .4277f,
+                              .4256f, .4235f, .4214f, .4193f, .4172f};
+  float ck[41];
+  for (int n = 0; n <= 40; ++n) ck[n] = c[n] * expf(3.f * p[n] * 2.30259f);   // setref.f90:559-600
+  if (cudaMemcpyToSymbol(kKoeC, ck, sizeof ck) != cudaSuccess) return CRESS_E_CUDA;
+  if (cudaMemcpyToSymbol(kKoeP, p, sizeof p) != cudaSuccess) return CRESS_E_CUDA;
+  return CRESS_OK;
+}
+
+int launch_cloudphy(const MicroArgs& a, cudaStream_t st) {
+  if (a.g.nk > kMaxNkFall - 1) return CRESS_E_UNSUPPORTED;
+  k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
+  dim3 b(32, 8, 1);
+  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
+  k_micro_src<<<gr, b, 0, st>>>(a);
+  dim3 b2(32, 4, 1);
+  dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 1);
+  k_micro_fall<<<gr2, b2, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+int launch_satadjst(const SatArgs& a, cudaStream_t st) {
+  dim3 b(32, 8, 1);
+  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
+  k_satadjst<<<gr, b, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+}  // namespace cress

@@ -1,0 +1,36 @@
+// Cold-rain microphysics kernels (internal interface).
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "hevi.cuh"
+
+namespace cress {
+
+struct MicroArgs {
+  Grid g;
+  const float* col;  // 1-D base columns (C_PTBR, C_RBR, C_PBR, C_JCB, C_RST used)
+  // past level t-dt (pp: pressure perturbation for p and the Exner function)
+  const float *ptpp, *qvp, *qcp, *qrp, *qip, *qsp, *qgp, *nip, *nsp, *ngp, *ppp;
+  // future level t+dt (updated)
+  float *ptpf, *qvf, *qcf, *qrf, *qif, *qsf, *qgf, *nif, *nsf, *ngf;
+  float* prec;       // 10 planes (px*py): prc, prr, pri, prs, prg x (rate, accumulated)
+  int* dtp_bits;     // domain minimum of the sedimentation step (float bits, positive)
+  float dtb;         // microphysics step = 2*dtb of the leapfrog (cloudphy.f90:282)
+  float dz, thresq;
+};
+
+// Koenig table upload (once per device); returns a CRESS status.
+int micro_init_tables();
+// s_cloudphy for cphopt=3: source terms and sedimentation (2 kernels).
+int launch_cloudphy(const MicroArgs& a, cudaStream_t st);
+
+struct SatArgs {
+  Grid g;
+  const float* col;  // C_PTBR, C_PBR
+  const float* pp;
+  float *ptp, *qv, *qc, *qi, *ni;
+  float thresq;
+};
+int launch_satadjst(const SatArgs& a, cudaStream_t st);
+
+}  // namespace cress

@@ -137,9 +137,39 @@ int cress_set_base_large(cress_ctx* ctx, const float* ubr, const float* vbr, con
  * SrcOrig/fdmdrv.f90:661-704): forcing of u, v, w, p', theta'
  * (s_forcedrv), nsstp HE-VI substeps of dts (s_smalldrv), the theta' step
  * (s_steps), the Asselin filter (s_timeflt), both periodic ghost planes
- * (bcycle, s_shift2nd) and the time-level rotation (s_swp2nxt).  dtb is
- * s_timeint's large step (half of dtbig on the first step). */
-int cress_large_step(cress_ctx* ctx, float dtb, int nsstp, float dts);
+ * (bcycle, s_shift2nd) and the time-level rotation (s_swp2nxt).  ctime is
+ * s_intgdrv's model time of the present level (ms); at ctime = 0 the
+ * Asselin filter is skipped (SrcOrig/intgdrv.f90:968).  dtb and dts are
+ * s_timeint's large and small steps (halves of dtbig, dtsml at ctime = 0,
+ * SrcOrig/timeint.f90:160-190).  With cphopt=3 the step is the moist one:
+ * moist buoyancy, the qv / species / number steps, s_cloudphy, the filter
+ * of the moist fields and s_satadjst on t and t+dt
+ * (SrcOrig/intgdrv.f90:832-998). */
+int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, float dts);
+
+/* Moist base state (cphopt=3): base pressure pbr and base water vapour qvbr
+ * (SrcOrig/setbase.f90:153-189), host arrays in reference layout. */
+int cress_set_base_moist(cress_ctx* ctx, const float* pbr, const float* qvbr);
+
+/* Cold-rain bulk microphysics on the device-resident state, replacing
+ * s_cloudphy for cphopt=3, haiopt=0 (SrcOrig/cloudphy.f90:277-466 ->
+ * s_coldblk, SrcOrig/coldblk.f90:321-481): process rates from the PAST
+ * level (theta', water species, ice numbers, p'), applied to the FUTURE
+ * level, then sedimentation with the domain-global sub-step
+ * (SrcOrig/fallblk.f90:298-543) accumulating surface precipitation.  dtb
+ * is the leapfrog large step (the scheme integrates over 2*dtb).  thresq is
+ * the namelist threshold of the mixing ratios. */
+int cress_cloudphy(cress_ctx* ctx, float dtb, float thresq);
+
+/* Saturation adjustment s_satadjst for cphopt=3 (SrcOrig/satadjst.f90:
+ * 154-189: s_siadjst then s_swadjst) on one time level (CRESS_NOW or
+ * CRESS_FUTURE) of theta', qv, qc, qi, ni, using that level's p'. */
+int cress_satadjst(cress_ctx* ctx, int level, float thresq);
+
+/* Surface precipitation planes prc, prr, pri, prs, prg, each as (rate,
+ * accumulated) on the (ni+2) x (nj+2) plane: 10 planes, host layout. */
+int cress_get_precip(cress_ctx* ctx, float* host);
+int cress_put_precip(cress_ctx* ctx, const float* host);
 
 /* Number of kernel launches the library issued since the context was
  * created (instrumentation for benchmarks). */

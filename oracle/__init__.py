@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle_cress.so")
 LIB_OMP = os.path.join(BUILD, "liboracle_cress_omp.so")
-SOURCES = ["oracle_capi.cpp", "oracle_dry.cpp"]
+SOURCES = ["oracle_capi.cpp", "oracle_dry.cpp", "oracle_moist.cpp"]
 HEADERS = [f for f in os.listdir(HERE) if f.endswith(".h")]
 
 _FP = ctypes.POINTER(ctypes.c_float)
@@ -112,6 +112,47 @@ def dry_steps(cfg, base, zph, past, now, nsteps, dtbig, dtsml, start=True, prec=
 def _fp(a):
     assert a.dtype == np.float32 and a.flags.c_contiguous
     return a.ctypes.data_as(_FP)
+
+
+MICRO_PAST = ["ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng", "pp"]
+MICRO_FUT = ["ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
+MICRO_BASE = ["ptbr", "rbr", "pbr", "jcb", "rst"]
+
+
+def cloudphy(dims, base, past, fut, prec, dtb, dz, thresq=1e-12, bits=32):
+    """One s_cloudphy call (cphopt=3) on the CPU.  past/fut: dicts of 3-D
+    float32 arrays (MICRO_PAST / MICRO_FUT); fut and prec (5 x 2 x (nj+2) x
+    (ni+2) float32: prc, prr, pri, prs, prg rate/accumulation) are updated
+    in place.  Returns npstp, the sedimentation sub-step count."""
+    ni, nj, nk = dims
+    L = lib()
+    L.oracle_cloudphy.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 3 + [ctypes.POINTER(_FP)] * 3 + [_FP]
+    b = [np.ascontiguousarray(base[n], np.float32) for n in MICRO_BASE]
+    p = [np.ascontiguousarray(past[n], np.float32) for n in MICRO_PAST]
+    for n in MICRO_FUT:
+        assert fut[n].dtype == np.float32 and fut[n].flags.c_contiguous
+    assert prec.dtype == np.float32 and prec.flags.c_contiguous and prec.size == 10 * (ni + 2) * (nj + 2)
+    f = [fut[n] for n in MICRO_FUT]
+    rc = L.oracle_cloudphy(bits, ni, nj, nk, float(dtb), float(dz), float(thresq),
+                           (_FP * len(b))(*[_fp(x) for x in b]), (_FP * len(p))(*[_fp(x) for x in p]),
+                           (_FP * len(f))(*[_fp(x) for x in f]), _fp(prec))
+    if rc < 0:
+        raise RuntimeError(f"oracle_cloudphy failed ({rc})")
+    return rc
+
+
+def satadjst(dims, ptbr, pbr, pp, st, thresq=1e-12):
+    """s_satadjst (cphopt=3) in place on st = dict with ptp, qv, qc, qi, ni."""
+    ni, nj, nk = dims
+    L = lib()
+    L.oracle_satadjst.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, _FP, _FP, _FP, ctypes.POINTER(_FP)]
+    L.oracle_satadjst.restype = None
+    s = [st[n] for n in ("ptp", "qv", "qc", "qi", "ni")]
+    for a in s:
+        assert a.dtype == np.float32 and a.flags.c_contiguous
+    L.oracle_satadjst(ni, nj, nk, float(thresq), _fp(np.ascontiguousarray(ptbr, np.float32)),
+                      _fp(np.ascontiguousarray(pbr, np.float32)), _fp(np.ascontiguousarray(pp, np.float32)),
+                      (_FP * 5)(*[_fp(a) for a in s]))
 
 
 def small_steps(cfg, base, frc, state, nsstp, dts, prec=32, fp64_solve=1, omp=False):

@@ -43,7 +43,7 @@ int run_dry(const int* io, const double* ro, const double* zph, const float* con
     const bool first = start && s == 0;
     const R dtb = first ? R(.5) * R(dtbig) : R(dtbig);
     const R dts = first ? R(.5) * R(dtsml) : R(dtsml);
-    intgdrv_dry<R>(r, dtb, nsstp, dts);
+    intgdrv_dry<R>(r, dtb, nsstp, dts, !first);   // no s_timeflt at ctime=0
   }
   F3<R>* so[] = {&r.p.u, &r.p.v, &r.p.w, &r.p.pp, &r.p.ptp, &r.c.u, &r.c.v, &r.c.w, &r.c.pp, &r.c.ptp};
   for (int n = 0; n < 10; ++n) so[n]->store(st[n]);

@@ -27,6 +27,9 @@ struct DryRun {
   std::vector<R> rbct;   // vspdmp coefficient rbct(k,2)
   R fc = R(0);           // 0.5*omega*sin(lat)
   Level<R> p, c, f;      // t-dt, t, t+dt
+  // moist buoyancy inputs at t (buoywb.f90:202-299); null for a dry run
+  const F3<R>* bqv = nullptr;
+  const F3<R>* bqall = nullptr;
   // scratch
   F3<R> ufrc, vfrc, wfrc, pfrc, ptfrc, wc, rxu, rxv, rxw, t1, t2, t3, t4, t5, jxu, jxv, jxw;
   SmallScratch<R> ss;
@@ -73,7 +76,7 @@ void forceuvw(DryRun<R>& r) {
   if (r.lo.vspopt >= 1)                                                 // forceuvw.f90:519
     vspuvw(o, r.lo, r.b, r.rbct, r.p.u, r.p.v, r.p.w, r.ufrc, r.vfrc, r.wfrc, r.t5);
   if (r.lo.coropt == 1) coriuv(o, r.fc, r.b, r.c.u, r.c.v, r.ufrc, r.vfrc, r.t1);   // :544
-  buoywb(o, false, r.b, r.c.ptp, (const F3<R>*)nullptr, (const F3<R>*)nullptr, r.wfrc, r.t1);  // :596
+  buoywb(o, r.bqv != nullptr, r.b, r.c.ptp, r.bqv, r.bqall, r.wfrc, r.t1);   // forceuvw.f90:596
   rstuvwc(o, r.b, r.c.u, r.c.v, r.wc, r.rxu, r.rxv, r.rxw);             // :614
   advuvw(o, r.rxu, r.rxv, r.rxw, r.c.u, r.c.v, r.c.w, r.ufrc, r.vfrc, r.wfrc, r.t1, r.t2, r.t3, r.t4);  // :626
 }
@@ -118,55 +121,93 @@ void forcept(DryRun<R>& r) {
   advbspt(o, r.b, r.c.w, r.ptfrc, r.t1);
 }
 
-// One large step (leapfrog from t-dt to t+dt with dtb, nsstp substeps of
-// dts): forcing, small steps, s_steps for theta' (steps.f90:506-574, 3979),
-// s_timeflt (timeflt.f90:335-404), shift2nd planes and swp2nxt rotation.
+// s_vbcs, SrcOrig/vbcs.f90:116-132: zero-gradient scalar below the ground
+// and above the lid.
 template <class R>
-void intgdrv_dry(DryRun<R>& r, R dtb, int nsstp, R dts) {
-  const Opts& o = r.o;
+void vbcs(const Opts& o, F3<R>& sf) {
   const int ni = o.ni, nj = o.nj, nk = o.nk;
+  for (int j = 1; j <= nj - 1; ++j)
+    for (int i = 1; i <= ni - 1; ++i) sf(i, j, 1) = sf(i, j, 2);
+  for (int j = 1; j <= nj - 1; ++j)
+    for (int i = 1; i <= ni - 1; ++i) sf(i, j, nk - 1) = sf(i, j, nk - 2);
+}
+
+// Phases of one large step (s_intgdrv, intgdrv.f90:866-1119), split so
+// the moist step can interleave its own parts.
+template <class R>
+void phase_forcing(DryRun<R>& r) {   // s_forcedrv (forcedrv.f90:548-608)
   forceuvw(r);
   forcep(r);
   forcept(r);
-  // s_smalldrv (smalldrv.f90:343-398): future = past, then the substeps.
+}
+
+template <class R>
+void phase_small(DryRun<R>& r, int nsstp, R dts) {   // s_smalldrv (smalldrv.f90:343-398)
   r.f.u = r.p.u; r.f.v = r.p.v; r.f.w = r.p.w; r.f.pp = r.p.pp;
-  phy2cnt(o, r.sthopt, r.b, r.f.w, r.wc);
+  phy2cnt(r.o, r.sthopt, r.b, r.f.w, r.wc);
   for (int n = 0; n < nsstp; ++n)
-    hevi<R>(o, r.sthopt, dts, r.b, r.ufrc, r.vfrc, r.wfrc, r.pfrc, r.f.ptp, r.f.u, r.f.v, r.f.w, r.wc,
+    hevi<R>(r.o, r.sthopt, dts, r.b, r.ufrc, r.vfrc, r.wfrc, r.pfrc, r.f.ptp, r.f.u, r.f.v, r.f.w, r.wc,
             r.f.pp, r.ss);
-  // s_steps (steps.f90:506-574): ptpf = ptpp + ptfrc * 2 dtb / rst
+}
+
+// s_steps for one scalar (steps.f90:506-590): f = p + frc*2dtb/rst, clipped
+// at zero for mixing ratios, then bcycle (3979) and vbcs (4362).
+template <class R>
+void step_scalar(const DryRun<R>& r, R dtb, const F3<R>& sp, const F3<R>& frc, F3<R>& sf, bool clip) {
+  const Opts& o = r.o;
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
   const R dtb2 = R(2) * dtb;
   for (int k = 2; k <= nk - 2; ++k)
     for (int j = 2; j <= nj - 2; ++j)
       for (int i = 2; i <= ni - 2; ++i) {
         const R dtdrst = dtb2 / r.b.rst(i, j, k);
-        r.f.ptp(i, j, k) = r.p.ptp(i, j, k) + r.ptfrc(i, j, k) * dtdrst;
+        const R v = sp(i, j, k) + frc(i, j, k) * dtdrst;
+        sf(i, j, k) = clip ? std::max(R(0), v) : v;
       }
-  bcycle(o, 2, 1, ni - 2, ni - 1, 2, 1, nj - 2, nj - 1, nk, r.f.ptp);   // steps.f90:3979
-  // s_timeflt (timeflt.f90:335-404)
-  const R fcoe = R(r.lo.filcoe), m1fc2 = R(1) - R(2) * R(r.lo.filcoe);
-  for (int k = 1; k <= nk - 1; ++k) {
-    for (int j = 1; j <= nj - 1; ++j)
-      for (int i = 1; i <= ni; ++i) r.c.u(i, j, k) = m1fc2 * r.c.u(i, j, k) + fcoe * (r.f.u(i, j, k) + r.p.u(i, j, k));
-    for (int j = 1; j <= nj; ++j)
-      for (int i = 1; i <= ni - 1; ++i) r.c.v(i, j, k) = m1fc2 * r.c.v(i, j, k) + fcoe * (r.f.v(i, j, k) + r.p.v(i, j, k));
-  }
-  for (int k = 1; k <= nk; ++k)
-    for (int j = 1; j <= nj - 1; ++j)
-      for (int i = 1; i <= ni - 1; ++i) r.c.w(i, j, k) = m1fc2 * r.c.w(i, j, k) + fcoe * (r.f.w(i, j, k) + r.p.w(i, j, k));
-  for (int k = 1; k <= nk - 1; ++k)
-    for (int j = 1; j <= nj - 1; ++j)
-      for (int i = 1; i <= ni - 1; ++i) {
-        r.c.pp(i, j, k) = m1fc2 * r.c.pp(i, j, k) + fcoe * (r.f.pp(i, j, k) + r.p.pp(i, j, k));
-        r.c.ptp(i, j, k) = m1fc2 * r.c.ptp(i, j, k) + fcoe * (r.f.ptp(i, j, k) + r.p.ptp(i, j, k));
-      }
-  // shift2nd on t and t+dt (intgdrv.f90:1005,1013): both periodic planes
+  bcycle(o, 2, 1, ni - 2, ni - 1, 2, 1, nj - 2, nj - 1, nk, sf);
+  vbcs(o, sf);
+}
+
+template <class R>
+void timeflt_field(const Opts& o, R filcoe, int ihi, int jhi, int khi, F3<R>& c, const F3<R>& f, const F3<R>& p) {
+  const R m1fc2 = R(1) - R(2) * filcoe;
+  for (int k = 1; k <= khi; ++k)
+    for (int j = 1; j <= jhi; ++j)
+      for (int i = 1; i <= ihi; ++i) c(i, j, k) = m1fc2 * c(i, j, k) + filcoe * (f(i, j, k) + p(i, j, k));
+}
+
+template <class R>
+void phase_timeflt(DryRun<R>& r) {   // s_timeflt (timeflt.f90:335-404)
+  const Opts& o = r.o;
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  const R fc = R(r.lo.filcoe);
+  timeflt_field(o, fc, ni, nj - 1, nk - 1, r.c.u, r.f.u, r.p.u);
+  timeflt_field(o, fc, ni - 1, nj, nk - 1, r.c.v, r.f.v, r.p.v);
+  timeflt_field(o, fc, ni - 1, nj - 1, nk, r.c.w, r.f.w, r.p.w);
+  timeflt_field(o, fc, ni - 1, nj - 1, nk - 1, r.c.pp, r.f.pp, r.p.pp);
+  timeflt_field(o, fc, ni - 1, nj - 1, nk - 1, r.c.ptp, r.f.ptp, r.p.ptp);
+}
+
+template <class R>
+void phase_halo(DryRun<R>& r) {   // shift2nd on t and t+dt (intgdrv.f90:1005,1013)
   for (Level<R>* L : {&r.c, &r.f}) {
-    halo_both(o, 'u', L->u); halo_both(o, 'v', L->v); halo_both(o, 's', L->w);
-    halo_both(o, 's', L->pp); halo_both(o, 's', L->ptp);
+    halo_both(r.o, 'u', L->u); halo_both(r.o, 'v', L->v); halo_both(r.o, 's', L->w);
+    halo_both(r.o, 's', L->pp); halo_both(r.o, 's', L->ptp);
   }
-  // swp2nxt (swp2nxt.f90:358-): past <- t, t <- t+dt
-  std::swap(r.p, r.c);
+}
+
+// One dry large step (leapfrog from t-dt to t+dt with dtb, nsstp
+// substeps of dts): forcing, small steps, s_steps for theta', s_timeflt
+// (skipped on the first step, ctime=0: intgdrv.f90:968), shift2nd planes
+// and the swp2nxt rotation.
+template <class R>
+void intgdrv_dry(DryRun<R>& r, R dtb, int nsstp, R dts, bool filter) {
+  phase_forcing(r);
+  phase_small(r, nsstp, dts);
+  step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false);
+  if (filter) phase_timeflt(r);
+  phase_halo(r);
+  std::swap(r.p, r.c);   // swp2nxt: past <- t, t <- t+dt
   std::swap(r.c, r.f);
 }
 

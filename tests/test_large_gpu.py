@@ -21,7 +21,7 @@ def region(name, ni, nj, nk):
     m = np.zeros((nk, nj + 2, ni + 2), bool)
     ih = ni + 1 if STAG[name] == "u" else ni
     jh = nj + 1 if STAG[name] == "v" else nj
-    k0, k1 = (1, nk) if name == "w" else (2, nk - 2)
+    k0, k1 = (1, nk) if name == "w" else (1, nk - 1)
     m[k0 - 1:k1, 0:jh + 1, 0:ih + 1] = True
     return m
 
@@ -51,7 +51,8 @@ def run_case(cress, oracle_lib, nx, ny, nz, nsteps, coropt=0, seed=3):
     nsstp = 20 * int(1.e2 * (dtbig + .001)) // int(1.e3 * (dtsml + .0001))
     for step in range(nsteps):
         first = step == 0
-        s.large_step(0.5 * dtbig if first else dtbig, nsstp, 0.5 * dtsml if first else dtsml)
+        s.large_step(round(step * dtbig * 1000), 0.5 * dtbig if first else dtbig, nsstp,
+                     0.5 * dtsml if first else dtsml)
     gp = [s.get_field(n, cress.PAST) for n in NAMES]
     gn = [s.get_field(n, cress.NOW) for n in NAMES]
     s.close()
