@@ -50,7 +50,7 @@ class Cfg(ctypes.Structure):
                 ("coropt", ctypes.c_int), ("tubopt", ctypes.c_int), ("cphopt", ctypes.c_int),
                 ("smhcoe", ctypes.c_float), ("smvcoe", ctypes.c_float), ("filcoe", ctypes.c_float),
                 ("fc", ctypes.c_float), ("vspvar", ctypes.c_char * 16),
-                ("reserved", ctypes.c_int * 8)]
+                ("thresq", ctypes.c_float), ("reserved", ctypes.c_int * 7)]
 
 
 _lib = None
@@ -107,7 +107,7 @@ class Solver:
 
     def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6,
                  tile=0, device=0, smtopt=3, smhcoe=0.001, smvcoe=0.0004, vspopt=2,
-                 vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1, cphopt=0):
+                 vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1, cphopt=0, thresq=1e-12):
         L = lib()
         c = Cfg()
         c.ni, c.nj, c.nk = ni, nj, nk
@@ -120,6 +120,7 @@ class Solver:
         c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = 2, smtopt, vspopt, coropt, 0, cphopt
         c.smhcoe, c.smvcoe, c.filcoe, c.fc = smhcoe, smvcoe, filcoe, fc
         c.vspvar = vspvar.encode()[:15]
+        c.thresq = thresq
         self.cfg = c
         self.shape = (nk, nj + 2, ni + 2)
         h = ctypes.c_void_p()

@@ -67,6 +67,11 @@ def base_columns(nk, dz, sthopt=0, dzmin=None, theta_sfc=300.0, dthdz=0.0, qv_sf
     f32 = lambda a: np.asarray(a, np.float32)
     c = {"jcb": f32(jcb), "ptbr": f32(theta), "pbr": f32(pbr), "rbr": f32(rbr),
          "zs": zs}
+    return _derived_columns(c, nk)
+
+
+def _derived_columns(c, nk):
+    """rst, rcsq and the u/v/w-point averages of jcb and rst."""
     c["rst"] = (np.abs(c["jcb"]) * c["rbr"]).astype(np.float32)
     c["rcsq"] = (np.float32(CP / CV) * c["pbr"]).astype(np.float32)
     for name in ("jcb", "rst"):
@@ -79,6 +84,97 @@ def base_columns(nk, dz, sthopt=0, dzmin=None, theta_sfc=300.0, dthdz=0.0, qv_sf
         c[name + "8u"] = (np.float32(0.5) * (c[name] + c[name])).astype(np.float32)
         c[name + "8v"] = c[name + "8u"].copy()
     return c
+
+
+def power_stretched_jcb(nk, ztop, dzmin, dzmax):
+    """Jacobian of a grid whose layer thickness grows from dzmin at the
+    ground to dzmax at the lid as dz(s) = dzmin + (dzmax-dzmin)*s**p,
+    s = 0..1 over the nz = nk-3 layers, p chosen so the layers sum to ztop.
+    Returns (jcb(k), mean spacing dz = ztop/nz)."""
+    n = nk - 3
+    dz = ztop / n
+    if not dzmin < dz < dzmax:
+        raise ValueError(f"{n} layers of {dzmin}..{dzmax} m cannot reach {ztop} m")
+    s = np.linspace(0.0, 1.0, n)
+    lo, hi = 0.01, 20.0
+    for _ in range(200):
+        p = 0.5 * (lo + hi)
+        tot = np.sum(dzmin + (dzmax - dzmin) * s ** p)
+        lo, hi = (p, hi) if tot > ztop else (lo, p)
+    jcb = np.ones(nk + 1)
+    jcb[2:2 + n] = (dzmin + (dzmax - dzmin) * s ** p) * (ztop / tot) / dz
+    jcb[1] = jcb[2]
+    jcb[nk - 1:] = jcb[nk - 2]
+    return jcb, dz
+
+
+EPSVA = RD / RV
+
+
+def moist_columns(nk, ztop=18000.0, dzmin=100.0, dzmax=500.0, theta_sfc=300.0, theta_tr=343.0,
+                  z_tr=12000.0, t_tr=213.0, qv_max=0.014, p_sfc=1.0e5):
+    """1-D base columns of the analytic supercell sounding on a stretched
+    grid: theta = theta_sfc + (theta_tr-theta_sfc)*(z/z_tr)**1.25 below the
+    tropopause z_tr, theta_tr*exp(g*(z-z_tr)/(cp*t_tr)) above; relative
+    humidity 1 - 0.75*(z/z_tr)**1.25 (0.25 above z_tr); qv capped at qv_max.
+    Hydrostatic in the virtual potential temperature, integrated in FP64
+    (Exner form, midpoint rule, qv iterated with p).  The base density
+    follows rbr = pbr/(rd*ptvbr*pibr), ptvbr = ptbr*(1+qvbr/epsva)/(1+qvbr)
+    (SrcOrig/setbase.f90:153-189)."""
+    jcb, dz = power_stretched_jcb(nk, ztop, dzmin, dzmax)
+    zw = np.zeros(nk + 1)
+    for k in range(3, nk + 1):
+        zw[k] = zw[k - 1] + jcb[k - 1] * dz
+    zs = np.zeros(nk + 1)
+    zs[1:nk] = 0.5 * (zw[1:nk] + zw[2:nk + 1])
+    zs[1] = -zs[2]
+    zs[nk] = zs[nk - 1] + jcb[nk - 1] * dz
+
+    def theta_of(z):
+        z = np.asarray(z, np.float64)
+        zc = np.clip(z, 0.0, None)
+        below = theta_sfc + (theta_tr - theta_sfc) * (np.minimum(zc, z_tr) / z_tr) ** 1.25
+        above = theta_tr * np.exp(G * (zc - z_tr) / (CP * t_tr))
+        return np.where(zc <= z_tr, below, above)
+
+    def rh_of(z):
+        zc = np.clip(np.asarray(z, np.float64), 0.0, z_tr)
+        return 1.0 - 0.75 * (zc / z_tr) ** 1.25
+
+    def qv_of(z, pi):
+        p = P0 * pi ** (CP / RD)
+        t = theta_of(z) * pi
+        return np.minimum(rh_of(z) * qvs_water(t, p), qv_max)
+
+    thv = lambda th, qv: th * (1.0 + qv / EPSVA) / (1.0 + qv)
+    pi = np.empty(nk + 1)
+    pi_s = (p_sfc / P0) ** (RD / CP)
+    # integrate from the ground (z = 0) to each scalar level
+    order = np.argsort(zs[1:]) + 1
+    z_prev, pi_prev = 0.0, pi_s
+    for k in [k for k in order if zs[k] >= 0.0]:
+        z0, z1 = z_prev, zs[k]
+        guess = pi_prev
+        for _ in range(8):
+            zm, pm = 0.5 * (z0 + z1), 0.5 * (pi_prev + guess)
+            guess = pi_prev - G * (z1 - z0) / (CP * thv(theta_of(zm), qv_of(zm, pm)))
+        pi[k] = guess
+        z_prev, pi_prev = z1, guess
+    k1 = 1   # the level below the ground, mirrored
+    guess = pi_s
+    for _ in range(8):
+        zm, pm = 0.5 * zs[k1], 0.5 * (pi_s + guess)
+        guess = pi_s - G * zs[k1] / (CP * thv(theta_of(zm), qv_of(zm, pm)))
+    pi[k1] = guess
+    pi[0] = pi[1]
+    theta = theta_of(zs)
+    qv = qv_of(zs, pi)
+    pbr = P0 * pi ** (CP / RD)
+    rbr = pbr / (RD * thv(theta, qv) * pi)
+    f32 = lambda a: np.asarray(a, np.float32)
+    c = {"jcb": f32(jcb), "ptbr": f32(theta), "pbr": f32(pbr), "rbr": f32(rbr), "qvbr": f32(qv),
+         "zs": zs, "zph": np.where(np.arange(nk + 1) == 1, -zw[3], zw), "dz": dz}
+    return _derived_columns(c, nk)
 
 
 def expand(colk, ni, nj, nk):
@@ -176,6 +272,73 @@ def dry_case(nx, ny, nz, dx, dz, sthopt=1, seed=0, ptp0=2.0, rad=None, u0=5.0, s
              periodic_fill(pp, "s"), periodic_fill(ptp, "s")]
     return dict(dims=(ni, nj, nk), base=base, cols=cols, zph=zph, level=level,
                 vspbar=vspbar, botbar=botbar)
+
+
+MOIST_NAMES = ["qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
+
+
+def supercell_case(nx, ny, nz, dx, ztop=18000.0, dzmin=100.0, dzmax=500.0, seed=0, ptp0=3.0,
+                   rad=(10000.0, 10000.0, 1400.0), zc=1400.0, shear=30.0, rcirc=7.0,
+                   noise=0.0, cloud=False):
+    """Moist supercell state (cold-rain microphysics, cphopt=3).
+
+    Base state: the analytic sounding of moist_columns on a grid stretched
+    from dzmin to dzmax up to ztop; quarter-circle hodograph of radius rcirc
+    over 0-2 km continuing straight to `shear` m/s of u at 6 km (constant
+    above).  Perturbation: +ptp0 K cos^2 ellipsoidal bubble of radii `rad`
+    centred at mid-domain, height zc, plus seeded uniform +-noise K.  With
+    cloud=True a seeded field of cloud, rain, ice, snow and graupel (with
+    ice numbers) and supersaturated pockets is added so every microphysical
+    process acts from the first step.  Returns a dict with dims, base (3-D,
+    incl. ubr, vbr, pbr, qvbr), cols, zph, dz (mean spacing), level (u, v,
+    w, pp, ptp) and moist (qv ... ng), past = present."""
+    ni, nj, nk = dims(nx, ny, nz)
+    cols = moist_columns(nk, ztop, dzmin, dzmax)
+    base = {n: expand(cols[n], ni, nj, nk) for n in BASE_NAMES + ["pbr", "qvbr"]}
+    zs = cols["zs"]
+    th = 0.5 * np.pi * np.clip(zs / 2000.0, 0.0, 1.0)
+    u = np.where(zs < 2000.0, rcirc * (1.0 - np.cos(th)),
+                 rcirc + (shear - rcirc) * np.clip((zs - 2000.0) / 4000.0, 0.0, 1.0))
+    v = rcirc * np.sin(th)
+    base["ubr"] = expand(u.astype(np.float32), ni, nj, nk)
+    base["vbr"] = expand(v.astype(np.float32), ni, nj, nk)
+    rng = np.random.default_rng(seed)
+    shp = (nk, nj + 2, ni + 2)
+    x = (np.arange(ni + 2) - 0.5 * (ni + 1)) * dx
+    y = (np.arange(nj + 2) - 0.5 * (nj + 1)) * dx
+    z = zs[1:nk + 1]
+    r = np.sqrt((x[None, None, :] / rad[0]) ** 2 + (y[None, :, None] / rad[1]) ** 2 +
+                ((z[:, None, None] - zc) / rad[2]) ** 2)
+    ptp = np.where(r < 1.0, ptp0 * np.cos(0.5 * np.pi * r) ** 2, 0.0)
+    if noise:
+        ptp = ptp + rng.uniform(-noise, noise, shp)
+    level = [base["ubr"].copy(), base["vbr"].copy(), np.zeros(shp, np.float32),
+             np.zeros(shp, np.float32), ptp.astype(np.float32)]
+    moist = {n: np.zeros(shp, np.float32) for n in MOIST_NAMES}
+    moist["qv"] = base["qvbr"].copy()
+    if cloud:
+        zz = z[:, None, None]
+        pbr = base["pbr"].astype(np.float64)
+        t = (base["ptbr"] * (pbr / P0) ** (RD / CP)).astype(np.float64)
+
+        def blob(lo, hi, zlo, zhi, amp):
+            b = np.clip((_noise(rng, shp, 1.0) - lo) / (hi - lo), 0.0, 1.0)
+            return amp * b * ((zz > zlo) & (zz < zhi))
+
+        moist["qv"] = np.minimum((0.8 + 0.3 * _noise(rng, shp, 1.0)) * qvs_water(t, pbr), 0.02)
+        moist["qc"] = blob(0.0, 0.6, 500.0, 9000.0, 1.5e-3)
+        moist["qr"] = blob(0.1, 0.8, 0.0, 6000.0, 2.0e-3)
+        moist["qi"] = blob(0.0, 0.7, 6000.0, 14000.0, 3.0e-4)
+        moist["qs"] = blob(0.0, 0.7, 4500.0, 12000.0, 1.0e-3)
+        moist["qg"] = blob(0.1, 0.8, 3000.0, 10000.0, 1.5e-3)
+        moist["ni"] = moist["qi"] / 1.0e-11 * (0.5 + rng.random(shp))
+        moist["ns"] = moist["qs"] / 5.0e-9 * (0.5 + rng.random(shp))
+        moist["ng"] = moist["qg"] / 5.0e-8 * (0.5 + rng.random(shp))
+    stag = ["u", "v", "s", "s", "s"]
+    level = [periodic_fill(np.asarray(a, np.float32), s) for a, s in zip(level, stag)]
+    moist = {n: periodic_fill(np.asarray(a, np.float32), "s") for n, a in moist.items()}
+    return dict(dims=(ni, nj, nk), base=base, cols=cols, zph=cols["zph"], dz=cols["dz"],
+                level=level, moist=moist)
 
 
 def qvs_water(t, p):

@@ -239,26 +239,32 @@ int Ctx::small_steps(int nsstp, float dts) {
   return CRESS_OK;
 }
 
-// One dry large step on the device-resident state (s_intgdrv order,
-// SrcOrig/intgdrv.f90:866-1119).
+// One large step on the device-resident state in s_intgdrv's order
+// (SrcOrig/intgdrv.f90:832-1119): forcing (moist buoyancy when cphopt=3),
+// small steps, the theta' step (inside k_force), the moist scalar steps,
+// s_cloudphy, s_timeflt (not at ctime=0), s_satadjst on t and t+dt,
+// periodic ghost planes, swp2nxt.
 int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
   if (!base_set || !large_set)
     return set_error(CRESS_E_STATE, "cress_large_step: base state (set_base3d, set_base_large) not set");
-  if (cfg.advopt != 2 || cfg.tubopt != 0 || cfg.cphopt != 0 ||
+  if (cfg.advopt != 2 || cfg.tubopt != 0 || !(cfg.cphopt == 0 || cfg.cphopt == 3) ||
       !(cfg.smtopt == 0 || cfg.smtopt % 10 == 2 || cfg.smtopt % 10 == 3) ||
       !(cfg.vspopt == 0 || cfg.vspopt == 2) || !(cfg.coropt == 0 || cfg.coropt == 1))
     return set_error(CRESS_E_UNSUPPORTED,
-                     "cress_large_step: needs advopt=2, tubopt=0, cphopt=0, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
+                     "cress_large_step: needs advopt=2, tubopt=0, cphopt 0/3, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
+  const bool moist = cfg.cphopt == 3;
+  if (moist && !moist_set) return set_error(CRESS_E_STATE, "cress_large_step: moist base state not set");
+  const int N = CRESS_NOW, P = CRESS_PAST, F = CRESS_FUTURE;
   ForceArgs f{};
   f.g = g;
   f.col = col_d;
-  f.u = lev[CRESS_U][CRESS_NOW]; f.v = lev[CRESS_V][CRESS_NOW]; f.w = lev[CRESS_W][CRESS_NOW];
-  f.pp = lev[CRESS_PP][CRESS_NOW]; f.ptp = lev[CRESS_PTP][CRESS_NOW];
-  f.up = lev[CRESS_U][CRESS_PAST]; f.vp = lev[CRESS_V][CRESS_PAST]; f.wp = lev[CRESS_W][CRESS_PAST];
-  f.ppp = lev[CRESS_PP][CRESS_PAST]; f.ptpp = lev[CRESS_PTP][CRESS_PAST];
+  f.u = lev[CRESS_U][N]; f.v = lev[CRESS_V][N]; f.w = lev[CRESS_W][N];
+  f.pp = lev[CRESS_PP][N]; f.ptp = lev[CRESS_PTP][N];
+  f.up = lev[CRESS_U][P]; f.vp = lev[CRESS_V][P]; f.wp = lev[CRESS_W][P];
+  f.ppp = lev[CRESS_PP][P]; f.ptpp = lev[CRESS_PTP][P];
   f.ufrc = lev[CRESS_U][CRESS_FORCING]; f.vfrc = lev[CRESS_V][CRESS_FORCING];
   f.wfrc = lev[CRESS_W][CRESS_FORCING]; f.pfrc = lev[CRESS_PP][CRESS_FORCING];
-  f.ptpf = lev[CRESS_PTP][CRESS_FUTURE];
+  f.ptpf = lev[CRESS_PTP][F];
   f.dxiv = 1.f / cfg.dx; f.dyiv = 1.f / cfg.dy; f.dziv = 1.f / cfg.dz;
   f.smhcoe = cfg.smhcoe; f.smvcoe = cfg.smvcoe;
   f.fc = cfg.fc;
@@ -267,41 +273,80 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
   f.ksp0 = ksp0;
   auto on = [&](int n) { return cfg.vspvar[n] == 'o' ? 1 : 0; };
   f.vsp_u = on(0); f.vsp_v = on(1); f.vsp_w = on(2); f.vsp_p = on(3); f.vsp_pt = on(4);
+  if (moist) {
+    f.qv = lev[CRESS_QV][N]; f.qc = lev[CRESS_QC][N]; f.qr = lev[CRESS_QR][N];
+    f.qi = lev[CRESS_QI][N]; f.qs = lev[CRESS_QS][N]; f.qg = lev[CRESS_QG][N];
+  }
   int rc = launch_force(f, stream);
   ++launches;
   if (rc) return set_error(rc, "forcing launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   if ((rc = small_steps(nsstp, dts))) return rc;
-  FilterArgs t{};
-  t.g = g;
-  t.u = lev[CRESS_U][CRESS_NOW]; t.v = lev[CRESS_V][CRESS_NOW]; t.w = lev[CRESS_W][CRESS_NOW];
-  t.pp = lev[CRESS_PP][CRESS_NOW]; t.ptp = lev[CRESS_PTP][CRESS_NOW];
-  t.uf = lev[CRESS_U][CRESS_FUTURE]; t.vf = lev[CRESS_V][CRESS_FUTURE]; t.wf = lev[CRESS_W][CRESS_FUTURE];
-  t.ppf = lev[CRESS_PP][CRESS_FUTURE]; t.ptpf = lev[CRESS_PTP][CRESS_FUTURE];
-  t.up = lev[CRESS_U][CRESS_PAST]; t.vp = lev[CRESS_V][CRESS_PAST]; t.wp = lev[CRESS_W][CRESS_PAST];
-  t.ppp = lev[CRESS_PP][CRESS_PAST]; t.ptpp = lev[CRESS_PTP][CRESS_PAST];
-  t.filcoe = cfg.filcoe;
+  if (moist) {
+    MoistScalarArgs m{};
+    m.g = g;
+    m.col = col_d;
+    m.u = lev[CRESS_U][N]; m.v = lev[CRESS_V][N]; m.w = lev[CRESS_W][N];
+    for (int n = 0; n < kMoistN; ++n) {
+      m.s[n] = lev[CRESS_QV + n][N];
+      m.sp[n] = lev[CRESS_QV + n][P];
+      m.sf[n] = lev[CRESS_QV + n][F];
+    }
+    m.dxiv = f.dxiv; m.dyiv = f.dyiv; m.dziv = f.dziv;
+    m.smhcoe = cfg.smhcoe; m.smvcoe = cfg.smvcoe; m.dtb2 = f.dtb2;
+    m.smtopt = cfg.smtopt; m.vspopt = cfg.vspopt; m.sthopt = cfg.sthopt; m.ksp0 = ksp0;
+    m.vsp_qv = on(5); m.vsp_q = on(6);
+    if ((rc = launch_moist_scalars(m, stream))) return set_error(rc, "moist scalar launch failed");
+    ++launches;
+    if ((rc = cloudphy(dtb, cfg.thresq))) return rc;
+  }
   if (filter) {
+    FilterArgs t{};
+    t.g = g;
+    t.u = lev[CRESS_U][N]; t.v = lev[CRESS_V][N]; t.w = lev[CRESS_W][N];
+    t.pp = lev[CRESS_PP][N]; t.ptp = lev[CRESS_PTP][N];
+    t.uf = lev[CRESS_U][F]; t.vf = lev[CRESS_V][F]; t.wf = lev[CRESS_W][F];
+    t.ppf = lev[CRESS_PP][F]; t.ptpf = lev[CRESS_PTP][F];
+    t.up = lev[CRESS_U][P]; t.vp = lev[CRESS_V][P]; t.wp = lev[CRESS_W][P];
+    t.ppp = lev[CRESS_PP][P]; t.ptpp = lev[CRESS_PTP][P];
+    t.filcoe = cfg.filcoe;
     if ((rc = launch_timeflt(t, stream))) return set_error(rc, "timeflt launch failed");
+    ++launches;
+  }
+  if (moist) {
+    MoistPostArgs m{};
+    m.g = g;
+    m.col = col_d;
+    for (int n = 0; n < kMoistN; ++n) {
+      m.c[n] = lev[CRESS_QV + n][N];
+      m.f[n] = lev[CRESS_QV + n][F];
+      m.p[n] = lev[CRESS_QV + n][P];
+    }
+    m.ptpc = lev[CRESS_PTP][N]; m.ppc = lev[CRESS_PP][N];
+    m.ptpf = lev[CRESS_PTP][F]; m.ppf = lev[CRESS_PP][F];
+    m.filcoe = cfg.filcoe; m.thresq = cfg.thresq; m.filter = filter ? 1 : 0;
+    if ((rc = launch_moist_post(m, stream))) return set_error(rc, "moist filter/adjustment launch failed");
     ++launches;
   }
   HaloArgs h{};
   h.g = g;
-  const int F[5] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP, CRESS_PTP};
-  const int S[5] = {STAG_U, STAG_V, STAG_S, STAG_S, STAG_S};
-  for (int lvl : {CRESS_NOW, CRESS_FUTURE})
-    for (int n = 0; n < 5; ++n) {
-      h.f[h.n] = lev[F[n]][lvl];
-      h.stag[h.n] = S[n];
+  const int nrot = moist ? 5 + kMoistN : 5;
+  int F5[5 + kMoistN] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP, CRESS_PTP};
+  int S5[5 + kMoistN] = {STAG_U, STAG_V, STAG_S, STAG_S, STAG_S};
+  for (int n = 0; n < kMoistN; ++n) { F5[5 + n] = CRESS_QV + n; S5[5 + n] = STAG_S; }
+  for (int lvl : {N, F})
+    for (int n = 0; n < nrot; ++n) {
+      h.f[h.n] = lev[F5[n]][lvl];
+      h.stag[h.n] = S5[n];
       ++h.n;
     }
   if ((rc = launch_halo(h, stream))) return set_error(rc, "halo launch failed");
   ++launches;
   // swp2nxt: past <- t, t <- t+dt (pointer rotation)
-  for (int n = 0; n < 5; ++n) {
-    float* p = lev[F[n]][CRESS_PAST];
-    lev[F[n]][CRESS_PAST] = lev[F[n]][CRESS_NOW];
-    lev[F[n]][CRESS_NOW] = lev[F[n]][CRESS_FUTURE];
-    lev[F[n]][CRESS_FUTURE] = p;
+  for (int n = 0; n < nrot; ++n) {
+    float* p = lev[F5[n]][P];
+    lev[F5[n]][P] = lev[F5[n]][N];
+    lev[F5[n]][N] = lev[F5[n]][F];
+    lev[F5[n]][F] = p;
   }
   return CRESS_OK;
 }
@@ -367,7 +412,7 @@ using namespace cress;
 extern "C" {
 
 const char* cress_last_error(void) { return g_last_error.c_str(); }
-int cress_abi_version(void) { return 1; }
+int cress_abi_version(void) { return 2; }
 
 int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   if (!cfg || !out) return set_error(CRESS_E_ARG, "cress_create: null argument");

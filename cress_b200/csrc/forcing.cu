@@ -24,9 +24,7 @@
 namespace cress {
 namespace {
 
-struct Pt {
-  long long id, px, pl;
-};
+constexpr float kEpsva = .622f;   // rd/rv, comphy.f90:79
 
 __device__ __forceinline__ float ld(const float* f, long long idx) { return __ldg(f + idx); }
 
@@ -167,10 +165,16 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
       f = smooth_into(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 1, A);
     }
     if (a.vspopt >= 1 && a.vsp_w && k >= a.ksp0) f = f - C(C_RBCT, k) * C(C_RST8W, k) * ld(a.wp, id);
-    if (k >= 3 && k <= nk - 2) {   // buoywb.f90:166-172,307-313 (dry)
-      const float b0 = g05 * C(C_RST, k - 1) * ld(a.ptp, id - pl) / C(C_PTBR, k - 1);
-      const float b1 = g05 * C(C_RST, k) * ld(a.ptp, id) / C(C_PTBR, k);
-      f = f + (b0 + b1);
+    if (k >= 3 && k <= nk - 2) {   // buoywb.f90:166-172 (dry), 202-299 (moist), 307-313
+      auto wb8s = [&](long long p, int kk) {
+        if (!a.qv) return g05 * C(C_RST, kk) * ld(a.ptp, p) / C(C_PTBR, kk);
+        const float qvbr = C(C_QVBR, kk);
+        const float qvd = ld(a.qv, p) - qvbr;
+        const float qall = (((ld(a.qc, p) + ld(a.qr, p)) + ld(a.qi, p)) + ld(a.qs, p)) + ld(a.qg, p);  // totalqwi.f90:163
+        return g05 * C(C_RST, kk) *
+               ((qvd / (kEpsva + qvbr) - (qvd + qall) / (1.f + qvbr)) + ld(a.ptp, p) / C(C_PTBR, kk));
+      };
+      f = f + (wb8s(id - pl, k - 1) + wb8s(id, k));
     }
     // advuvw.f90:685-852
     auto W = [&](long long p) { return ld(a.w, p); };
@@ -244,6 +248,80 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   }
 }
 
+// Forcing and s_steps of the nine moist scalars, one thread per scalar
+// point (i, j = 2..n-2, k = 2..nk-2), all nine fields per thread so the
+// advecting fluxes rst8u*u, rst8v*v, rst8w*wc are formed once:
+//   sfrc = advs (advs.f90:205-370) + smoo4qv / smoo4s of rbr*(qvp-qvbr) or
+//          rbr*sp (smoo4s.f90:184-296) + vspqv / vsps / vsps0
+//          (vspqv.f90:181-198, vsps.f90:181-198, vsps0.f90:114-124)
+//   sf = sp + sfrc*2dtb/rst, clipped at 0 for the mixing ratios
+//        (steps.f90:590-764), then vbcs at k=1, nk-1 (vbcs.f90:116-132).
+__global__ void __launch_bounds__(256) k_moist_scalars(const MoistScalarArgs a) {
+  const Grid g = a.g;
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > ni - 2 || j > nj - 2 || k > nk - 2) return;
+  const long long px = g.px, pl = g.plane;
+  const long long id = g.at(i, j, k);
+  const int nc = nk + 1;
+  auto C = [&](int f, int kk) { return __ldg(a.col + f * nc + kk); };
+  const float oned24 = 1.f / 24.f, fourd3 = 4.f / 3.f;
+  const float dxv24 = oned24 * a.dxiv, dyv24 = oned24 * a.dyiv;
+  const float dxv05n = -.5f * a.dxiv, dyv05n = -.5f * a.dyiv, dzv05n = -.5f * a.dziv;
+  const bool smooth = (a.smtopt % 10 == 2) || (a.smtopt % 10 == 3);
+  // rstuvwc.f90:172-210 fluxes at the faces the stencil touches
+  const float r8u = C(C_RST8U, k), r8v = C(C_RST8V, k);
+  const float fu_m1 = r8u * ld(a.u, id - 1), fu_0 = r8u * ld(a.u, id);
+  const float fu_p1 = r8u * ld(a.u, id + 1), fu_p2 = r8u * ld(a.u, id + 2);
+  const float fv_m1 = r8v * ld(a.v, id - px), fv_0 = r8v * ld(a.v, id);
+  const float fv_p1 = r8v * ld(a.v, id + px), fv_p2 = r8v * ld(a.v, id + 2 * px);
+  auto WC = [&](long long p, int kk) { return a.sthopt ? ld(a.w, p) / C(C_JCB8W, kk) : ld(a.w, p); };
+  const float fw_0 = C(C_RST8W, k) * WC(id, k), fw_1 = C(C_RST8W, k + 1) * WC(id + pl, k + 1);
+  const float rbct5 = .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1));
+  const float rst = C(C_RST, k);
+  const float dtdrst = a.dtb2 / rst;                                     // steps.f90:528
+#pragma unroll 1
+  for (int n = 0; n < kMoistN; ++n) {
+    const float* s = a.s[n];
+    const float s0 = ld(s, id);
+    // advs.f90:205-370, 4th-order horizontal, 2nd-order vertical
+    const float t1a = fu_0 * (s0 - ld(s, id - 1)) * dxv05n;
+    const float t1b = fu_p1 * (ld(s, id + 1) - s0) * dxv05n;
+    const float t2a = fv_0 * (s0 - ld(s, id - px)) * dyv05n;
+    const float t2b = fv_p1 * (ld(s, id + px) - s0) * dyv05n;
+    float f = (t1a + t1b) + (t2a + t2b);
+    const float w1a = (fu_m1 + fu_0) * (s0 - ld(s, id - 2)) * dxv24;
+    const float w1b = (fu_p1 + fu_p2) * (ld(s, id + 2) - s0) * dxv24;
+    const float w2a = (fv_m1 + fv_0) * (s0 - ld(s, id - 2 * px)) * dyv24;
+    const float w2b = (fv_p1 + fv_p2) * (ld(s, id + 2 * px) - s0) * dyv24;
+    f = fourd3 * f + ((w1a + w1b) + (w2a + w2b));
+    const float t3a = fw_0 * (s0 - ld(s, id - pl)) * dzv05n;
+    const float t3b = fw_1 * (ld(s, id + pl) - s0) * dzv05n;
+    f = f + (t3a + t3b);
+    const float* sp = a.sp[n];
+    const bool isqv = n == 0;
+    if (smooth) {
+      auto A = [&](int dx, int dy, int dz) {
+        const int kk = k + dz;
+        const float v = ld(sp, id + dx + dy * px + dz * pl);
+        return isqv ? C(C_RBR, kk) * (v - C(C_QVBR, kk)) : C(C_RBR, kk) * v;
+      };
+      f = smooth_into(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+    }
+    const float spv = ld(sp, id);
+    if (a.vspopt >= 1 && (isqv ? a.vsp_qv : a.vsp_q) && k >= a.ksp0 - 1)
+      f = f - rbct5 * rst * (isqv ? spv - C(C_QVBR, k) : spv);
+    float sf = spv + f * dtdrst;
+    if (n < 6) sf = fmaxf(0.f, sf);
+    float* out = a.sf[n];
+    out[id] = sf;
+    if (k == 2) out[id - pl] = sf;        // vbcs.f90:118
+    if (k == nk - 2) out[id + pl] = sf;   // vbcs.f90:132
+  }
+}
+
 // s_timeflt, SrcOrig/timeflt.f90:335-404 on the interior (ghosts are
 // refilled by k_halo afterwards).
 __global__ void __launch_bounds__(256) k_timeflt(const FilterArgs a) {
@@ -305,6 +383,13 @@ int launch_force(const ForceArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);
   dim3 gr((a.g.ni - 2 + 31) / 32, (a.g.nj - 2 + 7) / 8, a.g.nk - 2);
   k_force<<<gr, b, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+int launch_moist_scalars(const MoistScalarArgs& a, cudaStream_t st) {
+  dim3 b(32, 8, 1);
+  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 3);
+  k_moist_scalars<<<gr, b, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 

@@ -27,9 +27,28 @@ struct ForceArgs {
   float dtb2;                 // 2*dtb
   int smtopt, vspopt, coropt, sthopt, ksp0;
   int vsp_u, vsp_v, vsp_w, vsp_p, vsp_pt;  // vspvar switches
+  // moist buoyancy (buoywb.f90:202-299, cphopt != 0): qv and the five
+  // hydrometeor mixing ratios at t; null qv = dry buoyancy
+  const float* qv; const float* qc; const float* qr; const float* qi; const float* qs; const float* qg;
 };
 
 int launch_force(const ForceArgs& a, cudaStream_t st);
+
+// Forcing and leapfrog step of the nine moist scalars qv, qc, qr, qi, qs,
+// qg, ni, ns, ng (s_forceqv, s_forceq, s_steps).
+constexpr int kMoistN = 9;
+struct MoistScalarArgs {
+  Grid g;
+  const float* col;
+  const float* u; const float* v; const float* w;   // present winds (flux rst*u etc.)
+  const float* s[kMoistN];    // present level t
+  const float* sp[kMoistN];   // past level t-dt
+  float* sf[kMoistN];         // future level t+dt (output)
+  float dxiv, dyiv, dziv, smhcoe, smvcoe, dtb2;
+  int smtopt, vspopt, sthopt, ksp0;
+  int vsp_qv, vsp_q;          // vspvar(6:6), vspvar(7:7)
+};
+int launch_moist_scalars(const MoistScalarArgs& a, cudaStream_t st);
 
 struct FilterArgs {
   Grid g;
@@ -40,11 +59,12 @@ struct FilterArgs {
 };
 int launch_timeflt(const FilterArgs& a, cudaStream_t st);
 
-// Fill both periodic ghost layers of up to 8 fields (stag per field).
+// Fill both periodic ghost layers of up to kHaloMax fields (stag per field).
+constexpr int kHaloMax = 32;
 struct HaloArgs {
   Grid g;
-  float* f[16];
-  int stag[16];
+  float* f[kHaloMax];
+  int stag[kHaloMax];
   int n;
 };
 int launch_halo(const HaloArgs& a, cudaStream_t st);

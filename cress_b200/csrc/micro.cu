@@ -176,6 +176,47 @@ __global__ void __launch_bounds__(256) k_satadjst(const SatArgs a) {
   a.ptp[id] = ptp; a.qv[id] = qv; a.qc[id] = qc; a.qi[id] = qi; a.ni[id] = ni;
 }
 
+// s_timeflt for the moist fields (timeflt.f90:405-520) then s_satadjst on
+// t and t+dt (intgdrv.f90:985-998), interior points, k = 1..nk-1.
+__global__ void __launch_bounds__(256) k_moist_post(const MoistPostArgs a) {
+  const Grid g = a.g;
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (i > g.ni - 2 || j > g.nj - 2 || k > g.nk - 1) return;
+  const long long id = g.at(i, j, k);
+  const int nc = g.nk + 1;
+  float c[9];
+#pragma unroll
+  for (int n = 0; n < 9; ++n) c[n] = a.c[n][id];
+  if (a.filter) {
+    const float fc = a.filcoe, m1fc2 = 1.f - 2.f * a.filcoe;
+#pragma unroll
+    for (int n = 0; n < 9; ++n) {
+      c[n] = m1fc2 * c[n] + fc * (a.f[n][id] + __ldg(a.p[n] + id));
+      if (n != 0 && n != 1 && n != 3 && n != 6) a.c[n][id] = c[n];
+    }
+  }
+  const float rddvcp = 287.f / 1004.f, p0iv = 1.f / 1.e5f;
+  const float pbr = __ldg(a.col + C_PBR * nc + k), ptbr = __ldg(a.col + C_PTBR * nc + k);
+  {
+    const float p = pbr + a.ppc[id];                                    // getexner.f90:129
+    const float pi = expf(rddvcp * logf(p0iv * p));
+    float ptp = a.ptpc[id];
+    satadjst_cell(a.thresq, ptbr, pi, p, ptp, c[0], c[1], c[3], c[6]);
+    a.ptpc[id] = ptp;
+    a.c[0][id] = c[0]; a.c[1][id] = c[1]; a.c[3][id] = c[3]; a.c[6][id] = c[6];
+  }
+  {
+    const float p = pbr + a.ppf[id];
+    const float pi = expf(rddvcp * logf(p0iv * p));
+    float ptp = a.ptpf[id], qv = a.f[0][id], qc = a.f[1][id], qi = a.f[3][id], ni = a.f[6][id];
+    satadjst_cell(a.thresq, ptbr, pi, p, ptp, qv, qc, qi, ni);
+    a.ptpf[id] = ptp;
+    a.f[0][id] = qv; a.f[1][id] = qc; a.f[3][id] = qi; a.f[6][id] = ni;
+  }
+}
+
 }  // namespace
 
 int micro_init_tables() {
@@ -208,6 +249,13 @@ int launch_cloudphy(const MicroArgs& a, cudaStream_t st) {
   dim3 b2(32, 4, 1);
   dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 1);
   k_micro_fall<<<gr2, b2, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+int launch_moist_post(const MoistPostArgs& a, cudaStream_t st) {
+  dim3 b(32, 8, 1);
+  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
+  k_moist_post<<<gr, b, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 

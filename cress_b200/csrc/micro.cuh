@@ -33,4 +33,20 @@ struct SatArgs {
 };
 int launch_satadjst(const SatArgs& a, cudaStream_t st);
 
+// After the moist step's s_cloudphy: the Asselin filter of the nine moist
+// fields (when `filter`) and s_satadjst on t and t+dt, pointwise in one
+// pass.  Field order qv, qc, qr, qi, qs, qg, ni, ns, ng.
+struct MoistPostArgs {
+  Grid g;
+  const float* col;
+  float* c[9];          // t (filtered in place, then adjusted)
+  float* f[9];          // t+dt (adjusted)
+  const float* p[9];    // t-dt
+  float* ptpc; const float* ppc;   // theta', p' at t (already filtered)
+  float* ptpf; const float* ppf;   // theta', p' at t+dt
+  float filcoe, thresq;
+  int filter;
+};
+int launch_moist_post(const MoistPostArgs& a, cudaStream_t st);
+
 }  // namespace cress

@@ -58,12 +58,13 @@ typedef struct cress_cfg {
   int vspopt;           /* 0 none, 2 Rayleigh damping above botbar toward the base state */
   int coropt;           /* 0 none, 1 f-plane Coriolis on u, v */
   int tubopt;           /* 0 only (turbulence is not implemented on the GPU) */
-  int cphopt;           /* 0 only (dry) */
+  int cphopt;           /* 0 dry, 3 cold-rain bulk (haiopt=0) */
   float smhcoe, smvcoe; /* smoothing coefficients */
   float filcoe;         /* Asselin filter coefficient */
   float fc;             /* 0.5*omega*sin(lat) (SrcOrig/trilat.f90:118-134) */
-  char vspvar[16];      /* sponge switches u v w p pt ... ('o' on / 'x' off) */
-  int reserved[8];
+  char vspvar[16];      /* sponge switches u v w p pt qv q ... ('o' on / 'x' off) */
+  float thresq;         /* mixing-ratio threshold of the microphysics (namelist thresq) */
+  int reserved[7];
 } cress_cfg;
 
 typedef struct cress_ctx cress_ctx;

@@ -109,6 +109,44 @@ def dry_steps(cfg, base, zph, past, now, nsteps, dtbig, dtsml, start=True, prec=
         raise RuntimeError(f"oracle_dry_steps failed ({rc})")
 
 
+MOIST_BASE_NAMES = DRY_BASE_NAMES + ["pbr", "qvbr"]
+MOIST_STATE_NAMES = STATE_NAMES + ["qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
+
+
+def moist_steps(cfg, base, zph, past, now, prec, nsteps, dtbig, dtsml, start=True, prec_bits=32,
+                fp64_solve=1, omp=False):
+    """Run nsteps moist (cphopt=3) large steps on the CPU.  past/now: lists of
+    14 arrays in MOIST_STATE_NAMES order, updated in place; prec: the
+    5 x 2 x (nj+2) x (ni+2) precipitation planes (in/out).  Returns npstp
+    of the last step's sedimentation."""
+    L = lib(omp)
+    L.oracle_moist_steps.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(_FP), ctypes.POINTER(_FP), _FP, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    io = (ctypes.c_int * 10)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
+                             cfg.get("buyopt", 1), int(fp64_solve), cfg.get("sthopt", 0),
+                             cfg.get("smtopt", 3), cfg.get("vspopt", 2), cfg.get("coropt", 0))
+    ro = (ctypes.c_double * 11)(cfg["dx"], cfg["dy"], cfg["dz"], cfg.get("weicoe", 0.6),
+                                cfg.get("smhcoe", 0.001), cfg.get("smvcoe", 0.0004),
+                                cfg.get("filcoe", 0.1), cfg.get("vspbar", 0.0),
+                                cfg.get("botbar", 1e9), cfg.get("fc", 0.0), cfg.get("thresq", 1e-12))
+    z = np.ascontiguousarray(zph, np.float64)
+    b = [np.ascontiguousarray(base[n], np.float32) for n in MOIST_BASE_NAMES]
+    st = list(past) + list(now)
+    assert len(st) == 28
+    for s in st:
+        assert s.dtype == np.float32 and s.flags.c_contiguous
+    assert prec.dtype == np.float32 and prec.flags.c_contiguous
+    rc = L.oracle_moist_steps(prec_bits, io, ro, z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                              (_FP * len(b))(*[_fp(x) for x in b]),
+                              (_FP * len(st))(*[_fp(x) for x in st]), _fp(prec), int(nsteps),
+                              float(dtbig), float(dtsml), int(bool(start)))
+    if rc < 0:
+        raise RuntimeError(f"oracle_moist_steps failed ({rc})")
+    return rc
+
+
 def _fp(a):
     assert a.dtype == np.float32 and a.flags.c_contiguous
     return a.ctypes.data_as(_FP)

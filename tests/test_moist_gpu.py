@@ -1,0 +1,113 @@
+"""GPU parity of whole moist large steps (cphopt=3) against the CPU oracle.
+
+A supercell-type state on a stretched grid (analytic sounding, curved
+hodograph, warm bubble) with a seeded field of cloud, rain, ice, snow and
+graupel is advanced a few leapfrog steps by cress_large_step and by the
+oracle's restatement of s_intgdrv; both time levels of all 14 prognostic
+fields and the surface precipitation must agree.
+
+Tolerance.  The GPU computes in FP32 with FMA contraction and the CUDA
+math library (expf/logf/powf within 2 ulp); the oracle uses glibc and no
+contraction.  The microphysics has thresholds and limiters, so a cell
+near a branch point may take the other branch, and the dynamics carries
+such differences a few cells per step.  Per field we require
+  * 99.9% of cells within 1e-4 * max|field| of the oracle, and
+  * every cell within 1e-2 * max|field|,
+and the accumulated precipitation within 1e-3 of its maximum.  (Measured
+on a B200: every cell of every field within 2e-5 of its maximum.)
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["u", "v", "w", "pp", "ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
+STAG = {"u": "u", "v": "v"}
+# absolute floors (kg/kg for mixing ratios, /kg for numbers) under which a
+# difference is not significant, for fields that may be absent in a case
+FLOOR = {n: 1e-10 for n in NAMES[5:11]}
+FLOOR.update({n: 1e-3 for n in NAMES[11:]})
+
+
+def region(name, ni, nj, nk):
+    m = np.zeros((nk, nj + 2, ni + 2), bool)
+    st = STAG.get(name, "s")
+    i1 = ni - 1 if st == "u" else ni - 2
+    j1 = nj - 1 if st == "v" else nj - 2
+    k1 = nk if name == "w" else nk - 1
+    m[0:k1, 2:j1 + 1, 2:i1 + 1] = True
+    return m
+
+
+def run_case(cress, oracle_lib, nx, ny, nz, nsteps, seed=3, cloud=True, dtbig=5.0, dtsml=1.0):
+    from cress_b200 import cases
+    dx = 1000.0
+    case = cases.supercell_case(nx, ny, nz, dx, ztop=8000.0, seed=seed, cloud=cloud,
+                                rad=(6000.0, 6000.0, 1400.0))
+    ni, nj, nk = case["dims"]
+    dz, zph = case["dz"], case["zph"]
+    vspbar, botbar = 0.005, 0.6 * zph[nk - 1]
+    rbct, ksp0 = oracle_lib.vspdmp(nk, zph, vspbar, botbar)
+    cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=1, smtopt=3, vspopt=2, coropt=0,
+               vspbar=vspbar, botbar=botbar, thresq=1e-12)
+    init = list(case["level"]) + [case["moist"][n] for n in NAMES[5:]]
+    past = [a.copy() for a in init]
+    now = [a.copy() for a in init]
+    prec_ref = np.zeros((5, 2, nj + 2, ni + 2), np.float32)
+    oracle_lib.moist_steps(cfg, case["base"], zph, past, now, prec_ref, nsteps, dtbig, dtsml, start=True)
+
+    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, cphopt=3, thresq=1e-12)
+    s.set_base3d(case["base"])
+    s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
+    s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
+    for n, a in zip(NAMES, init):
+        s.put_field(n, cress.PAST, a)
+        s.put_field(n, cress.NOW, a)
+    nsstp = 20 * int(1.e2 * (dtbig + .001)) // int(1.e3 * (dtsml + .0001))
+    for step in range(nsteps):
+        first = step == 0
+        s.large_step(round(step * dtbig * 1000), 0.5 * dtbig if first else dtbig, nsstp,
+                     0.5 * dtsml if first else dtsml)
+    gp = [s.get_field(n, cress.PAST) for n in NAMES]
+    gn = [s.get_field(n, cress.NOW) for n in NAMES]
+    prec = s.get_precip()
+    s.close()
+    return (ni, nj, nk), (past, now, prec_ref), (gp, gn, prec)
+
+
+def errors(dims, ref, got):
+    """Per (level, field): (fraction within 1e-4 of scale, max err over the
+    scale; the floor of FLOOR added to both)."""
+    ni, nj, nk = dims
+    out = {}
+    for lvl in range(2):
+        for name, r, g in zip(NAMES, ref[lvl], got[lvl]):
+            m = region(name, ni, nj, nk)
+            floor = FLOOR.get(name, 0.0)
+            scale = float(np.abs(r[m]).max()) + 1e-30
+            err = np.maximum(np.abs(g[m] - r[m]) - floor, 0.0)
+            assert np.isfinite(g[m]).all(), (lvl, name)
+            out[(lvl, name)] = (float((err <= 1e-4 * scale).mean()), float(err.max()) / (scale + floor))
+    return out
+
+
+def check(dims, ref, got):
+    for (lvl, name), (frac, emax) in errors(dims, ref, got).items():
+        assert frac >= 0.999, f"level {lvl} {name}: only {frac:.4f} within 1e-4 (max rel {emax:.2e})"
+        assert emax <= 1e-2, f"level {lvl} {name}: max rel err {emax:.2e}"
+    ni, nj, nk = dims
+    sl = (slice(None), 1, slice(2, nj - 1), slice(2, ni - 1))
+    pr, pg = ref[2][sl], got[2][sl]
+    assert np.isfinite(pg).all()
+    assert float(np.abs(pg - pr).max()) <= 1e-3 * float(np.abs(pr).max()) + 1e-9
+
+
+def test_moist_large_steps_cloudy(cress, oracle_lib):
+    dims, ref, got = run_case(cress, oracle_lib, 40, 32, 24, 3)
+    check(dims, ref, got)
+
+
+def test_moist_large_steps_clear_ragged(cress, oracle_lib):
+    # no initial hydrometeors: only the bubble, vapour and saturation adjustment
+    dims, ref, got = run_case(cress, oracle_lib, 37, 29, 20, 2, seed=8, cloud=False)
+    check(dims, ref, got)

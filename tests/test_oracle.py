@@ -80,3 +80,33 @@ def test_fp64_solve_close_to_fp32_solve(oracle_lib):
     oracle_lib.small_steps(cfg, base, frc, b, 2, 0.5, prec=32, fp64_solve=1)
     w32, w64 = a[2], b[2]
     assert np.abs(w32 - w64).max() <= 1e-5 * np.abs(w64).max()
+
+
+def test_moist_step_fp32_vs_fp64_and_water(oracle_lib):
+    """The moist large step (cphopt=3) runs in both precisions and the two
+    agree to a small fraction of each field's range."""
+    from cress_b200 import cases
+    case = cases.supercell_case(16, 14, 14, 1000.0, ztop=5000.0, seed=2, cloud=True,
+                                rad=(4000.0, 4000.0, 1200.0))
+    ni, nj, nk = case["dims"]
+    zph = case["zph"]
+    botbar = 0.6 * zph[nk - 1]
+    rbct, ksp0 = oracle_lib.vspdmp(nk, zph, 0.005, botbar)
+    cfg = dict(ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=case["dz"], sthopt=1, vspbar=0.005,
+               botbar=botbar)
+    init = list(case["level"]) + [case["moist"][n] for n in oracle_lib.MOIST_STATE_NAMES[5:]]
+    runs = []
+    for bits in (32, 64):
+        past = [a.copy() for a in init]
+        now = [a.copy() for a in init]
+        prec = np.zeros((5, 2, nj + 2, ni + 2), np.float32)
+        npstp = oracle_lib.moist_steps(cfg, case["base"], zph, past, now, prec, 2, 5.0, 1.0,
+                                       prec_bits=bits)
+        assert npstp >= 1
+        runs.append((now, prec))
+    sl = (slice(0, nk - 1), slice(2, nj - 1), slice(2, ni - 1))
+    for name, a, b in zip(oracle_lib.MOIST_STATE_NAMES, runs[0][0], runs[1][0]):
+        assert np.isfinite(a).all(), name
+        scale = float(np.abs(b[sl]).max()) + 1e-12
+        assert float(np.abs(a[sl] - b[sl]).max()) <= 2e-2 * scale, name
+    assert float(np.abs(runs[0][1] - runs[1][1]).max()) <= 2e-2 * float(np.abs(runs[1][1]).max()) + 1e-9
