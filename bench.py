@@ -1,17 +1,22 @@
 """Benchmark: CReSS solver time integration on B200.
 
-Workload (default): one leapfrog large step of the dry solver (s_intgdrv:
-forcing of u, v, w, p', theta'; 20 HE-VI acoustic substeps; theta' step;
-Asselin filter; periodic ghost planes) on a 512x512x64 grid with the
-moist-supercell geometry (dx = 1 km, stretched dz, 18 km top), a warm
-bubble in a sheared flow.  Metric: cell-updates/s (interior cells x large
-steps / s).
+Workload (default): the moist supercell, 512x512x64 (dx = 1 km, dz
+stretched from 100 m to 500 m up to 18 km), cold-rain bulk microphysics
+(cphopt=3: qv, qc, qr, qi, qs, qg, ni, ns, ng), dtbig = 5 s with 10 HE-VI
+acoustic substeps.  One step = one leapfrog large step of s_intgdrv:
+forcing (advection, 4th-order smoothing, Rayleigh sponge, moist buoyancy),
+10 HE-VI substeps, theta' and the nine moist scalars' steps, s_cloudphy
+(process rates + sedimentation), the Asselin filter, saturation adjustment
+on t and t+dt, periodic ghost planes.  The state starts from a seeded
+cloudy field so the microphysics is active in a large share of the cells.
+Metric: cell-updates/s (interior cells x large steps / s).
 
 Prints ONE JSON line (rank 0).  Timing: CUDA events on the library's stream
 (a dedicated torch stream that the library is told to use), barrier +
 synchronize around the timed region, max over ranks.  Multi-GPU runs are
 independent replicas (one domain per GPU, no data-path collective):
-"scaling": "weak".
+"scaling": "weak".  --impl reference times the CPU restatement (OpenMP) of
+the same step on the host cores.
 """
 import argparse
 import json
@@ -23,13 +28,15 @@ import time
 
 import numpy as np
 
-CTIME = 1000   # any non-zero model time (ms): a step after the first
-
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 HEVI_BYTES_PER_CELL = 48  # u,v,w,p' read + write and 4 forcings read, float32
 METRIC = "cell-updates/s on 1 B200: plain vs learned-microphysics form at stated error"
+MOIST = ["qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
+NAMES = ["u", "v", "w", "pp", "ptp"] + MOIST
+VSPBAR = 0.005
+CTIME = 1000   # any non-zero model time (ms): a step after the first
 
 
 def measured_peaks():
@@ -87,13 +94,11 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def make_case(args, seed):
+def make_case(nx, ny, nz, dx, seed):
     from cress_b200 import cases
-    case = cases.dry_case(args.nx, args.ny, args.nz, args.dx, args.dz, sthopt=1, seed=seed,
-                          vspbar=0.005, shear=20.0)
-    ni, nj, nk = case["dims"]
-    zph = case["zph"]
-    case["botbar"] = 0.6 * zph[nk - 1]
+    case = cases.supercell_case(nx, ny, nz, dx, seed=seed, cloud=True)
+    nk = case["dims"][2]
+    case["botbar"] = 0.6 * case["zph"][nk - 1]
     return case
 
 
@@ -120,25 +125,25 @@ def nsstp_of(dtbig, dtsml):
     return 20 * int(1.e2 * (dtbig + .001)) // int(1.e3 * (dtsml + .0001))
 
 
-def cpu_dry(args, threads, nx, ny, nsteps):
-    """Oracle (C++ restatement, OpenMP) on a bounded sample: nx x ny x nz."""
+def cpu_moist(args, threads, nx, ny, nsteps):
+    """Oracle (C++ restatement, OpenMP) on a bounded sample: nx x ny x nz,
+    nsteps moist large steps.  Returns (cell-updates/s, seconds)."""
     import oracle
     os.environ["OMP_NUM_THREADS"] = str(threads)
     oracle.build()
-    sub = argparse.Namespace(**vars(args))
-    sub.nx, sub.ny = nx, ny
-    case = make_case(sub, 3)
+    case = make_case(nx, ny, args.nz, args.dx, 3)
     ni, nj, nk = case["dims"]
-    cfg = dict(ni=ni, nj=nj, nk=nk, dx=args.dx, dy=args.dx, dz=args.dz, sthopt=1, smtopt=3,
-               vspopt=2, coropt=0, vspbar=0.005, botbar=case["botbar"])
-    past = [a.copy() for a in case["level"]]
-    now = [a.copy() for a in case["level"]]
+    cfg = dict(ni=ni, nj=nj, nk=nk, dx=args.dx, dy=args.dx, dz=case["dz"], sthopt=1, smtopt=3,
+               vspopt=2, coropt=0, vspbar=VSPBAR, botbar=case["botbar"])
+    init = list(case["level"]) + [case["moist"][n] for n in MOIST]
+    past = [a.copy() for a in init]
+    now = [a.copy() for a in init]
+    prec = np.zeros((5, 2, nj + 2, ni + 2), np.float32)
     t0 = time.perf_counter()
-    oracle.dry_steps(cfg, case["base"], case["zph"], past, now, nsteps, args.dtbig, args.dtsml,
-                     start=False, omp=True)
+    oracle.moist_steps(cfg, case["base"], case["zph"], past, now, prec, nsteps, args.dtbig,
+                       args.dtsml, start=False, omp=True)
     dt = time.perf_counter() - t0
-    cells = nx * ny * args.nz * nsteps
-    return cells / dt, dt
+    return nx * ny * args.nz * nsteps / dt, dt
 
 
 def main():
@@ -151,12 +156,12 @@ def main():
     ap.add_argument("--ny", type=int, default=512)
     ap.add_argument("--nz", type=int, default=64)
     ap.add_argument("--dx", type=float, default=1000.0)
-    ap.add_argument("--dz", type=float, default=281.25)
     ap.add_argument("--dtbig", type=float, default=5.0)
-    ap.add_argument("--dtsml", type=float, default=0.5)
+    ap.add_argument("--dtsml", type=float, default=1.0)
     ap.add_argument("--tile", type=int, default=0)
-    ap.add_argument("--cpu-nx", type=int, default=128)
-    ap.add_argument("--cpu-ny", type=int, default=128)
+    ap.add_argument("--cpu-nx", type=int, default=256)
+    ap.add_argument("--cpu-ny", type=int, default=256)
+    ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
@@ -165,12 +170,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     nsstp = nsstp_of(args.dtbig, args.dtsml)
-    cfg_json = {"workload": f"dry large step (forcing + {nsstp} HE-VI substeps + theta' step + "
-                            f"Asselin filter + periodic halos), {args.nx}x{args.ny}x{args.nz}, "
-                            f"dx={args.dx:g} m, stretched dz, dtbig={args.dtbig:g} s, "
-                            f"dtsml={args.dtsml:g} s; warm bubble in 5-25 m/s shear",
+    cfg_json = {"workload": f"moist supercell large step (cold-rain bulk cphopt=3; forcing + "
+                            f"{nsstp} HE-VI substeps + 10 scalar steps + cloud physics + Asselin "
+                            f"filter + saturation adjustment + periodic halos), "
+                            f"{args.nx}x{args.ny}x{args.nz}, dx={args.dx:g} m, dz 100->500 m to "
+                            f"18 km, dtbig={args.dtbig:g} s, dtsml={args.dtsml:g} s; analytic "
+                            f"sounding, quarter-circle hodograph, +3 K bubble, seeded cloud field",
                 "nx": args.nx, "ny": args.ny, "nz": args.nz, "nsstp": nsstp,
-                "l2": "inputs larger than L2 (each field 72 MB)",
+                "microphysics": "plain (cold-rain bulk)",
+                "l2": "inputs larger than L2 (each field 72 MB at 512x512x64)",
                 "parallelism": f"replicas{world}"}
     cells = args.nx * args.ny * args.nz
 
@@ -179,13 +187,13 @@ def main():
             return
         threads = os.cpu_count() or 1
         vals = []
-        for n in range(args.warmup + args.steps):
-            v, dt = cpu_dry(args, threads, args.cpu_nx, args.cpu_ny, 1)
+        for _ in range(args.warmup + args.steps):
+            v, _dt = cpu_moist(args, threads, args.cpu_nx, args.cpu_ny, 1)
             vals.append(v)
         v = float(np.median(vals[args.warmup:]))
         cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} domain, one dry large step of "
-                         f"the C++ oracle (OpenMP, {threads} threads) per timed step"}
+               "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} supercell domain, one moist large "
+                         f"step of the C++ oracle (OpenMP, {threads} threads) per timed step"}
         print(json.dumps({"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": 0,
                           "steps": args.steps, "warmup": args.warmup, "impl": "reference",
                           "higher_is_better": True, "dtype": "f32", "data": "synthetic",
@@ -203,18 +211,19 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    case = make_case(args, 100 + rank)
+    case = make_case(args.nx, args.ny, args.nz, args.dx, 100 + rank)
     ni, nj, nk = case["dims"]
-    rbct, ksp0 = vspdmp_columns(nk, case["zph"], 0.005, case["botbar"])
-    s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, args.dz, sthopt=1, tile=args.tile,
-                          device=local)
+    rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, case["botbar"])
+    s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, case["dz"], sthopt=1, tile=args.tile,
+                          device=local, cphopt=3)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     s.set_stream(stream.cuda_stream)
     s.set_base3d(case["base"])
     s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
-    names = ["u", "v", "w", "pp", "ptp"]
-    for n, a in zip(names, case["level"]):
+    s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
+    init = list(case["level"]) + [case["moist"][n] for n in MOIST]
+    for n, a in zip(NAMES, init):
         s.put_field(n, cress_b200.PAST, a)
         s.put_field(n, cress_b200.NOW, a)
     s.sync()
@@ -232,7 +241,7 @@ def main():
         return float(t.item())
 
     s.large_step(0, 0.5 * args.dtbig, nsstp, 0.5 * args.dtsml)   # the first (half) step, ctime=0
-    for _ in range(args.warmup):
+    for _ in range(args.warmup - 1):
         s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
     barrier()
     l0 = s.launch_count()
@@ -262,20 +271,20 @@ def main():
     achieved = HEVI_BYTES_PER_CELL * cells / (hevi_ms * 1e-3) / 1e9
 
     # End to end through the public API with host buffers: every step the
-    # past and present levels (10 fields) go host->device from pinned
-    # memory, one large step runs, the new present level (5 fields) comes
+    # past and present levels (14 fields each) go host->device from pinned
+    # memory, one large step runs, the new present level (14 fields) comes
     # back.
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    past_h = [pin(a) for a in case["level"]]
-    now_h = [pin(a) for a in case["level"]]
-    out_h = [pin(np.empty_like(a)) for a in case["level"]]
+    past_h = [pin(a) for a in init]
+    now_h = [pin(a) for a in init]
+    out_h = [pin(np.empty_like(a)) for a in init]
 
     def e2e_step():
-        for n, a, b in zip(names, past_h, now_h):
+        for n, a, b in zip(NAMES, past_h, now_h):
             s.put_field(n, cress_b200.PAST, a)
             s.put_field(n, cress_b200.NOW, b)
         s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
-        for n, o in zip(names, out_h):
+        for n, o in zip(NAMES, out_h):
             s.get_field(n, cress_b200.NOW, out=o)
 
     for _ in range(args.warmup):
@@ -294,10 +303,11 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, dt = cpu_dry(args, threads, args.cpu_nx, args.cpu_ny, 1)
+        v, dt = cpu_moist(args, threads, args.cpu_nx, args.cpu_ny, args.cpu_steps)
         cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} domain, one dry large step of the "
-                         f"C++ oracle (OpenMP, {threads} threads), {dt:.2f} s"}
+               "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} supercell domain, {args.cpu_steps} "
+                         f"moist large steps of the C++ oracle (OpenMP, {threads} threads), "
+                         f"{dt:.2f} s"}
 
     if rank == 0:
         print(json.dumps({
