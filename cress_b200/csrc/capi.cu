@@ -15,6 +15,7 @@
 #include "hevi.cuh"
 #include "forcing.cuh"
 #include "micro.cuh"
+#include "mlp_impl.cuh"
 
 namespace cress {
 
@@ -46,8 +47,16 @@ float* Ctx::alloc_field() {
   return p;
 }
 
+void Ctx::free_learned() {
+  for (void* p : lb_owned) cudaFree(p);
+  lb_owned.clear();
+  lb = LearnedBuffers{};
+  mlp = nullptr;
+}
+
 Ctx::~Ctx() {
   cudaSetDevice(device);
+  free_learned();
   for (void* p : owned) cudaFree(p);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
@@ -370,7 +379,30 @@ int Ctx::cloudphy(float dtb, float thresq) {
   m.dtb = 2.f * dtb;        // cloudphy.f90:282
   m.dz = cfg.dz;
   m.thresq = thresq;
-  int rc = launch_cloudphy(m, stream);
+  int rc;
+  if (sampler) {
+    // tuples of the plain scheme on this step's state (before it changes)
+    const long long room = sampler->tcap - sampler->ntup;
+    if (room > 0) {
+      cudaMemsetAsync(count_d, 0, sizeof(unsigned long long), stream);
+      if ((rc = launch_collect_tuples(m, lev[CRESS_W][CRESS_NOW], sampler, sample_stride, sample_keep_zero,
+                                      sample_seed++, count_d, stream)))
+        return set_error(rc, "tuple sampling launch failed");
+      ++launches;
+      unsigned long long got = 0;
+      cudaMemcpyAsync(&got, count_d, sizeof(got), cudaMemcpyDeviceToHost, stream);
+      if ((rc = cuda_check(cudaStreamSynchronize(stream), "tuple sampling"))) return rc;
+      const long long add = (long long)got < room ? (long long)got : room;
+      sampler->ntup += add;
+      sampled += add;
+    }
+  }
+  if (mlp) {
+    rc = launch_cloudphy_learned(m, lev[CRESS_W][CRESS_NOW], mlp, lb, resid_tol, stream, &launches);
+    if (rc) return set_error(rc, "learned cloudphy failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return CRESS_OK;
+  }
+  rc = launch_cloudphy(m, stream);
   launches += 3;
   if (rc) return set_error(rc, "cloudphy launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   return CRESS_OK;
@@ -724,6 +756,92 @@ int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, floa
 long long cress_launch_count(const cress_ctx* ctx) {
   const Ctx* c = reinterpret_cast<const Ctx*>(ctx);
   return c ? c->launches : -1;
+}
+
+// Learned microphysics: MLP in place of the process rates of s_coldblk.
+int cress_set_learned_micro(cress_ctx* ctx, cress_mlp* mh, int chunk, float resid_tol) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->free_learned();
+  if (!mh) return CRESS_OK;
+  Mlp* m = reinterpret_cast<Mlp*>(mh);
+  if (c->cfg.cphopt != 3) return set_error(CRESS_E_STATE, "cress_set_learned_micro: context is not cphopt=3");
+  if (m->device != c->device) return set_error(CRESS_E_ARG, "MLP and context live on different devices");
+  if (chunk <= 0) chunk = 1 << 20;
+  chunk = (chunk + 127) / 128 * 128;
+  if (!(resid_tol > 0.f)) return set_error(CRESS_E_ARG, "resid_tol must be positive");
+  auto al = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    c->lb_owned.push_back(p);
+    return p;
+  };
+  LearnedBuffers& L = c->lb;
+  L.chunk = chunk;
+  L.xb = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpK1));
+  L.h0 = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpH));
+  L.h1 = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpH));
+  L.y = static_cast<float*>(al(sizeof(float) * (size_t)chunk * kMlpN4));
+  L.env = static_cast<unsigned char*>(al((size_t)chunk));
+  L.fb_list = static_cast<int*>(al(sizeof(int) * (size_t)chunk));
+  L.fb_count = static_cast<int*>(al(sizeof(int)));
+  L.stats = static_cast<unsigned long long*>(al(2 * sizeof(unsigned long long)));
+  L.err = static_cast<int*>(al(sizeof(int)));
+  if (!L.xb || !L.h0 || !L.h1 || !L.y || !L.env || !L.fb_list || !L.fb_count || !L.stats || !L.err) {
+    c->free_learned();
+    return set_error(CRESS_E_CUDA, "cudaMalloc of the learned-microphysics buffers failed");
+  }
+  cudaMemsetAsync(L.stats, 0, 2 * sizeof(unsigned long long), c->stream);
+  cudaMemsetAsync(L.err, 0, sizeof(int), c->stream);
+  c->mlp = m;
+  c->resid_tol = resid_tol;
+  return cuda_check(cudaStreamSynchronize(c->stream), "learned setup");
+}
+
+// Cells the MLP handled and cells sent to the plain scheme since the
+// learned form was enabled; a bounded-wait failure inside the GEMMs is
+// reported here as CRESS_E_TIMEOUT.
+int cress_learned_stats(cress_ctx* ctx, long long* mlp_cells, long long* fallback_cells) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !mlp_cells || !fallback_cells) return set_error(CRESS_E_ARG, "null argument");
+  if (!c->mlp) return set_error(CRESS_E_STATE, "learned microphysics is not enabled");
+  cudaSetDevice(c->device);
+  unsigned long long s[2] = {0, 0};
+  int e = 0;
+  cudaMemcpyAsync(s, c->lb.stats, sizeof(s), cudaMemcpyDeviceToHost, c->stream);
+  cudaMemcpyAsync(&e, c->lb.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  int rc = cuda_check(cudaStreamSynchronize(c->stream), "stats");
+  if (rc) return rc;
+  *mlp_cells = (long long)s[0];
+  *fallback_cells = (long long)s[1];
+  return e ? set_error(e, "a tensor-core GEMM of the learned form gave up waiting") : CRESS_OK;
+}
+
+// Sample (features, plain tendencies) tuples into the MLP's store on every
+// following s_cloudphy, 1 cell in `stride` (cells without any tendency 1 in
+// stride/keep_zero); NULL stops sampling.
+int cress_set_tuple_sampling(cress_ctx* ctx, cress_mlp* mh, int stride, float keep_zero, unsigned long long seed) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  c->sampler = nullptr;
+  if (!mh) return CRESS_OK;
+  Mlp* m = reinterpret_cast<Mlp*>(mh);
+  if (c->cfg.cphopt != 3) return set_error(CRESS_E_STATE, "cress_set_tuple_sampling: context is not cphopt=3");
+  if (m->device != c->device) return set_error(CRESS_E_ARG, "MLP and context live on different devices");
+  if (stride < 1 || keep_zero < 0.f || keep_zero > 1.f) return set_error(CRESS_E_ARG, "bad stride / keep_zero");
+  cudaSetDevice(c->device);
+  if (!c->count_d) {
+    if (cudaMalloc(&c->count_d, sizeof(unsigned long long)) != cudaSuccess)
+      return set_error(CRESS_E_CUDA, "cudaMalloc failed");
+    c->owned.push_back(c->count_d);
+  }
+  c->sampler = m;
+  c->sample_stride = stride;
+  c->sample_keep_zero = keep_zero;
+  c->sample_seed = seed;
+  return CRESS_OK;
 }
 
 }  // extern "C"

@@ -8,6 +8,7 @@
 #include <vector>
 #include "../../include/cress_b200.h"
 #include "common.cuh"
+#include "micro.cuh"
 
 namespace cress {
 
@@ -52,6 +53,19 @@ struct Ctx {
   float* prec_d = nullptr; // surface precipitation planes (10 x px*py)
   int* dtp_d = nullptr;    // sedimentation sub-step minimum (float bits)
   int cloudphy(float dtb, float thresq);
+  // learned microphysics (MLP in place of the process rates) and tuple
+  // sampling of the plain scheme for its training
+  Mlp* mlp = nullptr;
+  float resid_tol = 0.5f;
+  LearnedBuffers lb{};
+  std::vector<void*> lb_owned;
+  Mlp* sampler = nullptr;
+  int sample_stride = 64;
+  float sample_keep_zero = 0.1f;
+  unsigned long long sample_seed = 1;
+  unsigned long long* count_d = nullptr;
+  long long sampled = 0;
+  void free_learned();
   int satadjst(int level, float thresq);
   int tmap(const float* buf, int rows, CUtensorMap* out);
   int check_device_error();

@@ -19,6 +19,8 @@
 #include "hevi.cuh"
 #include "micro.cuh"
 #include "coldrain.cuh"
+#include "mlp.cuh"
+#include "mlp_impl.cuh"
 
 namespace cress {
 
@@ -263,6 +265,74 @@ int launch_satadjst(const SatArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);
   dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
   k_satadjst<<<gr, b, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+}  // namespace cress
+
+// Learned-form kernels (they use this file's Koenig tables and loaders).
+#include "micro_learned.cuh"
+
+namespace cress {
+
+int launch_collect_tuples(const MicroArgs& a, const float* w, Mlp* m, int stride, float keep_zero,
+                          unsigned long long seed, unsigned long long* count_d, cudaStream_t st) {
+  if (stride < 1) return CRESS_E_ARG;
+  k_micro_tuples<<<148 * 8, 128, 0, st>>>(a, w, m->tx, m->ty, count_d, m->tcap - m->ntup, stride, keep_zero,
+                                          seed);
+  return cudaGetLastError() == cudaSuccess ? CRESS_OK : CRESS_E_CUDA;
+}
+
+// s_cloudphy with the MLP in place of the process-rate part: chunks of
+// `L.chunk` interior cells go through features -> 4 tensor-core GEMMs ->
+// application; rejected cells run the plain process rates; then the plain
+// sedimentation.
+int launch_cloudphy_learned(const MicroArgs& a, const float* w, Mlp* m, const LearnedBuffers& L, float resid_tol,
+                            cudaStream_t st, long long* launches) {
+  if (a.g.nk > kMaxNkFall - 1) return CRESS_E_UNSUPPORTED;
+  k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
+  ++*launches;
+  const long long ncell = (long long)(a.g.ni - 3) * (a.g.nj - 3) * (a.g.nk - 1);
+  for (long long n0 = 0; n0 < ncell; n0 += L.chunk) {
+    const int cnt = (int)((ncell - n0) < L.chunk ? (ncell - n0) : L.chunk);
+    const int rows = (cnt + 127) / 128 * 128;
+    k_mlp_features<<<rows / 128, 128, 0, st>>>(a, w, n0, cnt, rows, m->norm_d, L.xb, L.env);
+    int rc;
+    const bf16* in = L.xb;
+    int kin = kMlpK1;
+    const bf16* wt[3] = {m->w.w1t, m->w.w2t, m->w.w3t};
+    const int boff[3] = {MlpLayout::B1, MlpLayout::B2, MlpLayout::B3};
+    bf16* outs[3] = {L.h0, L.h1, L.h0};
+    for (int l = 0; l < 3; ++l) {
+      GemmArgs g{};
+      g.M = rows; g.N = kMlpH; g.K = kin;
+      g.bias = m->params + boff[l];
+      g.act = 1;
+      g.out_bf = outs[l]; g.ldb = kMlpH;
+      g.err = L.err;
+      if ((rc = gemm_bf16(in, kin, wt[l], kin, g, st))) return rc;
+      in = outs[l];
+      kin = kMlpH;
+    }
+    GemmArgs g{};
+    g.M = rows; g.N = kMlpN4; g.K = kMlpH;
+    g.bias = m->params + MlpLayout::B4;
+    g.out_f32 = L.y; g.ldf = kMlpN4;
+    g.err = L.err;
+    if ((rc = gemm_bf16(in, kMlpH, m->w.w4t, kMlpH, g, st))) return rc;
+    cudaMemsetAsync(L.fb_count, 0, sizeof(int), st);
+    ApplyArgs p{};
+    p.y = L.y; p.env = L.env; p.norm = m->norm_d; p.n0 = n0; p.cnt = cnt; p.resid_tol = resid_tol;
+    p.fb_list = L.fb_list; p.fb_count = L.fb_count; p.fb_cap = L.chunk; p.stats = L.stats;
+    k_mlp_apply<<<(cnt + 127) / 128, 128, 0, st>>>(a, p);
+    k_micro_src_list<<<148 * 4, 128, 0, st>>>(a, n0, L.fb_list, L.fb_count, L.chunk);
+    *launches += 7;
+    if (cudaGetLastError() != cudaSuccess) return CRESS_E_CUDA;
+  }
+  dim3 b2(32, 4, 1);
+  dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 1);
+  k_micro_fall<<<gr2, b2, 0, st>>>(a);
+  ++*launches;
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 

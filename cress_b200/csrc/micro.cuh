@@ -1,5 +1,6 @@
 // Cold-rain microphysics kernels (internal interface).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "hevi.cuh"
@@ -48,5 +49,24 @@ struct MoistPostArgs {
   int filter;
 };
 int launch_moist_post(const MoistPostArgs& a, cudaStream_t st);
+
+// Learned form of the process-rate part (the MLP of mlp.cu).
+struct Mlp;
+struct LearnedBuffers {
+  int chunk = 0;                  // cells per inference chunk (multiple of 128)
+  __nv_bfloat16* xb = nullptr;    // [chunk][64] standardized inputs
+  __nv_bfloat16* h0 = nullptr;    // [chunk][256] activations (ping)
+  __nv_bfloat16* h1 = nullptr;    // [chunk][256] activations (pong)
+  float* y = nullptr;             // [chunk][64] outputs
+  unsigned char* env = nullptr;   // [chunk] inside the training envelope
+  int* fb_list = nullptr;         // [chunk] cells sent to the plain scheme
+  int* fb_count = nullptr;
+  unsigned long long* stats = nullptr;   // MLP cells, fallback cells
+  int* err = nullptr;
+};
+int launch_cloudphy_learned(const MicroArgs& a, const float* w, Mlp* m, const LearnedBuffers& L, float resid_tol,
+                            cudaStream_t st, long long* launches);
+int launch_collect_tuples(const MicroArgs& a, const float* w, Mlp* m, int stride, float keep_zero,
+                          unsigned long long seed, unsigned long long* count_d, cudaStream_t st);
 
 }  // namespace cress

@@ -1,0 +1,110 @@
+// 5th-generation tensor core (tcgen05) helpers for sm_100a: tensor-memory
+// allocation, BF16 x BF16 -> FP32 MMAs from shared-memory descriptors,
+// commits to mbarriers and tensor-memory loads for the epilogue.
+//
+// Shared-memory operands use the K-major, 128-byte-swizzle layout that a
+// TMA load with CU_TENSOR_MAP_SWIZZLE_128B produces: rows of 64 bf16 (128
+// bytes), 8-row groups 1024 bytes apart, the 16-byte chunk c of row r
+// stored at chunk position c ^ (r & 7).  Tiles start on 1024-byte
+// boundaries.
+#pragma once
+#include <cuda_bf16.h>
+#include <cstdint>
+#include "tma.cuh"
+
+namespace cress {
+
+// One warp allocates `ncols` (power of two, >= 32) tensor-memory columns;
+// the base address lands in *slot.
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// D[tmem] = A * B^T (+ D when accumulate != 0); A is M x 16 and B is N x 16
+// (one K step of 16 bf16), both K-major in shared memory.
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Arrive once on `bar` when every MMA this thread issued so far completes.
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+// Thread t of a warp reads tensor-memory lane (lane base + t), 32
+// consecutive 32-bit columns from `taddr` (lane base in bits 31..16).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+        "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+        "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor of a K-major, 128-byte-swizzled tile
+// starting at shared address `saddr` (1024-byte aligned, or advanced by a
+// multiple of 32 bytes inside the first row to select a K step): start
+// address >> 4 in bits 0..13, leading byte offset 1 (unused by swizzled
+// K-major layouts), stride byte offset 1024 >> 4 (8-row groups), layout
+// version 1, swizzle mode 2 (128 B) in bits 61..63.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;
+  return d;
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator (bits 4..5 = 1),
+// A and B BF16 (bits 7..9, 10..12 = 1), both K-major, N >> 3 in bits
+// 17..22, M >> 4 in bits 24..28.
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// 2-D tiled TMA load (inner coordinate x in elements; x * element size is
+// a multiple of 16 bytes by construction of the callers).
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Byte offset of element (row r, column c) of a K-major SW128 tile of
+// 64-column rows: the swizzle XORs the 16-byte chunk index with r & 7.
+__device__ __forceinline__ uint32_t sw128_offset(int r, int c) {
+  const int chunk = (c >> 3) ^ (r & 7);
+  return (uint32_t)(r * 128 + chunk * 16 + (c & 7) * 2);
+}
+
+}  // namespace cress

@@ -176,6 +176,64 @@ int cress_put_precip(cress_ctx* ctx, const float* host);
  * created (instrumentation for benchmarks). */
 long long cress_launch_count(const cress_ctx* ctx);
 
+/* ------------------------------------------------------------------------
+ * Learned cold-rain microphysics.  No counterpart in the reference: a
+ * per-cell MLP (16 inputs, 3 hidden layers of 256 with SiLU, 9 outputs;
+ * BF16 weights and activations, FP32 accumulation on the tensor cores)
+ * that replaces the process-rate part of s_coldblk (adjstni, srcblk,
+ * adjstni: SrcOrig/coldblk.f90:327-425).  It is trained by the library's
+ * own forward, backward and Adam kernels on tuples that the plain scheme
+ * produces on the device; in use, positivity and water conservation are
+ * enforced after inference, and cells outside the training envelope or
+ * failing the water-budget residual check run the plain scheme.
+ *
+ * Inputs (per cell, before standardization): T-273.16, ln p, rho, w,
+ * log10 of qv, qc, qr, qi, qs, qg (floor 1e-12), log10 of ni, ns, ng
+ * (floor 1), supersaturation over water and over ice (clipped to [-1,1]),
+ * log10 of the future level's total condensate.  Outputs: for the changes
+ * d of qv, qc, qr, qi, qs, qg, ni, ns, ng over 2*dtb, y = sign(d) *
+ * log10(1 + |d|/s) with s = 1e-9 (mixing ratios) or 1 (numbers).
+ * Normalisation block (cress_mlp_get_norm, 82 floats): input means (16),
+ * input scales (16), output means (9), output scales (9), input minimum
+ * (16) and maximum (16) of the training set (the envelope).
+ * Parameters (cress_mlp_param_count floats): W1 [256][64] (inputs padded
+ * to 64), b1 [256], W2 [256][256], b2, W3 [256][256], b3 (W_l stored
+ * [out][in]), W4 [256][64] ([in][out], outputs padded to 64), b4 [64].
+ * ---------------------------------------------------------------------- */
+typedef struct cress_mlp cress_mlp;
+
+int cress_mlp_param_count(void);
+int cress_mlp_create(int device, unsigned long long seed, cress_mlp** out);
+void cress_mlp_destroy(cress_mlp* m);
+int cress_mlp_get_params(cress_mlp* m, float* host);
+int cress_mlp_set_params(cress_mlp* m, const float* host);
+int cress_mlp_get_norm(cress_mlp* m, float* host);
+int cress_mlp_set_norm(cress_mlp* m, const float* host);
+/* Network function: x [n][16] standardized inputs -> y [n][9]. */
+int cress_mlp_forward(cress_mlp* m, int n, const float* x, float* y);
+/* Mean-square loss and its gradient w.r.t. every parameter for one batch
+ * (x [n][16], t [n][9] standardized; n a multiple of 128). */
+int cress_mlp_loss_grad(cress_mlp* m, int n, const float* x, const float* t, float* loss, float* grad);
+/* Tuple store (transformed, unstandardized features and targets). */
+int cress_mlp_reserve(cress_mlp* m, long long cap);
+int cress_mlp_add_tuples(cress_mlp* m, long long n, const float* x, const float* t);
+int cress_mlp_get_tuples(cress_mlp* m, long long first, long long n, float* x, float* t);
+long long cress_mlp_tuple_count(const cress_mlp* m);
+/* Normalisation and envelope from the stored tuples. */
+int cress_mlp_fit_norm(cress_mlp* m);
+/* `steps` Adam steps on random batches (batch % 128 == 0) of the store;
+ * losses (may be NULL) receives each step's loss. */
+int cress_mlp_train(cress_mlp* m, int steps, int batch, float lr, unsigned long long seed, float* losses);
+/* Use the MLP for the process rates in the context's s_cloudphy (NULL
+ * returns to the plain scheme).  chunk: cells per inference batch (0 =
+ * 2^20); resid_tol: relative tolerance of the water-budget residual. */
+int cress_set_learned_micro(cress_ctx* ctx, cress_mlp* m, int chunk, float resid_tol);
+int cress_learned_stats(cress_ctx* ctx, long long* mlp_cells, long long* fallback_cells);
+/* Sample training tuples of the plain scheme on every following
+ * s_cloudphy into the MLP's store (up to its reserved capacity): 1 cell
+ * in `stride`, cells with no tendency 1 in stride/keep_zero; NULL stops. */
+int cress_set_tuple_sampling(cress_ctx* ctx, cress_mlp* m, int stride, float keep_zero, unsigned long long seed);
+
 /* One HE-VI acoustic substep that allocates no device memory.  No
  * counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc from inside their time loop, such as a host model that keeps
