@@ -88,6 +88,25 @@ def lib():
     L.cress_satadjst.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]
     L.cress_get_precip.argtypes = [ctypes.c_void_p, _FP]
     L.cress_put_precip.argtypes = [ctypes.c_void_p, _FP]
+    vp, i, ll, ull, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_float
+    L.cress_mlp_param_count.restype = i
+    L.cress_mlp_create.argtypes = [i, ull, ctypes.POINTER(vp)]
+    L.cress_mlp_destroy.argtypes = [vp]
+    L.cress_mlp_destroy.restype = None
+    for name in ("cress_mlp_get_params", "cress_mlp_set_params", "cress_mlp_get_norm", "cress_mlp_set_norm"):
+        getattr(L, name).argtypes = [vp, _FP]
+    L.cress_mlp_forward.argtypes = [vp, i, _FP, _FP]
+    L.cress_mlp_loss_grad.argtypes = [vp, i, _FP, _FP, _FP, _FP]
+    L.cress_mlp_reserve.argtypes = [vp, ll]
+    L.cress_mlp_add_tuples.argtypes = [vp, ll, _FP, _FP]
+    L.cress_mlp_get_tuples.argtypes = [vp, ll, ll, _FP, _FP]
+    L.cress_mlp_tuple_count.argtypes = [vp]
+    L.cress_mlp_tuple_count.restype = ll
+    L.cress_mlp_fit_norm.argtypes = [vp]
+    L.cress_mlp_train.argtypes = [vp, i, i, f, ull, _FP]
+    L.cress_set_learned_micro.argtypes = [vp, vp, i, f]
+    L.cress_learned_stats.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
+    L.cress_set_tuple_sampling.argtypes = [vp, vp, i, f, ull]
     _lib = L
     return L
 
@@ -197,6 +216,22 @@ class Solver:
     def satadjst(self, level, thresq=1e-12):
         _check(lib().cress_satadjst(self._h, int(level), float(thresq)))
 
+    def set_learned_micro(self, mlp, chunk=0, resid_tol=0.5):
+        """Use `mlp` (an Mlp) for the process rates of s_cloudphy; None
+        returns to the plain scheme."""
+        _check(lib().cress_set_learned_micro(self._h, mlp._h if mlp else None, int(chunk), float(resid_tol)))
+        self._mlp = mlp
+
+    def learned_stats(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().cress_learned_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def set_tuple_sampling(self, mlp, stride=64, keep_zero=0.1, seed=1):
+        _check(lib().cress_set_tuple_sampling(self._h, mlp._h if mlp else None, int(stride),
+                                              float(keep_zero), int(seed)))
+        self._sampler = mlp
+
     def get_precip(self):
         ni, nj = self.shape[2] - 2, self.shape[1] - 2
         a = np.empty((5, 2, nj + 2, ni + 2), np.float32)
@@ -206,3 +241,88 @@ class Solver:
     def put_precip(self, a):
         a = np.ascontiguousarray(a, dtype=np.float32)
         _check(lib().cress_put_precip(self._h, fptr(a)))
+
+
+class Mlp:
+    """The learned-microphysics network on one device (see the cress_mlp_*
+    section of include/cress_b200.h for inputs, outputs and layouts)."""
+
+    NORM = 82
+    N_IN, N_OUT = 16, 9
+
+    def __init__(self, device=0, seed=1):
+        h = ctypes.c_void_p()
+        _check(lib().cress_mlp_create(int(device), int(seed), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cress_mlp_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @staticmethod
+    def param_count():
+        return lib().cress_mlp_param_count()
+
+    def get_params(self):
+        a = np.empty(self.param_count(), np.float32)
+        _check(lib().cress_mlp_get_params(self._h, fptr(a)))
+        return a
+
+    def set_params(self, a):
+        a = np.ascontiguousarray(a, np.float32)
+        assert a.size == self.param_count()
+        _check(lib().cress_mlp_set_params(self._h, fptr(a)))
+
+    def get_norm(self):
+        a = np.empty(self.NORM, np.float32)
+        _check(lib().cress_mlp_get_norm(self._h, fptr(a)))
+        return a
+
+    def set_norm(self, a):
+        a = np.ascontiguousarray(a, np.float32)
+        assert a.size == self.NORM
+        _check(lib().cress_mlp_set_norm(self._h, fptr(a)))
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.empty((x.shape[0], self.N_OUT), np.float32)
+        _check(lib().cress_mlp_forward(self._h, int(x.shape[0]), fptr(x), fptr(y)))
+        return y
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = np.zeros(1, np.float32)
+        g = np.empty(self.param_count(), np.float32)
+        _check(lib().cress_mlp_loss_grad(self._h, int(x.shape[0]), fptr(x), fptr(t), fptr(loss), fptr(g)))
+        return float(loss[0]), g
+
+    def reserve(self, cap):
+        _check(lib().cress_mlp_reserve(self._h, int(cap)))
+
+    def add_tuples(self, x, t):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        _check(lib().cress_mlp_add_tuples(self._h, int(x.shape[0]), fptr(x), fptr(t)))
+
+    def get_tuples(self, first=0, n=None):
+        if n is None:
+            n = self.tuple_count() - first
+        x = np.empty((n, self.N_IN), np.float32)
+        t = np.empty((n, self.N_OUT), np.float32)
+        _check(lib().cress_mlp_get_tuples(self._h, int(first), int(n), fptr(x), fptr(t)))
+        return x, t
+
+    def tuple_count(self):
+        return lib().cress_mlp_tuple_count(self._h)
+
+    def fit_norm(self):
+        _check(lib().cress_mlp_fit_norm(self._h))
+
+    def train(self, steps, batch=8192, lr=1e-3, seed=1):
+        losses = np.empty(max(int(steps), 1), np.float32)
+        _check(lib().cress_mlp_train(self._h, int(steps), int(batch), float(lr), int(seed), fptr(losses)))
+        return losses[:steps]

@@ -375,6 +375,7 @@ int Ctx::cloudphy(float dtb, float thresq) {
   m.qif = lev[CRESS_QI][F]; m.qsf = lev[CRESS_QS][F]; m.qgf = lev[CRESS_QG][F]; m.nif = lev[CRESS_NI][F];
   m.nsf = lev[CRESS_NS][F]; m.ngf = lev[CRESS_NG][F];
   m.prec = prec_d;
+  m.uspd = uspd_d;
   m.dtp_bits = dtp_d;
   m.dtb = 2.f * dtb;        // cloudphy.f90:282
   m.dz = cfg.dz;
@@ -505,6 +506,15 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
     c->owned.push_back(c->prec_d);
     c->owned.push_back(c->dtp_d);
     cudaMemsetAsync(c->prec_d, 0, pb, c->stream);
+    // fall speeds of the 8 sedimenting quantities (written by the process
+    // rates, read by the column sedimentation)
+    const size_t ub = sizeof(float) * 8 * (size_t)c->g.plane * c->g.nk;
+    if ((rc = cuda_check(cudaMalloc(&c->uspd_d, ub), "cudaMalloc fall speeds"))) {
+      delete c;
+      return rc;
+    }
+    c->owned.push_back(c->uspd_d);
+    cudaMemsetAsync(c->uspd_d, 0, ub, c->stream);
     if ((rc = micro_init_tables())) { delete c; return set_error(rc, "Koenig table upload failed"); }
   } else if (cfg->cphopt != 0) {
     delete c;

@@ -51,6 +51,7 @@ struct Ctx {
   bool large_set = false;  // cress_set_base_large was called
   bool moist_set = false;  // cress_set_base_moist was called
   float* prec_d = nullptr; // surface precipitation planes (10 x px*py)
+  float* uspd_d = nullptr; // fall speeds (8 fields)
   int* dtp_d = nullptr;    // sedimentation sub-step minimum (float bits)
   int cloudphy(float dtb, float thresq);
   // learned microphysics (MLP in place of the process rates) and tuple

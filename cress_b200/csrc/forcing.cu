@@ -249,8 +249,10 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
 }
 
 // Forcing and s_steps of the nine moist scalars, one thread per scalar
-// point (i, j = 2..n-2, k = 2..nk-2), all nine fields per thread so the
-// advecting fluxes rst8u*u, rst8v*v, rst8w*wc are formed once:
+// point (i, j = 2..n-2, k = 2..nk-2) and field (blockIdx.z runs over k
+// within a field, then over the fields), so the nine fields are in flight
+// at once; each thread forms its advecting fluxes rst8u*u, rst8v*v,
+// rst8w*wc (shared neighbours come from L1):
 //   sfrc = advs (advs.f90:205-370) + smoo4qv / smoo4s of rbr*(qvp-qvbr) or
 //          rbr*sp (smoo4s.f90:184-296) + vspqv / vsps / vsps0
 //          (vspqv.f90:181-198, vsps.f90:181-198, vsps0.f90:114-124)
@@ -261,8 +263,9 @@ __global__ void __launch_bounds__(256) k_moist_scalars(const MoistScalarArgs a) 
   const int ni = g.ni, nj = g.nj, nk = g.nk;
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = 2 + blockIdx.z;
-  if (i > ni - 2 || j > nj - 2 || k > nk - 2) return;
+  const int n = blockIdx.z / (nk - 3);
+  const int k = 2 + blockIdx.z % (nk - 3);
+  if (i > ni - 2 || j > nj - 2 || n >= kMoistN) return;
   const long long px = g.px, pl = g.plane;
   const long long id = g.at(i, j, k);
   const int nc = nk + 1;
@@ -282,8 +285,7 @@ __global__ void __launch_bounds__(256) k_moist_scalars(const MoistScalarArgs a) 
   const float rbct5 = .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1));
   const float rst = C(C_RST, k);
   const float dtdrst = a.dtb2 / rst;                                     // steps.f90:528
-#pragma unroll 1
-  for (int n = 0; n < kMoistN; ++n) {
+  {
     const float* s = a.s[n];
     const float s0 = ld(s, id);
     // advs.f90:205-370, 4th-order horizontal, 2nd-order vertical
@@ -388,7 +390,7 @@ int launch_force(const ForceArgs& a, cudaStream_t st) {
 
 int launch_moist_scalars(const MoistScalarArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 3);
+  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, (a.g.nk - 3) * kMoistN);
   k_moist_scalars<<<gr, b, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }

@@ -26,7 +26,6 @@ namespace cress {
 
 namespace {
 
-constexpr int kMaxNkFall = 160;   // column length the sedimentation kernel holds
 
 __device__ inline void load_cell(const MicroArgs& a, long long id, int k, MCell& c) {
   const int nc = a.g.nk + 1;
@@ -41,6 +40,16 @@ __device__ inline void load_cell(const MicroArgs& a, long long id, int k, MCell&
   c.qgp = __ldg(a.qgp + id); c.ncip = __ldg(a.nip + id); c.ncsp = __ldg(a.nsp + id);
   c.ncgp = __ldg(a.ngp + id);
   diagnw_cell(c.rbr, c.qrp, c.nccp, c.ncrp);                           // cloudphy.f90:366
+}
+
+// The fall speeds of the past level (termblk) in the order the
+// sedimentation kernel runs the species: cloud water, cloud ice, ice
+// number, rain, snow, graupel, snow number, graupel number.
+__device__ __forceinline__ void store_speeds(const MicroArgs& a, long long id, const MCell& c) {
+  const long long n3 = (long long)a.g.plane * a.g.nk;
+  float* u = a.uspd + id;
+  u[0] = c.ucq; u[n3] = c.uiq; u[2 * n3] = c.uin; u[3 * n3] = c.urq;
+  u[4 * n3] = c.usq; u[5 * n3] = c.ugq; u[6 * n3] = c.usn; u[7 * n3] = c.ugn;
 }
 
 __global__ void __launch_bounds__(256) k_micro_src(const MicroArgs a) {
@@ -59,6 +68,7 @@ __global__ void __launch_bounds__(256) k_micro_src(const MicroArgs a) {
     c.ncsf = a.nsf[id]; c.ncgf = a.ngf[id];
     adjstni_cell(c.rbr, c.rbv, c.qif, c.qsf, c.qgf, c.ncif, c.ncsf, c.ncgf);   // coldblk.f90:327
     termblk_cell(a.thresq, c);                                                // coldblk.f90:344
+    store_speeds(a, id, c);
     srcblk_cell(a.dtb, a.thresq, c);                                          // coldblk.f90:356
     adjstni_cell(c.rbr, c.rbv, c.qif, c.qsf, c.qgf, c.ncif, c.ncsf, c.ncgf);   // coldblk.f90:425
     a.ptpf[id] = c.ptpf; a.qvf[id] = c.qvf; a.qcf[id] = c.qcf; a.qrf[id] = c.qrf;
@@ -77,21 +87,12 @@ __global__ void __launch_bounds__(256) k_micro_src(const MicroArgs a) {
   if ((threadIdx.x & 31) == 0 && lim < 3.0e38f) atomicMin(a.dtp_bits, __float_as_int(lim));
 }
 
-// s_upwqp / s_upwnp on one column held in registers/local memory.
-__device__ inline void upw_column(int nk, float dziv, float dtp, const float* rbr, const float* rst,
-                                  const float* u, float* q, float* pr_rate, float* pr_acc) {
-  float flx[kMaxNkFall];
-  const float dzvdt = dziv * dtp;
-  for (int k = 1; k <= nk - 1; ++k) flx[k] = rbr[k] * u[k] * q[k];
-  for (int k = 1; k <= nk - 2; ++k) q[k] = fmaxf(q[k] + (flx[k + 1] - flx[k]) / rst[k] * dzvdt, 0.f);
-  q[nk - 1] = q[nk - 2];
-  if (pr_rate) {
-    const float rwiv05 = .5f / 1.e3f, dtp05 = .5f * dtp;
-    *pr_rate = (flx[1] + flx[2]) * rwiv05;
-    *pr_acc = *pr_acc + *pr_rate * dtp05;
-  }
-}
-
+// One thread per column.  For each species, npstp upwind sub-steps of
+// s_upwqp / s_upwnp (upwqp.f90:160-225, upwnp.f90:140-176) stream up the
+// column: the flux rbr*u*q of level k+1 is formed from the not yet updated
+// q(k+1) while q(k) is written, so a sub-step is one read and one write of
+// the column; the surface rate (flx(1)+flx(2))/2/rhow accumulates over
+// the sub-steps.
 __global__ void __launch_bounds__(128) k_micro_fall(const MicroArgs a) {
   const Grid g = a.g;
   const int nk = g.nk;
@@ -110,49 +111,54 @@ __global__ void __launch_bounds__(128) k_micro_fall(const MicroArgs a) {
     dtp = dtb;
   }
   const float dziv = 1.f / a.dz;
-  float rbr[kMaxNkFall], rst[kMaxNkFall], u[kMaxNkFall], q[kMaxNkFall];
+  const float dzvdt = dziv * dtp;
+  const float rwiv05 = .5f / 1.e3f, dtp05 = .5f * dtp;
   const int nc = nk + 1;
-  for (int k = 1; k <= nk - 1; ++k) {
-    rbr[k] = __ldg(a.col + C_RBR * nc + k);
-    rst[k] = __ldg(a.col + C_RST * nc + k);
-  }
+  const float* crbr = a.col + C_RBR * nc;
+  const float* crst = a.col + C_RST * nc;
   const long long id1 = g.at(i, j, 1);
   const long long pl = g.plane;
+  const long long n3 = pl * nk;
   const long long pp2 = (long long)g.px * g.py;
   const long long pid = (long long)j * g.px + i;
-  // Fall speeds of the past level (termblk, as in k_micro_src).
-  auto speeds = [&](int which) {
-    for (int k = 1; k <= nk - 1; ++k) {
-      MCell c;
-      load_cell(a, id1 + (k - 1) * pl, k, c);
-      termblk_cell(a.thresq, c);
-      float v = 0.f;
-      switch (which) {
-        case 0: v = c.ucq; break; case 1: v = c.uiq; break; case 2: v = c.uin; break;
-        case 3: v = c.urq; break; case 4: v = c.usq; break; case 5: v = c.ugq; break;
-        case 6: v = c.usn; break; default: v = c.ugn; break;
-      }
-      u[k] = v;
-    }
-  };
   float* const fields[8] = {a.qcf, a.qif, a.nif, a.qrf, a.qsf, a.qgf, a.nsf, a.ngf};
   const int pslot[8] = {0, 2, -1, 1, 3, 4, -1, -1};   // prc, pri, -, prr, prs, prg
+#pragma unroll 1
   for (int f = 0; f < 8; ++f) {
-    speeds(f);
-    float* fld = fields[f];
-    for (int k = 1; k <= nk - 1; ++k) q[k] = fld[id1 + (k - 1) * pl];
-    float rate = 0.f, acc = 0.f;
+    float* fld = fields[f] + id1;
+    const float* u = a.uspd + f * n3 + id1;
     const int s = pslot[f];
+    float rate = 0.f, acc = 0.f;
     if (s >= 0) { rate = a.prec[(2 * s) * pp2 + pid]; acc = a.prec[(2 * s + 1) * pp2 + pid]; }
-    for (int n = 0; n < npstp; ++n)
-      upw_column(nk, dziv, dtp, rbr, rst, u, q, s >= 0 ? &rate : nullptr, s >= 0 ? &acc : nullptr);
-    for (int k = 1; k <= nk - 1; ++k) fld[id1 + (k - 1) * pl] = q[k];
+#pragma unroll 1
+    for (int it = 0; it < npstp; ++it) {
+      float q0 = fld[0];
+      float f0 = __ldg(crbr + 1) * __ldg(u) * q0;
+      const float flx1 = f0;
+      float flx2 = 0.f, qn = 0.f;
+#pragma unroll 4
+      for (int k = 1; k <= nk - 2; ++k) {
+        const long long o = (long long)k * pl;             // level k+1
+        const float q1 = fld[o];
+        const float f1 = __ldg(crbr + k + 1) * __ldg(u + o) * q1;
+        if (k == 1) flx2 = f1;
+        qn = fmaxf(q0 + (f1 - f0) / __ldg(crst + k) * dzvdt, 0.f);
+        fld[o - pl] = qn;
+        q0 = q1;
+        f0 = f1;
+      }
+      fld[(long long)(nk - 2) * pl] = qn;                   // q(nk-1) = q(nk-2)
+      if (s >= 0) {
+        rate = (flx1 + flx2) * rwiv05;
+        acc = acc + rate * dtp05;
+      }
+    }
     if (s >= 0) { a.prec[(2 * s) * pp2 + pid] = rate; a.prec[(2 * s + 1) * pp2 + pid] = acc; }
   }
   // coldblk.f90:467-470: adjstni once more (flqcqi_opt=1)
   for (int k = 1; k <= nk - 1; ++k) {
     const long long id = id1 + (k - 1) * pl;
-    const float rb = rbr[k], rbv = 1.f / rb;
+    const float rb = __ldg(crbr + k), rbv = 1.f / rb;
     float nci = a.nif[id], ncs = a.nsf[id], ncg = a.ngf[id];
     adjstni_cell(rb, rbv, a.qif[id], a.qsf[id], a.qgf[id], nci, ncs, ncg);
     a.nif[id] = nci; a.nsf[id] = ncs; a.ngf[id] = ncg;
@@ -243,7 +249,6 @@ int micro_init_tables() {
 }
 
 int launch_cloudphy(const MicroArgs& a, cudaStream_t st) {
-  if (a.g.nk > kMaxNkFall - 1) return CRESS_E_UNSUPPORTED;
   k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
   dim3 b(32, 8, 1);
   dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
@@ -278,8 +283,9 @@ namespace cress {
 int launch_collect_tuples(const MicroArgs& a, const float* w, Mlp* m, int stride, float keep_zero,
                           unsigned long long seed, unsigned long long* count_d, cudaStream_t st) {
   if (stride < 1) return CRESS_E_ARG;
-  k_micro_tuples<<<148 * 8, 128, 0, st>>>(a, w, m->tx, m->ty, count_d, m->tcap - m->ntup, stride, keep_zero,
-                                          seed);
+  // append after the tuples already stored
+  k_micro_tuples<<<148 * 8, 128, 0, st>>>(a, w, m->tx + m->ntup * kMlpIn, m->ty + m->ntup * kMlpOut, count_d,
+                                          m->tcap - m->ntup, stride, keep_zero, seed);
   return cudaGetLastError() == cudaSuccess ? CRESS_OK : CRESS_E_CUDA;
 }
 
@@ -289,7 +295,6 @@ int launch_collect_tuples(const MicroArgs& a, const float* w, Mlp* m, int stride
 // sedimentation.
 int launch_cloudphy_learned(const MicroArgs& a, const float* w, Mlp* m, const LearnedBuffers& L, float resid_tol,
                             cudaStream_t st, long long* launches) {
-  if (a.g.nk > kMaxNkFall - 1) return CRESS_E_UNSUPPORTED;
   k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
   ++*launches;
   const long long ncell = (long long)(a.g.ni - 3) * (a.g.nj - 3) * (a.g.nk - 1);

@@ -15,6 +15,7 @@ struct MicroArgs {
   // future level t+dt (updated)
   float *ptpf, *qvf, *qcf, *qrf, *qif, *qsf, *qgf, *nif, *nsf, *ngf;
   float* prec;       // 10 planes (px*py): prc, prr, pri, prs, prg x (rate, accumulated)
+  float* uspd;       // 8 fall-speed fields (past level), written by the process-rate kernels
   int* dtp_bits;     // domain minimum of the sedimentation step (float bits, positive)
   float dtb;         // microphysics step = 2*dtb of the leapfrog (cloudphy.f90:282)
   float dz, thresq;

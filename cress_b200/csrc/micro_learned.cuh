@@ -138,6 +138,7 @@ __global__ void __launch_bounds__(128) k_mlp_features(const MicroArgs a, const f
       load_future(a, id, c);
       mlp_features(c, w_center(w, id, g.plane), f);
       termblk_cell(a.thresq, c);
+      store_speeds(a, id, c);
       const float dzjcb = a.dz * __ldg(a.col + C_JCB * (g.nk + 1) + k);
       lim = fminf(lim, dzjcb / (c.ucq + 1.e-20f));
       lim = fminf(lim, dzjcb / (c.urq + 1.e-20f));

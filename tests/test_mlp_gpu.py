@@ -1,0 +1,148 @@
+"""Learned microphysics on the GPU: the tensor-core forward pass and the
+hand-written backward pass against the CPU oracle (oracle/mlp.py, which
+rounds to BF16 at the same points), training on the device, and the
+learned form inside a moist large step.
+
+Tolerances: forward outputs within 2e-3 of the output range (a hidden
+activation whose FP32 sum lands on the other side of a BF16 rounding
+boundary moves by one BF16 ulp, 2^-8 relative); gradients within 5e-3 of
+each parameter block's largest entry.  (Measured on a B200: 4e-4 and 5e-4.)
+"""
+import numpy as np
+import pytest
+
+from oracle import mlp as M
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["u", "v", "w", "pp", "ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
+
+
+def random_params(seed, scale=1.0):
+    rng = np.random.default_rng(seed)
+    d = M.unpack(np.zeros(M.count()))
+    d["W1"][:, :M.NIN] = rng.uniform(-1, 1, (M.H, M.NIN)) * scale * np.sqrt(3 / M.NIN)
+    d["W2"][:] = rng.uniform(-1, 1, (M.H, M.H)) * scale * np.sqrt(3 / M.H)
+    d["W3"][:] = rng.uniform(-1, 1, (M.H, M.H)) * scale * np.sqrt(3 / M.H)
+    d["W4"][:, :M.NOUT] = rng.uniform(-1, 1, (M.H, M.NOUT)) * scale * np.sqrt(3 / M.H)
+    for b in ("b1", "b2", "b3"):
+        d[b][:] = rng.uniform(-0.2, 0.2, M.H)
+    d["b4"][:M.NOUT] = rng.uniform(-0.2, 0.2, M.NOUT)
+    return M.pack(d).astype(np.float32)
+
+
+def test_forward_matches_oracle(cress):
+    m = cress.Mlp(seed=3)
+    p = random_params(1)
+    m.set_params(p)
+    x = np.random.default_rng(2).standard_normal((300, 16)).astype(np.float32)
+    y = m.forward(x)
+    yr, _ = M.forward(p.astype(np.float64), x.astype(np.float64))
+    m.close()
+    scale = float(np.abs(yr).max())
+    assert np.isfinite(y).all()
+    assert float(np.abs(y - yr).max()) <= 2e-3 * scale
+
+
+def test_backward_matches_oracle(cress):
+    m = cress.Mlp(seed=3)
+    p = random_params(4)
+    m.set_params(p)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((256, 16)).astype(np.float32)
+    t = rng.standard_normal((256, 9)).astype(np.float32)
+    loss, g = m.loss_grad(x, t)
+    m.close()
+    lr, gr = M.loss_grad(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64))
+    assert abs(loss - lr) <= 1e-3 * abs(lr)
+    o = 0
+    for name, n in M.SIZES:
+        a, b = g[o:o + n], gr[o:o + n]
+        o += n
+        scale = float(np.abs(b).max()) + 1e-30
+        err = float(np.abs(a - b).max())
+        assert err <= 5e-3 * scale, f"{name}: max err {err:.3e} of scale {scale:.3e}"
+
+
+def test_training_reduces_loss(cress):
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal((40960, 16)).astype(np.float32)
+    t = np.stack([np.sin(x[:, 0]) + x[:, 1] * x[:, 2], np.tanh(x[:, 3] - x[:, 4]), x[:, 5] ** 2,
+                  np.cos(x[:, 6]), x[:, 7] * x[:, 8], np.abs(x[:, 9]), x[:, 10] - x[:, 11],
+                  np.sin(x[:, 12] * x[:, 13]), x[:, 14] + 0.5 * x[:, 15]], 1).astype(np.float32)
+    m = cress.Mlp(seed=11)
+    m.add_tuples(x, t)
+    m.fit_norm()
+    losses = m.train(400, batch=4096, lr=2e-3, seed=3)
+    m.close()
+    assert np.isfinite(losses).all()
+    first, last = float(np.mean(losses[:10])), float(np.mean(losses[-20:]))
+    assert last < 0.2 * first, (first, last)
+
+
+def _moist_solver(cress, oracle_lib, seed):
+    from cress_b200 import cases
+    case = cases.supercell_case(40, 32, 24, 1000.0, ztop=8000.0, seed=seed, cloud=True,
+                                rad=(6000.0, 6000.0, 1400.0))
+    ni, nj, nk = case["dims"]
+    zph = case["zph"]
+    rbct, ksp0 = oracle_lib.vspdmp(nk, zph, 0.005, 0.6 * zph[nk - 1])
+    s = cress.Solver(ni, nj, nk, 1000.0, 1000.0, case["dz"], sthopt=1, cphopt=3)
+    s.set_base3d(case["base"])
+    s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
+    s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
+    init = list(case["level"]) + [case["moist"][n] for n in NAMES[5:]]
+    for n, a in zip(NAMES, init):
+        s.put_field(n, cress.PAST, a)
+        s.put_field(n, cress.NOW, a)
+    return s, (ni, nj, nk)
+
+
+def test_learned_form_trained_on_plain_tuples(cress, oracle_lib):
+    """Tuples sampled from plain moist steps train the network; on held-out
+    tuples from another storm the trained network is far closer to the
+    plain scheme than the untrained one; the learned form then runs whole
+    large steps with non-negative species and every cell accounted for."""
+    m = cress.Mlp(seed=5)
+    m.reserve(400000)
+    s, dims = _moist_solver(cress, oracle_lib, 3)
+    s.set_tuple_sampling(m, stride=1, keep_zero=0.2, seed=9)
+    s.large_step(0, 2.5, 10, 0.5)
+    for n in range(1, 4):
+        s.large_step(n * 5000, 5.0, 10, 1.0)
+    s.set_tuple_sampling(None)
+    ntrain = m.tuple_count()
+    assert ntrain > 10000
+    # held-out tuples from a different storm
+    h = cress.Mlp(seed=6)
+    h.reserve(100000)
+    s2, _ = _moist_solver(cress, oracle_lib, 21)
+    s2.set_tuple_sampling(h, stride=2, keep_zero=0.2, seed=4)
+    s2.large_step(0, 2.5, 10, 0.5)
+    s2.large_step(5000, 5.0, 10, 1.0)
+    s2.close()
+    xh, th = h.get_tuples()
+    h.close()
+    m.fit_norm()
+    nm = m.get_norm()
+    xs = (xh - nm[0:16]) / nm[16:32]
+    ts = (th - nm[32:41]) / nm[41:50]
+    before = float(np.mean((m.forward(xs) - ts) ** 2))
+    losses = m.train(600, batch=8192, lr=1e-3, seed=2)
+    after = float(np.mean((m.forward(xs) - ts) ** 2))
+    assert np.isfinite(losses).all()
+    assert after < 0.5 * before, (before, after)
+    # the learned form inside whole large steps
+    s.set_learned_micro(m, chunk=32768, resid_tol=0.5)
+    ni, nj, nk = dims
+    for n in range(4, 6):
+        s.large_step(n * 5000, 5.0, 10, 1.0)
+    done, fallback = s.learned_stats()
+    assert done + fallback == 2 * (ni - 3) * (nj - 3) * (nk - 1)
+    for name in NAMES[5:]:
+        a = s.get_field(name, cress.NOW)[0:nk - 1, 2:nj - 1, 2:ni - 1]
+        assert np.isfinite(a).all() and float(a.min()) >= 0.0, name
+    for name in NAMES[:5]:
+        assert np.isfinite(s.get_field(name, cress.NOW)).all(), name
+    s.close()
+    m.close()

@@ -110,3 +110,25 @@ def test_moist_step_fp32_vs_fp64_and_water(oracle_lib):
         scale = float(np.abs(b[sl]).max()) + 1e-12
         assert float(np.abs(a[sl] - b[sl]).max()) <= 2e-2 * scale, name
     assert float(np.abs(runs[0][1] - runs[1][1]).max()) <= 2e-2 * float(np.abs(runs[1][1]).max()) + 1e-9
+
+
+def test_mlp_oracle_gradient_finite_differences():
+    """The oracle's backward pass (exact float64 mode) against central
+    differences on a sample of parameters."""
+    from oracle import mlp as M
+    rng = np.random.default_rng(1)
+    p = rng.uniform(-0.2, 0.2, M.count())
+    x = rng.standard_normal((8, 16))
+    t = rng.standard_normal((8, 9))
+    M.ROUND = False
+    try:
+        _, g = M.loss_grad(p, x, t)
+        idx = rng.choice(M.count(), 40, replace=False)
+        # keep to the parameters the padding does not zero out
+        for i in idx:
+            e = np.zeros_like(p)
+            e[i] = 1e-5
+            fd = (M.loss_grad(p + e, x, t)[0] - M.loss_grad(p - e, x, t)[0]) / 2e-5
+            assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+    finally:
+        M.ROUND = True
