@@ -146,6 +146,72 @@ def cpu_moist(args, threads, nx, ny, nsteps):
     return nx * ny * args.nz * nsteps / dt, dt
 
 
+def learned_leg(args, s, stream, nsstp, cells, plain_ms, barrier, max_over_ranks):
+    """The learned-microphysics form on the same domain.  Tuples of the plain
+    scheme are sampled over 4 plain steps, the MLP is trained on the device,
+    then the same `eval_steps` large steps run from one saved state with the
+    plain and the learned process rates; reports the learned form's
+    throughput (CUDA events) and its error against the plain form
+    (accumulated surface precipitation, hydrometeor RMS)."""
+    import torch
+    import cress_b200
+    m = cress_b200.Mlp(device=torch.cuda.current_device(), seed=7)
+    m.reserve(4_000_000)
+    s.set_tuple_sampling(m, stride=16, keep_zero=0.05, seed=3)
+    for _ in range(4):
+        s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+    s.set_tuple_sampling(None)
+    s.sync()
+    ntup = m.tuple_count()
+    m.fit_norm()
+    t0 = time.perf_counter()
+    losses = m.train(args.train_steps, batch=8192, lr=1e-3, seed=5)
+    train_s = time.perf_counter() - t0
+    saved = [s.get_field(n, lvl) for n in NAMES for lvl in (cress_b200.PAST, cress_b200.NOW)]
+    prec0 = s.get_precip()
+
+    def restore():
+        it = iter(saved)
+        for n in NAMES:
+            for lvl in (cress_b200.PAST, cress_b200.NOW):
+                s.put_field(n, lvl, next(it))
+        s.put_precip(prec0)
+
+    def run(learned_on):
+        restore()
+        s.set_learned_micro(m if learned_on else None, chunk=1 << 20, resid_tol=0.5)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.eval_steps):
+            s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+        e1.record(stream)
+        barrier()
+        t = max_over_ranks(e0.elapsed_time(e1)) / args.eval_steps
+        out = {n: s.get_field(n, cress_b200.NOW) for n in MOIST[1:6]}
+        stats = s.learned_stats() if learned_on else None
+        return t, out, s.get_precip(), stats
+
+    tp, qp, pp, _ = run(False)
+    tl, ql, pl, (ncl, nfb) = run(True)
+    s.set_learned_micro(None)
+    m.close()
+    sl = (slice(0, args.nz + 2), slice(2, args.ny + 2), slice(2, args.nx + 2))
+    rms = {n: float(np.sqrt(np.mean((ql[n][sl] - qp[n][sl]) ** 2)) /
+                    (np.sqrt(np.mean(qp[n][sl] ** 2)) + 1e-30)) for n in qp}
+    acc_p = float(pp[:, 1].sum())
+    acc_l = float(pl[:, 1].sum())
+    return {"value": cells / (tl * 1e-3), "unit": "cell-updates/s", "ms_per_step": tl,
+            "plain_ms_per_step_same_steps": tp, "speedup_vs_plain": tp / tl,
+            "mlp_cells": ncl, "fallback_cells": nfb,
+            "precip_accum_rel_diff": abs(acc_l - acc_p) / (abs(acc_p) + 1e-30),
+            "hydrometeor_rms_rel": rms,
+            "train": {"tuples": int(ntup), "steps": args.train_steps, "batch": 8192,
+                      "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-50:])),
+                      "seconds": train_s},
+            "eval_steps": args.eval_steps, "plain_ms_per_step_timed": plain_ms}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -163,6 +229,9 @@ def main():
     ap.add_argument("--cpu-ny", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--eval-steps", type=int, default=6)
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
@@ -270,6 +339,9 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = HEVI_BYTES_PER_CELL * cells / (hevi_ms * 1e-3) / 1e9
 
+    learned = None if args.no_learned else learned_leg(args, s, stream, nsstp, cells, ms / args.steps,
+                                                        barrier, max_over_ranks)
+
     # End to end through the public API with host buffers: every step the
     # past and present levels (14 fields each) go host->device from pinned
     # memory, one large step runs, the new present level (14 fields) comes
@@ -322,7 +394,7 @@ def main():
                          "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
-            "cpu_baseline": cpu}))
+            "cpu_baseline": cpu, "learned": learned}))
     if world > 1:
         dist.destroy_process_group()
 

@@ -56,13 +56,17 @@ __device__ __forceinline__ float smooth_into(float frc, int smtopt, float smhcoe
   return frc;
 }
 
+// blockIdx.z runs over k = 2..nk-1 within one output group, then over the
+// groups (0: ufrc, 1: vfrc, 2: wfrc, 3: pfrc and theta'), so the four
+// stencils of a point run in different threads.
 __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = 2 + blockIdx.z;
-  if (i > ni - 1 || j > nj - 1 || k > nk - 1) return;
+  const int grp = blockIdx.z / (nk - 2);
+  const int k = 2 + blockIdx.z % (nk - 2);
+  if (i > ni - 1 || j > nj - 1 || grp > 3) return;
   const long long px = g.px, pl = g.plane;
   const long long id = g.at(i, j, k);
   const int nc = nk + 1;
@@ -83,7 +87,7 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   auto RXW = [&](long long p, int kk) { return C(C_RST8W, kk) * WC(p, kk); };
 
   // ---------------------------------------------------------------- ufrc
-  if (j <= nj - 2 && k <= nk - 2) {
+  if (grp == 0 && j <= nj - 2 && k <= nk - 2) {
     float f = 0.f;
     if (smooth) {
       auto A = [&](int dx, int dy, int dz) {
@@ -119,7 +123,7 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
     a.ufrc[id] = f;
   }
   // ---------------------------------------------------------------- vfrc
-  if (i <= ni - 2 && k <= nk - 2) {
+  if (grp == 1 && i <= ni - 2 && k <= nk - 2) {
     float f = 0.f;
     if (smooth) {
       auto A = [&](int dx, int dy, int dz) {
@@ -155,7 +159,7 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
     a.vfrc[id] = f;
   }
   // ---------------------------------------------------------------- wfrc
-  if (i <= ni - 2 && j <= nj - 2) {
+  if (grp == 2 && i <= ni - 2 && j <= nj - 2) {
     float f = 0.f;
     if (smooth) {
       auto A = [&](int dx, int dy, int dz) {
@@ -195,7 +199,7 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
     a.wfrc[id] = f;
   }
   // ------------------------------------------------- pfrc, theta' step
-  if (i <= ni - 2 && j <= nj - 2 && k <= nk - 2) {
+  if (grp == 3 && i <= ni - 2 && j <= nj - 2 && k <= nk - 2) {
     // advs-type advection of s with fluxes FU/FV/FW (advs.f90:205-370)
     auto adv = [&](const float* s, auto FU, auto FV, auto FW) {
       auto S = [&](long long p) { return ld(s, p); };
@@ -357,14 +361,29 @@ __device__ __forceinline__ int wrap(int x, int n) {
   return 2 + r;
 }
 
-__global__ void __launch_bounds__(256) k_halo(const HaloArgs a) {
+// Threads run over the frame of possible ghost points only: the rows
+// j in {0, 1, nj-1, nj, nj+1} (all i) and the columns i in {0, 1, ni-1, ni,
+// ni+1} (j = 2..nj-2), one level per blockIdx.y; per field the staggering
+// decides which of them are ghosts.  Sources are never ghosts, so the
+// order of the copies does not matter.
+__global__ void __launch_bounds__(128) k_halo(const HaloArgs a) {
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj;
-  // threads cover the (ni+2) x (nj+2) plane; only ghost positions act
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = 1 + blockIdx.z;
-  if (i > ni + 1 || j > nj + 1 || k > g.nk) return;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = 1 + blockIdx.y;
+  const int rows = 5 * (ni + 2);
+  int i, j;
+  if (b < rows) {
+    const int r = b / (ni + 2);
+    i = b % (ni + 2);
+    j = r < 2 ? r : nj - 1 + (r - 2);
+  } else {
+    const int c = b - rows;
+    if (c >= 5 * (nj - 3)) return;
+    const int q = c / (nj - 3);
+    j = 2 + c % (nj - 3);
+    i = q < 2 ? q : ni - 1 + (q - 2);
+  }
   for (int n = 0; n < a.n; ++n) {
     const int st = a.stag[n];
     const bool gx = (st == STAG_U) ? (i <= 1 || i >= ni) : (i <= 1 || (i >= ni - 1 && i <= ni));
@@ -383,7 +402,7 @@ __global__ void __launch_bounds__(256) k_halo(const HaloArgs a) {
 
 int launch_force(const ForceArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni - 2 + 31) / 32, (a.g.nj - 2 + 7) / 8, a.g.nk - 2);
+  dim3 gr((a.g.ni - 2 + 31) / 32, (a.g.nj - 2 + 7) / 8, (a.g.nk - 2) * 4);
   k_force<<<gr, b, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
@@ -403,9 +422,9 @@ int launch_timeflt(const FilterArgs& a, cudaStream_t st) {
 }
 
 int launch_halo(const HaloArgs& a, cudaStream_t st) {
-  dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni + 2 + 31) / 32, (a.g.nj + 2 + 7) / 8, a.g.nk);
-  k_halo<<<gr, b, 0, st>>>(a);
+  const int frame = 5 * (a.g.ni + 2) + 5 * (a.g.nj - 3);
+  dim3 gr((frame + 127) / 128, a.g.nk, 1);
+  k_halo<<<gr, 128, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 

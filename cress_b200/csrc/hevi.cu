@@ -47,8 +47,12 @@ constexpr int r128(int n) { return (n + 31) / 32 * 32; }  // floats -> multiple 
 
 // FT: element type of the column store of eliminated right-hand sides
 // (double by default; float halves the store and doubles resident blocks,
-// with the elimination recurrence itself still in double).
-template <int TY, int S, typename FT = double>
+// with the elimination recurrence itself still in double).  GS: park the
+// eliminated right-hand sides (as float) in the new w array instead of
+// shared memory; the way down reads each one back just before it writes
+// the final w there (an L2 round trip), which frees the block's largest
+// shared-memory buffer for more resident blocks.
+template <int TY, int S, typename FT = double, bool GS = false>
 struct HeviLayout {
   using R = HeviRows<TY>;
   static constexpr int BX = kHeviBoxX;
@@ -67,14 +71,14 @@ struct HeviLayout {
   __host__ __device__ static size_t cols_floats(int nk) { return (size_t)((C_NFIELDS * (nk + 1) + 31) / 32 * 32); }
   __host__ __device__ static size_t bytes(int nk) {
     return 4 * ((size_t)S * stage + t3h_floats + cols_floats(nk)) + 8 * (size_t)S +
-           sizeof(FT) * (size_t)(nk - 4) * (kHeviTX * TY);
+           (GS ? 0 : sizeof(FT) * (size_t)(nk - 4) * (kHeviTX * TY));
   }
 };
 
-template <int TY, int S, typename FT>
-__global__ void __launch_bounds__(kHeviTX * TY)
+template <int TY, int S, typename FT, bool GS>
+__global__ void __launch_bounds__(kHeviTX * TY, GS ? 24 / TY : 1)
 k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
-  using L = HeviLayout<TY, S, FT>;
+  using L = HeviLayout<TY, S, FT, GS>;
   constexpr int TX = kHeviTX, BX = kHeviBoxX, NT = TX * TY;
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
@@ -239,7 +243,8 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
         // gaussel.f90:189-240 in double with the 1-D factors
         const double rr = (double)__ldg(a.thom_rr + k), aa = __ldg(a.thom_aa + k);
         const double f = (k == 3) ? (double)wrhs * aa : ((double)wrhs - rr * fprev) * aa;
-        fcol[(k - 3) * NT + tid] = (FT)f;
+        if constexpr (GS) a.w_new[id] = (float)f;
+        else fcol[(k - 3) * NT + tid] = (FT)f;
         fprev = f;
       }
       t3v_prev = t3v;
@@ -276,7 +281,7 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       if (k > 2) { fpn = a.p_new[idk - plane]; pon = a.p_old[idk - plane]; }
       float wk;
       if (k >= 3) {
-        const double f = (double)fcol[(k - 3) * NT + tid];
+        const double f = GS ? (double)a.w_new[idk] : (double)fcol[(k - 3) * NT + tid];
         const double wd = (k == nk - 2) ? f : f - __ldg(a.thom_cp + k) * wupd;                  // gaussel.f90:254
         wupd = wd;
         wk = (float)wd;
@@ -321,23 +326,19 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   }
 }
 
-template <int TY, int S, typename FT>
+template <int TY, int S, typename FT, bool GS = false>
 int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
-  using L = HeviLayout<TY, S, FT>;
+  using L = HeviLayout<TY, S, FT, GS>;
   const Grid& g = a.g;
   const int nx = g.ni - 3, ny = g.nj - 3;
   const size_t bytes = L::bytes(g.nk);
   if (bytes > 227 * 1024) return CRESS_E_UNSUPPORTED;
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(k_hevi_substep<TY, S, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             227 * 1024) != cudaSuccess)
-      return CRESS_E_CUDA;
-    attr_set = true;
-  }
+  if (cudaFuncSetAttribute(k_hevi_substep<TY, S, FT, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)bytes) != cudaSuccess)
+    return CRESS_E_CUDA;
   dim3 block(kHeviTX, TY);
   dim3 grid((nx + kHeviTX - 1) / kHeviTX, (ny + TY - 1) / TY);
-  k_hevi_substep<TY, S, FT><<<grid, block, bytes, st>>>(maps, a);
+  k_hevi_substep<TY, S, FT, GS><<<grid, block, bytes, st>>>(maps, a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
@@ -346,10 +347,11 @@ int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
 // Tile ids.  0-2 keep the eliminated right-hand sides as float between the
 // two sweeps (both recurrences still run in double): 3 blocks of 4 warps
 // fit per SM, the default.  3-5 store them as double (2 blocks per SM).
+// 6-8 park them (float) in the new w array (smaller blocks, more of them).
 int hevi_tile_rows(int tile) {
   switch (tile) {
-    case 1: case 4: return 2;
-    case 2: case 5: return 8;
+    case 1: case 4: case 8: return 2;
+    case 2: case 5: case 7: return 8;
     default: return 4;
   }
 }
@@ -361,6 +363,9 @@ int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaS
     case 3: return launch_t<4, 5, double>(a, maps, st);
     case 4: return launch_t<2, 6, double>(a, maps, st);
     case 5: return launch_t<8, 4, double>(a, maps, st);
+    case 6: return launch_t<4, 4, float, true>(a, maps, st);
+    case 7: return launch_t<8, 4, float, true>(a, maps, st);
+    case 8: return launch_t<2, 6, float, true>(a, maps, st);
     default: return launch_t<4, 4, float>(a, maps, st);
   }
 }
