@@ -344,15 +344,16 @@ int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
 
 }  // namespace
 
-// Tile ids.  0-2 keep the eliminated right-hand sides as float between the
-// two sweeps (both recurrences still run in double): 3 blocks of 4 warps
-// fit per SM, the default.  3-5 store them as double (2 blocks per SM).
-// 6-8 park them (float) in the new w array (smaller blocks, more of them).
+// Tile ids.  0 (the default) and 7: 32 x 8 columns per block, the
+// eliminated right-hand sides parked (float) in the new w array; 6 and 8:
+// the same with 32 x 4 and 32 x 2.  1, 2 and 9 keep them in shared memory
+// as float (32 x 2, 32 x 8, 32 x 4); 3-5 as double (both recurrences
+// always run in double).
 int hevi_tile_rows(int tile) {
   switch (tile) {
     case 1: case 4: case 8: return 2;
-    case 2: case 5: case 7: return 8;
-    default: return 4;
+    case 3: case 6: case 9: return 4;
+    default: return 8;
   }
 }
 
@@ -364,9 +365,9 @@ int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaS
     case 4: return launch_t<2, 6, double>(a, maps, st);
     case 5: return launch_t<8, 4, double>(a, maps, st);
     case 6: return launch_t<4, 4, float, true>(a, maps, st);
-    case 7: return launch_t<8, 4, float, true>(a, maps, st);
     case 8: return launch_t<2, 6, float, true>(a, maps, st);
-    default: return launch_t<4, 4, float>(a, maps, st);
+    case 9: return launch_t<4, 4, float>(a, maps, st);
+    default: return launch_t<8, 4, float, true>(a, maps, st);
   }
 }
 

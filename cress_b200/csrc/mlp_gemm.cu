@@ -4,11 +4,12 @@
 //
 // One CTA computes a 128 x BN tile of C.  Warp 0 (one lane) streams
 // 128 x 64 tiles of A and BN x 64 tiles of B with TMA (128-byte swizzle)
-// into a 4-stage ring; warp 1 (one lane) issues the tcgen05.mma K steps
-// (4 per stage) into a 128 x BN FP32 accumulator in tensor memory and
-// commits each stage back to its producer barrier; all four warps then
-// read the accumulator (warp w owns rows 32w..32w+31) and apply the
-// epilogue.  Every mbarrier wait is bounded: on timeout the kernel records
+// into a ring of stages (2 for BN = 256, so two CTAs share an SM and one's
+// epilogue overlaps the other's MMAs; 4 otherwise); warp 1 (one lane)
+// issues the tcgen05.mma K steps (4 per stage) into a 128 x BN FP32
+// accumulator in tensor memory and commits each stage back to its producer
+// barrier; all eight warps then read the accumulator (warp w owns rows
+// 32(w%4)..+31 and half of the columns) and apply the epilogue.  Every mbarrier wait is bounded: on timeout the kernel records
 // CRESS_E_TIMEOUT in the error word, waits (bounded) for its issued copies
 // and MMAs, frees tensor memory and returns.
 #include <cuda.h>
@@ -26,30 +27,35 @@ int set_error(int code, const char* fmt, ...);
 
 namespace {
 
-constexpr int kBM = 128, kBK = 64, kStages = 4;
+constexpr int kBM = 128, kBK = 64, kThreads = 256;
 
 template <int BN>
 struct GemmCfg {
+  static constexpr int S = BN == 256 ? 2 : 4;
   static constexpr int A_BYTES = kBM * kBK * 2;
   static constexpr int B_BYTES = BN * kBK * 2;
   static constexpr int STAGE = A_BYTES + B_BYTES;
-  static constexpr int SMEM = kStages * STAGE + 1024;
+  static constexpr int SMEM = S * STAGE + 1024;
   static constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
 };
 
-__device__ __forceinline__ float silu(float v) { return v / (1.f + expf(-v)); }
+// SiLU and its derivative with the fast exponential and division
+// intrinsics (relative error ~1e-6, far below the BF16 rounding of the
+// stored activations).
+__device__ __forceinline__ float silu(float v) { return __fdividef(v, 1.f + __expf(-v)); }
 __device__ __forceinline__ float dsilu(float z) {
-  const float s = 1.f / (1.f + expf(-z));
+  const float s = __fdividef(1.f, 1.f + __expf(-z));
   return s * (1.f + z * (1.f - s));
 }
 
 template <int BN>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kThreads, 2)
     k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, const GemmArgs g) {
   using Cfg = GemmCfg<BN>;
   extern __shared__ unsigned char dsm_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(dsm_raw) + 1023) &
                                                        ~static_cast<uintptr_t>(1023));
+  constexpr int kStages = Cfg::S;
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int fail;
@@ -117,16 +123,18 @@ __global__ void __launch_bounds__(128, 1)
   if (!good) {
     if (threadIdx.x == 0 && g.err) atomicExch(g.err, CRESS_E_TIMEOUT);
   } else {
-    const int row = m0 + warp * 32 + lane;
+    const int lg = warp & 3;                      // lane group of tensor memory this warp may read
+    const int row = m0 + lg * 32 + lane;
+    constexpr int HALF = BN / 2;
 #pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 32) {
-      uint32_t r[32];
-      tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), r);
+    for (int c0 = (warp >> 2) * HALF; c0 < (warp >> 2) * HALF + HALF; c0 += 16) {
+      uint32_t r[16];
+      tmem_ld16(tmem + (static_cast<uint32_t>(lg * 32) << 16) + static_cast<uint32_t>(c0), r);
       tmem_wait_ld();
       const int col0 = n0 + c0;
-      float a[32];
+      float a[16];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
+      for (int j = 0; j < 16; ++j) {
         float v = __uint_as_float(r[j]);
         if (g.bias) v += __ldg(g.bias + col0 + j);
         float o = v;
@@ -141,14 +149,14 @@ __global__ void __launch_bounds__(128, 1)
       if (g.out_f32) {
         float4* dst = reinterpret_cast<float4*>(g.out_f32 + (size_t)row * g.ldf + col0);
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
+        for (int q = 0; q < 4; ++q)
           dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
                                __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
       }
       if (g.out_bf) {
         uint4* dst = reinterpret_cast<uint4*>(g.out_bf + (size_t)row * g.ldb + col0);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 2; ++q) {
           uint32_t w[4];
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -160,7 +168,7 @@ __global__ void __launch_bounds__(128, 1)
       }
       if (g.out_bt) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) g.out_bt[(size_t)(col0 + j) * g.ldt + row] = __float2bfloat16_rn(a[j]);
+        for (int j = 0; j < 16; ++j) g.out_bt[(size_t)(col0 + j) * g.ldt + row] = __float2bfloat16_rn(a[j]);
       }
     }
   }
@@ -215,7 +223,7 @@ int launch_gemm(const bf16* A, int lda, const bf16* B, int ldb, const GemmArgs& 
       cudaSuccess)
     return set_error(CRESS_E_CUDA, "gemm smem attribute");
   dim3 grid(g.M / kBM, g.N / BN);
-  k_gemm_bf16<BN><<<grid, 128, Cfg::SMEM, st>>>(ta, tb, g);
+  k_gemm_bf16<BN><<<grid, kThreads, Cfg::SMEM, st>>>(ta, tb, g);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? CRESS_OK : set_error(CRESS_E_CUDA, "gemm launch: %s", cudaGetErrorString(e));
 }
