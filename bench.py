@@ -212,6 +212,74 @@ def learned_leg(args, s, stream, nsstp, cells, plain_ms, barrier, max_over_ranks
             "eval_steps": args.eval_steps, "plain_ms_per_step_timed": plain_ms}
 
 
+def ensemble_leg(args, rank):
+    """Batched ensemble: `members` supercell domains of uneven size (nx, ny
+    drawn from 96-192, nz = 48, dx = 1 km) with seeded bubble amplitude
+    (1-3 K), position and shear (10-30 m/s).  Each member has its own
+    stream; the large steps of all members are issued back to back (each
+    replayed from its CUDA graph) so they run concurrently, against the same
+    steps run member after member.  Wall time between device
+    synchronizations; reports aggregate cell-updates/s of both."""
+    import torch
+    import cress_b200
+    from cress_b200 import cases
+    rng = np.random.default_rng(1000 + rank)
+    nz, ksteps = 48, 5
+    members, total = [], 0
+    for mbr in range(args.members):
+        nx, ny = int(rng.integers(96, 193)), int(rng.integers(96, 193))
+        case = cases.supercell_case(nx, ny, nz, 1000.0, seed=int(rng.integers(1 << 30)),
+                                    ptp0=float(rng.uniform(1.0, 3.0)), shear=float(rng.uniform(10.0, 30.0)),
+                                    center=(float(rng.uniform(-20e3, 20e3)), float(rng.uniform(-20e3, 20e3))),
+                                    rad=(8000.0, 8000.0, 1400.0))
+        ni, nj, nk = case["dims"]
+        rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, 0.6 * case["zph"][nk - 1])
+        s = cress_b200.Solver(ni, nj, nk, 1000.0, 1000.0, case["dz"], sthopt=1, cphopt=3,
+                              device=torch.cuda.current_device())
+        s.set_base3d(case["base"])
+        s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
+        s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
+        init = list(case["level"]) + [case["moist"][n] for n in MOIST]
+        for n, a in zip(NAMES, init):
+            s.put_field(n, cress_b200.PAST, a)
+            s.put_field(n, cress_b200.NOW, a)
+        s.set_graphs(True)
+        s.large_step(0, 0.5 * args.dtbig, nsstp_of(args.dtbig, args.dtsml), 0.5 * args.dtsml)
+        members.append(s)
+        total += nx * ny * nz
+    nsstp = nsstp_of(args.dtbig, args.dtsml)
+    for _ in range(13):   # per pointer state (6): an eager step, a capture, then replays
+        for s in members:
+            s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+    torch.cuda.synchronize()
+
+    def timed(concurrent):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if concurrent:
+            for _ in range(ksteps):
+                for s in members:
+                    s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+            for s in members:
+                s.sync()
+        else:
+            for s in members:
+                for _ in range(ksteps):
+                    s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+                s.sync()
+        return time.perf_counter() - t0
+
+    t_seq = timed(False)
+    t_con = timed(True)
+    for s in members:
+        s.close()
+    return {"members": args.members, "nz": nz, "cells": total, "steps": ksteps,
+            "concurrent_cell_updates_per_s": total * ksteps / t_con,
+            "sequential_cell_updates_per_s": total * ksteps / t_seq,
+            "speedup": t_seq / t_con, "timing": "wall clock between device synchronizations",
+            "launch": "one CUDA-graph launch per member per large step, one stream per member"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,6 +298,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--members", type=int, default=32)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--eval-steps", type=int, default=6)
     args = ap.parse_args()
@@ -341,6 +411,7 @@ def main():
 
     learned = None if args.no_learned else learned_leg(args, s, stream, nsstp, cells, ms / args.steps,
                                                         barrier, max_over_ranks)
+    ensemble = None if args.no_ensemble else ensemble_leg(args, rank)
 
     # End to end through the public API with host buffers: every step the
     # past and present levels (14 fields each) go host->device from pinned
@@ -394,7 +465,7 @@ def main():
                          "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
-            "cpu_baseline": cpu, "learned": learned}))
+            "cpu_baseline": cpu, "learned": learned, "ensemble": ensemble}))
     if world > 1:
         dist.destroy_process_group()
 

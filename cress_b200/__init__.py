@@ -107,6 +107,7 @@ def lib():
     L.cress_set_learned_micro.argtypes = [vp, vp, i, f]
     L.cress_learned_stats.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
     L.cress_set_tuple_sampling.argtypes = [vp, vp, i, f, ull]
+    L.cress_set_graphs.argtypes = [vp, i]
     _lib = L
     return L
 
@@ -215,6 +216,10 @@ class Solver:
 
     def satadjst(self, level, thresq=1e-12):
         _check(lib().cress_satadjst(self._h, int(level), float(thresq)))
+
+    def set_graphs(self, on=True):
+        """Replay whole large steps from CUDA graphs."""
+        _check(lib().cress_set_graphs(self._h, int(bool(on))))
 
     def set_learned_micro(self, mlp, chunk=0, resid_tol=0.5):
         """Use `mlp` (an Mlp) for the process rates of s_cloudphy; None

@@ -279,14 +279,15 @@ MOIST_NAMES = ["qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
 
 def supercell_case(nx, ny, nz, dx, ztop=18000.0, dzmin=100.0, dzmax=500.0, seed=0, ptp0=3.0,
                    rad=(10000.0, 10000.0, 1400.0), zc=1400.0, shear=30.0, rcirc=7.0,
-                   noise=0.0, cloud=False):
+                   noise=0.0, cloud=False, center=(0.0, 0.0)):
     """Moist supercell state (cold-rain microphysics, cphopt=3).
 
     Base state: the analytic sounding of moist_columns on a grid stretched
     from dzmin to dzmax up to ztop; quarter-circle hodograph of radius rcirc
     over 0-2 km continuing straight to `shear` m/s of u at 6 km (constant
     above).  Perturbation: +ptp0 K cos^2 ellipsoidal bubble of radii `rad`
-    centred at mid-domain, height zc, plus seeded uniform +-noise K.  With
+    centred at mid-domain shifted by `center` (m), height zc, plus seeded
+    uniform +-noise K.  With
     cloud=True a seeded field of cloud, rain, ice, snow and graupel (with
     ice numbers) and supersaturated pockets is added so every microphysical
     process acts from the first step.  Returns a dict with dims, base (3-D,
@@ -304,8 +305,8 @@ def supercell_case(nx, ny, nz, dx, ztop=18000.0, dzmin=100.0, dzmax=500.0, seed=
     base["vbr"] = expand(v.astype(np.float32), ni, nj, nk)
     rng = np.random.default_rng(seed)
     shp = (nk, nj + 2, ni + 2)
-    x = (np.arange(ni + 2) - 0.5 * (ni + 1)) * dx
-    y = (np.arange(nj + 2) - 0.5 * (nj + 1)) * dx
+    x = (np.arange(ni + 2) - 0.5 * (ni + 1)) * dx - center[0]
+    y = (np.arange(nj + 2) - 0.5 * (nj + 1)) * dx - center[1]
     z = zs[1:nk + 1]
     r = np.sqrt((x[None, None, :] / rad[0]) ** 2 + (y[None, :, None] / rad[1]) ** 2 +
                 ((z[:, None, None] - zc) / rad[2]) ** 2)

@@ -54,8 +54,80 @@ void Ctx::free_learned() {
   mlp = nullptr;
 }
 
+std::vector<float*> Ctx::pointer_state() const {
+  std::vector<float*> s;
+  for (int f = 0; f < CRESS_NFIELD; ++f) {
+    for (int l = 0; l < 4; ++l) s.push_back(lev[f][l]);
+    s.push_back(spare[f]);
+  }
+  return s;
+}
+
+void Ctx::set_pointer_state(const std::vector<float*>& s) {
+  size_t n = 0;
+  for (int f = 0; f < CRESS_NFIELD; ++f) {
+    for (int l = 0; l < 4; ++l) lev[f][l] = s[n++];
+    spare[f] = s[n++];
+  }
+}
+
+void Ctx::free_graphs() {
+  for (auto& kv : grec)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  grec.clear();
+  gseen.clear();
+}
+
+// One large step, replayed from a CUDA graph when this pointer state and
+// these parameters were seen before: the first occurrence runs eagerly
+// (it fills the host-side caches: elimination factors, tensor maps), the
+// second is captured and instantiated, later ones launch the graph and
+// move the pointer state on as the eager step would.  Steps that sample
+// training tuples (they read a count back on the host) always run eagerly.
+int Ctx::step(bool filter, float dtb, int nsstp, float dts) {
+  if (!graphs || sampler) return large_step(filter, dtb, nsstp, dts);
+  const std::vector<float*> pre = pointer_state();
+  std::string key(reinterpret_cast<const char*>(pre.data()), pre.size() * sizeof(float*));
+  const struct { int filter, nsstp; float dtb, dts, resid; const void* mlp; int chunk; } p{
+      filter ? 1 : 0, nsstp, dtb, dts, resid_tol, mlp, lb.chunk};
+  key.append(reinterpret_cast<const char*>(&p), sizeof p);
+  auto it = grec.find(key);
+  if (it == grec.end()) {
+    if (gseen[key]++ == 0) return large_step(filter, dtb, nsstp, dts);
+    const long long l0 = launches;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      return large_step(filter, dtb, nsstp, dts);
+    }
+    const int rc = large_step(filter, dtb, nsstp, dts);
+    const cudaError_t e = cudaStreamEndCapture(stream, &graph);
+    GraphRec r;
+    if (rc || e != cudaSuccess || cudaGraphInstantiate(&r.exec, graph, 0) != cudaSuccess) {
+      // nothing ran: restore the pointer state and run eagerly
+      cudaGetLastError();
+      if (graph) cudaGraphDestroy(graph);
+      set_pointer_state(pre);
+      launches = l0;
+      graphs = false;
+      return large_step(filter, dtb, nsstp, dts);
+    }
+    cudaGraphDestroy(graph);
+    r.nlaunch = launches - l0;
+    launches = l0;
+    r.post = pointer_state();
+    it = grec.emplace(key, std::move(r)).first;
+  }
+  if (cudaGraphLaunch(it->second.exec, stream) != cudaSuccess)
+    return set_error(CRESS_E_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(cudaGetLastError()));
+  launches += it->second.nlaunch;
+  set_pointer_state(it->second.post);
+  return CRESS_OK;
+}
+
 Ctx::~Ctx() {
   cudaSetDevice(device);
+  free_graphs();
   free_learned();
   for (void* p : owned) cudaFree(p);
   if (own_stream) cudaStreamDestroy(own_stream);
@@ -760,7 +832,7 @@ int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, floa
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (!c) return set_error(CRESS_E_ARG, "null context");
   cudaSetDevice(c->device);
-  return c->large_step(ctime != 0, dtb, nsstp, dts);
+  return c->step(ctime != 0, dtb, nsstp, dts);
 }
 
 long long cress_launch_count(const cress_ctx* ctx) {
@@ -774,6 +846,7 @@ int cress_set_learned_micro(cress_ctx* ctx, cress_mlp* mh, int chunk, float resi
   if (!c) return set_error(CRESS_E_ARG, "null context");
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  c->free_graphs();   // captured steps refer to the old buffers
   c->free_learned();
   if (!mh) return CRESS_OK;
   Mlp* m = reinterpret_cast<Mlp*>(mh);
@@ -851,6 +924,18 @@ int cress_set_tuple_sampling(cress_ctx* ctx, cress_mlp* mh, int stride, float ke
   c->sample_stride = stride;
   c->sample_keep_zero = keep_zero;
   c->sample_seed = seed;
+  return CRESS_OK;
+}
+
+// Replay whole large steps from CUDA graphs (on) or launch every kernel
+// from the host (off, the default).
+int cress_set_graphs(cress_ctx* ctx, int on) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->free_graphs();
+  c->graphs = on != 0;
   return CRESS_OK;
 }
 

@@ -67,6 +67,20 @@ struct Ctx {
   unsigned long long* count_d = nullptr;
   long long sampled = 0;
   void free_learned();
+  // CUDA graphs of whole large steps, keyed by the time-level pointer state
+  // and the step parameters; each remembers the pointer state it leaves.
+  struct GraphRec {
+    cudaGraphExec_t exec = nullptr;
+    long long nlaunch = 0;
+    std::vector<float*> post;
+  };
+  bool graphs = false;
+  std::map<std::string, GraphRec> grec;
+  std::map<std::string, int> gseen;
+  std::vector<float*> pointer_state() const;
+  void set_pointer_state(const std::vector<float*>& s);
+  int step(bool filter, float dtb, int nsstp, float dts);
+  void free_graphs();
   int satadjst(int level, float thresq);
   int tmap(const float* buf, int rows, CUtensorMap* out);
   int check_device_error();

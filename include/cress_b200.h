@@ -148,6 +148,12 @@ int cress_set_base_large(cress_ctx* ctx, const float* ubr, const float* vbr, con
  * (SrcOrig/intgdrv.f90:832-998). */
 int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, float dts);
 
+/* Replay whole large steps from CUDA graphs (on != 0) instead of launching
+ * every kernel from the host: the second step with a given time-level
+ * state and parameters is captured, later ones launch the graph.  Results
+ * are bitwise identical to the eager path. */
+int cress_set_graphs(cress_ctx* ctx, int on);
+
 /* Moist base state (cphopt=3): base pressure pbr and base water vapour qvbr
  * (SrcOrig/setbase.f90:153-189), host arrays in reference layout. */
 int cress_set_base_moist(cress_ctx* ctx, const float* pbr, const float* qvbr);
