@@ -127,7 +127,8 @@ class Solver:
 
     def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6,
                  tile=0, device=0, smtopt=3, smhcoe=0.001, smvcoe=0.0004, vspopt=2,
-                 vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1, cphopt=0, thresq=1e-12):
+                 vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1, cphopt=0, thresq=1e-12,
+                 tubopt=0):
         L = lib()
         c = Cfg()
         c.ni, c.nj, c.nk = ni, nj, nk
@@ -137,7 +138,7 @@ class Solver:
         c.wbc = c.ebc = c.sbc = c.nbc = -1
         c.bbc = c.tbc = 2
         c.tile = tile
-        c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = 2, smtopt, vspopt, coropt, 0, cphopt
+        c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = 2, smtopt, vspopt, coropt, tubopt, cphopt
         c.smhcoe, c.smvcoe, c.filcoe, c.fc = smhcoe, smvcoe, filcoe, fc
         c.vspvar = vspvar.encode()[:15]
         c.thresq = thresq

@@ -328,11 +328,11 @@ int Ctx::small_steps(int nsstp, float dts) {
 int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
   if (!base_set || !large_set)
     return set_error(CRESS_E_STATE, "cress_large_step: base state (set_base3d, set_base_large) not set");
-  if (cfg.advopt != 2 || cfg.tubopt != 0 || !(cfg.cphopt == 0 || cfg.cphopt == 3) ||
+  if (cfg.advopt != 2 || !(cfg.tubopt == 0 || cfg.tubopt == 1) || !(cfg.cphopt == 0 || cfg.cphopt == 3) ||
       !(cfg.smtopt == 0 || cfg.smtopt % 10 == 2 || cfg.smtopt % 10 == 3) ||
       !(cfg.vspopt == 0 || cfg.vspopt == 2) || !(cfg.coropt == 0 || cfg.coropt == 1))
     return set_error(CRESS_E_UNSUPPORTED,
-                     "cress_large_step: needs advopt=2, tubopt=0, cphopt 0/3, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
+                     "cress_large_step: needs advopt=2, tubopt 0/1, cphopt 0/3, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
   const bool moist = cfg.cphopt == 3;
   if (moist && !moist_set) return set_error(CRESS_E_STATE, "cress_large_step: moist base state not set");
   const int N = CRESS_NOW, P = CRESS_PAST, F = CRESS_FUTURE;
@@ -358,7 +358,31 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
     f.qv = lev[CRESS_QV][N]; f.qc = lev[CRESS_QC][N]; f.qr = lev[CRESS_QR][N];
     f.qi = lev[CRESS_QI][N]; f.qs = lev[CRESS_QS][N]; f.qg = lev[CRESS_QG][N];
   }
-  int rc = launch_force(f, stream);
+  const float cpriv = 3.f;   // min(1/prnum, 3) with prnum = 0.33 (eddyvis.f90:219-222)
+  int rc;
+  if (cfg.tubopt == 1) {
+    // s_turbdrv up to s_eddyvis on the past level (forceuvw.f90:423-431)
+    TurbArgs t{};
+    t.g = g;
+    t.col = col_d;
+    t.up = lev[CRESS_U][P]; t.vp = lev[CRESS_V][P]; t.wp = lev[CRESS_W][P];
+    t.ptpp = lev[CRESS_PTP][P]; t.ppp = lev[CRESS_PP][P];
+    if (moist) {
+      t.qvp = lev[CRESS_QV][P]; t.qcp = lev[CRESS_QC][P]; t.qrp = lev[CRESS_QR][P];
+      t.qip = lev[CRESS_QI][P]; t.qsp = lev[CRESS_QS][P]; t.qgp = lev[CRESS_QG][P];
+    }
+    t.rkv = rkv_d;
+    t.dxiv = f.dxiv; t.dyiv = f.dyiv; t.dziv = f.dziv;
+    t.ds3 = cfg.dx * cfg.dy * cfg.dz;
+    t.ckmax = .125f / dtb;
+    t.cpriv = cpriv;
+    t.thresq = cfg.thresq;
+    if ((rc = launch_turb_visc(t, stream))) return set_error(rc, "eddy viscosity launch failed");
+    ++launches;
+    f.rkv = rkv_d;
+    f.cpriv = cpriv;
+  }
+  rc = launch_force(f, stream);
   ++launches;
   if (rc) return set_error(rc, "forcing launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   if ((rc = small_steps(nsstp, dts))) return rc;
@@ -376,6 +400,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
     m.smhcoe = cfg.smhcoe; m.smvcoe = cfg.smvcoe; m.dtb2 = f.dtb2;
     m.smtopt = cfg.smtopt; m.vspopt = cfg.vspopt; m.sthopt = cfg.sthopt; m.ksp0 = ksp0;
     m.vsp_qv = on(5); m.vsp_q = on(6);
+    m.rkv = f.rkv; m.cpriv = cpriv;
     if ((rc = launch_moist_scalars(m, stream))) return set_error(rc, "moist scalar launch failed");
     ++launches;
     if ((rc = cloudphy(dtb, cfg.thresq))) return rc;
@@ -591,6 +616,13 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   } else if (cfg->cphopt != 0) {
     delete c;
     return set_error(CRESS_E_UNSUPPORTED, "cphopt=%d: only 0 (dry) and 3 (cold rain) run on the GPU", cfg->cphopt);
+  }
+  if (cfg->tubopt == 1) {
+    c->rkv_d = c->alloc_field();   // Smagorinsky eddy viscosity
+    if (!c->rkv_d) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the eddy viscosity failed"); }
+  } else if (cfg->tubopt != 0) {
+    delete c;
+    return set_error(CRESS_E_UNSUPPORTED, "tubopt=%d: only 0 and 1 (Smagorinsky) run on the GPU", cfg->tubopt);
   }
   c->col_h.assign((size_t)C_NFIELDS_ALL * (cfg->nk + 1), 0.f);
   if ((rc = cuda_check(cudaMalloc(&c->col_d, sizeof(float) * c->col_h.size()), "cudaMalloc cols"))) {

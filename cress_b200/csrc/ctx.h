@@ -52,6 +52,7 @@ struct Ctx {
   bool moist_set = false;  // cress_set_base_moist was called
   float* prec_d = nullptr; // surface precipitation planes (10 x px*py)
   float* uspd_d = nullptr; // fall speeds (8 fields)
+  float* rkv_d = nullptr;  // Smagorinsky eddy viscosity (tubopt=1)
   int* dtp_d = nullptr;    // sedimentation sub-step minimum (float bits)
   int cloudphy(float dtb, float thresq);
   // learned microphysics (MLP in place of the process rates) and tuple

@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "forcing.cuh"
 #include "hevi.cuh"
+#include "turb.cuh"
 
 namespace cress {
 namespace {
@@ -59,6 +60,31 @@ __device__ __forceinline__ float smooth_into(float frc, int smtopt, float smhcoe
 // blockIdx.z runs over k = 2..nk-1 within one output group, then over the
 // groups (0: ufrc, 1: vfrc, 2: wfrc, 3: pfrc and theta'), so the four
 // stencils of a point run in different threads.
+// Turbulent mixing of a scalar S (the full field at t-dt, S(p, kk)) at the
+// point id of level k: s_eddydif / s_kh8uv diffusivities from the eddy
+// viscosity (rkh = priv*rkv/jcb, rkh8u = rkh(i-1)+rkh(i), rkv8w =
+// (rkh(k-1)+rkh(k))/2; eddydif.f90:154-260, kh8uv.f90:211-230) and the
+// flux divergence of s_turbflx / s_turbs (turbflx.f90:236-352,
+// turbs.f90:189-232), added to frc.
+template <class FS>
+__device__ __forceinline__ float turb_scalar(float frc, const float* rkv, const float* col, int nc, long long id,
+                                             int k, long long px, long long pl, float cpriv, float dxiv, float dyiv,
+                                             float dziv, const FS& S) {
+  auto C = [&](int f, int kk) { return __ldg(col + f * nc + kk); };
+  auto RKH = [&](long long p, int kk) { return cpriv * __ldg(rkv + p) / C(C_JCB, kk); };
+  const float jc = C(C_JCB, k);
+  const float dxv05 = .5f * dxiv, dyv05 = .5f * dyiv;
+  auto JS = [&](long long p) { return S(p, k) * jc; };
+  auto H1 = [&](long long p) { return (RKH(p - 1, k) + RKH(p, k)) * (JS(p) - JS(p - 1)) * dxv05; };
+  auto H2 = [&](long long p) { return (RKH(p - px, k) + RKH(p, k)) * (JS(p) - JS(p - px)) * dyv05; };
+  auto H3 = [&](long long p, int kk) {
+    return (.5f * (RKH(p - pl, kk - 1) + RKH(p, kk))) * (S(p, kk) - S(p - pl, kk - 1)) * dziv;
+  };
+  const float j8u = C(C_JCB8U, k), j8v = C(C_JCB8V, k);
+  return frc + ((H3(id + pl, k + 1) - H3(id, k)) * dziv +
+                ((j8u * H1(id + 1) - j8u * H1(id)) * dxiv + (j8v * H2(id + px) - j8v * H2(id)) * dyiv));
+}
+
 __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
@@ -87,8 +113,23 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   auto RXW = [&](long long p, int kk) { return C(C_RST8W, kk) * WC(p, kk); };
 
   // ---------------------------------------------------------------- ufrc
+  const Deform D{col, nc, nk, a.up, a.vp, a.wp, px, pl, dxiv, dyiv, dziv};
+  auto RKV = [&](long long p) { return __ldg(a.rkv + p); };
   if (grp == 0 && j <= nj - 2 && k <= nk - 2) {
     float f = 0.f;
+    if (a.rkv) {   // s_turbuvw u part (turbuvw.f90:288-333) with the stresses of s_strsten
+      const float jc = C(C_JCB, k), j8u = C(C_JCB8U, k);
+      auto A = [&](long long p) { return jc * (RKV(p) * D.s11(p, k)); };
+      auto T12 = [&](long long p) {
+        return .25f * D.s12(p, k) * ((RKV(p - 1 - px) + RKV(p)) + (RKV(p - 1) + RKV(p - px)));
+      };
+      auto Cc = [&](long long p) { return (j8u + j8u) * T12(p); };
+      auto T13 = [&](long long p, int kk) {
+        return .25f * D.s13(p, kk) * ((RKV(p - 1 - pl) + RKV(p)) + (RKV(p - 1) + RKV(p - pl)));
+      };
+      f = ((A(id) - A(id - 1)) * dxiv + (Cc(id + px) - Cc(id)) * (.5f * dyiv)) +
+          (T13(id + pl, k + 1) - T13(id, k)) * dziv;
+    }
     if (smooth) {
       auto A = [&](int dx, int dy, int dz) {
         const int kk = k + dz;
@@ -125,6 +166,19 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   // ---------------------------------------------------------------- vfrc
   if (grp == 1 && i <= ni - 2 && k <= nk - 2) {
     float f = 0.f;
+    if (a.rkv) {   // s_turbuvw v part (turbuvw.f90:795-840)
+      const float jc = C(C_JCB, k), j8v = C(C_JCB8V, k);
+      auto B = [&](long long p) { return jc * (RKV(p) * D.s22(p, k)); };
+      auto T12 = [&](long long p) {
+        return .25f * D.s12(p, k) * ((RKV(p - 1 - px) + RKV(p)) + (RKV(p - 1) + RKV(p - px)));
+      };
+      auto Cc = [&](long long p) { return (j8v + j8v) * T12(p); };
+      auto T23 = [&](long long p, int kk) {
+        return .25f * D.s23(p, kk) * ((RKV(p - px - pl) + RKV(p)) + (RKV(p - px) + RKV(p - pl)));
+      };
+      f = ((B(id) - B(id - px)) * dyiv + (Cc(id + 1) - Cc(id)) * (.5f * dxiv)) +
+          (T23(id + pl, k + 1) - T23(id, k)) * dziv;
+    }
     if (smooth) {
       auto A = [&](int dx, int dy, int dz) {
         const int kk = k + dz;
@@ -161,6 +215,20 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   // ---------------------------------------------------------------- wfrc
   if (grp == 2 && i <= ni - 2 && j <= nj - 2) {
     float f = 0.f;
+    if (a.rkv) {   // s_turbuvw w part (turbuvw.f90:1300-1330)
+      const float j8u = C(C_JCB8U, k - 1) + C(C_JCB8U, k), j8v = C(C_JCB8V, k - 1) + C(C_JCB8V, k);
+      auto T33 = [&](long long p, int kk) { return RKV(p) * D.s33(p, kk); };
+      auto T31 = [&](long long p) {
+        return .25f * D.s13(p, k) * ((RKV(p - 1 - pl) + RKV(p)) + (RKV(p - 1) + RKV(p - pl)));
+      };
+      auto T32 = [&](long long p) {
+        return .25f * D.s23(p, k) * ((RKV(p - px - pl) + RKV(p)) + (RKV(p - px) + RKV(p - pl)));
+      };
+      auto Aw = [&](long long p) { return j8u * T31(p); };
+      auto Cw = [&](long long p) { return j8v * T32(p); };
+      f = (T33(id, k) - T33(id - pl, k - 1)) * dziv +
+          ((Aw(id + 1) - Aw(id)) * (.5f * dxiv) + (Cw(id + px) - Cw(id)) * (.5f * dyiv));
+    }
     if (smooth) {
       auto A = [&](int dx, int dy, int dz) {
         const int kk = k + dz;
@@ -235,6 +303,10 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
       if (smooth) {
         auto A = [&](int dx, int dy, int dz) { return C(C_RBR, k + dz) * ld(a.ptpp, id + dx + dy * px + dz * pl); };
         f = smooth_into(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+      }
+      if (a.rkv) {   // forcept.f90:313-320, 383-393: mixing of the full theta at t-dt
+        auto S = [&](long long p, int kk) { return C(C_PTBR, kk) + ld(a.ptpp, p); };
+        f = turb_scalar(f, a.rkv, col, nc, id, k, px, pl, a.cpriv, dxiv, dyiv, dziv, S);
       }
       if (a.vspopt >= 1 && a.vsp_pt && k >= a.ksp0 - 1)
         f = f - .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1)) * C(C_RST, k) * ld(a.ptpp, id);
@@ -315,6 +387,10 @@ __global__ void __launch_bounds__(256) k_moist_scalars(const MoistScalarArgs a) 
         return isqv ? C(C_RBR, kk) * (v - C(C_QVBR, kk)) : C(C_RBR, kk) * v;
       };
       f = smooth_into(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+    }
+    if (a.rkv) {   // forceqv.f90:331-345, forceq.f90:438-452: mixing of the species at t-dt
+      auto S = [&](long long p, int) { return ld(sp, p); };
+      f = turb_scalar(f, a.rkv, a.col, nc, id, k, px, pl, a.cpriv, a.dxiv, a.dyiv, a.dziv, S);
     }
     const float spv = ld(sp, id);
     if (a.vspopt >= 1 && (isqv ? a.vsp_qv : a.vsp_q) && k >= a.ksp0 - 1)

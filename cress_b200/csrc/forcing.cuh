@@ -30,9 +30,26 @@ struct ForceArgs {
   // moist buoyancy (buoywb.f90:202-299, cphopt != 0): qv and the five
   // hydrometeor mixing ratios at t; null qv = dry buoyancy
   const float* qv; const float* qc; const float* qr; const float* qi; const float* qs; const float* qg;
+  // Smagorinsky turbulence (tubopt=1): eddy viscosity at scalar points from
+  // k_turb_visc (null: no turbulence) and 1/Pr (capped at 3)
+  const float* rkv;
+  float cpriv;
 };
 
 int launch_force(const ForceArgs& a, cudaStream_t st);
+
+// Smagorinsky eddy viscosity (s_turbdrv up to s_eddyvis: bruntv, defomten,
+// defomssq, eddyvis for tubopt=1, isoopt=1, flat terrain) from the past
+// level into rkv at the scalar points i, j = 1..n-1, k = 1..nk-1.
+struct TurbArgs {
+  Grid g;
+  const float* col;
+  const float *up, *vp, *wp, *ptpp, *ppp;                  // t-dt
+  const float *qvp, *qcp, *qrp, *qip, *qsp, *qgp;          // t-dt moist species (null: dry)
+  float* rkv;
+  float dxiv, dyiv, dziv, ds3, ckmax, cpriv, thresq;
+};
+int launch_turb_visc(const TurbArgs& a, cudaStream_t st);
 
 // Forcing and leapfrog step of the nine moist scalars qv, qc, qr, qi, qs,
 // qg, ni, ns, ng (s_forceqv, s_forceq, s_steps).
@@ -47,6 +64,8 @@ struct MoistScalarArgs {
   float dxiv, dyiv, dziv, smhcoe, smvcoe, dtb2;
   int smtopt, vspopt, sthopt, ksp0;
   int vsp_qv, vsp_q;          // vspvar(6:6), vspvar(7:7)
+  const float* rkv;           // eddy viscosity (tubopt=1) or null
+  float cpriv;
 };
 int launch_moist_scalars(const MoistScalarArgs& a, cudaStream_t st);
 

@@ -57,7 +57,7 @@ typedef struct cress_cfg {
   int smtopt;           /* 0 none, 2 horizontal, 3 horizontal + vertical 4th-order smoothing */
   int vspopt;           /* 0 none, 2 Rayleigh damping above botbar toward the base state */
   int coropt;           /* 0 none, 1 f-plane Coriolis on u, v */
-  int tubopt;           /* 0 only (turbulence is not implemented on the GPU) */
+  int tubopt;           /* 0 none, 1 Smagorinsky (isoopt=1, flat terrain, no surface flux) */
   int cphopt;           /* 0 dry, 3 cold-rain bulk (haiopt=0) */
   float smhcoe, smvcoe; /* smoothing coefficients */
   float filcoe;         /* Asselin filter coefficient */

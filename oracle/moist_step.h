@@ -178,7 +178,7 @@ template <class R>
 struct MoistRun {
   DryRun<R> r;
   MoistLevel<R> mp, mc, mf;
-  F3<R> qall, qfrc;
+  F3<R> qall, qallp, qfrc;
   std::vector<R> prec;   // 5 species x (rate, accumulation) planes
   R thresq = R(1.e-12);
   int npstp = 0;         // sedimentation sub-steps of the last step
@@ -186,7 +186,7 @@ struct MoistRun {
     const int ni = r.o.ni, nj = r.o.nj, nk = r.o.nk;
     r.alloc();
     mp.resize(ni, nj, nk); mc.resize(ni, nj, nk); mf.resize(ni, nj, nk);
-    qall.resize(ni, nj, nk); qfrc.resize(ni, nj, nk);
+    qall.resize(ni, nj, nk); qallp.resize(ni, nj, nk); qfrc.resize(ni, nj, nk);
     prec.assign((size_t)10 * (ni + 2) * (nj + 2), R(0));
   }
 };
@@ -215,6 +215,7 @@ void moist_scalar(MoistRun<R>& m, int n, R dtb) {
     smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 2, 2, nj - 2, 2, nk - 2, false, m.qfrc,
             r.t1, r.t2, r.t3);
   }
+  if (r.lo.tubopt == 1) turbs(o, r.b, sp, r.tw, m.qfrc);   // forceqv.f90:331-345, forceq.f90:438-452
   const char sw = isqv ? r.lo.vspvar[5] : r.lo.vspvar[6];
   if (r.lo.vspopt >= 1 && sw == 'o') {
     OMP_FOR for (int k = r.lo.ksp0 - 1; k <= nk - 2; ++k)
@@ -243,6 +244,13 @@ void intgdrv_moist(MoistRun<R>& m, R dtb, int nsstp, R dts, bool filter) {
                   m.mc.q[M_QG].d[n];
   r.bqv = &m.mc.q[M_QV];
   r.bqall = &m.qall;
+  for (size_t n = 0; n < m.qallp.size(); ++n)   // totalqwi at t-dt (intgdrv.f90:841)
+    m.qallp.d[n] = m.mp.q[M_QC].d[n] + m.mp.q[M_QR].d[n] + m.mp.q[M_QI].d[n] + m.mp.q[M_QS].d[n] +
+                   m.mp.q[M_QG].d[n];
+  r.tqv = &m.mp.q[M_QV];
+  r.tqall = &m.qallp;
+  r.thresq = m.thresq;
+  r.dtb_cur = dtb;
   phase_forcing(r);
   phase_small(r, nsstp, dts);
   step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false);
@@ -269,6 +277,8 @@ void intgdrv_moist(MoistRun<R>& m, R dtb, int nsstp, R dts, bool filter) {
   std::swap(m.mc, m.mf);
   r.bqv = nullptr;
   r.bqall = nullptr;
+  r.tqv = nullptr;
+  r.tqall = nullptr;
 }
 
 }  // namespace oracle

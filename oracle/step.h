@@ -5,6 +5,7 @@
 #pragma once
 #include <vector>
 #include "large.h"
+#include "turb.h"
 
 namespace oracle {
 
@@ -30,6 +31,13 @@ struct DryRun {
   // moist buoyancy inputs at t (buoywb.f90:202-299); null for a dry run
   const F3<R>* bqv = nullptr;
   const F3<R>* bqall = nullptr;
+  // Smagorinsky turbulence (tubopt=1): moist inputs at t-dt (bruntv.f90),
+  // null for a dry run; the step's dtb (eddyvis.f90: ckmax = 0.125/dtb)
+  const F3<R>* tqv = nullptr;
+  const F3<R>* tqall = nullptr;
+  R thresq = R(1.e-12);
+  R dtb_cur = R(0);
+  TurbWork<R> tw;
   // scratch
   F3<R> ufrc, vfrc, wfrc, pfrc, ptfrc, wc, rxu, rxv, rxw, t1, t2, t3, t4, t5, jxu, jxv, jxw;
   SmallScratch<R> ss;
@@ -40,6 +48,7 @@ struct DryRun {
                      &t5, &jxu, &jxv, &jxw})
       a->resize(ni, nj, nk);
     ss.resize(ni, nj, nk);
+    if (lo.tubopt == 1) tw.resize(ni, nj, nk);
   }
 };
 
@@ -51,6 +60,13 @@ void forceuvw(DryRun<R>& r) {
   const Opts& o = r.o;
   const int ni = o.ni, nj = o.nj, nk = o.nk;
   r.ufrc.fill(R(0)); r.vfrc.fill(R(0)); r.wfrc.fill(R(0));
+  if (r.lo.tubopt == 1) {                                               // forceuvw.f90:423-431, turbdrv.f90:245-287
+    bruntv(o, r.tqv != nullptr, r.thresq, r.b, r.p.pp, r.p.ptp, r.tqv, r.tqall, r.tw);
+    defomten(o, r.b, r.p.u, r.p.v, r.p.w, r.tw);
+    eddyvis(o, r.dtb_cur, r.b, r.tw);
+    strsten(o, r.tw);
+    turbuvw(o, r.b, r.tw, r.ufrc, r.vfrc, r.wfrc);
+  }
   phy2cnt(o, r.sthopt, r.b, r.c.w, r.wc);                               // forceuvw.f90:446
   if (r.lo.smtopt % 10 == 2 || r.lo.smtopt % 10 == 3) {                 // forceuvw.f90:469
     // smoo4uvw.f90:220-233: a = rst8u*(up-ubr)/jcb8u over k=1..nk-1, j=0..nj, i=0..ni+1
@@ -117,6 +133,13 @@ void forcept(DryRun<R>& r) {
     smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 2, 2, nj - 2, 2, nk - 2, false,
             r.ptfrc, r.t1, r.t2, r.t3);
   }
+  if (r.lo.tubopt == 1) {                                               // forcept.f90:313-320, 383-393
+    F3<R>& pt = r.tw.ptv;   // free after bruntv: the full potential temperature at t-dt
+    for (int k = 1; k <= nk - 1; ++k)
+      for (int j = 1; j <= nj - 1; ++j)
+        for (int i = 1; i <= ni - 1; ++i) pt(i, j, k) = r.b.ptbr(i, j, k) + r.p.ptp(i, j, k);
+    turbs(o, r.b, pt, r.tw, r.ptfrc);
+  }
   if (r.lo.vspopt >= 1 && r.lo.vspvar[4] == 'o') vsp_scalar(o, r.lo.ksp0, r.rbct, r.b.rst, r.p.ptp, r.ptfrc);
   advbspt(o, r.b, r.c.w, r.ptfrc, r.t1);
 }
@@ -137,6 +160,7 @@ void vbcs(const Opts& o, F3<R>& sf) {
 template <class R>
 void phase_forcing(DryRun<R>& r) {   // s_forcedrv (forcedrv.f90:548-608)
   forceuvw(r);
+  if (r.lo.tubopt == 1) eddydif(r.o, r.b, r.tw);   // forcedrv.f90:565-570
   forcep(r);
   forcept(r);
 }
@@ -202,6 +226,7 @@ void phase_halo(DryRun<R>& r) {   // shift2nd on t and t+dt (intgdrv.f90:1005,10
 // and the swp2nxt rotation.
 template <class R>
 void intgdrv_dry(DryRun<R>& r, R dtb, int nsstp, R dts, bool filter) {
+  r.dtb_cur = dtb;
   phase_forcing(r);
   phase_small(r, nsstp, dts);
   step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false);

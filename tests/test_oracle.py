@@ -132,3 +132,31 @@ def test_mlp_oracle_gradient_finite_differences():
             assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
     finally:
         M.ROUND = True
+
+
+def test_smagorinsky_fp32_vs_fp64_and_active(oracle_lib):
+    """Dry large steps with Smagorinsky turbulence (tubopt=1) in neutral
+    stratification: float and double agree to a small fraction of each
+    field's range, and the turbulence changes the result."""
+    from cress_b200 import cases
+    dx, dz = 500.0, 300.0
+    case = cases.dry_case(24, 20, 16, dx, dz, sthopt=1, seed=3, vspbar=0.005, dthdz=0.0, noise=0.5)
+    ni, nj, nk = case["dims"]
+    zph = case["zph"]
+    out = {}
+    for tub, prec in ((1, 32), (1, 64), (0, 32)):
+        cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=1, vspbar=0.005,
+                   botbar=0.6 * zph[nk - 1], tubopt=tub)
+        past = [a.copy() for a in case["level"]]
+        now = [a.copy() for a in case["level"]]
+        oracle_lib.dry_steps(cfg, case["base"], zph, past, now, 3, 2.0, 0.25, start=True, prec=prec)
+        out[(tub, prec)] = now
+    sl = (slice(0, nk - 1), slice(2, nj - 1), slice(2, ni - 1))
+    changed = 0.0
+    for n in range(5):
+        a, b, c = out[(1, 32)][n][sl], out[(1, 64)][n][sl], out[(0, 32)][n][sl]
+        scale = float(np.abs(b).max()) + 1e-12
+        assert np.isfinite(a).all()
+        assert float(np.abs(a - b).max()) <= 1e-3 * scale
+        changed = max(changed, float(np.abs(a - c).max()) / scale)
+    assert changed > 1e-3
