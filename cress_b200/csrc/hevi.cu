@@ -69,9 +69,12 @@ struct HeviLayout {
       4u * BX * (R::u + R::v + R::w + R::p + R::uf + R::vf + R::wf + R::pf);
   static constexpr int t3h_floats = r128((TY + 2) * BX);
   __host__ __device__ static size_t cols_floats(int nk) { return (size_t)((C_NFIELDS * (nk + 1) + 31) / 32 * 32); }
+  // ring, t3h (two buffers), columns, mbarriers, the elimination factors
+  // (aa, cp as double, rr as float) and the column store
   __host__ __device__ static size_t bytes(int nk) {
-    return 4 * ((size_t)S * stage + t3h_floats + cols_floats(nk)) + 8 * (size_t)S +
-           (GS ? 0 : sizeof(FT) * (size_t)(nk - 4) * (kHeviTX * TY));
+    return 4 * ((size_t)S * stage + 2 * (size_t)t3h_floats + cols_floats(nk)) + 8 * (size_t)S +
+           16 * (size_t)(nk + 2) + (GS ? 0 : sizeof(FT) * (size_t)(nk - 4) * (kHeviTX * TY)) +
+           4 * (size_t)(nk + 2);
   }
 };
 
@@ -94,12 +97,19 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
 
   extern __shared__ __align__(1024) float smem[];
   float* ring = smem;
-  float* t3h = ring + S * L::stage;                // [(TY+2)][BX], rows from j0-1, x from i0-2
-  float* cols = t3h + L::t3h_floats;               // [C_NFIELDS][nk+1]
+  float* t3hb = ring + S * L::stage;               // 2 x [(TY+2)][BX], rows from j0-1, x from i0-2
+  float* cols = t3hb + 2 * L::t3h_floats;          // [C_NFIELDS][nk+1]
   uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
-  FT* fcol = reinterpret_cast<FT*>(bars + S);  // [(nk-4)][NT]
+  double* thd = reinterpret_cast<double*>(bars + S);   // aa[k] then cp[k], k = 0..nk+1
+  FT* fcol = reinterpret_cast<FT*>(thd + 2 * (nk + 2));  // [(nk-4)][NT]
+  float* thr = reinterpret_cast<float*>(fcol) + (GS ? 0 : (sizeof(FT) / 4) * (size_t)(nk - 4) * NT);  // rr[k]
 
   for (int n = tid; n < C_NFIELDS * ncol; n += NT) cols[n] = __ldg(a.col + n);
+  for (int n = tid; n <= nk + 1; n += NT) {
+    thd[n] = __ldg(a.thom_aa + n);
+    thd[nk + 2 + n] = __ldg(a.thom_cp + n);
+    thr[n] = __ldg(a.thom_rr + n);
+  }
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -146,11 +156,10 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   long long id = g.at(i, j, 2);
 
   for (int k = 2; k <= nk - 2; ++k, id += plane) {
-    __syncthreads();  // the previous level's stage and t3h are no longer read
-    if (tid == 0 && k + S - 1 <= klast) {
-      fence_proxy_async_smem();
-      issue(k + S - 1);
-    }
+    // One barrier per level: t3h alternates between two buffers, and the
+    // stage of level k-1 is refilled only after this level's barrier, when
+    // every thread has finished level k-1.
+    float* t3h = t3hb + (k & 1) * L::t3h_floats;
     const int s0 = (k - 2) % S, s1 = (k - 1) % S;
     if (!fail) fail = !mbar_wait(&bars[s0], ((k - 2) / S) & 1);
     if (!fail) fail = !mbar_wait(&bars[s1], ((k - 1) / S) & 1);
@@ -193,6 +202,10 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       t3h[hy * BX + hx] = t3h_of(div3d_at(hx, hy), P[hy * BX + hx]);
     }
     __syncthreads();
+    if (tid == 0 && k + S - 1 <= klast) {
+      fence_proxy_async_smem();
+      issue(k + S - 1);
+    }
 
     // stepuv.f90:294,304 with pgrad.f90:379,389 on the four faces of the column
     const float tc = t3h[oy * BX + ox];
@@ -241,7 +254,7 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
         if (a.buyopt == 1) fw = fw + (wb8s_prev + wb8s);                                      // buoywsi.f90:205
         const float wrhs = wk + dts * fw * cols[C_IRST8W * ncol + k];                          // stepwi.f90:325
         // gaussel.f90:189-240 in double with the 1-D factors
-        const double rr = (double)__ldg(a.thom_rr + k), aa = __ldg(a.thom_aa + k);
+        const double rr = (double)thr[k], aa = thd[k];
         const double f = (k == 3) ? (double)wrhs * aa : ((double)wrhs - rr * fprev) * aa;
         if constexpr (GS) a.w_new[id] = (float)f;
         else fcol[(k - 3) * NT + tid] = (FT)f;
@@ -275,14 +288,20 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     double wupd = 0.0;        // w(k+1) as double for the recurrence
     float w3 = 0.f, wkend = 0.f, p2 = 0.f, p3 = 0.f, pkend = 0.f;
     long long idk = g.at(i, j, nk - 2);
-    float fpn = a.p_new[idk], pon = a.p_old[idk];
+    // loads run two levels ahead of their use (parked fp, old p', parked f)
+    float fp0 = a.p_new[idk], po0 = a.p_old[idk], fp1 = 0.f, po1 = 0.f;
+    float f0 = GS ? a.w_new[idk] : 0.f, f1 = 0.f;
+    if (nk - 3 >= 2) { fp1 = a.p_new[idk - plane]; po1 = a.p_old[idk - plane]; }
+    if (GS && nk - 3 >= 3) f1 = a.w_new[idk - plane];
     for (int k = nk - 2; k >= 2; --k, idk -= plane) {
-      const float fpb = fpn, po = pon;
-      if (k > 2) { fpn = a.p_new[idk - plane]; pon = a.p_old[idk - plane]; }
+      const float fpb = fp0, po = po0, fg = f0;
+      fp0 = fp1; po0 = po1; f0 = f1;
+      if (k - 2 >= 2) { fp1 = a.p_new[idk - 2 * plane]; po1 = a.p_old[idk - 2 * plane]; }
+      if (GS && k - 2 >= 3) f1 = a.w_new[idk - 2 * plane];
       float wk;
       if (k >= 3) {
-        const double f = GS ? (double)a.w_new[idk] : (double)fcol[(k - 3) * NT + tid];
-        const double wd = (k == nk - 2) ? f : f - __ldg(a.thom_cp + k) * wupd;                  // gaussel.f90:254
+        const double f = GS ? (double)fg : (double)fcol[(k - 3) * NT + tid];
+        const double wd = (k == nk - 2) ? f : f - thd[nk + 2 + k] * wupd;                     // gaussel.f90:254
         wupd = wd;
         wk = (float)wd;
         if (edge) store_periodic(a.w_new, g, STAG_S, i, j, k, wk);
@@ -344,16 +363,16 @@ int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
 
 }  // namespace
 
-// Tile ids.  0 (the default) and 7: 32 x 8 columns per block, the
-// eliminated right-hand sides parked (float) in the new w array; 6 and 8:
-// the same with 32 x 4 and 32 x 2.  1, 2 and 9 keep them in shared memory
-// as float (32 x 2, 32 x 8, 32 x 4); 3-5 as double (both recurrences
-// always run in double).
+// Tile ids.  0 (the default): 32 x 4 columns per block, 4-stage ring, the
+// eliminated right-hand sides parked (float) in the new w array; 6: the
+// same with a 5-stage ring; 7 and 8: 32 x 8 and 32 x 2.  1, 2 and 9 keep
+// them in shared memory as float (32 x 2, 32 x 8, 32 x 4); 3-5 as double
+// (both recurrences always run in double).
 int hevi_tile_rows(int tile) {
   switch (tile) {
     case 1: case 4: case 8: return 2;
-    case 3: case 6: case 9: return 4;
-    default: return 8;
+    case 2: case 5: case 7: return 8;
+    default: return 4;
   }
 }
 
@@ -364,10 +383,11 @@ int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaS
     case 3: return launch_t<4, 5, double>(a, maps, st);
     case 4: return launch_t<2, 6, double>(a, maps, st);
     case 5: return launch_t<8, 4, double>(a, maps, st);
-    case 6: return launch_t<4, 4, float, true>(a, maps, st);
+    case 6: return launch_t<4, 5, float, true>(a, maps, st);
+    case 7: return launch_t<8, 5, float, true>(a, maps, st);
     case 8: return launch_t<2, 6, float, true>(a, maps, st);
     case 9: return launch_t<4, 4, float>(a, maps, st);
-    default: return launch_t<8, 4, float, true>(a, maps, st);
+    default: return launch_t<4, 4, float, true>(a, maps, st);
   }
 }
 
