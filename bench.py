@@ -177,9 +177,9 @@ def learned_leg(args, s, stream, nsstp, cells, plain_ms, barrier, max_over_ranks
                 s.put_field(n, lvl, next(it))
         s.put_precip(prec0)
 
-    def run(learned_on):
+    def run(learned_on, chunk=0):
         restore()
-        s.set_learned_micro(m if learned_on else None, chunk=1 << 20, resid_tol=0.5)
+        s.set_learned_micro(m if learned_on else None, chunk=chunk, resid_tol=0.5)
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -193,6 +193,7 @@ def learned_leg(args, s, stream, nsstp, cells, plain_ms, barrier, max_over_ranks
         return t, out, s.get_precip(), stats
 
     tp, qp, pp, _ = run(False)
+    tc, _, _, _ = run(True, chunk=1 << 20)
     tl, ql, pl, (ncl, nfb) = run(True)
     s.set_learned_micro(None)
     m.close()
@@ -203,6 +204,7 @@ def learned_leg(args, s, stream, nsstp, cells, plain_ms, barrier, max_over_ranks
     acc_l = float(pl[:, 1].sum())
     return {"value": cells / (tl * 1e-3), "unit": "cell-updates/s", "ms_per_step": tl,
             "plain_ms_per_step_same_steps": tp, "speedup_vs_plain": tp / tl,
+            "inference": "fused", "chunked_ms_per_step": tc,
             "mlp_cells": ncl, "fallback_cells": nfb,
             "precip_accum_rel_diff": abs(acc_l - acc_p) / (abs(acc_p) + 1e-30),
             "hydrometeor_rms_rel": rms,

@@ -496,7 +496,8 @@ int Ctx::cloudphy(float dtb, float thresq) {
     }
   }
   if (mlp) {
-    rc = launch_cloudphy_learned(m, lev[CRESS_W][CRESS_NOW], mlp, lb, resid_tol, stream, &launches);
+    rc = lb.fused ? launch_cloudphy_fused(m, lev[CRESS_W][CRESS_NOW], mlp, lb, resid_tol, stream, &launches)
+                  : launch_cloudphy_learned(m, lev[CRESS_W][CRESS_NOW], mlp, lb, resid_tol, stream, &launches);
     if (rc) return set_error(rc, "learned cloudphy failed: %s", cudaGetErrorString(cudaGetLastError()));
     return CRESS_OK;
   }
@@ -884,9 +885,17 @@ int cress_set_learned_micro(cress_ctx* ctx, cress_mlp* mh, int chunk, float resi
   Mlp* m = reinterpret_cast<Mlp*>(mh);
   if (c->cfg.cphopt != 3) return set_error(CRESS_E_STATE, "cress_set_learned_micro: context is not cphopt=3");
   if (m->device != c->device) return set_error(CRESS_E_ARG, "MLP and context live on different devices");
-  if (chunk <= 0) chunk = 1 << 20;
-  chunk = (chunk + 127) / 128 * 128;
   if (!(resid_tol > 0.f)) return set_error(CRESS_E_ARG, "resid_tol must be positive");
+  // chunk 0: the fused kernel over all cells (the fallback list can hold
+  // every cell); chunk > 0: chunks of that many cells through the GEMMs
+  const bool fused = chunk <= 0;
+  const long long ncell = (long long)(c->g.ni - 3) * (c->g.nj - 3) * (c->g.nk - 1);
+  if (fused) {
+    if (ncell > 0x7FFFFFFFLL) return set_error(CRESS_E_ARG, "domain too large for the fused learned form");
+    chunk = (int)ncell;
+  } else {
+    chunk = (chunk + 127) / 128 * 128;
+  }
   auto al = [&](size_t bytes) -> void* {
     void* p = nullptr;
     if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
@@ -894,17 +903,20 @@ int cress_set_learned_micro(cress_ctx* ctx, cress_mlp* mh, int chunk, float resi
     return p;
   };
   LearnedBuffers& L = c->lb;
+  L.fused = fused;
   L.chunk = chunk;
-  L.xb = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpK1));
-  L.h0 = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpH));
-  L.h1 = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpH));
-  L.y = static_cast<float*>(al(sizeof(float) * (size_t)chunk * kMlpN4));
-  L.env = static_cast<unsigned char*>(al((size_t)chunk));
+  if (!fused) {
+    L.xb = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpK1));
+    L.h0 = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpH));
+    L.h1 = static_cast<__nv_bfloat16*>(al(sizeof(__nv_bfloat16) * (size_t)chunk * kMlpH));
+    L.y = static_cast<float*>(al(sizeof(float) * (size_t)chunk * kMlpN4));
+    L.env = static_cast<unsigned char*>(al((size_t)chunk));
+  }
   L.fb_list = static_cast<int*>(al(sizeof(int) * (size_t)chunk));
   L.fb_count = static_cast<int*>(al(sizeof(int)));
   L.stats = static_cast<unsigned long long*>(al(2 * sizeof(unsigned long long)));
   L.err = static_cast<int*>(al(sizeof(int)));
-  if (!L.xb || !L.h0 || !L.h1 || !L.y || !L.env || !L.fb_list || !L.fb_count || !L.stats || !L.err) {
+  if ((!fused && (!L.xb || !L.h0 || !L.h1 || !L.y || !L.env)) || !L.fb_list || !L.fb_count || !L.stats || !L.err) {
     c->free_learned();
     return set_error(CRESS_E_CUDA, "cudaMalloc of the learned-microphysics buffers failed");
   }

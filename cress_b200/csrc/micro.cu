@@ -277,6 +277,7 @@ int launch_satadjst(const SatArgs& a, cudaStream_t st) {
 
 // Learned-form kernels (they use this file's Koenig tables and loaders).
 #include "micro_learned.cuh"
+#include "mlp_fused.cuh"
 
 namespace cress {
 
@@ -338,6 +339,47 @@ int launch_cloudphy_learned(const MicroArgs& a, const float* w, Mlp* m, const Le
   dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 1);
   k_micro_fall<<<gr2, b2, 0, st>>>(a);
   ++*launches;
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+// s_cloudphy with the MLP in place of the process rates, fused: one
+// persistent kernel over all cells (features, 4 GEMMs, application), the
+// plain process rates on the rejected cells, the plain sedimentation.
+int launch_cloudphy_fused(const MicroArgs& a, const float* w, Mlp* m, const LearnedBuffers& L, float resid_tol,
+                          cudaStream_t st, long long* launches) {
+  k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
+  FusedMaps maps;
+  int rc;
+  if ((rc = encode_bf16_map(&maps.w1, m->w.w1t, kMlpH, kMlpK1, kMlpK1, kMlpH)) ||
+      (rc = encode_bf16_map(&maps.w2, m->w.w2t, kMlpH, kMlpH, kMlpH, kMlpH)) ||
+      (rc = encode_bf16_map(&maps.w3, m->w.w3t, kMlpH, kMlpH, kMlpH, kMlpH)) ||
+      (rc = encode_bf16_map(&maps.w4, m->w.w4t, kMlpN4, kMlpH, kMlpH, kMlpN4)))
+    return rc;
+  if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmem) != cudaSuccess)
+    return CRESS_E_CUDA;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  FusedArgs p{};
+  p.w = w;
+  p.norm = m->norm_d;
+  p.params = m->params;
+  p.ncell = (long long)(a.g.ni - 3) * (a.g.nj - 3) * (a.g.nk - 1);
+  p.resid_tol = resid_tol;
+  p.fb_list = L.fb_list;
+  p.fb_count = L.fb_count;
+  p.fb_cap = L.chunk;
+  p.stats = L.stats;
+  p.err = L.err;
+  cudaMemsetAsync(L.fb_count, 0, sizeof(int), st);
+  const long long ntiles = (p.ncell + kFusedTile - 1) / kFusedTile;
+  const int grid = (int)(ntiles < nsm ? ntiles : nsm);
+  k_mlp_fused<<<grid, kFusedThreads, kFusedSmem, st>>>(maps, a, p);
+  k_micro_src_list<<<nsm * 4, 128, 0, st>>>(a, 0, L.fb_list, L.fb_count, L.chunk);
+  dim3 b2(32, 4, 1);
+  dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 1);
+  k_micro_fall<<<gr2, b2, 0, st>>>(a);
+  *launches += 4;
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 

@@ -54,7 +54,8 @@ int launch_moist_post(const MoistPostArgs& a, cudaStream_t st);
 // Learned form of the process-rate part (the MLP of mlp.cu).
 struct Mlp;
 struct LearnedBuffers {
-  int chunk = 0;                  // cells per inference chunk (multiple of 128)
+  bool fused = false;             // one persistent fused kernel (fb_list holds every cell)
+  int chunk = 0;                  // cells per inference chunk (multiple of 128), chunked path
   __nv_bfloat16* xb = nullptr;    // [chunk][64] standardized inputs
   __nv_bfloat16* h0 = nullptr;    // [chunk][256] activations (ping)
   __nv_bfloat16* h1 = nullptr;    // [chunk][256] activations (pong)
@@ -67,6 +68,8 @@ struct LearnedBuffers {
 };
 int launch_cloudphy_learned(const MicroArgs& a, const float* w, Mlp* m, const LearnedBuffers& L, float resid_tol,
                             cudaStream_t st, long long* launches);
+int launch_cloudphy_fused(const MicroArgs& a, const float* w, Mlp* m, const LearnedBuffers& L, float resid_tol,
+                          cudaStream_t st, long long* launches);
 int launch_collect_tuples(const MicroArgs& a, const float* w, Mlp* m, int stride, float keep_zero,
                           unsigned long long seed, unsigned long long* count_d, cudaStream_t st);
 

@@ -185,70 +185,78 @@ struct ApplyArgs {
   unsigned long long* stats;   // [0] cells done by the MLP, [1] fallbacks
 };
 
-// Apply the predicted tendencies to the future level with positivity and
-// water conservation; cells outside the envelope or failing the residual
-// check go to the fallback list.
+// Apply the network's outputs ys (standardized) for interior cell n to the
+// future level, with positivity and water conservation: hydrometeor losses
+// are capped at what is present, vapour closes the water budget (the
+// network's own vapour change must agree within resid_tol), gains shrink
+// if vapour would go negative, theta' follows from the latent heats (lv,
+// lf at the cell's temperature, as in srcblk) and adjstni keeps the
+// numbers consistent.  Returns false (nothing written) when the cell must
+// run the plain process rates instead.
+__device__ inline bool mlp_apply_cell(const MicroArgs& a, long long n, const float* ys, bool ok, const float* norm,
+                                      float resid_tol) {
+  float d[kMlpOut];
+#pragma unroll
+  for (int m = 0; m < kMlpOut; ++m) {
+    const float yv = ys[m] * norm[kNormYstd + m] + norm[kNormYmean + m];
+    d[m] = tgt_inv(yv, m);
+    ok &= isfinite(d[m]);
+  }
+  if (!ok) return false;
+  int k;
+  const long long id = cell_index(a.g, n, k);
+  MCell c;
+  load_cell(a, id, k, c);
+  load_future(a, id, c);
+  float q[6] = {c.qvf, c.qcf, c.qrf, c.qif, c.qsf, c.qgf};
+  float gain = 0.f, loss = 0.f;
+#pragma unroll
+  for (int m = 1; m < 6; ++m) {
+    d[m] = fmaxf(d[m], -q[m]);
+    if (d[m] > 0.f) gain += d[m]; else loss -= d[m];
+  }
+  const float dqv_pred = d[0];
+  if (q[0] + loss - gain < 0.f && gain > 0.f) {
+    const float s = (q[0] + loss) / gain;
+#pragma unroll
+    for (int m = 1; m < 6; ++m)
+      if (d[m] > 0.f) d[m] *= s;
+    gain = q[0] + loss;
+  }
+  d[0] = loss - gain;
+  const float scale = fabsf(dqv_pred) + gain + loss;
+  if (fabsf(dqv_pred - d[0]) > resid_tol * scale + 1.e-10f) return false;
+  const float t = (c.ptbr + c.ptpp) * c.pi;
+  const float tcel = t - 273.16f;
+  const float lv = 2.50078e6f * expf((.167f + 3.67e-4f * t) * logf(273.16f / t));   // as srcblk
+  const float lf = 3.34e5f + (4.218e3f - 2.106e3f) * tcel;
+  const float cppiv = 1.f / (1004.f * c.pi);
+  a.ptpf[id] = c.ptpf + (lv * (-d[0]) + lf * (d[3] + d[4] + d[5])) * cppiv;
+  a.qvf[id] = q[0] + d[0];
+  a.qcf[id] = q[1] + d[1];
+  a.qrf[id] = q[2] + d[2];
+  const float qi = q[3] + d[3], qs = q[4] + d[4], qg = q[5] + d[5];
+  float nci = fmaxf(c.ncif + d[6], 0.f), ncs = fmaxf(c.ncsf + d[7], 0.f), ncg = fmaxf(c.ncgf + d[8], 0.f);
+  adjstni_cell(c.rbr, c.rbv, qi, qs, qg, nci, ncs, ncg);
+  a.qif[id] = qi; a.qsf[id] = qs; a.qgf[id] = qg;
+  a.nif[id] = nci; a.nsf[id] = ncs; a.ngf[id] = ncg;
+  return true;
+}
+
+// Apply one chunk's network outputs; cells outside the envelope or failing
+// the residual check go to the fallback list.
 __global__ void __launch_bounds__(128) k_mlp_apply(const MicroArgs a, const ApplyArgs p) {
   const Grid g = a.g;
   const long long ncell = (long long)(g.ni - 3) * (g.nj - 3) * (g.nk - 1);
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= p.cnt || p.n0 + r >= ncell) return;
   const long long n = p.n0 + r;
-  bool ok = p.env[r] != 0;
-  float d[kMlpOut];
-#pragma unroll
-  for (int m = 0; m < kMlpOut; ++m) {
-    const float yv = p.y[(size_t)r * kMlpN4 + m] * p.norm[kNormYstd + m] + p.norm[kNormYmean + m];
-    d[m] = tgt_inv(yv, m);
-    ok &= isfinite(d[m]);
-  }
-  int k;
-  const long long id = cell_index(g, n, k);
-  if (ok) {
-    MCell c;
-    load_cell(a, id, k, c);
-    load_future(a, id, c);
-    float q[6] = {c.qvf, c.qcf, c.qrf, c.qif, c.qsf, c.qgf};
-    // positivity of the hydrometeors
-    float gain = 0.f, loss = 0.f;
-#pragma unroll
-    for (int m = 1; m < 6; ++m) {
-      d[m] = fmaxf(d[m], -q[m]);
-      if (d[m] > 0.f) gain += d[m]; else loss -= d[m];
-    }
-    // vapour closes the water budget; the prediction must agree with it
-    const float dqv_pred = d[0];
-    if (q[0] + loss - gain < 0.f && gain > 0.f) {
-      const float s = (q[0] + loss) / gain;
-#pragma unroll
-      for (int m = 1; m < 6; ++m)
-        if (d[m] > 0.f) d[m] *= s;
-      gain = q[0] + loss;
-    }
-    d[0] = loss - gain;
-    const float scale = fabsf(dqv_pred) + gain + loss;
-    if (fabsf(dqv_pred - d[0]) > p.resid_tol * scale + 1.e-10f) ok = false;
-    if (ok) {
-      const float t = (c.ptbr + c.ptpp) * c.pi;
-      const float tcel = t - 273.16f;
-      const float lv = 2.50078e6f * expf((.167f + 3.67e-4f * t) * logf(273.16f / t));   // as srcblk
-      const float lf = 3.34e5f + (4.218e3f - 2.106e3f) * tcel;
-      const float cppiv = 1.f / (1004.f * c.pi);
-      a.ptpf[id] = c.ptpf + (lv * (-d[0]) + lf * (d[3] + d[4] + d[5])) * cppiv;
-      a.qvf[id] = q[0] + d[0];
-      a.qcf[id] = q[1] + d[1];
-      a.qrf[id] = q[2] + d[2];
-      const float qi = q[3] + d[3], qs = q[4] + d[4], qg = q[5] + d[5];
-      float nci = fmaxf(c.ncif + d[6], 0.f), ncs = fmaxf(c.ncsf + d[7], 0.f), ncg = fmaxf(c.ncgf + d[8], 0.f);
-      adjstni_cell(c.rbr, c.rbv, qi, qs, qg, nci, ncs, ncg);
-      a.qif[id] = qi; a.qsf[id] = qs; a.qgf[id] = qg;
-      a.nif[id] = nci; a.nsf[id] = ncs; a.ngf[id] = ncg;
-      atomicAdd(p.stats, 1ull);
-      return;
-    }
+  if (mlp_apply_cell(a, n, p.y + (size_t)r * kMlpN4, p.env[r] != 0, p.norm, p.resid_tol)) {
+    atomicAdd(p.stats, 1ull);
+    return;
   }
   const int slot = atomicAdd(p.fb_count, 1);
-  if (slot < p.fb_cap) p.fb_list[slot] = (int)(n - p.n0) + 0;   // relative to the chunk
+  if (slot < p.fb_cap) p.fb_list[slot] = (int)(n - p.n0);   // relative to the chunk
   atomicAdd(p.stats + 1, 1ull);
 }
 

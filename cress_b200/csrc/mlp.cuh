@@ -56,4 +56,8 @@ struct GemmArgs {
 };
 int gemm_bf16(const bf16* A, int lda, const bf16* B, int ldb, const GemmArgs& g, cudaStream_t st);
 
+// Tensor map of a row-major [rows][cols] BF16 matrix (leading dimension ld)
+// with boxes of box_rows x 64 and the 128-byte swizzle.
+int encode_bf16_map(CUtensorMap* m, const bf16* base, int rows, int cols, int ld, int box_rows);
+
 }  // namespace cress

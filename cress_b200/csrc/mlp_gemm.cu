@@ -232,6 +232,10 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 
 
 }  // namespace
 
+int encode_bf16_map(CUtensorMap* m, const bf16* base, int rows, int cols, int ld, int box_rows) {
+  return encode_bf16(m, base, rows, cols, ld, box_rows);
+}
+
 int gemm_bf16(const bf16* A, int lda, const bf16* B, int ldb, const GemmArgs& g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.M % kBM || g.K % kBK || g.N % 64)
     return set_error(CRESS_E_ARG, "gemm: M=%d N=%d K=%d (need M%%128, N%%64, K%%64 == 0)", g.M, g.N, g.K);

@@ -231,8 +231,10 @@ int cress_mlp_fit_norm(cress_mlp* m);
  * losses (may be NULL) receives each step's loss. */
 int cress_mlp_train(cress_mlp* m, int steps, int batch, float lr, unsigned long long seed, float* losses);
 /* Use the MLP for the process rates in the context's s_cloudphy (NULL
- * returns to the plain scheme).  chunk: cells per inference batch (0 =
- * 2^20); resid_tol: relative tolerance of the water-budget residual. */
+ * returns to the plain scheme).  chunk 0: one fused persistent kernel over
+ * all cells (activations stay on chip); chunk > 0: batches of that many
+ * cells through separate GEMM launches.  resid_tol: relative tolerance of
+ * the water-budget residual. */
 int cress_set_learned_micro(cress_ctx* ctx, cress_mlp* m, int chunk, float resid_tol);
 int cress_learned_stats(cress_ctx* ctx, long long* mlp_cells, long long* fallback_cells);
 /* Sample training tuples of the plain scheme on every following

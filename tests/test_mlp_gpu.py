@@ -146,3 +146,42 @@ def test_learned_form_trained_on_plain_tuples(cress, oracle_lib):
         assert np.isfinite(s.get_field(name, cress.NOW)).all(), name
     s.close()
     m.close()
+
+
+def test_fused_inference_matches_chunked(cress, oracle_lib):
+    """The fused persistent kernel (features, four tensor-core GEMMs with the
+    activations in shared memory, application) gives the same large steps
+    as the chunked path through separate GEMM launches."""
+    m = cress.Mlp(seed=8)
+    m.reserve(200000)
+    s, dims = _moist_solver(cress, oracle_lib, 4)
+    s.set_tuple_sampling(m, stride=1, keep_zero=0.2, seed=2)
+    s.large_step(0, 2.5, 10, 0.5)
+    s.large_step(5000, 5.0, 10, 1.0)
+    s.set_tuple_sampling(None)
+    s.close()
+    m.fit_norm()
+    m.train(200, batch=4096, lr=1e-3, seed=1)
+    out = []
+    for chunk in (16384, 0):
+        s, dims = _moist_solver(cress, oracle_lib, 4)
+        s.set_learned_micro(m, chunk=chunk, resid_tol=0.5)
+        s.large_step(0, 2.5, 10, 0.5)
+        s.large_step(5000, 5.0, 10, 1.0)
+        out.append(([s.get_field(n, cress.NOW) for n in NAMES], s.learned_stats(), s.get_precip()))
+        s.close()
+    m.close()
+    (a, sa, pa), (b, sb, pb) = out
+    ni, nj, nk = dims
+    ncell = (ni - 3) * (nj - 3) * (nk - 1)
+    assert sum(sa) == sum(sb) == 2 * ncell
+    # the two paths round the same products in the same order; a cell at the
+    # residual threshold may still take the other branch
+    assert abs(sa[1] - sb[1]) <= 2 + ncell // 1000, (sa, sb)
+    for name, x, y in zip(NAMES, a, b):
+        assert np.isfinite(y).all(), name
+        scale = float(np.abs(x).max()) + 1e-30
+        err = np.abs(x - y)
+        assert float((err <= 1e-5 * scale).mean()) >= 0.999, name
+        assert float(err.max()) <= 5e-2 * scale, name
+    assert float(np.abs(pa - pb).max()) <= 1e-3 * (float(np.abs(pa).max()) + 1e-30)
