@@ -401,7 +401,16 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
     m.smtopt = cfg.smtopt; m.vspopt = cfg.vspopt; m.sthopt = cfg.sthopt; m.ksp0 = ksp0;
     m.vsp_qv = on(5); m.vsp_q = on(6);
     m.rkv = f.rkv; m.cpriv = cpriv;
-    if ((rc = launch_moist_scalars(m, stream))) return set_error(rc, "moist scalar launch failed");
+    m.err = err_d;
+    MoistMaps mm;
+    for (int n = 0; n < kMoistN; ++n)
+      if ((rc = tmap(m.s[n], ScalarRows::s, &mm.s[n])) || (rc = tmap(m.sp[n], ScalarRows::s, &mm.sp[n]))) return rc;
+    if ((rc = tmap(m.u, ScalarRows::u, &mm.u)) || (rc = tmap(m.v, ScalarRows::v, &mm.v)) ||
+        (rc = tmap(m.w, ScalarRows::w, &mm.w)))
+      return rc;
+    if (m.rkv && (rc = tmap(m.rkv, ScalarRows::r, &mm.rkv))) return rc;
+    if (!m.rkv) mm.rkv = mm.w;
+    if ((rc = launch_moist_scalars(m, mm, stream))) return set_error(rc, "moist scalar launch failed");
     ++launches;
     if ((rc = cloudphy(dtb, cfg.thresq))) return rc;
   }

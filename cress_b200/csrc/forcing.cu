@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "forcing.cuh"
 #include "hevi.cuh"
+#include "stencil.cuh"
 #include "turb.cuh"
 
 namespace cress {
@@ -29,62 +30,9 @@ constexpr float kEpsva = .622f;   // rd/rv, comphy.f90:79
 
 __device__ __forceinline__ float ld(const float* f, long long idx) { return __ldg(f + idx); }
 
-// 4th-order smoothing increments (smoo4s.f90:199-296 and its u/v/w/p
-// variants) around `id`: A(dx,dy,dz) returns the smoothed quantity at an
-// offset.  wlev: the field sits on w levels (vertical ghost rule at nk).
-template <class FA>
-__device__ __forceinline__ float smooth_into(float frc, int smtopt, float smhcoe, float smvcoe, int k,
-                                             int kmin, int kmax, const FA& A) {
-  const float a0 = A(0, 0, 0);
-  auto t1 = [&](int x) { return (A(x + 1, 0, 0) + A(x - 1, 0, 0)) - 2.f * A(x, 0, 0); };
-  auto t2 = [&](int y) { return (A(0, y + 1, 0) + A(0, y - 1, 0)) - 2.f * A(0, y, 0); };
-  auto t3 = [&](int z) {
-    int kk = k + z;
-    if (kk < kmin) kk = kmin;   // tmp3(k=kmin-1) = tmp3(kmin)
-    if (kk > kmax) kk = kmax;   // tmp3(kmax+1) = tmp3(kmax)
-    const int d = kk - k;
-    return (A(0, 0, d + 1) + A(0, 0, d - 1)) - 2.f * A(0, 0, d);
-  };
-  (void)a0;
-  const float t10 = t1(0), t20 = t2(0), t30 = t3(0);
-  frc = frc + smhcoe * (t10 + t20) + smvcoe * t30;
-  if (smtopt % 10 == 2) {
-    frc = frc + smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1))));
-  } else {
-    frc = frc + (smvcoe * (t30 - (t3(1) + t3(-1))) +
-                 smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1)))));
-  }
-  return frc;
-}
-
 // blockIdx.z runs over k = 2..nk-1 within one output group, then over the
 // groups (0: ufrc, 1: vfrc, 2: wfrc, 3: pfrc and theta'), so the four
 // stencils of a point run in different threads.
-// Turbulent mixing of a scalar S (the full field at t-dt, S(p, kk)) at the
-// point id of level k: s_eddydif / s_kh8uv diffusivities from the eddy
-// viscosity (rkh = priv*rkv/jcb, rkh8u = rkh(i-1)+rkh(i), rkv8w =
-// (rkh(k-1)+rkh(k))/2; eddydif.f90:154-260, kh8uv.f90:211-230) and the
-// flux divergence of s_turbflx / s_turbs (turbflx.f90:236-352,
-// turbs.f90:189-232), added to frc.
-template <class FS>
-__device__ __forceinline__ float turb_scalar(float frc, const float* rkv, const float* col, int nc, long long id,
-                                             int k, long long px, long long pl, float cpriv, float dxiv, float dyiv,
-                                             float dziv, const FS& S) {
-  auto C = [&](int f, int kk) { return __ldg(col + f * nc + kk); };
-  auto RKH = [&](long long p, int kk) { return cpriv * __ldg(rkv + p) / C(C_JCB, kk); };
-  const float jc = C(C_JCB, k);
-  const float dxv05 = .5f * dxiv, dyv05 = .5f * dyiv;
-  auto JS = [&](long long p) { return S(p, k) * jc; };
-  auto H1 = [&](long long p) { return (RKH(p - 1, k) + RKH(p, k)) * (JS(p) - JS(p - 1)) * dxv05; };
-  auto H2 = [&](long long p) { return (RKH(p - px, k) + RKH(p, k)) * (JS(p) - JS(p - px)) * dyv05; };
-  auto H3 = [&](long long p, int kk) {
-    return (.5f * (RKH(p - pl, kk - 1) + RKH(p, kk))) * (S(p, kk) - S(p - pl, kk - 1)) * dziv;
-  };
-  const float j8u = C(C_JCB8U, k), j8v = C(C_JCB8V, k);
-  return frc + ((H3(id + pl, k + 1) - H3(id, k)) * dziv +
-                ((j8u * H1(id + 1) - j8u * H1(id)) * dxiv + (j8v * H2(id + px) - j8v * H2(id)) * dyiv));
-}
-
 __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
@@ -324,86 +272,6 @@ __global__ void __launch_bounds__(256) k_force(const ForceArgs a) {
   }
 }
 
-// Forcing and s_steps of the nine moist scalars, one thread per scalar
-// point (i, j = 2..n-2, k = 2..nk-2) and field (blockIdx.z runs over k
-// within a field, then over the fields), so the nine fields are in flight
-// at once; each thread forms its advecting fluxes rst8u*u, rst8v*v,
-// rst8w*wc (shared neighbours come from L1):
-//   sfrc = advs (advs.f90:205-370) + smoo4qv / smoo4s of rbr*(qvp-qvbr) or
-//          rbr*sp (smoo4s.f90:184-296) + vspqv / vsps / vsps0
-//          (vspqv.f90:181-198, vsps.f90:181-198, vsps0.f90:114-124)
-//   sf = sp + sfrc*2dtb/rst, clipped at 0 for the mixing ratios
-//        (steps.f90:590-764), then vbcs at k=1, nk-1 (vbcs.f90:116-132).
-__global__ void __launch_bounds__(256) k_moist_scalars(const MoistScalarArgs a) {
-  const Grid g = a.g;
-  const int ni = g.ni, nj = g.nj, nk = g.nk;
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int n = blockIdx.z / (nk - 3);
-  const int k = 2 + blockIdx.z % (nk - 3);
-  if (i > ni - 2 || j > nj - 2 || n >= kMoistN) return;
-  const long long px = g.px, pl = g.plane;
-  const long long id = g.at(i, j, k);
-  const int nc = nk + 1;
-  auto C = [&](int f, int kk) { return __ldg(a.col + f * nc + kk); };
-  const float oned24 = 1.f / 24.f, fourd3 = 4.f / 3.f;
-  const float dxv24 = oned24 * a.dxiv, dyv24 = oned24 * a.dyiv;
-  const float dxv05n = -.5f * a.dxiv, dyv05n = -.5f * a.dyiv, dzv05n = -.5f * a.dziv;
-  const bool smooth = (a.smtopt % 10 == 2) || (a.smtopt % 10 == 3);
-  // rstuvwc.f90:172-210 fluxes at the faces the stencil touches
-  const float r8u = C(C_RST8U, k), r8v = C(C_RST8V, k);
-  const float fu_m1 = r8u * ld(a.u, id - 1), fu_0 = r8u * ld(a.u, id);
-  const float fu_p1 = r8u * ld(a.u, id + 1), fu_p2 = r8u * ld(a.u, id + 2);
-  const float fv_m1 = r8v * ld(a.v, id - px), fv_0 = r8v * ld(a.v, id);
-  const float fv_p1 = r8v * ld(a.v, id + px), fv_p2 = r8v * ld(a.v, id + 2 * px);
-  auto WC = [&](long long p, int kk) { return a.sthopt ? ld(a.w, p) / C(C_JCB8W, kk) : ld(a.w, p); };
-  const float fw_0 = C(C_RST8W, k) * WC(id, k), fw_1 = C(C_RST8W, k + 1) * WC(id + pl, k + 1);
-  const float rbct5 = .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1));
-  const float rst = C(C_RST, k);
-  const float dtdrst = a.dtb2 / rst;                                     // steps.f90:528
-  {
-    const float* s = a.s[n];
-    const float s0 = ld(s, id);
-    // advs.f90:205-370, 4th-order horizontal, 2nd-order vertical
-    const float t1a = fu_0 * (s0 - ld(s, id - 1)) * dxv05n;
-    const float t1b = fu_p1 * (ld(s, id + 1) - s0) * dxv05n;
-    const float t2a = fv_0 * (s0 - ld(s, id - px)) * dyv05n;
-    const float t2b = fv_p1 * (ld(s, id + px) - s0) * dyv05n;
-    float f = (t1a + t1b) + (t2a + t2b);
-    const float w1a = (fu_m1 + fu_0) * (s0 - ld(s, id - 2)) * dxv24;
-    const float w1b = (fu_p1 + fu_p2) * (ld(s, id + 2) - s0) * dxv24;
-    const float w2a = (fv_m1 + fv_0) * (s0 - ld(s, id - 2 * px)) * dyv24;
-    const float w2b = (fv_p1 + fv_p2) * (ld(s, id + 2 * px) - s0) * dyv24;
-    f = fourd3 * f + ((w1a + w1b) + (w2a + w2b));
-    const float t3a = fw_0 * (s0 - ld(s, id - pl)) * dzv05n;
-    const float t3b = fw_1 * (ld(s, id + pl) - s0) * dzv05n;
-    f = f + (t3a + t3b);
-    const float* sp = a.sp[n];
-    const bool isqv = n == 0;
-    if (smooth) {
-      auto A = [&](int dx, int dy, int dz) {
-        const int kk = k + dz;
-        const float v = ld(sp, id + dx + dy * px + dz * pl);
-        return isqv ? C(C_RBR, kk) * (v - C(C_QVBR, kk)) : C(C_RBR, kk) * v;
-      };
-      f = smooth_into(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
-    }
-    if (a.rkv) {   // forceqv.f90:331-345, forceq.f90:438-452: mixing of the species at t-dt
-      auto S = [&](long long p, int) { return ld(sp, p); };
-      f = turb_scalar(f, a.rkv, a.col, nc, id, k, px, pl, a.cpriv, a.dxiv, a.dyiv, a.dziv, S);
-    }
-    const float spv = ld(sp, id);
-    if (a.vspopt >= 1 && (isqv ? a.vsp_qv : a.vsp_q) && k >= a.ksp0 - 1)
-      f = f - rbct5 * rst * (isqv ? spv - C(C_QVBR, k) : spv);
-    float sf = spv + f * dtdrst;
-    if (n < 6) sf = fmaxf(0.f, sf);
-    float* out = a.sf[n];
-    out[id] = sf;
-    if (k == 2) out[id - pl] = sf;        // vbcs.f90:118
-    if (k == nk - 2) out[id + pl] = sf;   // vbcs.f90:132
-  }
-}
-
 // s_timeflt, SrcOrig/timeflt.f90:335-404 on the interior (ghosts are
 // refilled by k_halo afterwards).
 __global__ void __launch_bounds__(256) k_timeflt(const FilterArgs a) {
@@ -480,13 +348,6 @@ int launch_force(const ForceArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);
   dim3 gr((a.g.ni - 2 + 31) / 32, (a.g.nj - 2 + 7) / 8, (a.g.nk - 2) * 4);
   k_force<<<gr, b, 0, st>>>(a);
-  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
-}
-
-int launch_moist_scalars(const MoistScalarArgs& a, cudaStream_t st) {
-  dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, (a.g.nk - 3) * kMoistN);
-  k_moist_scalars<<<gr, b, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 

@@ -66,8 +66,22 @@ struct MoistScalarArgs {
   int vsp_qv, vsp_q;          // vspvar(6:6), vspvar(7:7)
   const float* rkv;           // eddy viscosity (tubopt=1) or null
   float cpriv;
+  int* err;                   // device error word (a bounded wait gave up)
 };
-int launch_moist_scalars(const MoistScalarArgs& a, cudaStream_t st);
+
+// The scalar kernel stages 32 x kScalarTY tiles of every input level by
+// TMA (boxes kHeviBoxX wide, x from the tile's i0-2): the species at t and
+// t-dt and the eddy viscosity with two rows of y halo, u on the tile rows,
+// v from one row south to two rows north, w on the tile rows.
+constexpr int kScalarTY = 8;
+struct ScalarRows {
+  static constexpr int s = kScalarTY + 4, u = kScalarTY, v = kScalarTY + 3, w = kScalarTY, r = kScalarTY + 4;
+};
+struct MoistMaps {
+  CUtensorMap s[kMoistN], sp[kMoistN];
+  CUtensorMap u, v, w, rkv;   // rkv only with turbulence
+};
+int launch_moist_scalars(const MoistScalarArgs& a, const MoistMaps& maps, cudaStream_t st);
 
 struct FilterArgs {
   Grid g;

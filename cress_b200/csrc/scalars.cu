@@ -1,0 +1,239 @@
+// Forcing and leapfrog step of the nine moist scalars for sm_100a
+// (s_forceqv, s_forceq and their s_steps, cphopt=3):
+//   sfrc = advs (advs.f90:205-370, 4th-order horizontal, 2nd-order vertical)
+//        + smoo4qv / smoo4s of rbr*(qvp-qvbr) or rbr*sp (smoo4s.f90:184-296)
+//        + turbs of sp with the eddy diffusivity (forceqv.f90:331-345,
+//          forceq.f90:438-452; tubopt=1 only)
+//        + vspqv / vsps / vsps0 (vspqv.f90:181-198, vsps.f90:181-198, vsps0.f90:114-124)
+//   sf   = sp + sfrc*2dtb/rst, clipped at 0 for the mixing ratios
+//          (steps.f90:590-764), then vbcs at k = 1, nk-1 (vbcs.f90:116-132).
+//
+// Design (2.5-D).  A block owns a 32 x 8 tile of columns of ONE species
+// and marches k upward.  For every level 1..nk-1 one elected thread issues
+// TMA box loads of the species at t and t-dt (two rows of y halo), u, v, w
+// (and the eddy viscosity) into an S-stage shared-memory ring guarded by
+// mbarriers.  A level stays in the ring while the march needs it (k-2 ..
+// k+2 for the vertical smoothing), so every horizontal neighbour and every
+// vertical neighbour is read from shared memory, and HBM sees each input
+// once per species (the winds once per tile: the nine species of a tile
+// are neighbours in the grid, so their wind boxes are served from L2).
+// The terms are formed in the order of the reference expressions.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "common.cuh"
+#include "forcing.cuh"
+#include "hevi.cuh"
+#include "stencil.cuh"
+#include "tma.cuh"
+
+namespace cress {
+namespace {
+
+__host__ __device__ constexpr int r128f(int n) { return (n + 31) / 32 * 32; }  // floats -> multiple of 128 B
+
+template <int S, bool TURB>
+struct ScLayout {
+  using R = ScalarRows;
+  static constexpr int BX = kHeviBoxX;
+  static constexpr int oS = 0;
+  static constexpr int oSP = oS + r128f(BX * R::s);
+  static constexpr int oU = oSP + r128f(BX * R::s);
+  static constexpr int oV = oU + r128f(BX * R::u);
+  static constexpr int oW = oV + r128f(BX * R::v);
+  static constexpr int oR = oW + r128f(BX * R::w);
+  static constexpr int stage = oR + (TURB ? r128f(BX * R::r) : 0);   // floats per ring stage
+  static constexpr uint32_t tx_bytes = 4u * BX * (2 * R::s + R::u + R::v + R::w + (TURB ? R::r : 0));
+  __host__ __device__ static int cols_floats(int nk) { return r128f(C_NFIELDS_ALL * (nk + 1)); }
+  __host__ __device__ static size_t bytes(int nk) {
+    return 4 * ((size_t)S * stage + (size_t)cols_floats(nk)) + 8 * (size_t)S;
+  }
+};
+
+template <int S, bool TURB>
+__global__ void __launch_bounds__(kHeviTX * kScalarTY)
+k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
+  // level k+2 must have been issued (at k' = k+5-S) before level k waits for it
+  static_assert(S >= 6, "ring too shallow for the k-2..k+2 window");
+  using L = ScLayout<S, TURB>;
+  constexpr int TY = kScalarTY, BX = kHeviBoxX, NT = kHeviTX * TY;
+  const Grid g = a.g;
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const int n = blockIdx.x % kMoistN;                 // species; the nine of a tile are neighbours
+  const int i0 = 2 + (blockIdx.x / kMoistN) * kHeviTX, j0 = 2 + blockIdx.y * TY;
+  const int xb = i0 - 2;                              // box x origin (multiple of 32)
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kHeviTX + tx;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= ni - 2) && (j <= nj - 2);
+  const int nc = nk + 1;
+
+  extern __shared__ __align__(1024) float smem[];
+  float* ring = smem;
+  float* cols = ring + S * L::stage;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
+  for (int q = tid; q < C_NFIELDS_ALL * nc; q += NT) cols[q] = __ldg(a.col + q);
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  // Levels 1..nk-1 are staged; level lv lives in slot (lv-1) % S.
+  const int lmax = nk - 1;
+  const CUtensorMap* ms = &m.s[n];
+  const CUtensorMap* msp = &m.sp[n];
+  auto issue = [&](int lv) {
+    const int s = (lv - 1) % S;
+    float* st = ring + s * L::stage;
+    uint64_t* bar = &bars[s];
+    const int z = lv - 1;
+    mbar_arrive_expect_tx(bar, L::tx_bytes);
+    tma_load_3d(st + L::oS, ms, xb, j0 - 2, z, bar);
+    tma_load_3d(st + L::oSP, msp, xb, j0 - 2, z, bar);
+    tma_load_3d(st + L::oU, &m.u, xb, j0, z, bar);
+    tma_load_3d(st + L::oV, &m.v, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oW, &m.w, xb, j0, z, bar);
+    if constexpr (TURB) tma_load_3d(st + L::oR, &m.rkv, xb, j0 - 2, z, bar);
+  };
+  if (tid == 0)
+    for (int lv = 1; lv <= min(S, lmax); ++lv) issue(lv);
+
+  bool fail = false;
+  auto wait_level = [&](int lv) {
+    if (!fail && lv <= lmax) fail = !mbar_wait(&bars[(lv - 1) % S], ((lv - 1) / S) & 1);
+  };
+  for (int lv = 1; lv <= 3; ++lv) wait_level(lv);
+
+  auto C = [&](int f, int kk) { return cols[f * nc + kk]; };
+  const float oned24 = 1.f / 24.f, fourd3 = 4.f / 3.f;
+  const float dxv24 = oned24 * a.dxiv, dyv24 = oned24 * a.dyiv;
+  const float dxv05n = -.5f * a.dxiv, dyv05n = -.5f * a.dyiv, dzv05n = -.5f * a.dziv;
+  const bool smooth = (a.smtopt % 10 == 2) || (a.smtopt % 10 == 3);
+  const bool isqv = n == 0;
+  const bool vsp = a.vspopt >= 1 && (isqv ? a.vsp_qv : a.vsp_q);
+  float* out = a.sf[n];
+  // own column in the boxes: species/viscosity rows from j0-2, u and w
+  // rows from j0, v rows from j0-1
+  const int ox = tx + 2, oS = (ty + 2) * BX + ox, oU = ty * BX + ox, oV = (ty + 1) * BX + ox;
+  const long long plane = g.plane;
+  long long id = g.at(i, j, 2);
+  int slot = 1 % S;   // slot of level k (k = 2)
+
+  for (int k = 2; k <= nk - 2; ++k, id += plane) {
+    wait_level(k + 2);
+    // Every thread has finished level k-1, so the slot of level k-3 (last
+    // read as k'-2 at k' = k-1) may be refilled with level k+S-3.
+    __syncthreads();
+    if (tid == 0 && k >= 4 && k + S - 3 <= lmax) {
+      fence_proxy_async_smem();
+      issue(k + S - 3);
+    }
+    if (own && !fail) {
+      auto st = [&](int d) {   // stage of level k + d, d = -2..2
+        int s = slot + d;
+        s = s < 0 ? s + S : (s >= S ? s - S : s);
+        return ring + s * L::stage;
+      };
+      const float* st0 = st(0);
+      const float* S0 = st0 + L::oS;
+      const float* SP0 = st0 + L::oSP;
+      const float* U = st0 + L::oU;
+      const float* V = st0 + L::oV;
+      // rstuvwc.f90:172-210 fluxes at the faces the stencil touches
+      const float r8u = C(C_RST8U, k), r8v = C(C_RST8V, k);
+      const float fu_m1 = r8u * U[oU - 1], fu_0 = r8u * U[oU];
+      const float fu_p1 = r8u * U[oU + 1], fu_p2 = r8u * U[oU + 2];
+      const float fv_m1 = r8v * V[oV - BX], fv_0 = r8v * V[oV];
+      const float fv_p1 = r8v * V[oV + BX], fv_p2 = r8v * V[oV + 2 * BX];
+      auto WC = [&](float w, int kk) { return a.sthopt ? w / C(C_JCB8W, kk) : w; };
+      const float fw_0 = C(C_RST8W, k) * WC(st0[L::oW + oU], k);
+      const float fw_1 = C(C_RST8W, k + 1) * WC(st(1)[L::oW + oU], k + 1);
+      const float rbct5 = .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1));
+      const float rst = C(C_RST, k);
+      const float dtdrst = a.dtb2 / rst;                                     // steps.f90:528
+
+      // advs.f90:205-370
+      const float s0 = S0[oS];
+      const float t1a = fu_0 * (s0 - S0[oS - 1]) * dxv05n;
+      const float t1b = fu_p1 * (S0[oS + 1] - s0) * dxv05n;
+      const float t2a = fv_0 * (s0 - S0[oS - BX]) * dyv05n;
+      const float t2b = fv_p1 * (S0[oS + BX] - s0) * dyv05n;
+      float f = (t1a + t1b) + (t2a + t2b);
+      const float w1a = (fu_m1 + fu_0) * (s0 - S0[oS - 2]) * dxv24;
+      const float w1b = (fu_p1 + fu_p2) * (S0[oS + 2] - s0) * dxv24;
+      const float w2a = (fv_m1 + fv_0) * (s0 - S0[oS - 2 * BX]) * dyv24;
+      const float w2b = (fv_p1 + fv_p2) * (S0[oS + 2 * BX] - s0) * dyv24;
+      f = fourd3 * f + ((w1a + w1b) + (w2a + w2b));
+      const float t3a = fw_0 * (s0 - st(-1)[L::oS + oS]) * dzv05n;
+      const float t3b = fw_1 * (st(1)[L::oS + oS] - s0) * dzv05n;
+      f = f + (t3a + t3b);
+
+      // the species at t-dt at an offset (horizontal ones on level k only)
+      auto SPo = [&](int dx, int dy, int dz) {
+        return dz == 0 ? SP0[oS + dx + dy * BX] : st(dz)[L::oSP + oS];
+      };
+      if (smooth) {
+        auto A = [&](int dx, int dy, int dz) {
+          const int kk = k + dz;
+          const float v = SPo(dx, dy, dz);
+          return isqv ? C(C_RBR, kk) * (v - C(C_QVBR, kk)) : C(C_RBR, kk) * v;
+        };
+        f = smooth_into(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+      }
+      if constexpr (TURB) {
+        auto R = [&](int dx, int dy, int dz) {
+          return dz == 0 ? st0[L::oR + oS + dx + dy * BX] : st(dz)[L::oR + oS];
+        };
+        f = turb_scalar_at(f, C, k, a.cpriv, a.dxiv, a.dyiv, a.dziv, R, SPo);
+      }
+      const float spv = SP0[oS];
+      if (vsp && k >= a.ksp0 - 1) f = f - rbct5 * rst * (isqv ? spv - C(C_QVBR, k) : spv);
+      float sf = spv + f * dtdrst;
+      if (n < 6) sf = fmaxf(0.f, sf);
+      out[id] = sf;
+      if (k == 2) out[id - plane] = sf;        // vbcs.f90:118
+      if (k == nk - 2) out[id + plane] = sf;   // vbcs.f90:132
+    }
+    slot = slot + 1 == S ? 0 : slot + 1;
+  }
+
+  if (__syncthreads_or(fail)) {
+    // A bounded wait gave up: record it and let the copies still in flight
+    // land (bounded again) so no TMA write outlives the block.
+    if (tid == 0) {
+      if (a.err) atomicExch(a.err, 1);
+      const int last = min(nk - 2 + S - 3, lmax);   // highest level issued
+      for (int s = 0; s < S; ++s) {
+        int kl = -1;
+        for (int lv = 1; lv <= last; ++lv)
+          if ((lv - 1) % S == s) kl = lv;
+        if (kl >= 0) mbar_wait(&bars[s], ((kl - 1) / S) & 1);
+      }
+    }
+  }
+}
+
+template <int S, bool TURB>
+int launch_sc(const MoistScalarArgs& a, const MoistMaps& maps, cudaStream_t st) {
+  using L = ScLayout<S, TURB>;
+  const Grid& g = a.g;
+  const size_t bytes = L::bytes(g.nk);
+  if (bytes > 227 * 1024) return CRESS_E_UNSUPPORTED;
+  if (cudaFuncSetAttribute(k_scalars<S, TURB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+      cudaSuccess)
+    return CRESS_E_CUDA;
+  const int nx = g.ni - 3, ny = g.nj - 3;
+  dim3 block(kHeviTX, kScalarTY);
+  dim3 grid((nx + kHeviTX - 1) / kHeviTX * kMoistN, (ny + kScalarTY - 1) / kScalarTY);
+  k_scalars<S, TURB><<<grid, block, bytes, st>>>(maps, a);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+}  // namespace
+
+int launch_moist_scalars(const MoistScalarArgs& a, const MoistMaps& maps, cudaStream_t st) {
+  if (a.g.nk < 5) return CRESS_E_UNSUPPORTED;
+  return a.rkv ? launch_sc<7, true>(a, maps, st) : launch_sc<8, false>(a, maps, st);
+}
+
+}  // namespace cress

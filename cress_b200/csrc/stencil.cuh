@@ -1,0 +1,75 @@
+// Stencil helpers shared by the large-step kernels (internal): the
+// 4th-order numerical smoothing and the Smagorinsky mixing of a scalar,
+// written over accessor functors so that a kernel reading neighbours from
+// global memory and one reading them from a shared-memory tile form the
+// same terms in the same order.
+#pragma once
+#include "hevi.cuh"
+
+namespace cress {
+
+// 4th-order smoothing increments (smoo4s.f90:199-296 and its u/v/w/p
+// variants) around `id`: A(dx,dy,dz) returns the smoothed quantity at an
+// offset.  wlev: the field sits on w levels (vertical ghost rule at nk).
+template <class FA>
+__device__ __forceinline__ float smooth_into(float frc, int smtopt, float smhcoe, float smvcoe, int k,
+                                             int kmin, int kmax, const FA& A) {
+  const float a0 = A(0, 0, 0);
+  auto t1 = [&](int x) { return (A(x + 1, 0, 0) + A(x - 1, 0, 0)) - 2.f * A(x, 0, 0); };
+  auto t2 = [&](int y) { return (A(0, y + 1, 0) + A(0, y - 1, 0)) - 2.f * A(0, y, 0); };
+  auto t3 = [&](int z) {
+    int kk = k + z;
+    if (kk < kmin) kk = kmin;   // tmp3(k=kmin-1) = tmp3(kmin)
+    if (kk > kmax) kk = kmax;   // tmp3(kmax+1) = tmp3(kmax)
+    const int d = kk - k;
+    return (A(0, 0, d + 1) + A(0, 0, d - 1)) - 2.f * A(0, 0, d);
+  };
+  (void)a0;
+  const float t10 = t1(0), t20 = t2(0), t30 = t3(0);
+  frc = frc + smhcoe * (t10 + t20) + smvcoe * t30;
+  if (smtopt % 10 == 2) {
+    frc = frc + smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1))));
+  } else {
+    frc = frc + (smvcoe * (t30 - (t3(1) + t3(-1))) +
+                 smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1)))));
+  }
+  return frc;
+}
+
+// Turbulent mixing of a scalar S (the full field at t-dt) at a point of
+// level k: s_eddydif / s_kh8uv diffusivities from the eddy
+// viscosity (rkh = priv*rkv/jcb, rkh8u = rkh(i-1)+rkh(i), rkv8w =
+// (rkh(k-1)+rkh(k))/2; eddydif.f90:154-260, kh8uv.f90:211-230) and the
+// flux divergence of s_turbflx / s_turbs (turbflx.f90:236-352,
+// turbs.f90:189-232), added to frc.
+template <class FC, class FR, class FS>
+__device__ __forceinline__ float turb_scalar_at(float frc, const FC& C, int k, float cpriv, float dxiv, float dyiv,
+                                                float dziv, const FR& R, const FS& S) {
+  // R(dx, dy, dz): eddy viscosity, S(dx, dy, dz): the scalar, at an offset
+  // from the point (only dz = -1, 0, 1 on the point's own column)
+  auto RKH = [&](int dx, int dy, int dz) { return cpriv * R(dx, dy, dz) / C(C_JCB, k + dz); };
+  const float jc = C(C_JCB, k);
+  const float dxv05 = .5f * dxiv, dyv05 = .5f * dyiv;
+  auto JS = [&](int dx, int dy) { return S(dx, dy, 0) * jc; };
+  auto H1 = [&](int dx) { return (RKH(dx - 1, 0, 0) + RKH(dx, 0, 0)) * (JS(dx, 0) - JS(dx - 1, 0)) * dxv05; };
+  auto H2 = [&](int dy) { return (RKH(0, dy - 1, 0) + RKH(0, dy, 0)) * (JS(0, dy) - JS(0, dy - 1)) * dyv05; };
+  auto H3 = [&](int dz) {
+    return (.5f * (RKH(0, 0, dz - 1) + RKH(0, 0, dz))) * (S(0, 0, dz) - S(0, 0, dz - 1)) * dziv;
+  };
+  const float j8u = C(C_JCB8U, k), j8v = C(C_JCB8V, k);
+  return frc + ((H3(1) - H3(0)) * dziv + ((j8u * H1(1) - j8u * H1(0)) * dxiv + (j8v * H2(1) - j8v * H2(0)) * dyiv));
+}
+
+// The same at the point id of a global field: S(p, kk) is the scalar at the
+// linear index p of level kk.
+template <class FS>
+__device__ __forceinline__ float turb_scalar(float frc, const float* rkv, const float* col, int nc, long long id,
+                                             int k, long long px, long long pl, float cpriv, float dxiv, float dyiv,
+                                             float dziv, const FS& S) {
+  auto C = [&](int f, int kk) { return __ldg(col + f * nc + kk); };
+  auto R = [&](int dx, int dy, int dz) { return __ldg(rkv + id + dx + dy * px + dz * pl); };
+  auto SO = [&](int dx, int dy, int dz) { return S(id + dx + dy * px + dz * pl, k + dz); };
+  return turb_scalar_at(frc, C, k, cpriv, dxiv, dyiv, dziv, R, SO);
+}
+
+}  // namespace cress
