@@ -44,7 +44,10 @@ struct ScLayout {
   static constexpr int oR = oW + r128f(BX * R::w);
   static constexpr int stage = oR + (TURB ? r128f(BX * R::r) : 0);   // floats per ring stage
   static constexpr uint32_t tx_bytes = 4u * BX * (2 * R::s + R::u + R::v + R::w + (TURB ? R::r : 0));
-  __host__ __device__ static int cols_floats(int nk) { return r128f(C_NFIELDS_ALL * (nk + 1)); }
+  // 1-D columns stored k-major, colsT[k * NF + field], so a level's values
+  // sit at compile-time offsets from one pointer
+  static constexpr int NF = C_NFIELDS_ALL;
+  __host__ __device__ static int cols_floats(int nk) { return r128f(NF * (nk + 1)); }
   __host__ __device__ static size_t bytes(int nk) {
     return 4 * ((size_t)S * stage + (size_t)cols_floats(nk)) + 8 * (size_t)S;
   }
@@ -71,7 +74,10 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   float* ring = smem;
   float* cols = ring + S * L::stage;
   uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
-  for (int q = tid; q < C_NFIELDS_ALL * nc; q += NT) cols[q] = __ldg(a.col + q);
+  for (int q = tid; q < L::NF * nc; q += NT) {
+    const int f = q / nc, kk = q - f * nc;
+    cols[kk * L::NF + f] = __ldg(a.col + q);
+  }
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -104,7 +110,6 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   };
   for (int lv = 1; lv <= 3; ++lv) wait_level(lv);
 
-  auto C = [&](int f, int kk) { return cols[f * nc + kk]; };
   const float oned24 = 1.f / 24.f, fourd3 = 4.f / 3.f;
   const float dxv24 = oned24 * a.dxiv, dyv24 = oned24 * a.dyiv;
   const float dxv05n = -.5f * a.dxiv, dyv05n = -.5f * a.dyiv, dzv05n = -.5f * a.dziv;
@@ -117,7 +122,10 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   const int ox = tx + 2, oS = (ty + 2) * BX + ox, oU = ty * BX + ox, oV = (ty + 1) * BX + ox;
   const long long plane = g.plane;
   long long id = g.at(i, j, 2);
-  int slot = 1 % S;   // slot of level k (k = 2)
+  // stages of levels k-2 .. k+2 (those outside 1..nk-1 hold other levels
+  // and are read only by terms the reference's clamping discards)
+  auto slot_ptr = [&](int lv) { return ring + ((lv - 1 + S) % S) * L::stage; };
+  const float* stp[5] = {slot_ptr(0), slot_ptr(1), slot_ptr(2), slot_ptr(3), slot_ptr(4)};
 
   for (int k = 2; k <= nk - 2; ++k, id += plane) {
     wait_level(k + 2);
@@ -129,22 +137,20 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       issue(k + S - 3);
     }
     if (own && !fail) {
-      auto st = [&](int d) {   // stage of level k + d, d = -2..2
-        int s = slot + d;
-        s = s < 0 ? s + S : (s >= S ? s - S : s);
-        return ring + s * L::stage;
-      };
+      const float* ck = cols + k * L::NF;
+      auto C = [&](int f, int kk) { return ck[(kk - k) * L::NF + f]; };
+      auto st = [&](int d) { return stp[d + 2]; };
       const float* st0 = st(0);
-      const float* S0 = st0 + L::oS;
-      const float* SP0 = st0 + L::oSP;
-      const float* U = st0 + L::oU;
-      const float* V = st0 + L::oV;
+      const float* S0 = st0 + L::oS + oS;
+      const float* SP0 = st0 + L::oSP + oS;
+      const float* U = st0 + L::oU + oU;
+      const float* V = st0 + L::oV + oV;
       // rstuvwc.f90:172-210 fluxes at the faces the stencil touches
       const float r8u = C(C_RST8U, k), r8v = C(C_RST8V, k);
-      const float fu_m1 = r8u * U[oU - 1], fu_0 = r8u * U[oU];
-      const float fu_p1 = r8u * U[oU + 1], fu_p2 = r8u * U[oU + 2];
-      const float fv_m1 = r8v * V[oV - BX], fv_0 = r8v * V[oV];
-      const float fv_p1 = r8v * V[oV + BX], fv_p2 = r8v * V[oV + 2 * BX];
+      const float fu_m1 = r8u * U[-1], fu_0 = r8u * U[0];
+      const float fu_p1 = r8u * U[1], fu_p2 = r8u * U[2];
+      const float fv_m1 = r8v * V[-BX], fv_0 = r8v * V[0];
+      const float fv_p1 = r8v * V[BX], fv_p2 = r8v * V[2 * BX];
       auto WC = [&](float w, int kk) { return a.sthopt ? w / C(C_JCB8W, kk) : w; };
       const float fw_0 = C(C_RST8W, k) * WC(st0[L::oW + oU], k);
       const float fw_1 = C(C_RST8W, k + 1) * WC(st(1)[L::oW + oU], k + 1);
@@ -153,16 +159,16 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       const float dtdrst = a.dtb2 / rst;                                     // steps.f90:528
 
       // advs.f90:205-370
-      const float s0 = S0[oS];
-      const float t1a = fu_0 * (s0 - S0[oS - 1]) * dxv05n;
-      const float t1b = fu_p1 * (S0[oS + 1] - s0) * dxv05n;
-      const float t2a = fv_0 * (s0 - S0[oS - BX]) * dyv05n;
-      const float t2b = fv_p1 * (S0[oS + BX] - s0) * dyv05n;
+      const float s0 = S0[0];
+      const float t1a = fu_0 * (s0 - S0[-1]) * dxv05n;
+      const float t1b = fu_p1 * (S0[1] - s0) * dxv05n;
+      const float t2a = fv_0 * (s0 - S0[-BX]) * dyv05n;
+      const float t2b = fv_p1 * (S0[BX] - s0) * dyv05n;
       float f = (t1a + t1b) + (t2a + t2b);
-      const float w1a = (fu_m1 + fu_0) * (s0 - S0[oS - 2]) * dxv24;
-      const float w1b = (fu_p1 + fu_p2) * (S0[oS + 2] - s0) * dxv24;
-      const float w2a = (fv_m1 + fv_0) * (s0 - S0[oS - 2 * BX]) * dyv24;
-      const float w2b = (fv_p1 + fv_p2) * (S0[oS + 2 * BX] - s0) * dyv24;
+      const float w1a = (fu_m1 + fu_0) * (s0 - S0[-2]) * dxv24;
+      const float w1b = (fu_p1 + fu_p2) * (S0[2] - s0) * dxv24;
+      const float w2a = (fv_m1 + fv_0) * (s0 - S0[-2 * BX]) * dyv24;
+      const float w2b = (fv_p1 + fv_p2) * (S0[2 * BX] - s0) * dyv24;
       f = fourd3 * f + ((w1a + w1b) + (w2a + w2b));
       const float t3a = fw_0 * (s0 - st(-1)[L::oS + oS]) * dzv05n;
       const float t3b = fw_1 * (st(1)[L::oS + oS] - s0) * dzv05n;
@@ -170,7 +176,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
 
       // the species at t-dt at an offset (horizontal ones on level k only)
       auto SPo = [&](int dx, int dy, int dz) {
-        return dz == 0 ? SP0[oS + dx + dy * BX] : st(dz)[L::oSP + oS];
+        return dz == 0 ? SP0[dx + dy * BX] : st(dz)[L::oSP + oS];
       };
       if (smooth) {
         auto A = [&](int dx, int dy, int dz) {
@@ -178,7 +184,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
           const float v = SPo(dx, dy, dz);
           return isqv ? C(C_RBR, kk) * (v - C(C_QVBR, kk)) : C(C_RBR, kk) * v;
         };
-        f = smooth_into(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+        f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
       }
       if constexpr (TURB) {
         auto R = [&](int dx, int dy, int dz) {
@@ -186,7 +192,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
         };
         f = turb_scalar_at(f, C, k, a.cpriv, a.dxiv, a.dyiv, a.dziv, R, SPo);
       }
-      const float spv = SP0[oS];
+      const float spv = SP0[0];
       if (vsp && k >= a.ksp0 - 1) f = f - rbct5 * rst * (isqv ? spv - C(C_QVBR, k) : spv);
       float sf = spv + f * dtdrst;
       if (n < 6) sf = fmaxf(0.f, sf);
@@ -194,7 +200,9 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       if (k == 2) out[id - plane] = sf;        // vbcs.f90:118
       if (k == nk - 2) out[id + plane] = sf;   // vbcs.f90:132
     }
-    slot = slot + 1 == S ? 0 : slot + 1;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) stp[d] = stp[d + 1];
+    stp[4] = slot_ptr(k + 3);
   }
 
   if (__syncthreads_or(fail)) {

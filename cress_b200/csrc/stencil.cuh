@@ -36,6 +36,30 @@ __device__ __forceinline__ float smooth_into(float frc, int smtopt, float smhcoe
   return frc;
 }
 
+// The same increments where A may be evaluated at every dz in -2..2 (a
+// shared-memory ring that holds those levels, whatever they contain at the
+// ends of the column): the clamping of the vertical second difference at
+// kmin and kmax becomes a selection, so every offset is a compile-time
+// constant and the result is the one smooth_into forms.
+template <class FA>
+__device__ __forceinline__ float smooth_tile(float frc, int smtopt, float smhcoe, float smvcoe, int k, int kmin,
+                                             int kmax, const FA& A) {
+  auto t1 = [&](int x) { return (A(x + 1, 0, 0) + A(x - 1, 0, 0)) - 2.f * A(x, 0, 0); };
+  auto t2 = [&](int y) { return (A(0, y + 1, 0) + A(0, y - 1, 0)) - 2.f * A(0, y, 0); };
+  auto t3 = [&](int z) { return (A(0, 0, z + 1) + A(0, 0, z - 1)) - 2.f * A(0, 0, z); };
+  const float t10 = t1(0), t20 = t2(0), t30 = t3(0);
+  frc = frc + smhcoe * (t10 + t20) + smvcoe * t30;
+  if (smtopt % 10 == 2) {
+    frc = frc + smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1))));
+  } else {
+    const float t3p = k >= kmax ? t30 : t3(1);    // tmp3(kmax+1) = tmp3(kmax)
+    const float t3m = k <= kmin ? t30 : t3(-1);   // tmp3(kmin-1) = tmp3(kmin)
+    frc = frc + (smvcoe * (t30 - (t3p + t3m)) +
+                 smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1)))));
+  }
+  return frc;
+}
+
 // Turbulent mixing of a scalar S (the full field at t-dt) at a point of
 // level k: s_eddydif / s_kh8uv diffusivities from the eddy
 // viscosity (rkh = priv*rkv/jcb, rkh8u = rkh(i-1)+rkh(i), rkv8w =
