@@ -382,7 +382,17 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
     f.rkv = rkv_d;
     f.cpriv = cpriv;
   }
-  rc = launch_force(f, stream);
+  f.err = err_d;
+  {
+    const float* bufs[FB_NONE] = {lev[CRESS_U][N], lev[CRESS_V][N], lev[CRESS_W][N], lev[CRESS_PP][N],
+                                  lev[CRESS_PTP][N], lev[CRESS_U][P], lev[CRESS_V][P], lev[CRESS_W][P],
+                                  lev[CRESS_PP][P], lev[CRESS_PTP][P], f.rkv};
+    ForceMaps fm;
+    for (int gi = 0; gi < kForceGroups; ++gi)
+      for (int q = 0; q < force_nfields(gi, f.rkv != nullptr); ++q)
+        if ((rc = tmap(bufs[force_field_buf(gi, q)], force_field_rows(gi, q), &fm.m[gi][q]))) return rc;
+    rc = launch_force(f, fm, stream);
+  }
   ++launches;
   if (rc) return set_error(rc, "forcing launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   if ((rc = small_steps(nsstp, dts))) return rc;

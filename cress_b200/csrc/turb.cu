@@ -33,7 +33,10 @@ __global__ void __launch_bounds__(256) k_turb_visc(const TurbArgs a) {
   const long long id = g.at(i, j, k);
   const int nc = nk + 1;
   auto C = [&](int f, int kk) { return __ldg(a.col + f * nc + kk); };
-  const Deform D{a.col, nc, nk, a.up, a.vp, a.wp, px, pl, a.dxiv, a.dyiv, a.dziv};
+  auto U = [&](int x, int y, int z) { return __ldg(a.up + id + x + y * px + z * pl); };
+  auto V = [&](int x, int y, int z) { return __ldg(a.vp + id + x + y * px + z * pl); };
+  auto W = [&](int x, int y, int z) { return __ldg(a.wp + id + x + y * px + z * pl); };
+  const auto D = deform_at(C, U, V, W, k, nk, a.dxiv, a.dyiv, a.dziv);
   const float gdzv = 9.8f * a.dziv, gdzv05 = .5f * 9.8f * a.dziv;
   const bool moist = a.qvp != nullptr;
 
@@ -65,10 +68,10 @@ __global__ void __launch_bounds__(256) k_turb_visc(const TurbArgs a) {
     return gdzv * (l1.ptv - l0.ptv) / (C(C_JCB8W, kk) * (b0 + b1));
   };
 
-  const float s11 = D.s11(id, k), s22 = D.s22(id, k), s33 = D.s33(id, k);
-  const float s128s = (D.s12(id, k) + D.s12(id + 1 + px, k)) + (D.s12(id + 1, k) + D.s12(id + px, k));
-  const float s318s = (D.s31(id, k) + D.s31(id + 1 + pl, k + 1)) + (D.s31(id + pl, k + 1) + D.s31(id + 1, k));
-  const float s328s = (D.s32(id, k) + D.s32(id + px + pl, k + 1)) + (D.s32(id + pl, k + 1) + D.s32(id + px, k));
+  const float s11 = D.s11(0, 0, 0), s22 = D.s22(0, 0, 0), s33 = D.s33(0, 0, 0);
+  const float s128s = (D.s12(0, 0, 0) + D.s12(1, 1, 0)) + (D.s12(1, 0, 0) + D.s12(0, 1, 0));
+  const float s318s = (D.s31(0, 0, 0) + D.s31(1, 0, 1)) + (D.s31(0, 0, 1) + D.s31(1, 0, 0));
+  const float s328s = (D.s32(0, 0, 0) + D.s32(0, 1, 1)) + (D.s32(0, 0, 1) + D.s32(0, 1, 0));
   const float ssq = .5f * (s33 * s33 + (s11 * s11 + s22 * s22)) + .0625f * (s128s * s128s + (s318s * s318s + s328s * s328s));
   const float ln = expf((1.f / 3.f) * logf(a.ds3 * C(C_JCB, k)));
   const float ln2 = ln * ln;

@@ -3,67 +3,81 @@
 // kernel needs it, in the reference's operation order, instead of being
 // stored as the reference's t11..t32 arrays (SrcOrig/defomten.f90:305-1091,
 // trnopt=0, mfcopt=0, periodic, flat terrain).
+//
+// The winds and the 1-D columns come through accessors, so one set of
+// formulas serves kernels that read global memory and kernels that read a
+// shared-memory tile: U(x, y, z), V(.), W(.) give the past u, v, w at the
+// offset (x, y, z) from the kernel's point of level k, C(field, kk) a
+// column value of level kk.
 #pragma once
 #include "hevi.cuh"
 
 namespace cress {
 
-struct Deform {
-  const float* col;
-  int nc, nk;
-  const float *u, *v, *w;
-  long long px, pl;
+template <class FC, class FU, class FV, class FW>
+struct DeformAt {
+  const FC& C;
+  const FU& U;
+  const FV& V;
+  const FW& W;
+  int k, nk;
   float dxiv, dyiv, dziv;
 
-  __device__ __forceinline__ float C(int f, int k) const { return __ldg(col + f * nc + k); }
-  __device__ __forceinline__ float U(long long p) const { return __ldg(u + p); }
-  __device__ __forceinline__ float V(long long p) const { return __ldg(v + p); }
-  __device__ __forceinline__ float W(long long p) const { return __ldg(w + p); }
-
-  // s11, s22, s33 at the scalar point p of level k (defomten.f90:471-500, 667-686)
-  __device__ __forceinline__ float s11(long long p, int k) const {
-    const float j8u = C(C_JCB8U, k);
-    const float d = (U(p + 1) * j8u - U(p) * j8u) * dxiv;
-    return (2.f / C(C_JCB, k)) * d;
+  // s11, s22, s33 at the scalar point (x, y, z) (defomten.f90:471-500, 667-686)
+  __device__ __forceinline__ float s11(int x, int y, int z) const {
+    const int kk = k + z;
+    const float j8u = C(C_JCB8U, kk);
+    const float d = (U(x + 1, y, z) * j8u - U(x, y, z) * j8u) * dxiv;
+    return (2.f / C(C_JCB, kk)) * d;
   }
-  __device__ __forceinline__ float s22(long long p, int k) const {
-    const float j8v = C(C_JCB8V, k);
-    const float d = (V(p + px) * j8v - V(p) * j8v) * dyiv;
-    return (2.f / C(C_JCB, k)) * d;
+  __device__ __forceinline__ float s22(int x, int y, int z) const {
+    const int kk = k + z;
+    const float j8v = C(C_JCB8V, kk);
+    const float d = (V(x, y + 1, z) * j8v - V(x, y, z) * j8v) * dyiv;
+    return (2.f / C(C_JCB, kk)) * d;
   }
-  __device__ __forceinline__ float s33(long long p, int k) const {
-    return (2.f / C(C_JCB, k)) * (W(p + pl) - W(p)) * dziv;
+  __device__ __forceinline__ float s33(int x, int y, int z) const {
+    return (2.f / C(C_JCB, k + z)) * (W(x, y, z + 1) - W(x, y, z)) * dziv;
   }
-  // s12 at the u-v corner p = (i, j) of level k (defomten.f90:336-352, 471-480)
-  __device__ __forceinline__ float s12(long long p, int k) const {
-    const float jc = C(C_JCB, k), j8u = C(C_JCB8U, k), j8v = C(C_JCB8V, k);
+  // s12 at the u-v corner (x, y, z) (defomten.f90:336-352, 471-480)
+  __device__ __forceinline__ float s12(int x, int y, int z) const {
+    const int kk = k + z;
+    const float jc = C(C_JCB, kk), j8u = C(C_JCB8U, kk), j8v = C(C_JCB8V, kk);
     const float t3 = 4.f / ((jc + jc) + (jc + jc));
-    return t3 * ((U(p) * j8u - U(p - px) * j8u) * dyiv + (V(p) * j8v - V(p - 1) * j8v) * dxiv);
+    return t3 * ((U(x, y, z) * j8u - U(x, y - 1, z) * j8u) * dyiv + (V(x, y, z) * j8v - V(x - 1, y, z) * j8v) * dxiv);
   }
-  // s13 = s31 at the u-w point p of level kk = 2..nk-1 (defomten.f90:763-833)
-  __device__ __forceinline__ float s13(long long p, int kk) const {
-    const float j8w = C(C_JCB8W, kk);
+  // s13 = s31 at the u-w point (x, y, z), level 2..nk-1 (defomten.f90:763-833)
+  __device__ __forceinline__ float s13(int x, int y, int z) const {
+    const float j8w = C(C_JCB8W, k + z);
     const float t3 = 2.f / (j8w + j8w);
-    return ((W(p) * j8w - W(p - 1) * j8w) * dxiv + (U(p) - U(p - pl)) * dziv) * t3;
+    return ((W(x, y, z) * j8w - W(x - 1, y, z) * j8w) * dxiv + (U(x, y, z) - U(x, y, z - 1)) * dziv) * t3;
   }
-  // s23 = s32 at the v-w point p of level kk = 2..nk-1 (defomten.f90:934-986)
-  __device__ __forceinline__ float s23(long long p, int kk) const {
-    const float j8w = C(C_JCB8W, kk);
+  // s23 = s32 at the v-w point (x, y, z), level 2..nk-1 (defomten.f90:934-986)
+  __device__ __forceinline__ float s23(int x, int y, int z) const {
+    const float j8w = C(C_JCB8W, k + z);
     const float t3 = 2.f / (j8w + j8w);
-    return ((W(p) * j8w - W(p - px) * j8w) * dyiv + (V(p) - V(p - pl)) * dziv) * t3;
+    return ((W(x, y, z) * j8w - W(x, y - 1, z) * j8w) * dyiv + (V(x, y, z) - V(x, y, z - 1)) * dziv) * t3;
   }
-  // s31, s32 with the rigid-lid images of s_bcten at kk = 1 and nk
+  // s31, s32 with the rigid-lid images of s_bcten at levels 1 and nk
   // (bcten.f90:126-160: ten(1) = -ten(3), ten(nk) = -ten(nk-2))
-  __device__ __forceinline__ float s31(long long p, int kk) const {
-    if (kk == 1) return -s13(p + 2 * pl, 3);
-    if (kk == nk) return -s13(p - 2 * pl, nk - 2);
-    return s13(p, kk);
+  __device__ __forceinline__ float s31(int x, int y, int z) const {
+    const int kk = k + z;
+    if (kk == 1) return -s13(x, y, z + 2);
+    if (kk == nk) return -s13(x, y, z - 2);
+    return s13(x, y, z);
   }
-  __device__ __forceinline__ float s32(long long p, int kk) const {
-    if (kk == 1) return -s23(p + 2 * pl, 3);
-    if (kk == nk) return -s23(p - 2 * pl, nk - 2);
-    return s23(p, kk);
+  __device__ __forceinline__ float s32(int x, int y, int z) const {
+    const int kk = k + z;
+    if (kk == 1) return -s23(x, y, z + 2);
+    if (kk == nk) return -s23(x, y, z - 2);
+    return s23(x, y, z);
   }
 };
+
+template <class FC, class FU, class FV, class FW>
+__device__ __forceinline__ DeformAt<FC, FU, FV, FW> deform_at(const FC& C, const FU& U, const FV& V, const FW& W,
+                                                              int k, int nk, float dxiv, float dyiv, float dziv) {
+  return DeformAt<FC, FU, FV, FW>{C, U, V, W, k, nk, dxiv, dyiv, dziv};
+}
 
 }  // namespace cress
