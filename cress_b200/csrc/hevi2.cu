@@ -1,0 +1,391 @@
+// Fused HE-VI acoustic substep for sm_100a, two rows per thread (the
+// default tile).  Same operators, order of terms and boundary rules as
+// k_hevi_substep (hevi.cu: s_hevi, SrcOrig/hevi.f90:339-426, impopt=1,
+// flat terrain, periodic lateral boundaries, rigid lid):
+//   pgrad + diver3d, stepuv, diverpih + diver2d, diverpiv, advbspi,
+//   pgradiv, buoywsi, stepwi with the FP64 Thomas solve (gaussel), steppi.
+//
+// Design.  A block of 32 x 4 threads owns a 32 x 8 tile of columns; thread
+// (tx, ty) owns the columns (i0+tx, j0+2ty) and (i0+tx, j0+2ty+1) and
+// marches both up k, then down.  Levels stream through an S-stage TMA ring
+// as in k_hevi_substep.  Per level and thread:
+//   * the damped pressure of its two columns (registers and shared memory)
+//     plus at most one of the 80 halo points of the tile;
+//   * the west u face of each column; the east face is the west face of
+//     the next lane (a shuffle), only lane 31 forms its own;
+//   * three v faces (south of the first row, between the rows, north of the
+//     second), where one thread per row would form four;
+//   * two independent Thomas recurrences (instruction-level parallelism).
+// Per-level constants come from a k-major table in shared memory, so each
+// is one load at a fixed offset.  Eliminated right-hand sides are parked
+// (float) in the new w array and the backward pressure tendency in the new
+// p' array, as in the GS variant of k_hevi_substep.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "common.cuh"
+#include "hevi.cuh"
+#include "tma.cuh"
+
+namespace cress {
+
+namespace {
+
+constexpr int kH2TY = 8;      // tile rows
+constexpr int kH2Rows = 4;    // thread rows (two tile rows each)
+constexpr int kHNF = 24;      // stride (floats) of the k-major column table (>= C_NFIELDS)
+
+__host__ __device__ constexpr int r128h(int n) { return (n + 31) / 32 * 32; }
+
+template <int S>
+struct H2Layout {
+  using R = HeviRows<kH2TY>;
+  static constexpr int BX = kHeviBoxX;
+  static constexpr int oU = 0;
+  static constexpr int oV = oU + r128h(BX * R::u);
+  static constexpr int oW = oV + r128h(BX * R::v);
+  static constexpr int oP = oW + r128h(BX * R::w);
+  static constexpr int oUF = oP + r128h(BX * R::p);
+  static constexpr int oVF = oUF + r128h(BX * R::uf);
+  static constexpr int oWF = oVF + r128h(BX * R::vf);
+  static constexpr int oPF = oWF + r128h(BX * R::wf);
+  static constexpr int stage = oPF + r128h(BX * R::pf);
+  static constexpr uint32_t tx_bytes =
+      4u * BX * (R::u + R::v + R::w + R::p + R::uf + R::vf + R::wf + R::pf);
+  static constexpr int t3h_floats = r128h((kH2TY + 2) * BX);
+  __host__ __device__ static int cols_floats(int nk) { return r128h(kHNF * (nk + 2)); }
+  // ring, t3h (two buffers), k-major columns, mbarriers, aa and cp
+  // (double), rr (float)
+  __host__ __device__ static size_t bytes(int nk) {
+    return 4 * ((size_t)S * stage + 2 * (size_t)t3h_floats + (size_t)cols_floats(nk)) + 8 * (size_t)S +
+           16 * (size_t)(nk + 2) + 4 * (size_t)(nk + 2);
+  }
+};
+
+template <int S>
+__global__ void __launch_bounds__(kHeviTX * kH2Rows, 4)
+k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
+  using L = H2Layout<S>;
+  constexpr int TX = kHeviTX, TY = kH2TY, BX = kHeviBoxX, NT = TX * kH2Rows;
+  const unsigned full = 0xffffffffu;
+  const Grid g = a.g;
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = 2 + blockIdx.x * TX, j0 = 2 + blockIdx.y * TY;
+  const int xb = i0 - 2;  // box x origin (multiple of 32)
+  const int ilast = min(i0 + TX - 1, ni - 2), jlast = min(j0 + TY - 1, nj - 2);
+  const int i = i0 + tx, jA = j0 + 2 * ty, jB = jA + 1;
+  const bool ownA = (i <= ilast) && (jA <= jlast), ownB = (i <= ilast) && (jB <= jlast);
+  const int ncol = nk + 1;
+  // Columns whose values the periodic wrap also copies into ghost cells.
+  const bool ei = (i <= 3) || (i >= ni - 2);
+  const bool edgeA = ei || (jA <= 3) || (jA >= nj - 2), edgeB = ei || (jB <= 3) || (jB >= nj - 2);
+
+  extern __shared__ __align__(1024) float smem[];
+  float* ring = smem;
+  float* t3hb = ring + S * L::stage;          // 2 x [(TY+2)][BX], rows from j0-1, x from i0-2
+  float* cols = t3hb + 2 * L::t3h_floats;     // cols[k * kHNF + field]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
+  double* thd = reinterpret_cast<double*>(bars + S);       // aa[k] then cp[k], k = 0..nk+1
+  float* thr = reinterpret_cast<float*>(thd + 2 * (nk + 2));  // rr[k]
+
+  for (int n = tid; n < C_NFIELDS * ncol; n += NT) {
+    const int f = n / ncol, kk = n - f * ncol;
+    cols[kk * kHNF + f] = __ldg(a.col + n);
+  }
+  for (int n = tid; n <= nk + 1; n += NT) {
+    thd[n] = __ldg(a.thom_aa + n);
+    thd[nk + 2 + n] = __ldg(a.thom_cp + n);
+    thr[n] = __ldg(a.thom_rr + n);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  // Levels 2..nk-1 are staged (w is needed one level above the top update).
+  const int klast = nk - 1;
+  auto issue = [&](int k) {
+    const int s = (k - 2) % S;
+    float* st = ring + s * L::stage;
+    uint64_t* bar = &bars[s];
+    const int z = k - 1;
+    mbar_arrive_expect_tx(bar, L::tx_bytes);
+    tma_load_3d(st + L::oU, &m.u, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oV, &m.v, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oW, &m.w, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oP, &m.p, xb, j0 - 1, z, bar);
+    tma_load_3d(st + L::oUF, &m.uf, xb, j0, z, bar);
+    tma_load_3d(st + L::oVF, &m.vf, xb, j0, z, bar);
+    tma_load_3d(st + L::oWF, &m.wf, xb, j0, z, bar);
+    tma_load_3d(st + L::oPF, &m.pf, xb, j0, z, bar);
+  };
+  if (tid == 0)
+    for (int k = 2; k <= min(S, klast); ++k) issue(k);
+
+  // Halo point of the damped-pressure plane handled by this thread (box
+  // coordinates): rows south/north of the tile, columns west/east of it.
+  constexpr int NH = 2 * TX + 2 * TY;
+  int hx = 0, hy = 0;
+  {
+    int n = tid;
+    if (n < TX) { hx = n + 2; hy = 0; }
+    else if ((n -= TX) < TX) { hx = n + 2; hy = TY + 1; }
+    else if ((n -= TX) < TY) { hx = 1; hy = n + 1; }
+    else { n -= TY; hx = TX + 2; hy = n + 1; }
+  }
+  const bool has_halo = tid < NH;
+  const int ox = tx + 2;
+  const int oyA = 2 * ty + 1, oyB = oyA + 1;   // own rows in the boxes that start at j0-1
+  const int fyA = 2 * ty, fyB = fyA + 1;       // own rows in the forcing boxes (from j0)
+  const float dts = a.dts, dxiv = a.dxiv, dyiv = a.dyiv, dziv = a.dziv;
+  const float weic1m = 1.f - a.weicoe;
+  float t3vA_prev = 0.f, fpdvjA_prev = 0.f, wb8sA_prev = 0.f;
+  float t3vB_prev = 0.f, fpdvjB_prev = 0.f, wb8sB_prev = 0.f;
+  double fA_prev = 0.0, fB_prev = 0.0;
+  bool fail = false;
+  const long long plane = g.plane, px = g.px;
+  long long idA = g.at(i, jA, 2);
+
+  for (int k = 2; k <= nk - 2; ++k, idA += plane) {
+    const long long idB = idA + px;
+    // One barrier per level: t3h alternates between two buffers, and the
+    // stage of level k-1 is refilled only after this level's barrier.
+    float* t3h = t3hb + (k & 1) * L::t3h_floats;
+    const int s0 = (k - 2) % S, s1 = (k - 1) % S;
+    if (!fail && k == 2) fail = !mbar_wait(&bars[s0], 0);
+    if (!fail) fail = !mbar_wait(&bars[s1], ((k - 1) / S) & 1);
+    const float* st0 = ring + s0 * L::stage;
+    const float* U = st0 + L::oU;
+    const float* V = st0 + L::oV;
+    const float* W0 = st0 + L::oW;
+    const float* W1 = ring + s1 * L::stage + L::oW;
+    const float* P = st0 + L::oP;
+    const float* UF = st0 + L::oUF;
+    const float* VF = st0 + L::oVF;
+    const float* WF = st0 + L::oWF;
+    const float* PF = st0 + L::oPF;
+    const float* ck = cols + k * kHNF;
+    const float* ck1 = ck + kHNF;
+    const float rst8u = ck[C_RST8U], rst8v = ck[C_RST8V];
+    const float rst8wk = ck[C_RST8W], rst8wk1 = ck1[C_RST8W];
+    const float jcbk = ck[C_JCB], ijcbk = ck[C_IJCB];
+    const float irst8u = ck[C_IRST8U], irst8v = ck[C_IRST8V];
+    const float ij8wk = ck[C_IJCB8W], ij8wk1 = ck1[C_IJCB8W];
+
+    // diver3d.f90:318 (with phy2cnt.f90:219 for the contravariant w)
+    auto div3d_at = [&](int x, int y) {
+      float wck = W0[y * BX + x], wck1 = W1[y * BX + x];
+      if (a.sthopt) { wck = wck * ij8wk; wck1 = wck1 * ij8wk1; }
+      return (rst8wk * wck - rst8wk1 * wck1) * dziv +
+             ((rst8u * U[y * BX + x] - rst8u * U[y * BX + x + 1]) * dxiv +
+              (rst8v * V[y * BX + x] - rst8v * V[(y + 1) * BX + x]) * dyiv);
+    };
+    // pgrad.f90:300,341,363
+    auto t3h_of = [&](float div, float pp) {
+      float th = (a.divopt == 2) ? pp + a.divch * div * ijcbk
+               : (a.divopt >= 1) ? pp + a.divcv * jcbk * div : pp;
+      return jcbk * th;
+    };
+    const float divA = div3d_at(ox, oyA), ppA = P[oyA * BX + ox];
+    const float divB = div3d_at(ox, oyB), ppB = P[oyB * BX + ox];
+    const float tcA = t3h_of(divA, ppA), tcB = t3h_of(divB, ppB);
+    t3h[oyA * BX + ox] = tcA;
+    t3h[oyB * BX + ox] = tcB;
+    const float t3vA = (a.divopt >= 1) ? ppA + a.divcv * jcbk * divA : ppA;  // pgrad.f90:300
+    const float t3vB = (a.divopt >= 1) ? ppB + a.divcv * jcbk * divB : ppB;
+    if (has_halo) t3h[hy * BX + hx] = t3h_of(div3d_at(hx, hy), P[hy * BX + hx]);
+    __syncthreads();
+    if (tid == 0 && k + S - 1 <= klast) {
+      fence_proxy_async_smem();
+      issue(k + S - 1);
+    }
+
+    // stepuv.f90:294,304 with pgrad.f90:379,389: west u faces, the east
+    // face from the next lane (lane 31 forms its own)
+    const float unA0 = U[oyA * BX + ox] + dts * (UF[fyA * BX + ox] + (t3h[oyA * BX + ox - 1] - tcA) * dxiv) * irst8u;
+    const float unB0 = U[oyB * BX + ox] + dts * (UF[fyB * BX + ox] + (t3h[oyB * BX + ox - 1] - tcB) * dxiv) * irst8u;
+    float unA1 = __shfl_down_sync(full, unA0, 1);
+    float unB1 = __shfl_down_sync(full, unB0, 1);
+    if (tx == TX - 1) {
+      unA1 = U[oyA * BX + ox + 1] + dts * (UF[fyA * BX + ox + 1] + (tcA - t3h[oyA * BX + ox + 1]) * dxiv) * irst8u;
+      unB1 = U[oyB * BX + ox + 1] + dts * (UF[fyB * BX + ox + 1] + (tcB - t3h[oyB * BX + ox + 1]) * dxiv) * irst8u;
+    }
+    // v faces south of row A, between the rows, north of row B
+    const float vf0 = V[oyA * BX + ox] + dts * (VF[fyA * BX + ox] + (t3h[(oyA - 1) * BX + ox] - tcA) * dyiv) * irst8v;
+    const float vf1 = V[oyB * BX + ox] + dts * (VF[fyB * BX + ox] + (tcA - tcB) * dyiv) * irst8v;
+    const float vf2 = V[(oyB + 1) * BX + ox] + dts * (VF[(fyB + 1) * BX + ox] + (tcB - t3h[(oyB + 1) * BX + ox]) * dyiv) * irst8v;
+
+    const float jcb8u = ck[C_JCB8U], jcb8v = ck[C_JCB8V];
+    const float rcsq = ck[C_RCSQ], rst = ck[C_RST], rbr = ck[C_RBR], ircsq = ck[C_IRCSQ];
+    const float irst8w = ck[C_IRST8W];
+    // one row: the stores of stepuv and everything up to the forward
+    // elimination step
+    auto row = [&](bool own, bool edge, int j, long long id, int oy, int fy, float un0, float un1, float vn0,
+                   float vn1, float ppo, float t3v, float& t3v_prev, float& fpdvj_prev, float& wb8s_prev,
+                   double& fprev) {
+      if (!own) return;
+      if (edge) {
+        store_periodic(a.u_new, g, STAG_U, i, j, k, un0);
+        store_periodic(a.v_new, g, STAG_V, i, j, k, vn0);
+      } else {
+        a.u_new[id] = un0;
+        a.v_new[id] = vn0;
+      }
+      if (k == 2) { store_periodic(a.u_new, g, STAG_U, i, j, 1, un0);          // vbcu.f90:120
+                    store_periodic(a.v_new, g, STAG_V, i, j, 1, vn0); }
+      if (k == nk - 2) { store_periodic(a.u_new, g, STAG_U, i, j, nk - 1, un0); // vbcu.f90:134
+                         store_periodic(a.v_new, g, STAG_V, i, j, nk - 1, vn0); }
+      if (i == ilast && i + 1 == ni - 1) {  // stepuv.f90:293 updates u(ni-1) too
+        store_periodic(a.u_new, g, STAG_U, i + 1, j, k, un1);
+        if (k == 2) store_periodic(a.u_new, g, STAG_U, i + 1, j, 1, un1);
+        if (k == nk - 2) store_periodic(a.u_new, g, STAG_U, i + 1, j, nk - 1, un1);
+      }
+      if (j == jlast && j + 1 == nj - 1) {  // stepuv.f90:302 updates v(nj-1) too
+        store_periodic(a.v_new, g, STAG_V, i, j + 1, k, vn1);
+        if (k == 2) store_periodic(a.v_new, g, STAG_V, i, j + 1, 1, vn1);
+        if (k == nk - 2) store_periodic(a.v_new, g, STAG_V, i, j + 1, nk - 1, vn1);
+      }
+      float phd = (jcb8u * un0 - jcb8u * un1) * dxiv + (jcb8v * vn0 - jcb8v * vn1) * dyiv;  // diver2d.f90:288
+      phd = rcsq * phd;                                                                       // diverpih.f90:208
+      const float wk = W0[oy * BX + ox], wk1 = W1[oy * BX + ox];
+      const float pvd = rcsq * (wk - wk1) * dziv;                                             // diverpiv.f90:124
+      const float fp = PF[fy * BX + ox] + phd + weic1m * (a.g05 * (wk + wk1) * rst + pvd);    // advbspi.f90:158
+      a.p_new[id] = fp;  // parked until the way down
+      const float fpdvj = fp * ijcbk;                                                          // pgradiv.f90:149
+      const float wb8s = (ppo * rst + fp * rbr * a.dtw) * ircsq * a.g05n;                     // buoywsi.f90:171
+      if (k >= 3) {
+        const float wpg = (t3v_prev - t3v) * dziv;                                            // pgrad.f90:320
+        float fw = WF[fy * BX + ox] + wpg + (fpdvj_prev - fpdvj) * a.dtdzw;                   // pgradiv.f90:163
+        if (a.buyopt == 1) fw = fw + (wb8s_prev + wb8s);                                      // buoywsi.f90:205
+        const float wrhs = wk + dts * fw * irst8w;                                            // stepwi.f90:325
+        // gaussel.f90:189-240 in double with the 1-D factors
+        const double rr = (double)thr[k], aa = thd[k];
+        const double f = (k == 3) ? (double)wrhs * aa : ((double)wrhs - rr * fprev) * aa;
+        a.w_new[id] = (float)f;   // parked until the way down
+        fprev = f;
+      }
+      t3v_prev = t3v;
+      fpdvj_prev = fpdvj;
+      wb8s_prev = wb8s;
+    };
+    row(ownA, edgeA, jA, idA, oyA, fyA, unA0, unA1, vf0, vf1, ppA, t3vA, t3vA_prev, fpdvjA_prev, wb8sA_prev, fA_prev);
+    row(ownB, edgeB, jB, idB, oyB, fyB, unB0, unB1, vf1, vf2, ppB, t3vB, t3vB_prev, fpdvjB_prev, wb8sB_prev, fB_prev);
+  }
+
+  if (__syncthreads_or(fail)) {
+    // A bounded wait gave up: record it, let the copies still in flight
+    // land (bounded again) so no TMA write outlives the block, and leave.
+    if (tid == 0) {
+      atomicExch(a.err, 1);
+      const int kmax = min(nk - 2 + S - 1, klast);
+      for (int s = 0; s < S; ++s) {
+        int kl = -1;
+        for (int k = 2; k <= kmax; ++k)
+          if ((k - 2) % S == s) kl = k;
+        if (kl >= 0) mbar_wait(&bars[s], ((kl - 2) / S) & 1);
+      }
+    }
+    return;
+  }
+
+  // --- way down: back substitution, w boundary rows, p' update, both rows
+  // interleaved; loads run two levels ahead of their use ------------------
+  struct Col {
+    float wup = 0.f;        // w(k+1) as float; w(nk-1) = 0 (vbcw.f90:481)
+    double wupd = 0.0;      // w(k+1) as double for the recurrence
+    float w3 = 0.f, wkend = 0.f, p2 = 0.f, p3 = 0.f, pkend = 0.f;
+    float fp0 = 0.f, po0 = 0.f, f0 = 0.f, fp1 = 0.f, po1 = 0.f, f1 = 0.f;
+    long long idk = 0;
+  };
+  Col cA, cB;
+  auto start = [&](Col& c, bool own, long long id_top) {
+    c.idk = id_top;
+    if (!own) return;
+    c.fp0 = a.p_new[id_top]; c.po0 = a.p_old[id_top]; c.f0 = a.w_new[id_top];
+    if (nk - 3 >= 2) { c.fp1 = a.p_new[id_top - plane]; c.po1 = a.p_old[id_top - plane]; }
+    if (nk - 3 >= 3) c.f1 = a.w_new[id_top - plane];
+  };
+  start(cA, ownA, g.at(i, jA, nk - 2));
+  start(cB, ownB, g.at(i, jB, nk - 2));
+  auto down = [&](Col& c, bool own, bool edge, int j, int k) {
+    if (!own) return;
+    const float fpb = c.fp0, po = c.po0, fg = c.f0;
+    c.fp0 = c.fp1; c.po0 = c.po1; c.f0 = c.f1;
+    const long long idk = c.idk;
+    if (k - 2 >= 2) { c.fp1 = a.p_new[idk - 2 * plane]; c.po1 = a.p_old[idk - 2 * plane]; }
+    if (k - 2 >= 3) c.f1 = a.w_new[idk - 2 * plane];
+    const float* ckd = cols + k * kHNF;
+    float wk;
+    if (k >= 3) {
+      const double wd = (k == nk - 2) ? (double)fg : (double)fg - thd[nk + 2 + k] * c.wupd;   // gaussel.f90:254
+      c.wupd = wd;
+      wk = (float)wd;
+      if (edge) store_periodic(a.w_new, g, STAG_S, i, j, k, wk);
+      else a.w_new[idk] = wk;
+      if (k == 3) c.w3 = wk;
+      if (k == nk - 2) c.wkend = wk;
+    } else {
+      wk = 0.f;  // vbcw.f90:317 (flat terrain)
+    }
+    const float rcsq = ckd[C_RCSQ], rst = ckd[C_RST];
+    const float pvd = rcsq * (wk - c.wup) * dziv;                                   // diverpiv.f90:124
+    const float fp = fpb + a.weicoe * (a.g05 * (wk + c.wup) * rst + pvd);            // advbspi.f90:175
+    const float pn = po + dts * fp * ckd[C_IJCB];                                   // steppi.f90:217
+    if (edge) store_periodic(a.p_new, g, STAG_S, i, j, k, pn);
+    else a.p_new[idk] = pn;
+    if (k == 2) c.p2 = pn;
+    if (k == 3) c.p3 = pn;
+    if (k == nk - 2) c.pkend = pn;
+    c.wup = wk;
+    c.idk = idk - plane;
+  };
+  for (int k = nk - 2; k >= 2; --k) {
+    down(cA, ownA, edgeA, jA, k);
+    down(cB, ownB, edgeB, jB, k);
+  }
+  // vbcw.f90:285,317,471,481 (flat terrain; wc = w / jcb8w when stretched),
+  // vbcp.f90:126-160, and level nk of u, v, p' carried over (the small step
+  // does not touch it)
+  auto finish = [&](const Col& c, bool own, int j) {
+    if (!own) return;
+    const float j8w3 = cols[3 * kHNF + C_JCB8W], j8wt = cols[(nk - 2) * kHNF + C_JCB8W];
+    const float wc3 = a.sthopt ? c.w3 / j8w3 : c.w3;
+    const float wct = a.sthopt ? c.wkend / j8wt : c.wkend;
+    store_periodic(a.w_new, g, STAG_S, i, j, 1, -j8w3 * wc3 - 0.f);
+    store_periodic(a.w_new, g, STAG_S, i, j, 2, 0.f);
+    store_periodic(a.w_new, g, STAG_S, i, j, nk - 1, 0.f);
+    store_periodic(a.w_new, g, STAG_S, i, j, nk, -j8wt * wct - 0.f);
+    store_periodic(a.p_new, g, STAG_S, i, j, 1, (a.bbc == 2) ? 2.f * c.p2 - c.p3 : c.p2);
+    store_periodic(a.p_new, g, STAG_S, i, j, nk - 1, c.pkend);
+    store_periodic(a.p_new, g, STAG_S, i, j, nk, a.p_old[g.at(i, j, nk)]);
+    store_periodic(a.u_new, g, STAG_U, i, j, nk, a.u_old[g.at(i, j, nk)]);
+    store_periodic(a.v_new, g, STAG_V, i, j, nk, a.v_old[g.at(i, j, nk)]);
+    if (i == ilast && i + 1 == ni - 1)
+      store_periodic(a.u_new, g, STAG_U, i + 1, j, nk, a.u_old[g.at(i + 1, j, nk)]);
+    if (j == jlast && j + 1 == nj - 1)
+      store_periodic(a.v_new, g, STAG_V, i, j + 1, nk, a.v_old[g.at(i, j + 1, nk)]);
+  };
+  finish(cA, ownA, jA);
+  finish(cB, ownB, jB);
+}
+
+}  // namespace
+
+int launch_hevi2(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
+  constexpr int S = 4;
+  using L = H2Layout<S>;
+  const Grid& g = a.g;
+  const int nx = g.ni - 3, ny = g.nj - 3;
+  const size_t bytes = L::bytes(g.nk);
+  if (bytes > 227 * 1024) return CRESS_E_UNSUPPORTED;
+  if (cudaFuncSetAttribute(k_hevi2<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+    return CRESS_E_CUDA;
+  dim3 block(kHeviTX, kH2Rows);
+  dim3 grid((nx + kHeviTX - 1) / kHeviTX, (ny + kH2TY - 1) / kH2TY);
+  k_hevi2<S><<<grid, block, bytes, st>>>(maps, a);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+}  // namespace cress
