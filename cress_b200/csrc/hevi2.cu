@@ -62,7 +62,10 @@ struct H2Layout {
   }
 };
 
-template <int S>
+// DIV = divopt, STH = stretched grid (sthopt != 0), BUY = buyopt == 1: the
+// options are template parameters, so the level loop carries no branches
+// on them.
+template <int S, int DIV, bool STH, bool BUY>
 __global__ void __launch_bounds__(kHeviTX * kH2Rows, 4)
 k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   using L = H2Layout<S>;
@@ -80,6 +83,9 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   // Columns whose values the periodic wrap also copies into ghost cells.
   const bool ei = (i <= 3) || (i >= ni - 2);
   const bool edgeA = ei || (jA <= 3) || (jA >= nj - 2), edgeB = ei || (jB <= 3) || (jB >= nj - 2);
+  // the faces stepuv also updates at i = ni-1 and j = nj-1 (stepuv.f90:293,302)
+  const bool xlast = (i == ilast) && (i + 1 == ni - 1);
+  const bool ylastA = (jA == jlast) && (jA + 1 == nj - 1), ylastB = (jB == jlast) && (jB + 1 == nj - 1);
 
   extern __shared__ __align__(1024) float smem[];
   float* ring = smem;
@@ -145,11 +151,12 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   float t3vB_prev = 0.f, fpdvjB_prev = 0.f, wb8sB_prev = 0.f;
   double fA_prev = 0.0, fB_prev = 0.0;
   bool fail = false;
-  const long long plane = g.plane, px = g.px;
-  long long idA = g.at(i, jA, 2);
+  // 32-bit element indices (the launcher checks that every field fits)
+  const int plane = (int)g.plane, px = g.px;
+  int idA = (int)g.at(i, jA, 2);
 
   for (int k = 2; k <= nk - 2; ++k, idA += plane) {
-    const long long idB = idA + px;
+    const int idB = idA + px;
     // One barrier per level: t3h alternates between two buffers, and the
     // stage of level k-1 is refilled only after this level's barrier.
     float* t3h = t3hb + (k & 1) * L::t3h_floats;
@@ -177,15 +184,17 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     // diver3d.f90:318 (with phy2cnt.f90:219 for the contravariant w)
     auto div3d_at = [&](int x, int y) {
       float wck = W0[y * BX + x], wck1 = W1[y * BX + x];
-      if (a.sthopt) { wck = wck * ij8wk; wck1 = wck1 * ij8wk1; }
+      if constexpr (STH) { wck = wck * ij8wk; wck1 = wck1 * ij8wk1; }
       return (rst8wk * wck - rst8wk1 * wck1) * dziv +
              ((rst8u * U[y * BX + x] - rst8u * U[y * BX + x + 1]) * dxiv +
               (rst8v * V[y * BX + x] - rst8v * V[(y + 1) * BX + x]) * dyiv);
     };
     // pgrad.f90:300,341,363
     auto t3h_of = [&](float div, float pp) {
-      float th = (a.divopt == 2) ? pp + a.divch * div * ijcbk
-               : (a.divopt >= 1) ? pp + a.divcv * jcbk * div : pp;
+      float th;
+      if constexpr (DIV == 2) th = pp + a.divch * div * ijcbk;
+      else if constexpr (DIV == 1) th = pp + a.divcv * jcbk * div;
+      else th = pp;
       return jcbk * th;
     };
     const float divA = div3d_at(ox, oyA), ppA = P[oyA * BX + ox];
@@ -193,8 +202,8 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     const float tcA = t3h_of(divA, ppA), tcB = t3h_of(divB, ppB);
     t3h[oyA * BX + ox] = tcA;
     t3h[oyB * BX + ox] = tcB;
-    const float t3vA = (a.divopt >= 1) ? ppA + a.divcv * jcbk * divA : ppA;  // pgrad.f90:300
-    const float t3vB = (a.divopt >= 1) ? ppB + a.divcv * jcbk * divB : ppB;
+    const float t3vA = (DIV >= 1) ? ppA + a.divcv * jcbk * divA : ppA;  // pgrad.f90:300
+    const float t3vB = (DIV >= 1) ? ppB + a.divcv * jcbk * divB : ppB;
     if (has_halo) t3h[hy * BX + hx] = t3h_of(div3d_at(hx, hy), P[hy * BX + hx]);
     __syncthreads();
     if (tid == 0 && k + S - 1 <= klast) {
@@ -222,9 +231,10 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     const float irst8w = ck[C_IRST8W];
     // one row: the stores of stepuv and everything up to the forward
     // elimination step
-    auto row = [&](bool own, bool edge, int j, long long id, int oy, int fy, float un0, float un1, float vn0,
-                   float vn1, float ppo, float t3v, float& t3v_prev, float& fpdvj_prev, float& wb8s_prev,
-                   double& fprev) {
+    const bool kend = (k == 2) || (k == nk - 2);
+    auto row = [&](bool own, bool edge, bool ylast, int j, int id, int oy, int fy, float un0, float un1,
+                   float vn0, float vn1, float ppo, float t3v, float& t3v_prev, float& fpdvj_prev,
+                   float& wb8s_prev, double& fprev) {
       if (!own) return;
       if (edge) {
         store_periodic(a.u_new, g, STAG_U, i, j, k, un0);
@@ -233,19 +243,14 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
         a.u_new[id] = un0;
         a.v_new[id] = vn0;
       }
-      if (k == 2) { store_periodic(a.u_new, g, STAG_U, i, j, 1, un0);          // vbcu.f90:120
-                    store_periodic(a.v_new, g, STAG_V, i, j, 1, vn0); }
-      if (k == nk - 2) { store_periodic(a.u_new, g, STAG_U, i, j, nk - 1, un0); // vbcu.f90:134
-                         store_periodic(a.v_new, g, STAG_V, i, j, nk - 1, vn0); }
-      if (i == ilast && i + 1 == ni - 1) {  // stepuv.f90:293 updates u(ni-1) too
-        store_periodic(a.u_new, g, STAG_U, i + 1, j, k, un1);
-        if (k == 2) store_periodic(a.u_new, g, STAG_U, i + 1, j, 1, un1);
-        if (k == nk - 2) store_periodic(a.u_new, g, STAG_U, i + 1, j, nk - 1, un1);
-      }
-      if (j == jlast && j + 1 == nj - 1) {  // stepuv.f90:302 updates v(nj-1) too
-        store_periodic(a.v_new, g, STAG_V, i, j + 1, k, vn1);
-        if (k == 2) store_periodic(a.v_new, g, STAG_V, i, j + 1, 1, vn1);
-        if (k == nk - 2) store_periodic(a.v_new, g, STAG_V, i, j + 1, nk - 1, vn1);
+      if (xlast) store_periodic(a.u_new, g, STAG_U, i + 1, j, k, un1);
+      if (ylast) store_periodic(a.v_new, g, STAG_V, i, j + 1, k, vn1);
+      if (kend) {   // vbcu.f90:120,134 (and vbcv): levels 1 and nk-1 copy levels 2 and nk-2
+        const int kc = k == 2 ? 1 : nk - 1;
+        store_periodic(a.u_new, g, STAG_U, i, j, kc, un0);
+        store_periodic(a.v_new, g, STAG_V, i, j, kc, vn0);
+        if (xlast) store_periodic(a.u_new, g, STAG_U, i + 1, j, kc, un1);
+        if (ylast) store_periodic(a.v_new, g, STAG_V, i, j + 1, kc, vn1);
       }
       float phd = (jcb8u * un0 - jcb8u * un1) * dxiv + (jcb8v * vn0 - jcb8v * vn1) * dyiv;  // diver2d.f90:288
       phd = rcsq * phd;                                                                       // diverpih.f90:208
@@ -258,7 +263,7 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       if (k >= 3) {
         const float wpg = (t3v_prev - t3v) * dziv;                                            // pgrad.f90:320
         float fw = WF[fy * BX + ox] + wpg + (fpdvj_prev - fpdvj) * a.dtdzw;                   // pgradiv.f90:163
-        if (a.buyopt == 1) fw = fw + (wb8s_prev + wb8s);                                      // buoywsi.f90:205
+        if constexpr (BUY) fw = fw + (wb8s_prev + wb8s);                                      // buoywsi.f90:205
         const float wrhs = wk + dts * fw * irst8w;                                            // stepwi.f90:325
         // gaussel.f90:189-240 in double with the 1-D factors
         const double rr = (double)thr[k], aa = thd[k];
@@ -270,8 +275,10 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       fpdvj_prev = fpdvj;
       wb8s_prev = wb8s;
     };
-    row(ownA, edgeA, jA, idA, oyA, fyA, unA0, unA1, vf0, vf1, ppA, t3vA, t3vA_prev, fpdvjA_prev, wb8sA_prev, fA_prev);
-    row(ownB, edgeB, jB, idB, oyB, fyB, unB0, unB1, vf1, vf2, ppB, t3vB, t3vB_prev, fpdvjB_prev, wb8sB_prev, fB_prev);
+    row(ownA, edgeA, ylastA, jA, idA, oyA, fyA, unA0, unA1, vf0, vf1, ppA, t3vA, t3vA_prev, fpdvjA_prev,
+        wb8sA_prev, fA_prev);
+    row(ownB, edgeB, ylastB, jB, idB, oyB, fyB, unB0, unB1, vf1, vf2, ppB, t3vB, t3vB_prev, fpdvjB_prev,
+        wb8sB_prev, fB_prev);
   }
 
   if (__syncthreads_or(fail)) {
@@ -290,102 +297,124 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     return;
   }
 
-  // --- way down: back substitution, w boundary rows, p' update, both rows
-  // interleaved; loads run two levels ahead of their use ------------------
+  // --- way down: back substitution, p' update, both rows interleaved;
+  // loads run two levels ahead (their level clamped at 2, where the values
+  // are not used).  cp(nk-2) = 0 makes the recurrence the identity at the
+  // top level, so every level 3..nk-2 takes the same path. -------------
   struct Col {
     float wup = 0.f;        // w(k+1) as float; w(nk-1) = 0 (vbcw.f90:481)
     double wupd = 0.0;      // w(k+1) as double for the recurrence
-    float w3 = 0.f, wkend = 0.f, p2 = 0.f, p3 = 0.f, pkend = 0.f;
+    float wkend = 0.f, p3 = 0.f, pkend = 0.f;
     float fp0 = 0.f, po0 = 0.f, f0 = 0.f, fp1 = 0.f, po1 = 0.f, f1 = 0.f;
-    long long idk = 0;
+    int idk = 0;
   };
   Col cA, cB;
-  auto start = [&](Col& c, bool own, long long id_top) {
+  auto start = [&](Col& c, bool own, int id_top) {
     c.idk = id_top;
     if (!own) return;
     c.fp0 = a.p_new[id_top]; c.po0 = a.p_old[id_top]; c.f0 = a.w_new[id_top];
-    if (nk - 3 >= 2) { c.fp1 = a.p_new[id_top - plane]; c.po1 = a.p_old[id_top - plane]; }
-    if (nk - 3 >= 3) c.f1 = a.w_new[id_top - plane];
+    c.fp1 = a.p_new[id_top - plane]; c.po1 = a.p_old[id_top - plane]; c.f1 = a.w_new[id_top - plane];
   };
-  start(cA, ownA, g.at(i, jA, nk - 2));
-  start(cB, ownB, g.at(i, jB, nk - 2));
+  const int idtopA = (int)g.at(i, jA, nk - 2);
+  start(cA, ownA, idtopA);
+  start(cB, ownB, idtopA + px);
+  // the p' update of steppi from w(k) and w(k+1) (diverpiv.f90:124,
+  // advbspi.f90:175, steppi.f90:217)
+  auto pnew = [&](const Col& c, float wk, float fpb, float po, int k) {
+    const float* ckd = cols + k * kHNF;
+    const float pvd = ckd[C_RCSQ] * (wk - c.wup) * dziv;
+    const float fp = fpb + a.weicoe * (a.g05 * (wk + c.wup) * ckd[C_RST] + pvd);
+    return po + dts * fp * ckd[C_IJCB];
+  };
   auto down = [&](Col& c, bool own, bool edge, int j, int k) {
     if (!own) return;
     const float fpb = c.fp0, po = c.po0, fg = c.f0;
     c.fp0 = c.fp1; c.po0 = c.po1; c.f0 = c.f1;
-    const long long idk = c.idk;
-    if (k - 2 >= 2) { c.fp1 = a.p_new[idk - 2 * plane]; c.po1 = a.p_old[idk - 2 * plane]; }
-    if (k - 2 >= 3) c.f1 = a.w_new[idk - 2 * plane];
-    const float* ckd = cols + k * kHNF;
-    float wk;
-    if (k >= 3) {
-      const double wd = (k == nk - 2) ? (double)fg : (double)fg - thd[nk + 2 + k] * c.wupd;   // gaussel.f90:254
-      c.wupd = wd;
-      wk = (float)wd;
-      if (edge) store_periodic(a.w_new, g, STAG_S, i, j, k, wk);
-      else a.w_new[idk] = wk;
-      if (k == 3) c.w3 = wk;
-      if (k == nk - 2) c.wkend = wk;
+    const int idk = c.idk;
+    const int idl = idk - (k - 2 >= 2 ? 2 : k - 2) * plane;   // level max(k-2, 2)
+    c.fp1 = a.p_new[idl]; c.po1 = a.p_old[idl]; c.f1 = a.w_new[idl];
+    const double wd = (double)fg - thd[nk + 2 + k] * c.wupd;   // gaussel.f90:254
+    c.wupd = wd;
+    const float wk = (float)wd;
+    const float pn = pnew(c, wk, fpb, po, k);
+    if (edge) {
+      store_periodic(a.w_new, g, STAG_S, i, j, k, wk);
+      store_periodic(a.p_new, g, STAG_S, i, j, k, pn);
     } else {
-      wk = 0.f;  // vbcw.f90:317 (flat terrain)
+      a.w_new[idk] = wk;
+      a.p_new[idk] = pn;
     }
-    const float rcsq = ckd[C_RCSQ], rst = ckd[C_RST];
-    const float pvd = rcsq * (wk - c.wup) * dziv;                                   // diverpiv.f90:124
-    const float fp = fpb + a.weicoe * (a.g05 * (wk + c.wup) * rst + pvd);            // advbspi.f90:175
-    const float pn = po + dts * fp * ckd[C_IJCB];                                   // steppi.f90:217
-    if (edge) store_periodic(a.p_new, g, STAG_S, i, j, k, pn);
-    else a.p_new[idk] = pn;
-    if (k == 2) c.p2 = pn;
-    if (k == 3) c.p3 = pn;
-    if (k == nk - 2) c.pkend = pn;
+    if (k == nk - 2) { c.wkend = wk; c.pkend = pn; }
+    c.p3 = pn;   // the value of level 3 after the loop
     c.wup = wk;
     c.idk = idk - plane;
   };
-  for (int k = nk - 2; k >= 2; --k) {
+  for (int k = nk - 2; k >= 3; --k) {
     down(cA, ownA, edgeA, jA, k);
     down(cB, ownB, edgeB, jB, k);
   }
-  // vbcw.f90:285,317,471,481 (flat terrain; wc = w / jcb8w when stretched),
-  // vbcp.f90:126-160, and level nk of u, v, p' carried over (the small step
-  // does not touch it)
-  auto finish = [&](const Col& c, bool own, int j) {
+  // level 2: w(2) = 0 (vbcw.f90:317, flat terrain), then the boundary rows
+  // of vbcw.f90:285,317,471,481 (wc = w / jcb8w when stretched) and
+  // vbcp.f90:126-160, and level nk of u, v, p' carried over (the small
+  // step does not touch it)
+  auto finish = [&](Col& c, bool own, bool edge, bool ylast, int j) {
     if (!own) return;
+    const float p2 = pnew(c, 0.f, c.fp0, c.po0, 2);
+    if (edge) store_periodic(a.p_new, g, STAG_S, i, j, 2, p2);
+    else a.p_new[c.idk] = p2;
+    const float w3 = c.wup;
     const float j8w3 = cols[3 * kHNF + C_JCB8W], j8wt = cols[(nk - 2) * kHNF + C_JCB8W];
-    const float wc3 = a.sthopt ? c.w3 / j8w3 : c.w3;
-    const float wct = a.sthopt ? c.wkend / j8wt : c.wkend;
+    const float wc3 = STH ? w3 / j8w3 : w3;
+    const float wct = STH ? c.wkend / j8wt : c.wkend;
     store_periodic(a.w_new, g, STAG_S, i, j, 1, -j8w3 * wc3 - 0.f);
     store_periodic(a.w_new, g, STAG_S, i, j, 2, 0.f);
     store_periodic(a.w_new, g, STAG_S, i, j, nk - 1, 0.f);
     store_periodic(a.w_new, g, STAG_S, i, j, nk, -j8wt * wct - 0.f);
-    store_periodic(a.p_new, g, STAG_S, i, j, 1, (a.bbc == 2) ? 2.f * c.p2 - c.p3 : c.p2);
+    store_periodic(a.p_new, g, STAG_S, i, j, 1, (a.bbc == 2) ? 2.f * p2 - c.p3 : p2);
     store_periodic(a.p_new, g, STAG_S, i, j, nk - 1, c.pkend);
     store_periodic(a.p_new, g, STAG_S, i, j, nk, a.p_old[g.at(i, j, nk)]);
     store_periodic(a.u_new, g, STAG_U, i, j, nk, a.u_old[g.at(i, j, nk)]);
     store_periodic(a.v_new, g, STAG_V, i, j, nk, a.v_old[g.at(i, j, nk)]);
-    if (i == ilast && i + 1 == ni - 1)
-      store_periodic(a.u_new, g, STAG_U, i + 1, j, nk, a.u_old[g.at(i + 1, j, nk)]);
-    if (j == jlast && j + 1 == nj - 1)
-      store_periodic(a.v_new, g, STAG_V, i, j + 1, nk, a.v_old[g.at(i, j + 1, nk)]);
+    if (xlast) store_periodic(a.u_new, g, STAG_U, i + 1, j, nk, a.u_old[g.at(i + 1, j, nk)]);
+    if (ylast) store_periodic(a.v_new, g, STAG_V, i, j + 1, nk, a.v_old[g.at(i, j + 1, nk)]);
   };
-  finish(cA, ownA, jA);
-  finish(cB, ownB, jB);
+  finish(cA, ownA, edgeA, ylastA, jA);
+  finish(cB, ownB, edgeB, ylastB, jB);
 }
 
-}  // namespace
-
-int launch_hevi2(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
+template <int DIV, bool STH, bool BUY>
+int launch_h2(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
   constexpr int S = 4;
   using L = H2Layout<S>;
   const Grid& g = a.g;
   const int nx = g.ni - 3, ny = g.nj - 3;
   const size_t bytes = L::bytes(g.nk);
   if (bytes > 227 * 1024) return CRESS_E_UNSUPPORTED;
-  if (cudaFuncSetAttribute(k_hevi2<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_hevi2<S, DIV, STH, BUY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+      cudaSuccess)
     return CRESS_E_CUDA;
   dim3 block(kHeviTX, kH2Rows);
   dim3 grid((nx + kHeviTX - 1) / kHeviTX, (ny + kH2TY - 1) / kH2TY);
-  k_hevi2<S><<<grid, block, bytes, st>>>(maps, a);
+  k_hevi2<S, DIV, STH, BUY><<<grid, block, bytes, st>>>(maps, a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+template <int DIV>
+int launch_h2_div(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
+  const bool sth = a.sthopt != 0, buy = a.buyopt == 1;
+  if (sth) return buy ? launch_h2<DIV, true, true>(a, maps, st) : launch_h2<DIV, true, false>(a, maps, st);
+  return buy ? launch_h2<DIV, false, true>(a, maps, st) : launch_h2<DIV, false, false>(a, maps, st);
+}
+
+}  // namespace
+
+int launch_hevi2(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
+  if (a.g.count() >= (1LL << 31) || a.g.nk < 6) return CRESS_E_UNSUPPORTED;   // 32-bit indices; levels 2..nk-2 >= 3
+  switch (a.divopt) {
+    case 2: return launch_h2_div<2>(a, maps, st);
+    case 1: return launch_h2_div<1>(a, maps, st);
+    default: return launch_h2_div<0>(a, maps, st);
+  }
 }
 
 }  // namespace cress
