@@ -521,7 +521,7 @@ int Ctx::cloudphy(float dtb, float thresq) {
     return CRESS_OK;
   }
   rc = launch_cloudphy(m, stream);
-  launches += 3;
+  launches += 4;
   if (rc) return set_error(rc, "cloudphy launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   return CRESS_OK;
 }

@@ -9,11 +9,12 @@
 // sedimentation CFL limit dz*jcb/(u+eps) into one domain minimum
 // (the chkfall allreduce of SrcOrig/fallblk.f90:439) with a warp reduction
 // and one atomicMin per warp.
-// k_micro_fall (one thread per column): recovers npstp and dtp from that
-// minimum (fallblk.f90:441-449), recomputes the past-level fall speeds,
-// runs the upwind sedimentation sub-steps of every species column
-// (upwqp.f90:160-225, upwnp.f90:140-176) with the surface precipitation
-// rate and accumulation, and the final adjstni (coldblk.f90:469).
+// k_micro_fall (one thread per column and sedimenting species; the eight
+// species are independent): recovers npstp and dtp from that minimum
+// (fallblk.f90:441-449) and runs the upwind sedimentation sub-steps of its
+// species column (upwqp.f90:160-225, upwnp.f90:140-176) with the past-level
+// fall speeds k_micro_src stored, and the surface precipitation rate and
+// accumulation; k_adjstni then applies the final adjstni (coldblk.f90:469).
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "hevi.cuh"
@@ -52,7 +53,7 @@ __device__ __forceinline__ void store_speeds(const MicroArgs& a, long long id, c
   u[4 * n3] = c.usq; u[5 * n3] = c.ugq; u[6 * n3] = c.usn; u[7 * n3] = c.ugn;
 }
 
-__global__ void __launch_bounds__(256) k_micro_src(const MicroArgs a) {
+__global__ void __launch_bounds__(256, 3) k_micro_src(const MicroArgs a) {
   const Grid g = a.g;
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -87,8 +88,8 @@ __global__ void __launch_bounds__(256) k_micro_src(const MicroArgs a) {
   if ((threadIdx.x & 31) == 0 && lim < 3.0e38f) atomicMin(a.dtp_bits, __float_as_int(lim));
 }
 
-// One thread per column.  For each species, npstp upwind sub-steps of
-// s_upwqp / s_upwnp (upwqp.f90:160-225, upwnp.f90:140-176) stream up the
+// One thread per column and species (blockIdx.z).  npstp upwind sub-steps
+// of s_upwqp / s_upwnp (upwqp.f90:160-225, upwnp.f90:140-176) stream up the
 // column: the flux rbr*u*q of level k+1 is formed from the not yet updated
 // q(k+1) while q(k) is written, so a sub-step is one read and one write of
 // the column; the surface rate (flx(1)+flx(2))/2/rhow accumulates over
@@ -98,6 +99,7 @@ __global__ void __launch_bounds__(128) k_micro_fall(const MicroArgs a) {
   const int nk = g.nk;
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int f = blockIdx.z;
   if (i > g.ni - 2 || j > g.nj - 2) return;
   // fallblk.f90:421-449
   const float dtb = a.dtb;
@@ -121,13 +123,14 @@ __global__ void __launch_bounds__(128) k_micro_fall(const MicroArgs a) {
   const long long n3 = pl * nk;
   const long long pp2 = (long long)g.px * g.py;
   const long long pid = (long long)j * g.px + i;
-  float* const fields[8] = {a.qcf, a.qif, a.nif, a.qrf, a.qsf, a.qgf, a.nsf, a.ngf};
-  const int pslot[8] = {0, 2, -1, 1, 3, 4, -1, -1};   // prc, pri, -, prr, prs, prg
-#pragma unroll 1
-  for (int f = 0; f < 8; ++f) {
-    float* fld = fields[f] + id1;
+  // species f: qc, qi, ni, qr, qs, qg, ns, ng; its precipitation slot
+  // (prc, pri, -, prr, prs, prg, -, -)
+  float* const field = f == 0 ? a.qcf : f == 1 ? a.qif : f == 2 ? a.nif : f == 3 ? a.qrf
+                     : f == 4 ? a.qsf : f == 5 ? a.qgf : f == 6 ? a.nsf : a.ngf;
+  const int s = f == 0 ? 0 : f == 1 ? 2 : f == 3 ? 1 : f == 4 ? 3 : f == 5 ? 4 : -1;
+  {
+    float* fld = field + id1;
     const float* u = a.uspd + f * n3 + id1;
-    const int s = pslot[f];
     float rate = 0.f, acc = 0.f;
     if (s >= 0) { rate = a.prec[(2 * s) * pp2 + pid]; acc = a.prec[(2 * s + 1) * pp2 + pid]; }
 #pragma unroll 1
@@ -155,14 +158,21 @@ __global__ void __launch_bounds__(128) k_micro_fall(const MicroArgs a) {
     }
     if (s >= 0) { a.prec[(2 * s) * pp2 + pid] = rate; a.prec[(2 * s + 1) * pp2 + pid] = acc; }
   }
-  // coldblk.f90:467-470: adjstni once more (flqcqi_opt=1)
-  for (int k = 1; k <= nk - 1; ++k) {
-    const long long id = id1 + (k - 1) * pl;
-    const float rb = __ldg(crbr + k), rbv = 1.f / rb;
-    float nci = a.nif[id], ncs = a.nsf[id], ncg = a.ngf[id];
-    adjstni_cell(rb, rbv, a.qif[id], a.qsf[id], a.qgf[id], nci, ncs, ncg);
-    a.nif[id] = nci; a.nsf[id] = ncs; a.ngf[id] = ncg;
-  }
+}
+
+// coldblk.f90:467-470: adjstni once more after the sedimentation
+// (flqcqi_opt=1), interior points, k = 1..nk-1.
+__global__ void __launch_bounds__(256) k_adjstni(const MicroArgs a) {
+  const Grid g = a.g;
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (i > g.ni - 2 || j > g.nj - 2 || k > g.nk - 1) return;
+  const long long id = g.at(i, j, k);
+  const float rb = __ldg(a.col + C_RBR * (g.nk + 1) + k), rbv = 1.f / rb;
+  float nci = a.nif[id], ncs = a.nsf[id], ncg = a.ngf[id];
+  adjstni_cell(rb, rbv, a.qif[id], a.qsf[id], a.qgf[id], nci, ncs, ncg);
+  a.nif[id] = nci; a.nsf[id] = ncs; a.ngf[id] = ncg;
 }
 
 __global__ void k_init_dtp(int* dtp_bits, float v) { *dtp_bits = __float_as_int(v); }
@@ -248,14 +258,22 @@ int micro_init_tables() {
   return CRESS_OK;
 }
 
+// s_fallblk for the eight species, then the final adjstni (two launches).
+static void launch_fall(const MicroArgs& a, cudaStream_t st) {
+  dim3 b2(32, 4, 1);
+  dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 8);
+  k_micro_fall<<<gr2, b2, 0, st>>>(a);
+  dim3 b(32, 8, 1);
+  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
+  k_adjstni<<<gr, b, 0, st>>>(a);
+}
+
 int launch_cloudphy(const MicroArgs& a, cudaStream_t st) {
   k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
   dim3 b(32, 8, 1);
   dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
   k_micro_src<<<gr, b, 0, st>>>(a);
-  dim3 b2(32, 4, 1);
-  dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 1);
-  k_micro_fall<<<gr2, b2, 0, st>>>(a);
+  launch_fall(a, st);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
@@ -335,10 +353,8 @@ int launch_cloudphy_learned(const MicroArgs& a, const float* w, Mlp* m, const Le
     *launches += 7;
     if (cudaGetLastError() != cudaSuccess) return CRESS_E_CUDA;
   }
-  dim3 b2(32, 4, 1);
-  dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 1);
-  k_micro_fall<<<gr2, b2, 0, st>>>(a);
-  ++*launches;
+  launch_fall(a, st);
+  *launches += 2;
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
@@ -376,10 +392,8 @@ int launch_cloudphy_fused(const MicroArgs& a, const float* w, Mlp* m, const Lear
   const int grid = (int)(ntiles < nsm ? ntiles : nsm);
   k_mlp_fused<<<grid, kFusedThreads, kFusedSmem, st>>>(maps, a, p);
   k_micro_src_list<<<nsm * 4, 128, 0, st>>>(a, 0, L.fb_list, L.fb_count, L.chunk);
-  dim3 b2(32, 4, 1);
-  dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 1);
-  k_micro_fall<<<gr2, b2, 0, st>>>(a);
-  *launches += 4;
+  launch_fall(a, st);
+  *launches += 5;
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
