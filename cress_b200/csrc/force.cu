@@ -37,8 +37,7 @@
 namespace cress {
 namespace {
 
-constexpr float kEpsva = .622f;   // rd/rv, comphy.f90:79
-constexpr int kNF = C_NFIELDS_ALL;
+constexpr int kNF = kLevelStride;   // stride of the k-major level table
 
 __host__ __device__ constexpr int r128c(int n) { return (n + 31) / 32 * 32; }  // floats -> multiple of 128 B
 
@@ -95,12 +94,9 @@ __device__ __forceinline__ void force_group(const ForceMaps& m, const ForceArgs&
   const int nc = nk + 1;
 
   float* ring = smem;
-  float* cols = ring + S * FRing<T>::stage_max();   // colsT[k * kNF + field]
+  float* cols = ring + S * FRing<T>::stage_max();   // level table: cols[k * kNF + field]
   uint64_t* bars = reinterpret_cast<uint64_t*>(cols + r128c(kNF * nc));
-  for (int q = tid; q < kNF * nc; q += NT) {
-    const int f = q / nc, kk = q - f * nc;
-    cols[kk * kNF + f] = __ldg(a.col + q);
-  }
+  fill_level_table(cols, a.col, nk, a.dtb2, tid, NT);
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -171,7 +167,7 @@ __device__ __forceinline__ void force_group(const ForceMaps& m, const ForceArgs&
       auto RXU = [&](int dx, int dy, int dz) { return C(C_RST8U, k + dz) * Uc(dx, dy, dz); };
       auto RXV = [&](int dx, int dy, int dz) { return C(C_RST8V, k + dz) * Vc(dx, dy, dz); };
       auto WC = [&](int dx, int dy, int dz) {
-        return a.sthopt ? Wc(dx, dy, dz) / C(C_JCB8W, k + dz) : Wc(dx, dy, dz);
+        return a.sthopt ? Wc(dx, dy, dz) * C(C_IJCB8W, k + dz) : Wc(dx, dy, dz);
       };
       auto RXW = [&](int dx, int dy, int dz) { return C(C_RST8W, k + dz) * WC(dx, dy, dz); };
 
@@ -198,7 +194,7 @@ __device__ __forceinline__ void force_group(const ForceMaps& m, const ForceArgs&
         if (smooth) {
           auto A = [&](int dx, int dy, int dz) {
             const int kk = k + dz;
-            return C(C_RST8U, kk) * (UP(dx, dy, dz) - C(C_UBR, kk)) / C(C_JCB8U, kk);
+            return C(C_RST8U, kk) * (UP(dx, dy, dz) - C(C_UBR, kk)) * C(D_IJCB8U, kk);
           };
           f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
         }
@@ -250,7 +246,7 @@ __device__ __forceinline__ void force_group(const ForceMaps& m, const ForceArgs&
         if (smooth) {
           auto A = [&](int dx, int dy, int dz) {
             const int kk = k + dz;
-            return C(C_RST8V, kk) * (VP(dx, dy, dz) - C(C_VBR, kk)) / C(C_JCB8V, kk);
+            return C(C_RST8V, kk) * (VP(dx, dy, dz) - C(C_VBR, kk)) * C(D_IJCB8V, kk);
           };
           f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
         }
@@ -303,7 +299,7 @@ __device__ __forceinline__ void force_group(const ForceMaps& m, const ForceArgs&
         if (smooth) {
           auto A = [&](int dx, int dy, int dz) {
             const int kk = k + dz;
-            return C(C_RST8W, kk) * WP(dx, dy, dz) / C(C_JCB8W, kk);
+            return C(C_RST8W, kk) * WP(dx, dy, dz) * C(C_IJCB8W, kk);
           };
           f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 1, A);
         }
@@ -313,14 +309,13 @@ __device__ __forceinline__ void force_group(const ForceMaps& m, const ForceArgs&
         float wbk = 0.f;
         if (k <= nk - 2) {
           if (!a.qv) {
-            wbk = g05 * C(C_RST, k) * __ldg(a.ptp + id) / C(C_PTBR, k);
+            wbk = g05 * C(C_RST, k) * __ldg(a.ptp + id) * C(D_IPTBR, k);
           } else {
-            const float qvbr = C(C_QVBR, k);
-            const float qvd = __ldg(a.qv + id) - qvbr;
+            const float qvd = __ldg(a.qv + id) - C(C_QVBR, k);
             const float qall = (((__ldg(a.qc + id) + __ldg(a.qr + id)) + __ldg(a.qi + id)) + __ldg(a.qs + id)) +
                                __ldg(a.qg + id);   // totalqwi.f90:163
             wbk = g05 * C(C_RST, k) *
-                  ((qvd / (kEpsva + qvbr) - (qvd + qall) / (1.f + qvbr)) + __ldg(a.ptp + id) / C(C_PTBR, k));
+                  ((qvd * C(D_IEPSQV, k) - (qvd + qall) * C(D_I1QV, k)) + __ldg(a.ptp + id) * C(D_IPTBR, k));
           }
         }
         if (k >= 3 && k <= nk - 2) f = f + (wb_prev + wbk);
@@ -389,7 +384,7 @@ __device__ __forceinline__ void force_group(const ForceMaps& m, const ForceArgs&
             return (C(C_RBR, kk - 1) + C(C_RBR, kk)) * Wc(0, 0, z) * (C(C_PTBR, kk - 1) - C(C_PTBR, kk)) * dziv25;
           };
           f = f + (pta8w(0) + pta8w(1));
-          const float dtdrst = a.dtb2 / C(C_RST, k);                     // steps.f90:528
+          const float dtdrst = C(D_DTDRST, k);                          // steps.f90:528
           const float ptpf = SP(0, 0, 0) + f * dtdrst;                    // steps.f90:568
           a.ptpf[id] = ptpf;
           if (k == 2) a.ptpf[id - plane] = ptpf;                          // vbcs.f90:118

@@ -11,6 +11,51 @@ namespace cress {
 // same table: the Rayleigh coefficient rbct(k) (vspdmp.f90:269-292).
 enum ColFieldLarge { C_RBCT = C_NFIELDS, C_NFIELDS_ALL };
 
+// Per-level values the large-step kernels derive from the columns, once per
+// block, into a k-major shared-memory table: quotients of constants by
+// columns (the same IEEE divisions the stencils would repeat per point) and
+// reciprocals of the per-level divisors of field values, which the stencils
+// multiply by (a field value of exactly zero would otherwise send every
+// such division through its slow path).
+enum ColDerived {
+  D_IJCB8U = C_NFIELDS_ALL, D_IJCB8V, D_IPTBR, D_IEPSQV, D_I1QV, D_DTDRST, D_2JCB, D_4JCB, D_2J8W, D_NFIELDS
+};
+constexpr int kLevelStride = 32;   // floats per level of the table (>= D_NFIELDS)
+
+// Column field f (base or derived) of level kk; B(f, kk) reads a base column.
+template <class FB>
+__device__ __forceinline__ float level_value(int f, int kk, const FB& B, float dtb2) {
+  switch (f) {
+    case D_IJCB8U: return 1.f / B(C_JCB8U, kk);
+    case D_IJCB8V: return 1.f / B(C_JCB8V, kk);
+    case D_IPTBR: return 1.f / B(C_PTBR, kk);
+    case D_IEPSQV: return 1.f / (.622f + B(C_QVBR, kk));   // epsva = rd/rv, comphy.f90:79
+    case D_I1QV: return 1.f / (1.f + B(C_QVBR, kk));
+    case D_DTDRST: return dtb2 / B(C_RST, kk);             // steps.f90:528
+    case D_2JCB: return 2.f / B(C_JCB, kk);                 // defomten.f90:471-500
+    case D_4JCB: {
+      const float jc = B(C_JCB, kk);
+      return 4.f / ((jc + jc) + (jc + jc));                 // defomten.f90:336-352
+    }
+    case D_2J8W: {
+      const float j8w = B(C_JCB8W, kk);
+      return 2.f / (j8w + j8w);                             // defomten.f90:763-833
+    }
+    default: return B(f, kk);
+  }
+}
+
+// Fill table[kk * kLevelStride + f], kk = 0..nk, from col[f * (nk+1) + kk].
+__device__ __forceinline__ void fill_level_table(float* table, const float* col, int nk, float dtb2, int tid,
+                                                 int nt) {
+  const int nc = nk + 1;
+  auto B = [&](int f, int kk) { return __ldg(col + f * nc + kk); };
+  for (int q = tid; q < nc * kLevelStride; q += nt) {
+    const int kk = q / kLevelStride, f = q - kk * kLevelStride;
+    table[q] = f < D_NFIELDS ? level_value(f, kk, B, dtb2) : 0.f;
+  }
+}
+
 struct ForceArgs {
   Grid g;
   const float* col;           // 1-D columns, C_NFIELDS_ALL x (nk+1)

@@ -44,9 +44,10 @@ struct ScLayout {
   static constexpr int oR = oW + r128f(BX * R::w);
   static constexpr int stage = oR + (TURB ? r128f(BX * R::r) : 0);   // floats per ring stage
   static constexpr uint32_t tx_bytes = 4u * BX * (2 * R::s + R::u + R::v + R::w + (TURB ? R::r : 0));
-  // 1-D columns stored k-major, colsT[k * NF + field], so a level's values
-  // sit at compile-time offsets from one pointer
-  static constexpr int NF = C_NFIELDS_ALL;
+  // 1-D columns and their derived values stored k-major (the level table,
+  // cols[k * NF + field]), so a level's values sit at compile-time offsets
+  // from one pointer
+  static constexpr int NF = kLevelStride;
   __host__ __device__ static int cols_floats(int nk) { return r128f(NF * (nk + 1)); }
   __host__ __device__ static size_t bytes(int nk) {
     return 4 * ((size_t)S * stage + (size_t)cols_floats(nk)) + 8 * (size_t)S;
@@ -74,10 +75,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   float* ring = smem;
   float* cols = ring + S * L::stage;
   uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
-  for (int q = tid; q < L::NF * nc; q += NT) {
-    const int f = q / nc, kk = q - f * nc;
-    cols[kk * L::NF + f] = __ldg(a.col + q);
-  }
+  fill_level_table(cols, a.col, nk, a.dtb2, tid, NT);
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -151,12 +149,12 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       const float fu_p1 = r8u * U[1], fu_p2 = r8u * U[2];
       const float fv_m1 = r8v * V[-BX], fv_0 = r8v * V[0];
       const float fv_p1 = r8v * V[BX], fv_p2 = r8v * V[2 * BX];
-      auto WC = [&](float w, int kk) { return a.sthopt ? w / C(C_JCB8W, kk) : w; };
+      auto WC = [&](float w, int kk) { return a.sthopt ? w * C(C_IJCB8W, kk) : w; };
       const float fw_0 = C(C_RST8W, k) * WC(st0[L::oW + oU], k);
       const float fw_1 = C(C_RST8W, k + 1) * WC(st(1)[L::oW + oU], k + 1);
       const float rbct5 = .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1));
       const float rst = C(C_RST, k);
-      const float dtdrst = a.dtb2 / rst;                                     // steps.f90:528
+      const float dtdrst = C(D_DTDRST, k);                                  // steps.f90:528
 
       // advs.f90:205-370
       const float s0 = S0[0];

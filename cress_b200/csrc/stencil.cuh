@@ -71,7 +71,7 @@ __device__ __forceinline__ float turb_scalar_at(float frc, const FC& C, int k, f
                                                 float dziv, const FR& R, const FS& S) {
   // R(dx, dy, dz): eddy viscosity, S(dx, dy, dz): the scalar, at an offset
   // from the point (only dz = -1, 0, 1 on the point's own column)
-  auto RKH = [&](int dx, int dy, int dz) { return cpriv * R(dx, dy, dz) / C(C_JCB, k + dz); };
+  auto RKH = [&](int dx, int dy, int dz) { return cpriv * R(dx, dy, dz) * C(C_IJCB, k + dz); };
   const float jc = C(C_JCB, k);
   const float dxv05 = .5f * dxiv, dyv05 = .5f * dyiv;
   auto JS = [&](int dx, int dy) { return S(dx, dy, 0) * jc; };
@@ -82,18 +82,6 @@ __device__ __forceinline__ float turb_scalar_at(float frc, const FC& C, int k, f
   };
   const float j8u = C(C_JCB8U, k), j8v = C(C_JCB8V, k);
   return frc + ((H3(1) - H3(0)) * dziv + ((j8u * H1(1) - j8u * H1(0)) * dxiv + (j8v * H2(1) - j8v * H2(0)) * dyiv));
-}
-
-// The same at the point id of a global field: S(p, kk) is the scalar at the
-// linear index p of level kk.
-template <class FS>
-__device__ __forceinline__ float turb_scalar(float frc, const float* rkv, const float* col, int nc, long long id,
-                                             int k, long long px, long long pl, float cpriv, float dxiv, float dyiv,
-                                             float dziv, const FS& S) {
-  auto C = [&](int f, int kk) { return __ldg(col + f * nc + kk); };
-  auto R = [&](int dx, int dy, int dz) { return __ldg(rkv + id + dx + dy * px + dz * pl); };
-  auto SO = [&](int dx, int dy, int dz) { return S(id + dx + dy * px + dz * pl, k + dz); };
-  return turb_scalar_at(frc, C, k, cpriv, dxiv, dyiv, dziv, R, SO);
 }
 
 }  // namespace cress

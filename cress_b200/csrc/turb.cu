@@ -32,7 +32,8 @@ __global__ void __launch_bounds__(256) k_turb_visc(const TurbArgs a) {
   const long long px = g.px, pl = g.plane;
   const long long id = g.at(i, j, k);
   const int nc = nk + 1;
-  auto C = [&](int f, int kk) { return __ldg(a.col + f * nc + kk); };
+  auto B = [&](int f, int kk) { return __ldg(a.col + f * nc + kk); };
+  auto C = [&](int f, int kk) { return level_value(f, kk, B, 0.f); };
   auto U = [&](int x, int y, int z) { return __ldg(a.up + id + x + y * px + z * pl); };
   auto V = [&](int x, int y, int z) { return __ldg(a.vp + id + x + y * px + z * pl); };
   auto W = [&](int x, int y, int z) { return __ldg(a.wp + id + x + y * px + z * pl); };
