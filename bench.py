@@ -58,28 +58,31 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.rows = []
-        self._stop = threading.Event()
-        self._t = threading.Thread(target=self._run, daemon=True)
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                      "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self._p = None
 
     def __enter__(self):
-        self._t.start()
+        # one nvidia-smi in its own sampling loop (every 50 ms) for the
+        # whole timed region
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                        "--format=csv,noheader,nounits", "-lms", "50"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._p = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is None:
+            return
+        self._p.terminate()
+        try:
+            out, _ = self._p.communicate(timeout=10)
+        except Exception:
+            self._p.kill()
+            out, _ = self._p.communicate()
+        for line in (out or "").splitlines():
+            if line.strip():
+                self.rows.append([x.strip() for x in line.split(",")])
 
     def summary(self):
         if not self.rows:
@@ -294,7 +297,8 @@ def main():
     ap.add_argument("--dx", type=float, default=1000.0)
     ap.add_argument("--dtbig", type=float, default=5.0)
     ap.add_argument("--dtsml", type=float, default=1.0)
-    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--tile", type=int, default=-1,
+                    help="HE-VI tile shape; -1 (default): chosen by the autotuner on the live state")
     ap.add_argument("--cpu-nx", type=int, default=256)
     ap.add_argument("--cpu-ny", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=3)
@@ -357,7 +361,7 @@ def main():
     case = make_case(args.nx, args.ny, args.nz, args.dx, 100 + rank)
     ni, nj, nk = case["dims"]
     rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, case["botbar"])
-    s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, case["dz"], sthopt=1, tile=args.tile,
+    s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, case["dz"], sthopt=1, tile=max(args.tile, 0),
                           device=local, cphopt=3)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -384,6 +388,11 @@ def main():
         return float(t.item())
 
     s.large_step(0, 0.5 * args.dtbig, nsstp, 0.5 * args.dtsml)   # the first (half) step, ctime=0
+    tune = None
+    if args.tile < 0:
+        best, tms = s.autotune(nsstp=nsstp, dts=args.dtsml, reps=2)
+        tune = {"tile": best, "ms_per_substep": [round(t, 4) for t in tms]}
+    cfg_json["hevi_tile"] = tune["tile"] if tune else args.tile
     if not args.no_graphs:
         # capture the CUDA graphs of the time-level rotation's 6 pointer
         # states (an eager step and a capture each) before the warm-up
@@ -393,6 +402,7 @@ def main():
     for _ in range(args.warmup - 1):
         s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
     barrier()
+    d0 = s.diagnostics(cress_b200.NOW)
     l0 = s.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -402,6 +412,12 @@ def main():
         e1.record(stream)
         barrier()
     launches = s.launch_count() - l0
+    d1 = s.diagnostics(cress_b200.NOW)
+    budget = {"water_kg": [d0["water"], d1["water"]], "precip_kg": [d0["precip"], d1["precip"]],
+              "mass_kg": [d0["mass"], d1["mass"]],
+              "water_drift_rel": ((d1["water"] + d1["precip"]) - (d0["water"] + d0["precip"])) / d0["water"],
+              "mass_drift_rel": (d1["mass"] - d0["mass"]) / d0["mass"], "max_w": d1["max_w"],
+              "nonfinite": int(d1["nonfinite"]), "over": f"{args.steps} timed steps (FP64 sums on the device)"}
     ms = max_over_ranks(e0.elapsed_time(e1))
     value = world * cells * args.steps / (ms * 1e-3)
 
@@ -471,11 +487,12 @@ def main():
             "sim_s_per_wall_s": args.dtbig / (ms / args.steps * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "kernel": "k_hevi_substep",
+                         "kernel": "k_hevi2" if cfg_json["hevi_tile"] == 0 else "k_hevi_substep",
                          "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
-            "cpu_baseline": cpu, "learned": learned, "ensemble": ensemble}))
+            "cpu_baseline": cpu, "learned": learned, "ensemble": ensemble,
+            "budget": budget, "autotune": tune}))
     if world > 1:
         dist.destroy_process_group()
 

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libcress_b200.so")
 FIELDS = ["u", "v", "w", "pp", "ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 PAST, NOW, FUTURE, FORCING = 0, 1, 2, 3
+NTILES = 11   # HE-VI tile shapes (cress_cfg.tile)
 # enum cress_base order
 BASE_NAMES = ["jcb", "jcb8u", "jcb8v", "jcb8w", "rbr", "ptbr", "rst", "rst8u", "rst8v",
               "rst8w", "rcsq"]
@@ -108,6 +109,8 @@ def lib():
     L.cress_learned_stats.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
     L.cress_set_tuple_sampling.argtypes = [vp, vp, i, f, ull]
     L.cress_set_graphs.argtypes = [vp, i]
+    L.cress_diagnostics.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double)]
+    L.cress_autotune.argtypes = [vp, i, f, i, ctypes.POINTER(i), ctypes.POINTER(f)]
     _lib = L
     return L
 
@@ -237,6 +240,27 @@ class Solver:
         _check(lib().cress_set_tuple_sampling(self._h, mlp._h if mlp else None, int(stride),
                                               float(keep_zero), int(seed)))
         self._sampler = mlp
+
+    DIAG_NAMES = ("water", "precip", "mass", "max_u", "max_v", "max_w", "max_ptp", "nonfinite")
+
+    def diagnostics(self, level=NOW, check=True):
+        """FP64 domain sums and maxima of one time level as a dict (see
+        cress_diagnostics); with check=True a non-finite value raises
+        CressError (CRESS_E_NONFINITE)."""
+        out = (ctypes.c_double * 8)()
+        rc = lib().cress_diagnostics(self._h, int(level), out)
+        if check or rc != 5:
+            _check(rc)
+        return dict(zip(self.DIAG_NAMES, list(out)))
+
+    def autotune(self, nsstp=10, dts=1.0, reps=3):
+        """Time every HE-VI tile shape on the current state and keep the
+        fastest; returns (best tile, milliseconds per substep per tile,
+        -1 for shapes the grid cannot use)."""
+        best = ctypes.c_int(-1)
+        ms = (ctypes.c_float * NTILES)()
+        _check(lib().cress_autotune(self._h, int(nsstp), float(dts), int(reps), ctypes.byref(best), ms))
+        return best.value, list(ms)
 
     def get_precip(self):
         ni, nj = self.shape[2] - 2, self.shape[1] - 2

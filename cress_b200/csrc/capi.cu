@@ -12,6 +12,7 @@
 #include "../../include/cress_b200.h"
 #include "common.cuh"
 #include "ctx.h"
+#include "diag.cuh"
 #include "hevi.cuh"
 #include "forcing.cuh"
 #include "micro.cuh"
@@ -555,6 +556,91 @@ int Ctx::check_device_error() {
   return CRESS_OK;
 }
 
+// Domain diagnostics of one time level (diag.cu): out[0..2] FP64 water,
+// precipitated water and mass (kg), out[3..6] max |u|, |v|, |w|, |theta'|,
+// out[7] the number of non-finite values.
+int Ctx::diagnostics(int level, double* out) {
+  if (level < CRESS_PAST || level > CRESS_FUTURE)
+    return set_error(CRESS_E_ARG, "cress_diagnostics: level %d (0..2)", level);
+  if (!base_set) return set_error(CRESS_E_STATE, "cress_diagnostics: base state not set");
+  int rc;
+  if (!diag_d) {
+    if ((rc = cuda_check(cudaMalloc(&diag_d, sizeof(DiagAcc)), "cudaMalloc diagnostics"))) return rc;
+    owned.push_back(diag_d);
+  }
+  DiagArgs a{};
+  a.g = g;
+  a.col = col_d;
+  a.u = lev[CRESS_U][level]; a.v = lev[CRESS_V][level]; a.w = lev[CRESS_W][level];
+  a.pp = lev[CRESS_PP][level]; a.ptp = lev[CRESS_PTP][level];
+  if (cfg.cphopt == 3) {
+    for (int n = 0; n < 6; ++n) a.q[n] = lev[CRESS_QV + n][level];
+    for (int n = 0; n < 3; ++n) a.n[n] = lev[CRESS_NI + n][level];
+    a.prec = prec_d;
+  }
+  a.dv = (double)cfg.dx * (double)cfg.dy * (double)cfg.dz;
+  a.dxdy = (double)cfg.dx * (double)cfg.dy;
+  a.acc = static_cast<DiagAcc*>(diag_d);
+  if ((rc = cuda_check(cudaMemsetAsync(diag_d, 0, sizeof(DiagAcc), stream), "clear diagnostics"))) return rc;
+  if ((rc = launch_diag(a, stream))) return set_error(rc, "diagnostics launch failed");
+  DiagAcc h{};
+  if ((rc = cuda_check(cudaMemcpyAsync(&h, diag_d, sizeof h, cudaMemcpyDeviceToHost, stream), "read diagnostics")) ||
+      (rc = cuda_check(cudaStreamSynchronize(stream), "sync")))
+    return rc;
+  for (int n = 0; n < 3; ++n) out[n] = h.sum[n];
+  for (int n = 0; n < 4; ++n) {
+    float f;
+    std::memcpy(&f, &h.maxbits[n], 4);
+    out[3 + n] = f;
+  }
+  out[7] = (double)h.nonfinite;
+  if (h.nonfinite)
+    return set_error(CRESS_E_NONFINITE, "%llu non-finite values in time level %d", h.nonfinite, level);
+  return CRESS_OK;
+}
+
+// Time every HE-VI tile variant over `reps` small-step loops of nsstp
+// substeps on the current state (the loop writes only the future level and
+// its spare, so the state the next large step starts from is untouched),
+// keep the fastest as cfg.tile and drop graphs captured with another tile.
+int Ctx::autotune(int nsstp, float dts, int reps, int* best, float* ms) {
+  if (nsstp < 1 || reps < 1) return set_error(CRESS_E_ARG, "cress_autotune: nsstp=%d reps=%d", nsstp, reps);
+  const int keep = cfg.tile;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return set_error(CRESS_E_CUDA, "cudaEventCreate failed");
+  float best_ms = 0.f;
+  int best_tile = -1, rc = CRESS_OK;
+  for (int t = 0; t < CRESS_NTILES; ++t) {
+    cfg.tile = t;
+    if (ms) ms[t] = -1.f;
+    rc = small_steps(nsstp, dts);   // warm-up; a shape the grid cannot use is skipped
+    if (rc == CRESS_E_UNSUPPORTED) { rc = CRESS_OK; continue; }
+    if (rc) break;
+    cudaEventRecord(e0, stream);
+    for (int r = 0; r < reps && !rc; ++r) rc = small_steps(nsstp, dts);
+    cudaEventRecord(e1, stream);
+    if (rc) break;
+    if ((rc = cuda_check(cudaEventSynchronize(e1), "autotune sync"))) break;
+    if ((rc = check_device_error())) break;
+    float t_ms = 0.f;
+    cudaEventElapsedTime(&t_ms, e0, e1);
+    t_ms /= (float)(reps * nsstp);
+    if (ms) ms[t] = t_ms;
+    if (best_tile < 0 || t_ms < best_ms) { best_ms = t_ms; best_tile = t; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc || best_tile < 0) {
+    cfg.tile = keep;
+    return rc ? rc : set_error(CRESS_E_UNSUPPORTED, "cress_autotune: no tile shape fits this grid");
+  }
+  cfg.tile = best_tile;
+  free_graphs();
+  if (best) *best = best_tile;
+  return CRESS_OK;
+}
+
 }  // namespace cress
 
 using namespace cress;
@@ -1000,6 +1086,21 @@ int cress_set_graphs(cress_ctx* ctx, int on) {
   c->free_graphs();
   c->graphs = on != 0;
   return CRESS_OK;
+}
+
+int cress_diagnostics(cress_ctx* ctx, int level, double* out) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !out) return set_error(CRESS_E_ARG, "cress_diagnostics: null argument");
+  cudaSetDevice(c->device);
+  return c->diagnostics(level, out);
+}
+
+int cress_autotune(cress_ctx* ctx, int nsstp, float dts, int reps, int* best_tile, float* ms_per_substep) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "cress_autotune: null context");
+  if (!c->base_set) return set_error(CRESS_E_STATE, "cress_autotune: base state not set");
+  cudaSetDevice(c->device);
+  return c->autotune(nsstp, dts, reps, best_tile, ms_per_substep);
 }
 
 }  // extern "C"

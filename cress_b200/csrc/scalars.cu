@@ -69,7 +69,6 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kHeviTX + tx;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= ni - 2) && (j <= nj - 2);
-  const int nc = nk + 1;
 
   extern __shared__ __align__(1024) float smem[];
   float* ring = smem;

@@ -148,6 +148,30 @@ int cress_set_base_large(cress_ctx* ctx, const float* ubr, const float* vbr, con
  * (SrcOrig/intgdrv.f90:832-998). */
 int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, float dts);
 
+/* Domain diagnostics of one time level (level 0..2), in FP64 on the
+ * device over the physical cells i = 2..ni-2, j = 2..nj-2, k = 2..nk-2:
+ *   out[0] water of qv+qc+qr+qi+qs+qg, sum rst (q...) dx dy dz      (kg)
+ *   out[1] precipitated water, sum of the accumulated surface
+ *          precipitation of the five species times rhow dx dy       (kg)
+ *   out[2] mass, sum rst (1 + p'/rcsq) dx dy dz                     (kg)
+ *   out[3..6] max |u|, |v|, |w|, |theta'|
+ *   out[7] number of non-finite values in the level's prognostic fields
+ * (out[0..1] are 0 without microphysics).  Returns CRESS_E_NONFINITE when
+ * out[7] > 0 (the blow-up detector; the reference's own monitor is the
+ * max/min printout of SrcOrig/mxndrv.f90).  out holds 8 doubles. */
+int cress_diagnostics(cress_ctx* ctx, int level, double* out);
+
+/* Number of HE-VI tile shapes (cress_cfg.tile = 0 .. CRESS_NTILES-1). */
+#define CRESS_NTILES 11
+
+/* Autotuner: times every HE-VI tile shape (xy tile, ring depth, column
+ * store) over `reps` small-step loops of nsstp substeps of length dts on
+ * the current state, which it leaves untouched (only the future level is
+ * written), and keeps the fastest as the context's tile.  best_tile and
+ * ms_per_substep[CRESS_NTILES] (milliseconds per substep, -1 for shapes
+ * this grid cannot use) may be null. */
+int cress_autotune(cress_ctx* ctx, int nsstp, float dts, int reps, int* best_tile, float* ms_per_substep);
+
 /* Replay whole large steps from CUDA graphs (on != 0) instead of launching
  * every kernel from the host: the second step with a given time-level
  * state and parameters is captured, later ones launch the graph.  Results
