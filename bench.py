@@ -32,6 +32,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 HEVI_BYTES_PER_CELL = 48  # u,v,w,p' read + write and 4 forcings read, float32
+# DRAM bytes per cell of one k_hevi2 launch from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum = 632.6 MB over 384*384*63 cells at 384x384x64,
+# profiles/hevi_substep_384x384x64.md); the traffic grows with the cells
+HEVI2_TRAFFIC_PER_CELL = 632.6e6 / (384 * 384 * 63)
 METRIC = "cell-updates/s on 1 B200: plain vs learned-microphysics form at stated error"
 MOIST = ["qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
 NAMES = ["u", "v", "w", "pp", "ptp"] + MOIST
@@ -486,7 +490,10 @@ def main():
             "data": "synthetic", "config": cfg_json,
             "sim_s_per_wall_s": args.dtbig / (ms / args.steps * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "frac": achieved / peak,
+                         "traffic": HEVI2_TRAFFIC_PER_CELL * cells if cfg_json["hevi_tile"] == 0 else None,
+                         "traffic_source": "ncu dram bytes per cell at 384x384x64 scaled to this grid",
+                         "peak_source": peak_kind,
                          "kernel": "k_hevi2" if cfg_json["hevi_tile"] == 0 else "k_hevi_substep",
                          "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
                          "ms_per_launch": hevi_ms},

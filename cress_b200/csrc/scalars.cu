@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "forcing.cuh"
 #include "hevi.cuh"
+#include "f2.cuh"
 #include "stencil.cuh"
 #include "tma.cuh"
 
@@ -32,18 +33,26 @@ namespace {
 
 __host__ __device__ constexpr int r128f(int n) { return (n + 31) / 32 * 32; }  // floats -> multiple of 128 B
 
+// Species per block: the three of a group share the staged winds (and the
+// eddy viscosity) and the block's barriers.
+constexpr int kScGroup = 3;
+static_assert(kMoistN % kScGroup == 0, "species groups must tile the nine species");
+
 template <int S, bool TURB>
 struct ScLayout {
   using R = ScalarRows;
   static constexpr int BX = kHeviBoxX;
+  static constexpr int sbox = r128f(BX * R::s);
+  // species q of the group at oS + q * 2 * sbox (t), + sbox (t-dt)
   static constexpr int oS = 0;
-  static constexpr int oSP = oS + r128f(BX * R::s);
-  static constexpr int oU = oSP + r128f(BX * R::s);
+  static constexpr int oSP = sbox;
+  static constexpr int oU = kScGroup * 2 * sbox;
   static constexpr int oV = oU + r128f(BX * R::u);
   static constexpr int oW = oV + r128f(BX * R::v);
   static constexpr int oR = oW + r128f(BX * R::w);
   static constexpr int stage = oR + (TURB ? r128f(BX * R::r) : 0);   // floats per ring stage
-  static constexpr uint32_t tx_bytes = 4u * BX * (2 * R::s + R::u + R::v + R::w + (TURB ? R::r : 0));
+  static constexpr uint32_t tx_bytes =
+      4u * BX * (kScGroup * 2 * R::s + R::u + R::v + R::w + (TURB ? R::r : 0));
   // 1-D columns and their derived values stored k-major (the level table,
   // cols[k * NF + field]), so a level's values sit at compile-time offsets
   // from one pointer
@@ -54,21 +63,28 @@ struct ScLayout {
   }
 };
 
+// Threads: 16 x 8 x 3; thread (tx, ty, tz) owns the pair of columns
+// i0+2tx, i0+2tx+1 of row j0+ty of species 3g+tz and computes both with
+// packed FP32x2 arithmetic (f2.cuh), so each operation serves two points.
+constexpr int kScPairs = kHeviTX / 2;
+
 template <int S, bool TURB>
-__global__ void __launch_bounds__(kHeviTX * kScalarTY)
+__global__ void __launch_bounds__(kScPairs * kScalarTY * kScGroup)
 k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   // level k+2 must have been issued (at k' = k+5-S) before level k waits for it
   static_assert(S >= 6, "ring too shallow for the k-2..k+2 window");
   using L = ScLayout<S, TURB>;
-  constexpr int TY = kScalarTY, BX = kHeviBoxX, NT = kHeviTX * TY;
+  constexpr int TY = kScalarTY, BX = kHeviBoxX, NT = kScPairs * TY * kScGroup;
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
-  const int n = blockIdx.x % kMoistN;                 // species; the nine of a tile are neighbours
-  const int i0 = 2 + (blockIdx.x / kMoistN) * kHeviTX, j0 = 2 + blockIdx.y * TY;
+  constexpr int NG = kMoistN / kScGroup;               // species groups
+  const int grp = blockIdx.x % NG;                     // the groups of a tile are neighbours
+  const int q = threadIdx.z, n = grp * kScGroup + q;   // this thread's species
+  const int i0 = 2 + (blockIdx.x / NG) * kHeviTX, j0 = 2 + blockIdx.y * TY;
   const int xb = i0 - 2;                              // box x origin (multiple of 32)
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kHeviTX + tx;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = (i <= ni - 2) && (j <= nj - 2);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = (q * TY + ty) * kScPairs + tx;
+  const int i = i0 + 2 * tx, j = j0 + ty;
+  const bool ownA = (i <= ni - 2) && (j <= nj - 2), ownB = (i + 1 <= ni - 2) && (j <= nj - 2);
 
   extern __shared__ __align__(1024) float smem[];
   float* ring = smem;
@@ -83,16 +99,16 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
 
   // Levels 1..nk-1 are staged; level lv lives in slot (lv-1) % S.
   const int lmax = nk - 1;
-  const CUtensorMap* ms = &m.s[n];
-  const CUtensorMap* msp = &m.sp[n];
   auto issue = [&](int lv) {
     const int s = (lv - 1) % S;
     float* st = ring + s * L::stage;
     uint64_t* bar = &bars[s];
     const int z = lv - 1;
     mbar_arrive_expect_tx(bar, L::tx_bytes);
-    tma_load_3d(st + L::oS, ms, xb, j0 - 2, z, bar);
-    tma_load_3d(st + L::oSP, msp, xb, j0 - 2, z, bar);
+    for (int p = 0; p < kScGroup; ++p) {
+      tma_load_3d(st + L::oS + p * 2 * L::sbox, &m.s[grp * kScGroup + p], xb, j0 - 2, z, bar);
+      tma_load_3d(st + L::oSP + p * 2 * L::sbox, &m.sp[grp * kScGroup + p], xb, j0 - 2, z, bar);
+    }
     tma_load_3d(st + L::oU, &m.u, xb, j0, z, bar);
     tma_load_3d(st + L::oV, &m.v, xb, j0 - 1, z, bar);
     tma_load_3d(st + L::oW, &m.w, xb, j0, z, bar);
@@ -114,9 +130,12 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   const bool isqv = n == 0;
   const bool vsp = a.vspopt >= 1 && (isqv ? a.vsp_qv : a.vsp_q);
   float* out = a.sf[n];
-  // own column in the boxes: species/viscosity rows from j0-2, u and w
-  // rows from j0, v rows from j0-1
-  const int ox = tx + 2, oS = (ty + 2) * BX + ox, oU = ty * BX + ox, oV = (ty + 1) * BX + ox;
+  // own pair in the boxes (x offset even, so every pair load is 8-byte
+  // aligned): species/viscosity rows from j0-2, u and w rows from j0, v
+  // rows from j0-1
+  const int ox = 2 * tx + 2, oU = ty * BX + ox, oV = (ty + 1) * BX + ox;
+  const int oS = q * 2 * L::sbox + (ty + 2) * BX + ox;   // own pair of this species' boxes
+  const int oR = (ty + 2) * BX + ox;                     // own pair of the viscosity box
   const long long plane = g.plane;
   long long id = g.at(i, j, 2);
   // stages of levels k-2 .. k+2 (those outside 1..nk-1 hold other levels
@@ -133,7 +152,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       fence_proxy_async_smem();
       issue(k + S - 3);
     }
-    if (own && !fail) {
+    if ((ownA || ownB) && !fail) {
       const float* ck = cols + k * L::NF;
       auto C = [&](int f, int kk) { return ck[(kk - k) * L::NF + f]; };
       auto st = [&](int d) { return stp[d + 2]; };
@@ -144,58 +163,63 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       const float* V = st0 + L::oV + oV;
       // rstuvwc.f90:172-210 fluxes at the faces the stencil touches
       const float r8u = C(C_RST8U, k), r8v = C(C_RST8V, k);
-      const float fu_m1 = r8u * U[-1], fu_0 = r8u * U[0];
-      const float fu_p1 = r8u * U[1], fu_p2 = r8u * U[2];
-      const float fv_m1 = r8v * V[-BX], fv_0 = r8v * V[0];
-      const float fv_p1 = r8v * V[BX], fv_p2 = r8v * V[2 * BX];
-      auto WC = [&](float w, int kk) { return a.sthopt ? w * C(C_IJCB8W, kk) : w; };
-      const float fw_0 = C(C_RST8W, k) * WC(st0[L::oW + oU], k);
-      const float fw_1 = C(C_RST8W, k + 1) * WC(st(1)[L::oW + oU], k + 1);
+      const F2 fu_m1 = r8u * pair_at(U, -1), fu_0 = r8u * ld2(U);
+      const F2 fu_p1 = r8u * pair_at(U, 1), fu_p2 = r8u * ld2(U + 2);
+      const F2 fv_m1 = r8v * ld2(V - BX), fv_0 = r8v * ld2(V);
+      const F2 fv_p1 = r8v * ld2(V + BX), fv_p2 = r8v * ld2(V + 2 * BX);
+      auto WC = [&](F2 w, int kk) { return a.sthopt ? w * C(C_IJCB8W, kk) : w; };
+      const F2 fw_0 = C(C_RST8W, k) * WC(ld2(st0 + L::oW + oU), k);
+      const F2 fw_1 = C(C_RST8W, k + 1) * WC(ld2(st(1) + L::oW + oU), k + 1);
       const float rbct5 = .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1));
       const float rst = C(C_RST, k);
       const float dtdrst = C(D_DTDRST, k);                                  // steps.f90:528
 
       // advs.f90:205-370
-      const float s0 = S0[0];
-      const float t1a = fu_0 * (s0 - S0[-1]) * dxv05n;
-      const float t1b = fu_p1 * (S0[1] - s0) * dxv05n;
-      const float t2a = fv_0 * (s0 - S0[-BX]) * dyv05n;
-      const float t2b = fv_p1 * (S0[BX] - s0) * dyv05n;
-      float f = (t1a + t1b) + (t2a + t2b);
-      const float w1a = (fu_m1 + fu_0) * (s0 - S0[-2]) * dxv24;
-      const float w1b = (fu_p1 + fu_p2) * (S0[2] - s0) * dxv24;
-      const float w2a = (fv_m1 + fv_0) * (s0 - S0[-2 * BX]) * dyv24;
-      const float w2b = (fv_p1 + fv_p2) * (S0[2 * BX] - s0) * dyv24;
+      const F2 s0 = ld2(S0);
+      const F2 t1a = fu_0 * (s0 - pair_at(S0, -1)) * dxv05n;
+      const F2 t1b = fu_p1 * (pair_at(S0, 1) - s0) * dxv05n;
+      const F2 t2a = fv_0 * (s0 - ld2(S0 - BX)) * dyv05n;
+      const F2 t2b = fv_p1 * (ld2(S0 + BX) - s0) * dyv05n;
+      F2 f = (t1a + t1b) + (t2a + t2b);
+      const F2 w1a = (fu_m1 + fu_0) * (s0 - ld2(S0 - 2)) * dxv24;
+      const F2 w1b = (fu_p1 + fu_p2) * (ld2(S0 + 2) - s0) * dxv24;
+      const F2 w2a = (fv_m1 + fv_0) * (s0 - ld2(S0 - 2 * BX)) * dyv24;
+      const F2 w2b = (fv_p1 + fv_p2) * (ld2(S0 + 2 * BX) - s0) * dyv24;
       f = fourd3 * f + ((w1a + w1b) + (w2a + w2b));
-      const float t3a = fw_0 * (s0 - st(-1)[L::oS + oS]) * dzv05n;
-      const float t3b = fw_1 * (st(1)[L::oS + oS] - s0) * dzv05n;
+      const F2 t3a = fw_0 * (s0 - ld2(st(-1) + L::oS + oS)) * dzv05n;
+      const F2 t3b = fw_1 * (ld2(st(1) + L::oS + oS) - s0) * dzv05n;
       f = f + (t3a + t3b);
 
       // the species at t-dt at an offset (horizontal ones on level k only)
       auto SPo = [&](int dx, int dy, int dz) {
-        return dz == 0 ? SP0[dx + dy * BX] : st(dz)[L::oSP + oS];
+        return dz == 0 ? pair_at(SP0 + dy * BX, dx) : ld2(st(dz) + L::oSP + oS);
       };
       if (smooth) {
         auto A = [&](int dx, int dy, int dz) {
           const int kk = k + dz;
-          const float v = SPo(dx, dy, dz);
+          const F2 v = SPo(dx, dy, dz);
           return isqv ? C(C_RBR, kk) * (v - C(C_QVBR, kk)) : C(C_RBR, kk) * v;
         };
         f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
       }
       if constexpr (TURB) {
         auto R = [&](int dx, int dy, int dz) {
-          return dz == 0 ? st0[L::oR + oS + dx + dy * BX] : st(dz)[L::oR + oS];
+          return dz == 0 ? pair_at(st0 + L::oR + oR + dy * BX, dx) : ld2(st(dz) + L::oR + oR);
         };
         f = turb_scalar_at(f, C, k, a.cpriv, a.dxiv, a.dyiv, a.dziv, R, SPo);
       }
-      const float spv = SP0[0];
+      const F2 spv = ld2(SP0);
       if (vsp && k >= a.ksp0 - 1) f = f - rbct5 * rst * (isqv ? spv - C(C_QVBR, k) : spv);
-      float sf = spv + f * dtdrst;
-      if (n < 6) sf = fmaxf(0.f, sf);
-      out[id] = sf;
-      if (k == 2) out[id - plane] = sf;        // vbcs.f90:118
-      if (k == nk - 2) out[id + plane] = sf;   // vbcs.f90:132
+      F2 sf = spv + f * dtdrst;
+      if (n < 6) sf = fmax2(sf, 0.f);
+      // the pair's first index is even, so the pair store is 8-byte aligned
+      auto put = [&](long long at) {
+        if (ownB) *reinterpret_cast<float2*>(out + at) = sf.v;
+        else out[at] = sf.v.x;
+      };
+      put(id);
+      if (k == 2) put(id - plane);        // vbcs.f90:118
+      if (k == nk - 2) put(id + plane);   // vbcs.f90:132
     }
 #pragma unroll
     for (int d = 0; d < 4; ++d) stp[d] = stp[d + 1];
@@ -228,8 +252,8 @@ int launch_sc(const MoistScalarArgs& a, const MoistMaps& maps, cudaStream_t st) 
       cudaSuccess)
     return CRESS_E_CUDA;
   const int nx = g.ni - 3, ny = g.nj - 3;
-  dim3 block(kHeviTX, kScalarTY);
-  dim3 grid((nx + kHeviTX - 1) / kHeviTX * kMoistN, (ny + kScalarTY - 1) / kScalarTY);
+  dim3 block(kScPairs, kScalarTY, kScGroup);
+  dim3 grid((nx + kHeviTX - 1) / kHeviTX * (kMoistN / kScGroup), (ny + kScalarTY - 1) / kScalarTY);
   k_scalars<S, TURB><<<grid, block, bytes, st>>>(maps, a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
@@ -238,7 +262,7 @@ int launch_sc(const MoistScalarArgs& a, const MoistMaps& maps, cudaStream_t st) 
 
 int launch_moist_scalars(const MoistScalarArgs& a, const MoistMaps& maps, cudaStream_t st) {
   if (a.g.nk < 5) return CRESS_E_UNSUPPORTED;
-  return a.rkv ? launch_sc<7, true>(a, maps, st) : launch_sc<8, false>(a, maps, st);
+  return a.rkv ? launch_sc<6, true>(a, maps, st) : launch_sc<6, false>(a, maps, st);
 }
 
 }  // namespace cress

@@ -1,59 +1,35 @@
 // Stencil helpers shared by the large-step kernels (internal): the
 // 4th-order numerical smoothing and the Smagorinsky mixing of a scalar,
-// written over accessor functors so that a kernel reading neighbours from
-// global memory and one reading them from a shared-memory tile form the
-// same terms in the same order.
+// written over accessor functors so that every kernel that uses them forms
+// the same terms in the same order, whatever memory its neighbours come
+// from and whether it computes one point or a pair (F2).
 #pragma once
 #include "hevi.cuh"
 
 namespace cress {
 
 // 4th-order smoothing increments (smoo4s.f90:199-296 and its u/v/w/p
-// variants) around `id`: A(dx,dy,dz) returns the smoothed quantity at an
-// offset.  wlev: the field sits on w levels (vertical ghost rule at nk).
-template <class FA>
-__device__ __forceinline__ float smooth_into(float frc, int smtopt, float smhcoe, float smvcoe, int k,
-                                             int kmin, int kmax, const FA& A) {
-  const float a0 = A(0, 0, 0);
-  auto t1 = [&](int x) { return (A(x + 1, 0, 0) + A(x - 1, 0, 0)) - 2.f * A(x, 0, 0); };
-  auto t2 = [&](int y) { return (A(0, y + 1, 0) + A(0, y - 1, 0)) - 2.f * A(0, y, 0); };
-  auto t3 = [&](int z) {
-    int kk = k + z;
-    if (kk < kmin) kk = kmin;   // tmp3(k=kmin-1) = tmp3(kmin)
-    if (kk > kmax) kk = kmax;   // tmp3(kmax+1) = tmp3(kmax)
-    const int d = kk - k;
-    return (A(0, 0, d + 1) + A(0, 0, d - 1)) - 2.f * A(0, 0, d);
-  };
-  (void)a0;
-  const float t10 = t1(0), t20 = t2(0), t30 = t3(0);
-  frc = frc + smhcoe * (t10 + t20) + smvcoe * t30;
-  if (smtopt % 10 == 2) {
-    frc = frc + smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1))));
-  } else {
-    frc = frc + (smvcoe * (t30 - (t3(1) + t3(-1))) +
-                 smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1)))));
-  }
-  return frc;
-}
-
-// The same increments where A may be evaluated at every dz in -2..2 (a
-// shared-memory ring that holds those levels, whatever they contain at the
-// ends of the column): the clamping of the vertical second difference at
-// kmin and kmax becomes a selection, so every offset is a compile-time
-// constant and the result is the one smooth_into forms.
-template <class FA>
-__device__ __forceinline__ float smooth_tile(float frc, int smtopt, float smhcoe, float smvcoe, int k, int kmin,
-                                             int kmax, const FA& A) {
+// variants) added to frc at a point of level k: A(dx, dy, dz) returns the
+// smoothed quantity at an offset, and may be evaluated at every dz in
+// -2..2 (a shared-memory ring that holds those levels, whatever they
+// contain at the ends of the column).  The reference clamps the vertical
+// second difference at kmin and kmax (tmp3(kmin-1) = tmp3(kmin),
+// tmp3(kmax+1) = tmp3(kmax)); here that is a selection, so every offset is
+// a compile-time constant.
+// T is float, or F2 (f2.cuh) for two points at once.
+template <class T, class FA>
+__device__ __forceinline__ T smooth_tile(T frc, int smtopt, float smhcoe, float smvcoe, int k, int kmin, int kmax,
+                                         const FA& A) {
   auto t1 = [&](int x) { return (A(x + 1, 0, 0) + A(x - 1, 0, 0)) - 2.f * A(x, 0, 0); };
   auto t2 = [&](int y) { return (A(0, y + 1, 0) + A(0, y - 1, 0)) - 2.f * A(0, y, 0); };
   auto t3 = [&](int z) { return (A(0, 0, z + 1) + A(0, 0, z - 1)) - 2.f * A(0, 0, z); };
-  const float t10 = t1(0), t20 = t2(0), t30 = t3(0);
+  const T t10 = t1(0), t20 = t2(0), t30 = t3(0);
   frc = frc + smhcoe * (t10 + t20) + smvcoe * t30;
   if (smtopt % 10 == 2) {
     frc = frc + smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1))));
   } else {
-    const float t3p = k >= kmax ? t30 : t3(1);    // tmp3(kmax+1) = tmp3(kmax)
-    const float t3m = k <= kmin ? t30 : t3(-1);   // tmp3(kmin-1) = tmp3(kmin)
+    const T t3p = k >= kmax ? t30 : t3(1);    // tmp3(kmax+1) = tmp3(kmax)
+    const T t3m = k <= kmin ? t30 : t3(-1);   // tmp3(kmin-1) = tmp3(kmin)
     frc = frc + (smvcoe * (t30 - (t3p + t3m)) +
                  smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1)))));
   }
@@ -66,9 +42,9 @@ __device__ __forceinline__ float smooth_tile(float frc, int smtopt, float smhcoe
 // (rkh(k-1)+rkh(k))/2; eddydif.f90:154-260, kh8uv.f90:211-230) and the
 // flux divergence of s_turbflx / s_turbs (turbflx.f90:236-352,
 // turbs.f90:189-232), added to frc.
-template <class FC, class FR, class FS>
-__device__ __forceinline__ float turb_scalar_at(float frc, const FC& C, int k, float cpriv, float dxiv, float dyiv,
-                                                float dziv, const FR& R, const FS& S) {
+template <class T, class FC, class FR, class FS>
+__device__ __forceinline__ T turb_scalar_at(T frc, const FC& C, int k, float cpriv, float dxiv, float dyiv,
+                                            float dziv, const FR& R, const FS& S) {
   // R(dx, dy, dz): eddy viscosity, S(dx, dy, dz): the scalar, at an offset
   // from the point (only dz = -1, 0, 1 on the point's own column)
   auto RKH = [&](int dx, int dy, int dz) { return cpriv * R(dx, dy, dz) * C(C_IJCB, k + dz); };
