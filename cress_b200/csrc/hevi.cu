@@ -312,7 +312,6 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
         wk = 0.f;  // vbcw.f90:317 (flat terrain)
       }
       const float rcsq = cols[C_RCSQ * ncol + k], rst = cols[C_RST * ncol + k];
-      const float jcb = cols[C_JCB * ncol + k];
       const float pvd = rcsq * (wk - wup) * dziv;                                              // diverpiv.f90:124
       const float fp = fpb + a.weicoe * (a.g05 * (wk + wup) * rst + pvd);                        // advbspi.f90:175
       const float pn = po + dts * fp * cols[C_IJCB * ncol + k];                                                     // steppi.f90:217

@@ -16,7 +16,8 @@
 //   * three v faces (south of the first row, between the rows, north of the
 //     second), where one thread per row would form four;
 //   * two independent Thomas recurrences (instruction-level parallelism).
-// Per-level constants come from a k-major table in shared memory, so each
+// The two rows' single-precision arithmetic runs as packed FP32x2
+// instructions (f2.cuh), one instruction for both rows.  Per-level constants come from a k-major table in shared memory, so each
 // is one load at a fixed offset.  Eliminated right-hand sides are parked
 // (float) in the new w array and the backward pressure tendency in the new
 // p' array, as in the GS variant of k_hevi_substep.
@@ -24,6 +25,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "common.cuh"
+#include "f2.cuh"
 #include "hevi.cuh"
 #include "tma.cuh"
 
@@ -147,8 +149,7 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   const int fyA = 2 * ty, fyB = fyA + 1;       // own rows in the forcing boxes (from j0)
   const float dts = a.dts, dxiv = a.dxiv, dyiv = a.dyiv, dziv = a.dziv;
   const float weic1m = 1.f - a.weicoe;
-  float t3vA_prev = 0.f, fpdvjA_prev = 0.f, wb8sA_prev = 0.f;
-  float t3vB_prev = 0.f, fpdvjB_prev = 0.f, wb8sB_prev = 0.f;
+  F2 t3v_prev = f2(0.f), fpdvj_prev = f2(0.f), wb8s_prev = f2(0.f);   // rows A, B
   double fA_prev = 0.0, fB_prev = 0.0;
   bool fail = false;
   // 32-bit element indices (the launcher checks that every field fits)
@@ -197,13 +198,23 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       else th = pp;
       return jcbk * th;
     };
-    const float divA = div3d_at(ox, oyA), ppA = P[oyA * BX + ox];
-    const float divB = div3d_at(ox, oyB), ppB = P[oyB * BX + ox];
-    const float tcA = t3h_of(divA, ppA), tcB = t3h_of(divB, ppB);
-    t3h[oyA * BX + ox] = tcA;
-    t3h[oyB * BX + ox] = tcB;
-    const float t3vA = (DIV >= 1) ? ppA + a.divcv * jcbk * divA : ppA;  // pgrad.f90:300
-    const float t3vB = (DIV >= 1) ? ppB + a.divcv * jcbk * divB : ppB;
+    // rows A and B of the thread packed into the two lanes of F2 (f2.cuh):
+    // every operation below is one packed instruction for both rows
+    auto col2 = [&](const float* base, int oy) { return f2(base[oy * BX + ox], base[(oy + 1) * BX + ox]); };
+    F2 wc0 = col2(W0, oyA), wc1 = col2(W1, oyA);
+    if constexpr (STH) { wc0 = wc0 * ij8wk; wc1 = wc1 * ij8wk1; }
+    const F2 div = (rst8wk * wc0 - rst8wk1 * wc1) * dziv +
+                   ((rst8u * col2(U, oyA) - rst8u * col2(U + 1, oyA)) * dxiv +
+                    (rst8v * col2(V, oyA) - rst8v * col2(V + BX, oyA)) * dyiv);      // diver3d.f90:318
+    const F2 pp = col2(P, oyA);
+    F2 th;                                                                         // pgrad.f90:341,363
+    if constexpr (DIV == 2) th = pp + a.divch * div * ijcbk;
+    else if constexpr (DIV == 1) th = pp + a.divcv * jcbk * div;
+    else th = pp;
+    const F2 tc = jcbk * th;
+    t3h[oyA * BX + ox] = tc.v.x;
+    t3h[oyB * BX + ox] = tc.v.y;
+    const F2 t3v = (DIV >= 1) ? pp + a.divcv * jcbk * div : pp;                    // pgrad.f90:300
     if (has_halo) t3h[hy * BX + hx] = t3h_of(div3d_at(hx, hy), P[hy * BX + hx]);
     __syncthreads();
     if (tid == 0 && k + S - 1 <= klast) {
@@ -213,72 +224,69 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
 
     // stepuv.f90:294,304 with pgrad.f90:379,389: west u faces, the east
     // face from the next lane (lane 31 forms its own)
-    const float unA0 = U[oyA * BX + ox] + dts * (UF[fyA * BX + ox] + (t3h[oyA * BX + ox - 1] - tcA) * dxiv) * irst8u;
-    const float unB0 = U[oyB * BX + ox] + dts * (UF[fyB * BX + ox] + (t3h[oyB * BX + ox - 1] - tcB) * dxiv) * irst8u;
-    float unA1 = __shfl_down_sync(full, unA0, 1);
-    float unB1 = __shfl_down_sync(full, unB0, 1);
-    if (tx == TX - 1) {
-      unA1 = U[oyA * BX + ox + 1] + dts * (UF[fyA * BX + ox + 1] + (tcA - t3h[oyA * BX + ox + 1]) * dxiv) * irst8u;
-      unB1 = U[oyB * BX + ox + 1] + dts * (UF[fyB * BX + ox + 1] + (tcB - t3h[oyB * BX + ox + 1]) * dxiv) * irst8u;
-    }
-    // v faces south of row A, between the rows, north of row B
-    const float vf0 = V[oyA * BX + ox] + dts * (VF[fyA * BX + ox] + (t3h[(oyA - 1) * BX + ox] - tcA) * dyiv) * irst8v;
-    const float vf1 = V[oyB * BX + ox] + dts * (VF[fyB * BX + ox] + (tcA - tcB) * dyiv) * irst8v;
-    const float vf2 = V[(oyB + 1) * BX + ox] + dts * (VF[(fyB + 1) * BX + ox] + (tcB - t3h[(oyB + 1) * BX + ox]) * dyiv) * irst8v;
+    const F2 un0 = col2(U, oyA) + dts * (col2(UF, fyA) + (col2(t3h - 1, oyA) - tc) * dxiv) * irst8u;
+    F2 un1 = f2(__shfl_down_sync(full, un0.v.x, 1), __shfl_down_sync(full, un0.v.y, 1));
+    if (tx == TX - 1)
+      un1 = col2(U + 1, oyA) + dts * (col2(UF + 1, fyA) + (tc - col2(t3h + 1, oyA)) * dxiv) * irst8u;
+    // v faces south of rows A and B (the one between the rows serves both),
+    // and north of row B
+    const F2 vs = col2(V, oyA) + dts * (col2(VF, fyA) + (f2(t3h[(oyA - 1) * BX + ox], tc.v.x) - tc) * dyiv) * irst8v;
+    const float vf2 = V[(oyB + 1) * BX + ox] +
+                      dts * (VF[(fyB + 1) * BX + ox] + (tc.v.y - t3h[(oyB + 1) * BX + ox]) * dyiv) * irst8v;
+    const F2 vn = f2(vs.v.y, vf2);
 
     const float jcb8u = ck[C_JCB8U], jcb8v = ck[C_JCB8V];
     const float rcsq = ck[C_RCSQ], rst = ck[C_RST], rbr = ck[C_RBR], ircsq = ck[C_IRCSQ];
     const float irst8w = ck[C_IRST8W];
-    // one row: the stores of stepuv and everything up to the forward
-    // elimination step
+    // the stores of stepuv for one row
     const bool kend = (k == 2) || (k == nk - 2);
-    auto row = [&](bool own, bool edge, bool ylast, int j, int id, int oy, int fy, float un0, float un1,
-                   float vn0, float vn1, float ppo, float t3v, float& t3v_prev, float& fpdvj_prev,
-                   float& wb8s_prev, double& fprev) {
-      if (!own) return;
+    auto store_uv = [&](bool edge, bool ylast, int j, int id, float u0, float u1, float v0, float v1) {
       if (edge) {
-        store_periodic(a.u_new, g, STAG_U, i, j, k, un0);
-        store_periodic(a.v_new, g, STAG_V, i, j, k, vn0);
+        store_periodic(a.u_new, g, STAG_U, i, j, k, u0);
+        store_periodic(a.v_new, g, STAG_V, i, j, k, v0);
       } else {
-        a.u_new[id] = un0;
-        a.v_new[id] = vn0;
+        a.u_new[id] = u0;
+        a.v_new[id] = v0;
       }
-      if (xlast) store_periodic(a.u_new, g, STAG_U, i + 1, j, k, un1);
-      if (ylast) store_periodic(a.v_new, g, STAG_V, i, j + 1, k, vn1);
+      if (xlast) store_periodic(a.u_new, g, STAG_U, i + 1, j, k, u1);
+      if (ylast) store_periodic(a.v_new, g, STAG_V, i, j + 1, k, v1);
       if (kend) {   // vbcu.f90:120,134 (and vbcv): levels 1 and nk-1 copy levels 2 and nk-2
         const int kc = k == 2 ? 1 : nk - 1;
-        store_periodic(a.u_new, g, STAG_U, i, j, kc, un0);
-        store_periodic(a.v_new, g, STAG_V, i, j, kc, vn0);
-        if (xlast) store_periodic(a.u_new, g, STAG_U, i + 1, j, kc, un1);
-        if (ylast) store_periodic(a.v_new, g, STAG_V, i, j + 1, kc, vn1);
+        store_periodic(a.u_new, g, STAG_U, i, j, kc, u0);
+        store_periodic(a.v_new, g, STAG_V, i, j, kc, v0);
+        if (xlast) store_periodic(a.u_new, g, STAG_U, i + 1, j, kc, u1);
+        if (ylast) store_periodic(a.v_new, g, STAG_V, i, j + 1, kc, v1);
       }
-      float phd = (jcb8u * un0 - jcb8u * un1) * dxiv + (jcb8v * vn0 - jcb8v * vn1) * dyiv;  // diver2d.f90:288
-      phd = rcsq * phd;                                                                       // diverpih.f90:208
-      const float wk = W0[oy * BX + ox], wk1 = W1[oy * BX + ox];
-      const float pvd = rcsq * (wk - wk1) * dziv;                                             // diverpiv.f90:124
-      const float fp = PF[fy * BX + ox] + phd + weic1m * (a.g05 * (wk + wk1) * rst + pvd);    // advbspi.f90:158
-      a.p_new[id] = fp;  // parked until the way down
-      const float fpdvj = fp * ijcbk;                                                          // pgradiv.f90:149
-      const float wb8s = (ppo * rst + fp * rbr * a.dtw) * ircsq * a.g05n;                     // buoywsi.f90:171
-      if (k >= 3) {
-        const float wpg = (t3v_prev - t3v) * dziv;                                            // pgrad.f90:320
-        float fw = WF[fy * BX + ox] + wpg + (fpdvj_prev - fpdvj) * a.dtdzw;                   // pgradiv.f90:163
-        if constexpr (BUY) fw = fw + (wb8s_prev + wb8s);                                      // buoywsi.f90:205
-        const float wrhs = wk + dts * fw * irst8w;                                            // stepwi.f90:325
-        // gaussel.f90:189-240 in double with the 1-D factors
-        const double rr = (double)thr[k], aa = thd[k];
-        const double f = (k == 3) ? (double)wrhs * aa : ((double)wrhs - rr * fprev) * aa;
-        a.w_new[id] = (float)f;   // parked until the way down
-        fprev = f;
-      }
-      t3v_prev = t3v;
-      fpdvj_prev = fpdvj;
-      wb8s_prev = wb8s;
     };
-    row(ownA, edgeA, ylastA, jA, idA, oyA, fyA, unA0, unA1, vf0, vf1, ppA, t3vA, t3vA_prev, fpdvjA_prev,
-        wb8sA_prev, fA_prev);
-    row(ownB, edgeB, ylastB, jB, idB, oyB, fyB, unB0, unB1, vf1, vf2, ppB, t3vB, t3vB_prev, fpdvjB_prev,
-        wb8sB_prev, fB_prev);
+    if (ownA) store_uv(edgeA, ylastA, jA, idA, un0.v.x, un1.v.x, vs.v.x, vn.v.x);
+    if (ownB) store_uv(edgeB, ylastB, jB, idB, un0.v.y, un1.v.y, vs.v.y, vn.v.y);
+
+    F2 phd = (jcb8u * un0 - jcb8u * un1) * dxiv + (jcb8v * vs - jcb8v * vn) * dyiv;    // diver2d.f90:288
+    phd = rcsq * phd;                                                                   // diverpih.f90:208
+    const F2 wk = col2(W0, oyA), wk1 = col2(W1, oyA);
+    const F2 pvd = rcsq * (wk - wk1) * dziv;                                            // diverpiv.f90:124
+    const F2 fp = col2(PF, fyA) + phd + weic1m * (a.g05 * (wk + wk1) * rst + pvd);      // advbspi.f90:158
+    if (ownA) a.p_new[idA] = fp.v.x;   // parked until the way down
+    if (ownB) a.p_new[idB] = fp.v.y;
+    const F2 fpdvj = fp * ijcbk;                                                        // pgradiv.f90:149
+    const F2 wb8s = (pp * rst + fp * rbr * a.dtw) * ircsq * a.g05n;                     // buoywsi.f90:171
+    if (k >= 3) {
+      const F2 wpg = (t3v_prev - t3v) * dziv;                                           // pgrad.f90:320
+      F2 fw = col2(WF, fyA) + wpg + (fpdvj_prev - fpdvj) * a.dtdzw;                     // pgradiv.f90:163
+      if constexpr (BUY) fw = fw + (wb8s_prev + wb8s);                                  // buoywsi.f90:205
+      const F2 wrhs = wk + dts * fw * irst8w;                                           // stepwi.f90:325
+      // gaussel.f90:189-240 in double with the 1-D factors, one recurrence per row
+      const double rr = (double)thr[k], aa = thd[k];
+      const double fA = (k == 3) ? (double)wrhs.v.x * aa : ((double)wrhs.v.x - rr * fA_prev) * aa;
+      const double fB = (k == 3) ? (double)wrhs.v.y * aa : ((double)wrhs.v.y - rr * fB_prev) * aa;
+      if (ownA) a.w_new[idA] = (float)fA;   // parked until the way down
+      if (ownB) a.w_new[idB] = (float)fB;
+      fA_prev = fA;
+      fB_prev = fB;
+    }
+    t3v_prev = t3v;
+    fpdvj_prev = fpdvj;
+    wb8s_prev = wb8s;
   }
 
   if (__syncthreads_or(fail)) {
