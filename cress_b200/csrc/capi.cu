@@ -389,12 +389,12 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
                                   lev[CRESS_PTP][N], lev[CRESS_U][P], lev[CRESS_V][P], lev[CRESS_W][P],
                                   lev[CRESS_PP][P], lev[CRESS_PTP][P], f.rkv};
     ForceMaps fm;
-    for (int gi = 0; gi < kForceGroups; ++gi)
-      for (int q = 0; q < force_nfields(gi, f.rkv != nullptr); ++q)
-        if ((rc = tmap(bufs[force_field_buf(gi, q)], force_field_rows(gi, q), &fm.m[gi][q]))) return rc;
+    for (int sg = 0; sg < 2; ++sg)
+      for (int q = 0; q < force_nslots(sg, f.rkv != nullptr); ++q)
+        if ((rc = tmap(bufs[force_slot_buf(sg, q)], force_slot_rows(sg, q), &fm.m[sg][q]))) return rc;
     rc = launch_force(f, fm, stream);
   }
-  ++launches;
+  launches += 2;
   if (rc) return set_error(rc, "forcing launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   if ((rc = small_steps(nsstp, dts))) return rc;
   if (moist) {

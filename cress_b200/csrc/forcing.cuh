@@ -82,45 +82,33 @@ struct ForceArgs {
   int* err;                   // device error word (a bounded wait gave up)
 };
 
-// The forcing kernel computes five output groups (u, v, w, p', theta'),
-// each from its own list of staged fields: 32 x kForceTY tiles of every
-// level are copied by TMA into a shared-memory ring (boxes kHeviBoxX wide,
-// x from the tile's i0-2; rows from j0 + force_field_r0 on,
-// force_field_rows of them).  Slot q of group G reads force_field_buf.
+// The forcing runs as two kernels over 32 x kForceTY tiles: the momentum
+// kernel (output groups u, v, w in one block) and the scalar kernel
+// (groups p' and theta').  Each stages its fields (slots) level by level
+// by TMA into a shared-memory ring: boxes kHeviBoxX wide, x from the
+// tile's i0-2, rows from j0 + force_slot_r0 on, force_slot_rows of them.
 constexpr int kForceTY = 8;
-constexpr int kForceGroups = 5;
-constexpr int kForceFields = 7;
+constexpr int kForceSlots = 8;
 enum ForceBuf { FB_U, FB_V, FB_W, FB_PP, FB_PTP, FB_UP, FB_VP, FB_WP, FB_PPP, FB_PTPP, FB_RKV, FB_NONE };
-// number of staged fields of group g (with turbulence: turb != 0)
-__host__ __device__ constexpr int force_nfields(int g, bool turb) {
-  return g <= 2 ? (turb ? 7 : 4) : (g == 3 ? 5 : (turb ? 6 : 5));
+// staged fields of kernel sg (0 momentum, 1 scalar), with turbulence: turb
+__host__ __device__ constexpr int force_nslots(int sg, bool turb) { return sg == 0 ? (turb ? 7 : 6) : (turb ? 8 : 7); }
+// momentum: u, v, w, up, vp, wp | rkv       scalar: pp, ptp, ppp, ptpp, u, v, w | rkv
+__host__ __device__ constexpr int force_slot_buf(int sg, int s) {
+  return sg == 0 ? (s == 0 ? FB_U : s == 1 ? FB_V : s == 2 ? FB_W : s == 3 ? FB_UP : s == 4 ? FB_VP : s == 5 ? FB_WP : FB_RKV)
+                 : (s == 0 ? FB_PP : s == 1 ? FB_PTP : s == 2 ? FB_PPP : s == 3 ? FB_PTPP : s == 4 ? FB_U
+                    : s == 5 ? FB_V : s == 6 ? FB_W : FB_RKV);
 }
-__host__ __device__ constexpr int force_field_buf(int g, int q) {
-  // u: u, v, w, up | vp, wp, rkv    v: v, u, w, vp | up, wp, rkv
-  // w: w, u, v, wp | up, vp, rkv    p': pp, u, v, w, ppp    theta': ptp, u, v, w, ptpp | rkv
-  return g == 0 ? (q == 0 ? FB_U : q == 1 ? FB_V : q == 2 ? FB_W : q == 3 ? FB_UP : q == 4 ? FB_VP : q == 5 ? FB_WP : FB_RKV)
-       : g == 1 ? (q == 0 ? FB_V : q == 1 ? FB_U : q == 2 ? FB_W : q == 3 ? FB_VP : q == 4 ? FB_UP : q == 5 ? FB_WP : FB_RKV)
-       : g == 2 ? (q == 0 ? FB_W : q == 1 ? FB_U : q == 2 ? FB_V : q == 3 ? FB_WP : q == 4 ? FB_UP : q == 5 ? FB_VP : FB_RKV)
-       : g == 3 ? (q == 0 ? FB_PP : q == 1 ? FB_U : q == 2 ? FB_V : q == 3 ? FB_W : q == 4 ? FB_PPP : FB_NONE)
-                : (q == 0 ? FB_PTP : q == 1 ? FB_U : q == 2 ? FB_V : q == 3 ? FB_W : q == 4 ? FB_PTPP : q == 5 ? FB_RKV : FB_NONE);
+// first box row relative to j0 and the number of rows: the momentum slots
+// and the scalars' own variables carry two rows of y halo; the scalars'
+// winds and viscosity what their stencils reach
+__host__ __device__ constexpr int force_slot_r0(int sg, int s) {
+  return (sg == 0 || s < 4) ? -2 : (s == 4 || s == 6) ? 0 : -1;
 }
-// first box row relative to j0 and the number of rows
-__host__ __device__ constexpr int force_field_r0(int g, int q) {
-  return g == 0 ? (q == 0 ? -2 : q == 1 ? -1 : q == 2 ? 0 : q == 3 ? -2 : q == 4 ? 0 : q == 5 ? 0 : -1)
-       : g == 1 ? (q == 0 ? -2 : q == 1 ? -1 : q == 2 ? -1 : q == 3 ? -2 : -1)
-       : g == 2 ? (q == 0 ? -2 : q == 1 ? 0 : q == 2 ? -1 : q == 3 ? -2 : q == 4 ? 0 : q == 5 ? 0 : -1)
-       : g == 3 ? (q == 0 ? -2 : q == 1 ? 0 : q == 2 ? -1 : q == 3 ? 0 : -2)
-                : (q == 0 ? -2 : q == 1 ? 0 : q == 2 ? -1 : q == 3 ? 0 : q == 4 ? -2 : -1);
-}
-__host__ __device__ constexpr int force_field_rows(int g, int q) {
-  return kForceTY + (g == 0 ? (q == 0 ? 4 : q == 1 ? 3 : q == 2 ? 0 : q == 3 ? 4 : q == 4 ? 1 : q == 5 ? 0 : 2)
-                   : g == 1 ? (q == 0 ? 4 : q == 3 ? 4 : 1)
-                   : g == 2 ? (q == 0 ? 4 : q == 1 ? 0 : q == 2 ? 3 : q == 3 ? 4 : q == 4 ? 0 : q == 5 ? 1 : 2)
-                   : g == 3 ? (q == 0 ? 4 : q == 1 ? 0 : q == 2 ? 3 : q == 3 ? 0 : 4)
-                            : (q == 0 ? 4 : q == 1 ? 0 : q == 2 ? 3 : q == 3 ? 0 : q == 4 ? 4 : 2));
+__host__ __device__ constexpr int force_slot_rows(int sg, int s) {
+  return kForceTY + ((sg == 0 || s < 4) ? 4 : (s == 4 || s == 6) ? 0 : s == 5 ? 3 : 2);
 }
 struct ForceMaps {
-  CUtensorMap m[kForceGroups][kForceFields];
+  CUtensorMap m[2][kForceSlots];
 };
 
 int launch_force(const ForceArgs& a, const ForceMaps& maps, cudaStream_t st);
