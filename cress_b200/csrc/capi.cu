@@ -261,6 +261,33 @@ int Ctx::tmap(const float* buf, int rows, CUtensorMap* out) {
   return CRESS_OK;
 }
 
+// The level table of the large-step kernels for a step of 2*dtb = dtb2
+// (forcing.cuh: columns, reciprocals, derived quotients), formed on the
+// host with the same IEEE operations the device would use and kept per
+// distinct dtb2 (the half first step and the regular one).
+int Ctx::level_table(float dtb2, const float** out) {
+  uint32_t key;
+  std::memcpy(&key, &dtb2, 4);
+  auto it = level_tables.find(key);
+  if (it != level_tables.end()) { *out = it->second; return CRESS_OK; }
+  const int nk = g.nk, nc = nk + 1;
+  auto B = [&](int f, int kk) { return col_h[(size_t)f * nc + kk]; };
+  std::vector<float> t((size_t)nc * kLevelStride, 0.f);
+  for (int kk = 0; kk < nc; ++kk)
+    for (int f = 0; f < D_NFIELDS; ++f) t[(size_t)kk * kLevelStride + f] = level_value(f, kk, B, dtb2);
+  float* d = nullptr;
+  int rc;
+  if ((rc = cuda_check(cudaMalloc(&d, sizeof(float) * t.size()), "cudaMalloc level table"))) return rc;
+  owned.push_back(d);
+  if ((rc = cuda_check(cudaMemcpyAsync(d, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice, stream),
+                       "copy level table")) ||
+      (rc = cuda_check(cudaStreamSynchronize(stream), "sync level table")))
+    return rc;
+  level_tables.emplace(key, d);
+  *out = d;
+  return CRESS_OK;
+}
+
 int Ctx::small_steps(int nsstp, float dts) {
   if (!base_set) return set_error(CRESS_E_STATE, "cress_small_steps: base state not set");
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_small_steps: nsstp=%d", nsstp);
@@ -351,6 +378,8 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
   f.smhcoe = cfg.smhcoe; f.smvcoe = cfg.smvcoe;
   f.fc = cfg.fc;
   f.dtb2 = 2.f * dtb;
+  int rc;
+  if ((rc = level_table(f.dtb2, &f.lvl))) return rc;
   f.smtopt = cfg.smtopt; f.vspopt = cfg.vspopt; f.coropt = cfg.coropt; f.sthopt = cfg.sthopt;
   f.ksp0 = ksp0;
   auto on = [&](int n) { return cfg.vspvar[n] == 'o' ? 1 : 0; };
@@ -360,7 +389,6 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
     f.qi = lev[CRESS_QI][N]; f.qs = lev[CRESS_QS][N]; f.qg = lev[CRESS_QG][N];
   }
   const float cpriv = 3.f;   // min(1/prnum, 3) with prnum = 0.33 (eddyvis.f90:219-222)
-  int rc;
   if (cfg.tubopt == 1) {
     // s_turbdrv up to s_eddyvis on the past level (forceuvw.f90:423-431)
     TurbArgs t{};
@@ -413,6 +441,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
     m.vsp_qv = on(5); m.vsp_q = on(6);
     m.rkv = f.rkv; m.cpriv = cpriv;
     m.err = err_d;
+    m.lvl = f.lvl;
     MoistMaps mm;
     for (int n = 0; n < kMoistN; ++n)
       if ((rc = tmap(m.s[n], ScalarRows::s, &mm.s[n])) || (rc = tmap(m.sp[n], ScalarRows::s, &mm.sp[n]))) return rc;

@@ -45,6 +45,8 @@ struct Ctx {
   int put_host(float* dst, const float* host);
   int get_host(float* host, const float* src);
   int thomas_for(float dts, const ThomasSet** out);
+  std::map<uint32_t, float*> level_tables;   // level table per 2*dtb (bits)
+  int level_table(float dtb2, const float** out);
   int small_steps(int nsstp, float dts);
   int large_step(bool filter, float dtb, int nsstp, float dts);
   int ksp0 = 2;            // first Rayleigh-damped level

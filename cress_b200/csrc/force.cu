@@ -63,7 +63,7 @@ struct FLayout {
     return b;
   }
   static size_t bytes(int nk) {
-    return 4 * ((size_t)S * stage + (size_t)r128c(kNF * (nk + 1))) + 8 * (size_t)S;
+    return 4 * (size_t)S * stage + 8 * (size_t)S;
   }
 };
 
@@ -87,7 +87,7 @@ __device__ __forceinline__ F2 gld2(const float* p) { return F2{__ldg(reinterpret
 // index of the pair's first point (even), ownB whether the second point is
 // owned too, wb_prev the w group's buoyancy term of the level below.
 template <int G, bool T>
-__device__ __forceinline__ void force_point(const ForceArgs& a, const float* const* stp, const float* cols,
+__device__ __forceinline__ void force_point(const ForceArgs& a, const float* const* stp,
                                             int rowbase, long long id, int k, bool ownB, F2& wb_prev) {
   constexpr int SG = G <= 2 ? 0 : 1;
   using L = FLayout<SG, T>;
@@ -102,8 +102,8 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
   const float dxv05n = -.5f * dxiv, dyv05n = -.5f * dyiv, dzv05n = -.5f * dziv;
   const bool smooth = (a.smtopt % 10 == 2) || (a.smtopt % 10 == 3);
   const float g05 = .5f * 9.8f;
-  const float* ck = cols + k * kNF;
-  auto C = [&](int f, int kk) { return ck[(kk - k) * kNF + f]; };
+  const float* ck = a.lvl + k * kNF;
+  auto C = [&](int f, int kk) { return __ldg(ck + (kk - k) * kNF + f); };
   // field q of this group at the offset (dx, dy, dz), both points
   auto X = [&](int q, int dx, int dy, int dz) {
     const int s = force_slot(G, q);
@@ -356,7 +356,7 @@ template <int SG, bool T>
 __global__ void __launch_bounds__(kFPairs * kForceTY * (SG == 0 ? 3 : 2))
 k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
   using L = FLayout<SG, T>;
-  constexpr int S = L::S, BX = kHeviBoxX, TY = kForceTY, NT = kFPairs * TY * L::ngroups;
+  constexpr int S = L::S, BX = kHeviBoxX, TY = kForceTY;
   // level k+2 must have been issued (at k' = k+5-S) before level k waits for it
   static_assert(S >= 6, "ring too shallow for the k-2..k+2 window");
   const Grid g = a.g;
@@ -372,13 +372,10 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
   const int imaxg = G == 0 ? ni - 1 : ni - 2, jmaxg = G == 1 ? nj - 1 : nj - 2, kmaxg = G == 2 ? nk - 1 : nk - 2;
   const bool ownA = (i <= imaxg) && (j <= jmaxg), ownB = (i + 1 <= imaxg) && (j <= jmaxg);
   const int kmax = SG == 0 ? nk - 1 : nk - 2, lmax = SG == 0 ? nk : nk - 1;
-  const int nc = nk + 1;
 
   extern __shared__ __align__(1024) float fsmem[];
   float* ring = fsmem;
-  float* cols = ring + S * L::stage;                // level table: cols[k * kNF + field]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(cols + r128c(kNF * nc));
-  fill_level_table(cols, a.col, nk, a.dtb2, tid, NT);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + S * L::stage);
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -424,12 +421,12 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
     }
     if ((ownA || ownB) && !fail && k <= kmaxg) {
       if constexpr (SG == 0) {
-        if (gz == 0) force_point<0, T>(a, stp, cols, rowbase, id, k, ownB, wb_prev);
-        else if (gz == 1) force_point<1, T>(a, stp, cols, rowbase, id, k, ownB, wb_prev);
-        else force_point<2, T>(a, stp, cols, rowbase, id, k, ownB, wb_prev);
+        if (gz == 0) force_point<0, T>(a, stp, rowbase, id, k, ownB, wb_prev);
+        else if (gz == 1) force_point<1, T>(a, stp, rowbase, id, k, ownB, wb_prev);
+        else force_point<2, T>(a, stp, rowbase, id, k, ownB, wb_prev);
       } else {
-        if (gz == 0) force_point<3, T>(a, stp, cols, rowbase, id, k, ownB, wb_prev);
-        else force_point<4, T>(a, stp, cols, rowbase, id, k, ownB, wb_prev);
+        if (gz == 0) force_point<3, T>(a, stp, rowbase, id, k, ownB, wb_prev);
+        else force_point<4, T>(a, stp, rowbase, id, k, ownB, wb_prev);
       }
     }
 #pragma unroll

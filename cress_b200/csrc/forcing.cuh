@@ -11,20 +11,22 @@ namespace cress {
 // same table: the Rayleigh coefficient rbct(k) (vspdmp.f90:269-292).
 enum ColFieldLarge { C_RBCT = C_NFIELDS, C_NFIELDS_ALL };
 
-// Per-level values the large-step kernels derive from the columns, once per
-// block, into a k-major shared-memory table: quotients of constants by
-// columns (the same IEEE divisions the stencils would repeat per point) and
-// reciprocals of the per-level divisors of field values, which the stencils
-// multiply by (a field value of exactly zero would otherwise send every
-// such division through its slow path).
+// Per-level values the large-step kernels read from a k-major table (the
+// level table, table[k * kLevelStride + field], built on the host once per
+// large-step length and kept on the device): the 1-D columns, quotients of
+// constants by columns (the same IEEE divisions the stencils would repeat
+// per point) and reciprocals of the per-level divisors of field values,
+// which the stencils multiply by (a field value of exactly zero would
+// otherwise send every such division through its slow path).
 enum ColDerived {
   D_IJCB8U = C_NFIELDS_ALL, D_IJCB8V, D_IPTBR, D_IEPSQV, D_I1QV, D_DTDRST, D_2JCB, D_4JCB, D_2J8W, D_NFIELDS
 };
 constexpr int kLevelStride = 32;   // floats per level of the table (>= D_NFIELDS)
 
 // Column field f (base or derived) of level kk; B(f, kk) reads a base column.
+#pragma nv_exec_check_disable
 template <class FB>
-__device__ __forceinline__ float level_value(int f, int kk, const FB& B, float dtb2) {
+__host__ __device__ __forceinline__ float level_value(int f, int kk, const FB& B, float dtb2) {
   switch (f) {
     case D_IJCB8U: return 1.f / B(C_JCB8U, kk);
     case D_IJCB8V: return 1.f / B(C_JCB8V, kk);
@@ -45,20 +47,10 @@ __device__ __forceinline__ float level_value(int f, int kk, const FB& B, float d
   }
 }
 
-// Fill table[kk * kLevelStride + f], kk = 0..nk, from col[f * (nk+1) + kk].
-__device__ __forceinline__ void fill_level_table(float* table, const float* col, int nk, float dtb2, int tid,
-                                                 int nt) {
-  const int nc = nk + 1;
-  auto B = [&](int f, int kk) { return __ldg(col + f * nc + kk); };
-  for (int q = tid; q < nc * kLevelStride; q += nt) {
-    const int kk = q / kLevelStride, f = q - kk * kLevelStride;
-    table[q] = f < D_NFIELDS ? level_value(f, kk, B, dtb2) : 0.f;
-  }
-}
-
 struct ForceArgs {
   Grid g;
   const float* col;           // 1-D columns, C_NFIELDS_ALL x (nk+1)
+  const float* lvl;           // level table (nk+1) x kLevelStride for this dtb
   // present level t
   const float* u; const float* v; const float* w; const float* pp; const float* ptp;
   // past level t-dt
@@ -132,6 +124,7 @@ constexpr int kMoistN = 9;
 struct MoistScalarArgs {
   Grid g;
   const float* col;
+  const float* lvl;           // level table (nk+1) x kLevelStride for this dtb
   const float* u; const float* v; const float* w;   // present winds (flux rst*u etc.)
   const float* s[kMoistN];    // present level t
   const float* sp[kMoistN];   // past level t-dt

@@ -53,14 +53,8 @@ struct ScLayout {
   static constexpr int stage = oR + (TURB ? r128f(BX * R::r) : 0);   // floats per ring stage
   static constexpr uint32_t tx_bytes =
       4u * BX * (kScGroup * 2 * R::s + R::u + R::v + R::w + (TURB ? R::r : 0));
-  // 1-D columns and their derived values stored k-major (the level table,
-  // cols[k * NF + field]), so a level's values sit at compile-time offsets
-  // from one pointer
-  static constexpr int NF = kLevelStride;
-  __host__ __device__ static int cols_floats(int nk) { return r128f(NF * (nk + 1)); }
-  __host__ __device__ static size_t bytes(int nk) {
-    return 4 * ((size_t)S * stage + (size_t)cols_floats(nk)) + 8 * (size_t)S;
-  }
+  static constexpr int NF = kLevelStride;   // stride of the level table
+  __host__ __device__ static size_t bytes(int) { return 4 * (size_t)S * stage + 8 * (size_t)S; }
 };
 
 // Threads: 16 x 8 x 3; thread (tx, ty, tz) owns the pair of columns
@@ -74,7 +68,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   // level k+2 must have been issued (at k' = k+5-S) before level k waits for it
   static_assert(S >= 6, "ring too shallow for the k-2..k+2 window");
   using L = ScLayout<S, TURB>;
-  constexpr int TY = kScalarTY, BX = kHeviBoxX, NT = kScPairs * TY * kScGroup;
+  constexpr int TY = kScalarTY, BX = kHeviBoxX;
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
   constexpr int NG = kMoistN / kScGroup;               // species groups
@@ -88,9 +82,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
 
   extern __shared__ __align__(1024) float smem[];
   float* ring = smem;
-  float* cols = ring + S * L::stage;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
-  fill_level_table(cols, a.col, nk, a.dtb2, tid, NT);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + S * L::stage);
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -153,8 +145,8 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       issue(k + S - 3);
     }
     if ((ownA || ownB) && !fail) {
-      const float* ck = cols + k * L::NF;
-      auto C = [&](int f, int kk) { return ck[(kk - k) * L::NF + f]; };
+      const float* ck = a.lvl + k * L::NF;
+      auto C = [&](int f, int kk) { return __ldg(ck + (kk - k) * L::NF + f); };
       auto st = [&](int d) { return stp[d + 2]; };
       const float* st0 = st(0);
       const float* S0 = st0 + L::oS + oS;
