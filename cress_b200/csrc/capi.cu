@@ -297,6 +297,11 @@ int Ctx::small_steps(int nsstp, float dts) {
   HeviArgs a{};
   a.g = g;
   a.col = col_d;
+  if (level_tables.empty()) {   // any level table serves: the small step reads only its columns
+    const float* t = nullptr;
+    if ((rc = level_table(0.f, &t))) return rc;
+  }
+  a.lvl = level_tables.begin()->second;
   a.thom_rr = th->rr; a.thom_aa = th->aa; a.thom_cp = th->cp;
   a.err = err_d;
   a.dts = dts;

@@ -21,7 +21,7 @@ enum ColFieldLarge { C_RBCT = C_NFIELDS, C_NFIELDS_ALL };
 enum ColDerived {
   D_IJCB8U = C_NFIELDS_ALL, D_IJCB8V, D_IPTBR, D_IEPSQV, D_I1QV, D_DTDRST, D_2JCB, D_4JCB, D_2J8W, D_NFIELDS
 };
-constexpr int kLevelStride = 32;   // floats per level of the table (>= D_NFIELDS)
+static_assert(kLevelStride >= D_NFIELDS, "level table stride too small");
 
 // Column field f (base or derived) of level kk; B(f, kk) reads a base column.
 #pragma nv_exec_check_disable

@@ -363,25 +363,27 @@ int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
 }  // namespace
 
 // Tile ids.  0 (the default): k_hevi2 (hevi2.cu), 32 x 8 columns per block
-// with two rows per thread.  10: 32 x 4 columns, 4-stage ring, the
+// with two rows per thread; 11: the same with a 3-stage ring and the level
+// table read from global memory (more resident blocks).  10: 32 x 4 columns, 4-stage ring, the
 // eliminated right-hand sides parked (float) in the new w array; 6: the
 // same with a 5-stage ring; 7 and 8: 32 x 8 and 32 x 2.  1, 2 and 9 keep
 // them in shared memory as float (32 x 2, 32 x 8, 32 x 4); 3-5 as double
 // (both recurrences always run in double).
 int hevi_tile_rows(int tile) {
   switch (tile) {
-    case 0: return 8;
+    case 0: case 11: return 8;
     case 1: case 4: case 8: return 2;
     case 2: case 5: case 7: return 8;
     default: return 4;
   }
 }
 
-int launch_hevi2(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st);
+int launch_hevi2(const HeviArgs& a, const HeviMaps& maps, int variant, cudaStream_t st);
 
 int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st) {
   switch (tile) {
-    case 0: return launch_hevi2(a, maps, st);
+    case 0: return launch_hevi2(a, maps, 0, st);
+    case 11: return launch_hevi2(a, maps, 1, st);
     case 1: return launch_t<2, 5, float>(a, maps, st);
     case 2: return launch_t<8, 4, float>(a, maps, st);
     case 3: return launch_t<4, 5, double>(a, maps, st);

@@ -16,6 +16,11 @@ enum ColField {
   C_IRST8U, C_IRST8V, C_IJCB, C_IRCSQ, C_IRST8W, C_IJCB8W, C_NFIELDS
 };
 
+// Stride (floats) of the k-major level table (table[k * kLevelStride +
+// field]) the large-step kernels and the global-table HE-VI variant read:
+// the ColField columns, then the derived values of forcing.cuh.
+constexpr int kLevelStride = 32;
+
 // Width (floats) of every TMA box of the HE-VI kernel: x from i0-2 (a
 // multiple of 32, so 16-byte aligned) to i0+33, covering the 32-column
 // tile with the x halos the stencils need.
@@ -38,6 +43,7 @@ struct HeviArgs {
   const float* u_old; const float* v_old; const float* p_old;
   float* u_new; float* v_new; float* w_new; float* p_new;
   const float* col;       // 1-D base columns
+  const float* lvl;       // the same k-major (level table, stride kLevelStride) or null
   const float* thom_rr;   // [k] sub-diagonal a_k of the w system (float, as formed by stepwi)
   const double* thom_aa;  // [k] 1/(b_k - a_k c'_{k-1})
   const double* thom_cp;  // [k] c'_k

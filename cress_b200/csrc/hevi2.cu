@@ -57,8 +57,10 @@ struct H2Layout {
   static constexpr int t3h_floats = r128h((kH2TY + 2) * BX);
   __host__ __device__ static int cols_floats(int nk) { return r128h(kHNF * (nk + 2)); }
   // ring, t3h (two buffers), k-major columns, mbarriers, aa and cp
-  // (double), rr (float)
-  __host__ __device__ static size_t bytes(int nk) {
+  // (double), rr (float); with the level table in global memory (GT) only
+  // the ring, t3h and the mbarriers
+  __host__ __device__ static size_t bytes(int nk, bool gt) {
+    if (gt) return 4 * ((size_t)S * stage + 2 * (size_t)t3h_floats) + 8 * (size_t)S;
     return 4 * ((size_t)S * stage + 2 * (size_t)t3h_floats + (size_t)cols_floats(nk)) + 8 * (size_t)S +
            16 * (size_t)(nk + 2) + 4 * (size_t)(nk + 2);
   }
@@ -66,9 +68,11 @@ struct H2Layout {
 
 // DIV = divopt, STH = stretched grid (sthopt != 0), BUY = buyopt == 1: the
 // options are template parameters, so the level loop carries no branches
-// on them.
-template <int S, int DIV, bool STH, bool BUY>
-__global__ void __launch_bounds__(kHeviTX * kH2Rows, 4)
+// on them.  GT: the per-level columns and the elimination factors are read
+// from global memory (the level table, a.lvl) instead of being copied into
+// shared memory, which leaves room for more resident blocks.
+template <int S, int DIV, bool STH, bool BUY, bool GT>
+__global__ void __launch_bounds__(kHeviTX * kH2Rows, GT ? 5 : 4)
 k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   using L = H2Layout<S>;
   constexpr int TX = kHeviTX, TY = kH2TY, BX = kHeviBoxX, NT = TX * kH2Rows;
@@ -92,20 +96,26 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   extern __shared__ __align__(1024) float smem[];
   float* ring = smem;
   float* t3hb = ring + S * L::stage;          // 2 x [(TY+2)][BX], rows from j0-1, x from i0-2
-  float* cols = t3hb + 2 * L::t3h_floats;     // cols[k * kHNF + field]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(cols + L::cols_floats(nk));
+  float* cols = t3hb + 2 * L::t3h_floats;     // cols[k * kHNF + field] (shared-table variant)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(GT ? cols : cols + L::cols_floats(nk));
   double* thd = reinterpret_cast<double*>(bars + S);       // aa[k] then cp[k], k = 0..nk+1
   float* thr = reinterpret_cast<float*>(thd + 2 * (nk + 2));  // rr[k]
-
-  for (int n = tid; n < C_NFIELDS * ncol; n += NT) {
-    const int f = n / ncol, kk = n - f * ncol;
-    cols[kk * kHNF + f] = __ldg(a.col + n);
+  if constexpr (!GT) {
+    for (int n = tid; n < C_NFIELDS * ncol; n += NT) {
+      const int f = n / ncol, kk = n - f * ncol;
+      cols[kk * kHNF + f] = __ldg(a.col + n);
+    }
+    for (int n = tid; n <= nk + 1; n += NT) {
+      thd[n] = __ldg(a.thom_aa + n);
+      thd[nk + 2 + n] = __ldg(a.thom_cp + n);
+      thr[n] = __ldg(a.thom_rr + n);
+    }
   }
-  for (int n = tid; n <= nk + 1; n += NT) {
-    thd[n] = __ldg(a.thom_aa + n);
-    thd[nk + 2 + n] = __ldg(a.thom_cp + n);
-    thr[n] = __ldg(a.thom_rr + n);
-  }
+  // column field f of level kk, and the elimination factors
+  auto CK = [&](int kk, int f) { return GT ? __ldg(a.lvl + kk * kLevelStride + f) : cols[kk * kHNF + f]; };
+  auto TH_AA = [&](int kk) { return GT ? __ldg(a.thom_aa + kk) : thd[kk]; };
+  auto TH_CP = [&](int kk) { return GT ? __ldg(a.thom_cp + kk) : thd[nk + 2 + kk]; };
+  auto TH_RR = [&](int kk) { return GT ? __ldg(a.thom_rr + kk) : thr[kk]; };
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -174,13 +184,11 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     const float* VF = st0 + L::oVF;
     const float* WF = st0 + L::oWF;
     const float* PF = st0 + L::oPF;
-    const float* ck = cols + k * kHNF;
-    const float* ck1 = ck + kHNF;
-    const float rst8u = ck[C_RST8U], rst8v = ck[C_RST8V];
-    const float rst8wk = ck[C_RST8W], rst8wk1 = ck1[C_RST8W];
-    const float jcbk = ck[C_JCB], ijcbk = ck[C_IJCB];
-    const float irst8u = ck[C_IRST8U], irst8v = ck[C_IRST8V];
-    const float ij8wk = ck[C_IJCB8W], ij8wk1 = ck1[C_IJCB8W];
+    const float rst8u = CK(k, C_RST8U), rst8v = CK(k, C_RST8V);
+    const float rst8wk = CK(k, C_RST8W), rst8wk1 = CK(k + 1, C_RST8W);
+    const float jcbk = CK(k, C_JCB), ijcbk = CK(k, C_IJCB);
+    const float irst8u = CK(k, C_IRST8U), irst8v = CK(k, C_IRST8V);
+    const float ij8wk = CK(k, C_IJCB8W), ij8wk1 = CK(k + 1, C_IJCB8W);
 
     // diver3d.f90:318 (with phy2cnt.f90:219 for the contravariant w)
     auto div3d_at = [&](int x, int y) {
@@ -235,9 +243,9 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
                       dts * (VF[(fyB + 1) * BX + ox] + (tc.v.y - t3h[(oyB + 1) * BX + ox]) * dyiv) * irst8v;
     const F2 vn = f2(vs.v.y, vf2);
 
-    const float jcb8u = ck[C_JCB8U], jcb8v = ck[C_JCB8V];
-    const float rcsq = ck[C_RCSQ], rst = ck[C_RST], rbr = ck[C_RBR], ircsq = ck[C_IRCSQ];
-    const float irst8w = ck[C_IRST8W];
+    const float jcb8u = CK(k, C_JCB8U), jcb8v = CK(k, C_JCB8V);
+    const float rcsq = CK(k, C_RCSQ), rst = CK(k, C_RST), rbr = CK(k, C_RBR), ircsq = CK(k, C_IRCSQ);
+    const float irst8w = CK(k, C_IRST8W);
     // the stores of stepuv for one row
     const bool kend = (k == 2) || (k == nk - 2);
     auto store_uv = [&](bool edge, bool ylast, int j, int id, float u0, float u1, float v0, float v1) {
@@ -276,7 +284,7 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       if constexpr (BUY) fw = fw + (wb8s_prev + wb8s);                                  // buoywsi.f90:205
       const F2 wrhs = wk + dts * fw * irst8w;                                           // stepwi.f90:325
       // gaussel.f90:189-240 in double with the 1-D factors, one recurrence per row
-      const double rr = (double)thr[k], aa = thd[k];
+      const double rr = (double)TH_RR(k), aa = TH_AA(k);
       const double fA = (k == 3) ? (double)wrhs.v.x * aa : ((double)wrhs.v.x - rr * fA_prev) * aa;
       const double fB = (k == 3) ? (double)wrhs.v.y * aa : ((double)wrhs.v.y - rr * fB_prev) * aa;
       if (ownA) a.w_new[idA] = (float)fA;   // parked until the way down
@@ -329,10 +337,9 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   // the p' update of steppi from w(k) and w(k+1) (diverpiv.f90:124,
   // advbspi.f90:175, steppi.f90:217)
   auto pnew = [&](const Col& c, float wk, float fpb, float po, int k) {
-    const float* ckd = cols + k * kHNF;
-    const float pvd = ckd[C_RCSQ] * (wk - c.wup) * dziv;
-    const float fp = fpb + a.weicoe * (a.g05 * (wk + c.wup) * ckd[C_RST] + pvd);
-    return po + dts * fp * ckd[C_IJCB];
+    const float pvd = CK(k, C_RCSQ) * (wk - c.wup) * dziv;
+    const float fp = fpb + a.weicoe * (a.g05 * (wk + c.wup) * CK(k, C_RST) + pvd);
+    return po + dts * fp * CK(k, C_IJCB);
   };
   auto down = [&](Col& c, bool own, bool edge, int j, int k) {
     if (!own) return;
@@ -341,7 +348,7 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     const int idk = c.idk;
     const int idl = idk - (k - 2 >= 2 ? 2 : k - 2) * plane;   // level max(k-2, 2)
     c.fp1 = a.p_new[idl]; c.po1 = a.p_old[idl]; c.f1 = a.w_new[idl];
-    const double wd = (double)fg - thd[nk + 2 + k] * c.wupd;   // gaussel.f90:254
+    const double wd = (double)fg - TH_CP(k) * c.wupd;   // gaussel.f90:254
     c.wupd = wd;
     const float wk = (float)wd;
     const float pn = pnew(c, wk, fpb, po, k);
@@ -371,7 +378,7 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     if (edge) store_periodic(a.p_new, g, STAG_S, i, j, 2, p2);
     else a.p_new[c.idk] = p2;
     const float w3 = c.wup;
-    const float j8w3 = cols[3 * kHNF + C_JCB8W], j8wt = cols[(nk - 2) * kHNF + C_JCB8W];
+    const float j8w3 = CK(3, C_JCB8W), j8wt = CK(nk - 2, C_JCB8W);
     const float wc3 = STH ? w3 / j8w3 : w3;
     const float wct = STH ? c.wkend / j8wt : c.wkend;
     store_periodic(a.w_new, g, STAG_S, i, j, 1, -j8w3 * wc3 - 0.f);
@@ -390,39 +397,46 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   finish(cB, ownB, edgeB, ylastB, jB);
 }
 
-template <int DIV, bool STH, bool BUY>
+template <int S, bool GT, int DIV, bool STH, bool BUY>
 int launch_h2(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
-  constexpr int S = 4;
   using L = H2Layout<S>;
   const Grid& g = a.g;
   const int nx = g.ni - 3, ny = g.nj - 3;
-  const size_t bytes = L::bytes(g.nk);
+  const size_t bytes = L::bytes(g.nk, GT);
   if (bytes > 227 * 1024) return CRESS_E_UNSUPPORTED;
-  if (cudaFuncSetAttribute(k_hevi2<S, DIV, STH, BUY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
-      cudaSuccess)
+  auto kern = k_hevi2<S, DIV, STH, BUY, GT>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
     return CRESS_E_CUDA;
   dim3 block(kHeviTX, kH2Rows);
   dim3 grid((nx + kHeviTX - 1) / kHeviTX, (ny + kH2TY - 1) / kH2TY);
-  k_hevi2<S, DIV, STH, BUY><<<grid, block, bytes, st>>>(maps, a);
+  kern<<<grid, block, bytes, st>>>(maps, a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
-template <int DIV>
+template <int S, bool GT, int DIV>
 int launch_h2_div(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
   const bool sth = a.sthopt != 0, buy = a.buyopt == 1;
-  if (sth) return buy ? launch_h2<DIV, true, true>(a, maps, st) : launch_h2<DIV, true, false>(a, maps, st);
-  return buy ? launch_h2<DIV, false, true>(a, maps, st) : launch_h2<DIV, false, false>(a, maps, st);
+  if (sth) return buy ? launch_h2<S, GT, DIV, true, true>(a, maps, st) : launch_h2<S, GT, DIV, true, false>(a, maps, st);
+  return buy ? launch_h2<S, GT, DIV, false, true>(a, maps, st) : launch_h2<S, GT, DIV, false, false>(a, maps, st);
+}
+
+template <int S, bool GT>
+int launch_h2_opts(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
+  switch (a.divopt) {
+    case 2: return launch_h2_div<S, GT, 2>(a, maps, st);
+    case 1: return launch_h2_div<S, GT, 1>(a, maps, st);
+    default: return launch_h2_div<S, GT, 0>(a, maps, st);
+  }
 }
 
 }  // namespace
 
-int launch_hevi2(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
+// variant 0: 4-stage ring, level table in shared memory; 1: 3-stage ring,
+// level table and elimination factors read from global memory (needs a.lvl)
+int launch_hevi2(const HeviArgs& a, const HeviMaps& maps, int variant, cudaStream_t st) {
   if (a.g.count() >= (1LL << 31) || a.g.nk < 6) return CRESS_E_UNSUPPORTED;   // 32-bit indices; levels 2..nk-2 >= 3
-  switch (a.divopt) {
-    case 2: return launch_h2_div<2>(a, maps, st);
-    case 1: return launch_h2_div<1>(a, maps, st);
-    default: return launch_h2_div<0>(a, maps, st);
-  }
+  if (variant == 1) return a.lvl ? launch_h2_opts<3, true>(a, maps, st) : CRESS_E_UNSUPPORTED;
+  return launch_h2_opts<4, false>(a, maps, st);
 }
 
 }  // namespace cress

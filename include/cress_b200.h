@@ -51,7 +51,7 @@ typedef struct cress_cfg {
   float weicoe;         /* implicit weight beta (SrcOrig/advbspi.f90:140) */
   int wbc, ebc, sbc, nbc;  /* lateral BCs after chknlslv: -1 = periodic */
   int bbc, tbc;         /* 2 = rigid (SrcOrig/vbcw.f90:201) */
-  int tile;             /* HE-VI tile shape id (0 = default: 32x8, two rows per thread; 1-10 other shapes) */
+  int tile;             /* HE-VI tile shape id (0 = default: 32x8, two rows per thread; 1-11 other shapes) */
   /* large step (SrcOrig/forcedrv.f90:548-608, SrcOrig/timeflt.f90:335) */
   int advopt;           /* 2 only: 4th-order horizontal advection */
   int smtopt;           /* 0 none, 2 horizontal, 3 horizontal + vertical 4th-order smoothing */
@@ -162,7 +162,7 @@ int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, floa
 int cress_diagnostics(cress_ctx* ctx, int level, double* out);
 
 /* Number of HE-VI tile shapes (cress_cfg.tile = 0 .. CRESS_NTILES-1). */
-#define CRESS_NTILES 11
+#define CRESS_NTILES 12
 
 /* Autotuner: times every HE-VI tile shape (xy tile, ring depth, column
  * store) over `reps` small-step loops of nsstp substeps of length dts on

@@ -48,7 +48,7 @@ def test_one_substep(cress, oracle_lib, sthopt):
     check(ni, nj, nk, ref, out, 1)
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
+@pytest.mark.parametrize("tile", list(range(12)))
 def test_ragged_domain_tiles(cress, oracle_lib, tile):
     # nx, ny not multiples of the tile: partial edge tiles on both axes
     ni, nj, nk, ref, out = run_pair(cress, oracle_lib, 45, 37, 21, 3, tile=tile, seed=5)
