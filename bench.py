@@ -301,6 +301,8 @@ def main():
     ap.add_argument("--dx", type=float, default=1000.0)
     ap.add_argument("--dtbig", type=float, default=5.0)
     ap.add_argument("--dtsml", type=float, default=1.0)
+    ap.add_argument("--impopt", type=int, default=1, choices=[0, 1],
+                    help="small step: 1 HE-VI (the configuration's), 0 HE-VE (needs --dtsml short enough)")
     ap.add_argument("--tile", type=int, default=-1,
                     help="HE-VI tile shape; -1 (default): chosen by the autotuner on the live state")
     ap.add_argument("--cpu-nx", type=int, default=256)
@@ -365,7 +367,7 @@ def main():
     case = make_case(args.nx, args.ny, args.nz, args.dx, 100 + rank)
     ni, nj, nk = case["dims"]
     rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, case["botbar"])
-    s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, case["dz"], sthopt=1, tile=max(args.tile, 0),
+    s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, case["dz"], sthopt=1, tile=max(args.tile, 0), impopt=args.impopt,
                           device=local, cphopt=3)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -393,10 +395,11 @@ def main():
 
     s.large_step(0, 0.5 * args.dtbig, nsstp, 0.5 * args.dtsml)   # the first (half) step, ctime=0
     tune = None
-    if args.tile < 0:
+    if args.tile < 0 and args.impopt == 1:
         best, tms = s.autotune(nsstp=nsstp, dts=args.dtsml, reps=2)
         tune = {"tile": best, "ms_per_substep": [round(t, 4) for t in tms]}
-    cfg_json["hevi_tile"] = tune["tile"] if tune else args.tile
+    cfg_json["hevi_tile"] = tune["tile"] if tune else max(args.tile, 0)
+    cfg_json["small_step"] = "HE-VI (impopt=1)" if args.impopt == 1 else "HE-VE (impopt=0)"
     if not args.no_graphs:
         # capture the CUDA graphs of the time-level rotation's 6 pointer
         # states (an eager step and a capture each) before the warm-up
@@ -491,10 +494,12 @@ def main():
             "sim_s_per_wall_s": args.dtbig / (ms / args.steps * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": HEVI2_TRAFFIC_PER_CELL * cells if cfg_json["hevi_tile"] == 0 else None,
+                         "traffic": (HEVI2_TRAFFIC_PER_CELL * cells
+                                     if cfg_json["hevi_tile"] == 0 and args.impopt == 1 else None),
                          "traffic_source": "ncu dram bytes per cell at 384x384x64 scaled to this grid",
                          "peak_source": peak_kind,
-                         "kernel": "k_hevi2" if cfg_json["hevi_tile"] == 0 else "k_hevi_substep",
+                         "kernel": ("k_heve" if args.impopt == 0 else
+                                    "k_hevi2" if cfg_json["hevi_tile"] == 0 else "k_hevi_substep"),
                          "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),

@@ -128,7 +128,7 @@ def fptr(a):
 class Solver:
     """One domain on one GPU (a cress_ctx)."""
 
-    def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6,
+    def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6, impopt=1,
                  tile=0, device=0, smtopt=3, smhcoe=0.001, smvcoe=0.0004, vspopt=2,
                  vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1, cphopt=0, thresq=1e-12,
                  tubopt=0):
@@ -136,7 +136,7 @@ class Solver:
         c = Cfg()
         c.ni, c.nj, c.nk = ni, nj, nk
         c.dx, c.dy, c.dz = dx, dy, dz
-        c.sthopt, c.impopt, c.divopt, c.buyopt, c.gwmopt = sthopt, 1, divopt, buyopt, 0
+        c.sthopt, c.impopt, c.divopt, c.buyopt, c.gwmopt = sthopt, impopt, divopt, buyopt, 0
         c.weicoe = weicoe
         c.wbc = c.ebc = c.sbc = c.nbc = -1
         c.bbc = c.tbc = 2

@@ -291,8 +291,9 @@ int Ctx::level_table(float dtb2, const float** out) {
 int Ctx::small_steps(int nsstp, float dts) {
   if (!base_set) return set_error(CRESS_E_STATE, "cress_small_steps: base state not set");
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_small_steps: nsstp=%d", nsstp);
+  const bool heve = cfg.impopt == 0;
   const ThomasSet* th = nullptr;
-  int rc = thomas_for(dts, &th);
+  int rc = heve ? CRESS_OK : thomas_for(dts, &th);
   if (rc) return rc;
   HeviArgs a{};
   a.g = g;
@@ -302,7 +303,7 @@ int Ctx::small_steps(int nsstp, float dts) {
     if ((rc = level_table(0.f, &t))) return rc;
   }
   a.lvl = level_tables.begin()->second;
-  a.thom_rr = th->rr; a.thom_aa = th->aa; a.thom_cp = th->cp;
+  if (th) { a.thom_rr = th->rr; a.thom_aa = th->aa; a.thom_cp = th->cp; }
   a.err = err_d;
   a.dts = dts;
   a.dxiv = 1.f / cfg.dx; a.dyiv = 1.f / cfg.dy; a.dziv = 1.f / cfg.dz;
@@ -314,7 +315,7 @@ int Ctx::small_steps(int nsstp, float dts) {
   a.g05 = .5f * kG;
   a.g05n = -.5f * kG;
   a.divopt = cfg.divopt; a.buyopt = cfg.buyopt; a.sthopt = cfg.sthopt; a.bbc = cfg.bbc;
-  const int TY = hevi_tile_rows(cfg.tile);
+  const int TY = hevi_tile_rows(heve ? 0 : cfg.tile);
   HeviMaps maps;
   if ((rc = tmap(lev[CRESS_U][CRESS_FORCING], TY, &maps.uf)) ||
       (rc = tmap(lev[CRESS_V][CRESS_FORCING], TY + 1, &maps.vf)) ||
@@ -334,9 +335,18 @@ int Ctx::small_steps(int nsstp, float dts) {
     if ((rc = tmap(olds[0], TY + 2, &maps.u)) || (rc = tmap(olds[1], TY + 3, &maps.v)) ||
         (rc = tmap(olds[2], TY + 2, &maps.w)) || (rc = tmap(olds[3], TY + 2, &maps.p)))
       return rc;
-    rc = launch_hevi_substep(a, maps, cfg.tile, stream);
+    if (heve) {
+      // the first substep forms the contravariant w of levels 2 and nk-1
+      // from the past w (phy2cnt before the loop, smalldrv.f90:358)
+      a.wc_from_w = s == 0;
+      a.wc_old = wcside[s & 1];
+      a.wc_new = wcside[(s + 1) & 1];
+      rc = launch_heve_substep(a, maps, stream);
+    } else {
+      rc = launch_hevi_substep(a, maps, cfg.tile, stream);
+    }
     ++launches;
-    if (rc) return set_error(rc, "HE-VI substep launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    if (rc) return set_error(rc, "small-step launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     for (int n = 0; n < 4; ++n) {
       float* t = news[n];
       news[n] = (s == 0) ? spare[F[n]] : olds[n];
@@ -639,6 +649,7 @@ int Ctx::diagnostics(int level, double* out) {
 // keep the fastest as cfg.tile and drop graphs captured with another tile.
 int Ctx::autotune(int nsstp, float dts, int reps, int* best, float* ms) {
   if (nsstp < 1 || reps < 1) return set_error(CRESS_E_ARG, "cress_autotune: nsstp=%d reps=%d", nsstp, reps);
+  if (cfg.impopt == 0) return set_error(CRESS_E_UNSUPPORTED, "cress_autotune: the HE-VE step has one tile shape");
   const int keep = cfg.tile;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
@@ -689,8 +700,8 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   *out = nullptr;
   if (cfg->ni < 8 || cfg->nj < 8 || cfg->nk < 8)
     return set_error(CRESS_E_ARG, "cress_create: dims too small (%d,%d,%d)", cfg->ni, cfg->nj, cfg->nk);
-  if (cfg->impopt != 1 || cfg->gwmopt != 0)
-    return set_error(CRESS_E_UNSUPPORTED, "only impopt=1, gwmopt=0 run on the GPU");
+  if ((cfg->impopt != 0 && cfg->impopt != 1) || cfg->gwmopt != 0)
+    return set_error(CRESS_E_UNSUPPORTED, "only impopt=0 (HE-VE) or 1 (HE-VI), gwmopt=0 run on the GPU");
   if (!(cfg->wbc == -1 && cfg->ebc == -1 && cfg->sbc == -1 && cfg->nbc == -1))
     return set_error(CRESS_E_UNSUPPORTED, "only periodic lateral boundaries (-1) run on the GPU");
   if (cfg->bbc != 2 || cfg->tbc != 2)
@@ -776,6 +787,16 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   }
   c->owned.push_back(c->err_d);
   cudaMemsetAsync(c->err_d, 0, sizeof(int), c->stream);
+  if (cfg->impopt == 0) {   // HE-VE side buffers (two planes each)
+    for (int b = 0; b < 2; ++b) {
+      if ((rc = cuda_check(cudaMalloc(&c->wcside[b], sizeof(float) * 2 * c->g.plane), "cudaMalloc wc planes"))) {
+        delete c;
+        return rc;
+      }
+      c->owned.push_back(c->wcside[b]);
+      cudaMemsetAsync(c->wcside[b], 0, sizeof(float) * 2 * c->g.plane, c->stream);
+    }
+  }
   *out = reinterpret_cast<cress_ctx*>(c);
   return CRESS_OK;
 }

@@ -32,6 +32,9 @@ struct Ctx {
   // ping-pong partner of the future level during the small-step loop.
   float* lev[CRESS_NFIELD][4];
   float* spare[CRESS_NFIELD];
+  // HE-VE (impopt=0): contravariant w of levels 2 and nk-1, two planes per
+  // buffer, ping-pong between substeps
+  float* wcside[2] = {nullptr, nullptr};
   std::vector<float> col_h;   // 1-D base columns on the host
   float* col_d = nullptr;
   bool base_set = false;

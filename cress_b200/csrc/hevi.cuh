@@ -48,6 +48,13 @@ struct HeviArgs {
   const double* thom_aa;  // [k] 1/(b_k - a_k c'_{k-1})
   const double* thom_cp;  // [k] c'_k
   int* err;               // device error word (nonzero: a bounded wait gave up)
+  // HE-VE only: the contravariant w of levels 2 and nk-1 (two planes of
+  // px*py each), which the reference keeps from the explicit update while
+  // the rigid lid sets w itself to 0 there; read from wc_old (or formed
+  // from w_old when wc_from_w), written to wc_new
+  const float* wc_old;
+  float* wc_new;
+  int wc_from_w;
   float dts, dxiv, dyiv, dziv, divch, divcv, weicoe, dtdzw, dtw, g05, g05n;
   int divopt, buyopt, sthopt, bbc;
 };
@@ -57,5 +64,8 @@ int hevi_tile_rows(int tile);
 // Launch one substep; `maps` must describe the buffers in `a` with the
 // box rows of HeviRows<hevi_tile_rows(tile)>.
 int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st);
+// One HE-VE substep (impopt=0, s_heve); the maps are those of tile 0's
+// box rows (HeviRows<8>) and a.lvl must hold the level table.
+int launch_heve_substep(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st);
 
 }  // namespace cress

@@ -44,7 +44,7 @@ typedef struct cress_cfg {
   int ni, nj, nk;       /* array dims: ni = xdim = nx+3, nk = zdim (SrcOrig/setdim.f90:196-199) */
   float dx, dy, dz;     /* grid spacing; dz is the mean spacing when sthopt=1 */
   int sthopt;           /* 0 uniform, >=1 stretched vertical grid (jcb varies in k) */
-  int impopt;           /* 1 = HE-VI with Thomas solve (the only small-step scheme on the GPU) */
+  int impopt;           /* 1 = HE-VI (implicit vertical, Thomas solve), 0 = HE-VE (explicit) */
   int divopt;           /* divergence damping 0/1/2 (SrcOrig/pgrad.f90:260-349) */
   int buyopt;           /* 1 = buoyancy in the small step (SrcOrig/hevi.f90:377) */
   int gwmopt;           /* 0 only */
@@ -112,10 +112,11 @@ int cress_put_field(cress_ctx* ctx, int field, int level, const float* host);
 int cress_get_field(cress_ctx* ctx, int field, int level, float* host);
 
 /* Acoustic small-step loop on the device-resident state: replaces the body
- * of s_smalldrv (SrcOrig/smalldrv.f90:343-398) for impopt=1: future u, v,
- * w, p' start from the past level, then nsstp HE-VI substeps of dts
- * (SrcOrig/hevi.f90:339-426) run with the forcing level's u, v, w, p'
- * forcings (ufrc, vfrc, wfrc, pfrc).  The result is the FUTURE level. */
+ * of s_smalldrv (SrcOrig/smalldrv.f90:343-398): future u, v, w, p' start
+ * from the past level, then nsstp substeps of dts run with the forcing
+ * level's u, v, w, p' forcings (ufrc, vfrc, wfrc, pfrc), HE-VI
+ * (SrcOrig/hevi.f90:339-426) for impopt=1 or HE-VE (SrcOrig/heve.f90:
+ * 337-406) for impopt=0.  The result is the FUTURE level. */
 int cress_small_steps(cress_ctx* ctx, int nsstp, float dts);
 
 /* Same call with host arrays, as s_smalldrv receives them: copies

@@ -89,10 +89,10 @@ def dry_steps(cfg, base, zph, past, now, nsteps, dtbig, dtsml, start=True, prec=
                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(_FP), ctypes.POINTER(_FP), ctypes.c_int,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int]
-    io = (ctypes.c_int * 11)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
+    io = (ctypes.c_int * 12)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
                              cfg.get("buyopt", 1), int(fp64_solve), cfg.get("sthopt", 0),
                              cfg.get("smtopt", 3), cfg.get("vspopt", 2), cfg.get("coropt", 0),
-                             cfg.get("tubopt", 0))
+                             cfg.get("tubopt", 0), cfg.get("impopt", 1))
     ro = (ctypes.c_double * 10)(cfg["dx"], cfg["dy"], cfg["dz"], cfg.get("weicoe", 0.6),
                                 cfg.get("smhcoe", 0.001), cfg.get("smvcoe", 0.0004),
                                 cfg.get("filcoe", 0.1), cfg.get("vspbar", 0.0),
@@ -125,10 +125,10 @@ def moist_steps(cfg, base, zph, past, now, prec, nsteps, dtbig, dtsml, start=Tru
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(_FP), ctypes.POINTER(_FP), _FP, ctypes.c_int,
                                      ctypes.c_double, ctypes.c_double, ctypes.c_int]
-    io = (ctypes.c_int * 11)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
+    io = (ctypes.c_int * 12)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
                              cfg.get("buyopt", 1), int(fp64_solve), cfg.get("sthopt", 0),
                              cfg.get("smtopt", 3), cfg.get("vspopt", 2), cfg.get("coropt", 0),
-                             cfg.get("tubopt", 0))
+                             cfg.get("tubopt", 0), cfg.get("impopt", 1))
     ro = (ctypes.c_double * 11)(cfg["dx"], cfg["dy"], cfg["dz"], cfg.get("weicoe", 0.6),
                                 cfg.get("smhcoe", 0.001), cfg.get("smvcoe", 0.0004),
                                 cfg.get("filcoe", 0.1), cfg.get("vspbar", 0.0),
@@ -196,14 +196,15 @@ def satadjst(dims, ptbr, pbr, pp, st, thresq=1e-12):
 
 
 def small_steps(cfg, base, frc, state, nsstp, dts, prec=32, fp64_solve=1, omp=False):
-    """Run s_smalldrv's loop (phy2cnt + nsstp x s_hevi) on the CPU.
+    """Run s_smalldrv's loop (phy2cnt + nsstp x s_hevi, or s_heve when
+    cfg["impopt"] == 0) on the CPU.
 
-    cfg: dict with ni,nj,nk,dx,dy,dz,sthopt,divopt,buyopt,weicoe.
+    cfg: dict with ni,nj,nk,dx,dy,dz,sthopt,divopt,buyopt,weicoe[,impopt].
     base: dict of 3-D float32 arrays (BASE_NAMES); frc: [ufrc,vfrc,wfrc,pfrc];
     state: [uf,vf,wf,ppf] (updated in place).
     """
-    io = (ctypes.c_int * 10)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
-                             cfg.get("buyopt", 1), 0, 1, 2, 2, int(fp64_solve))
+    io = (ctypes.c_int * 11)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
+                             cfg.get("buyopt", 1), 0, 1, 2, 2, int(fp64_solve), cfg.get("impopt", 1))
     ro = (ctypes.c_double * 4)(cfg["dx"], cfg["dy"], cfg["dz"], cfg.get("weicoe", 0.6))
     b = [np.ascontiguousarray(base[n], np.float32) for n in BASE_NAMES]
     f = [np.ascontiguousarray(x, np.float32) for x in frc]

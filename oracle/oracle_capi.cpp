@@ -24,7 +24,7 @@ Opts make_opts(const int* io, const double* ro) {
   Opts o;
   o.ni = io[0]; o.nj = io[1]; o.nk = io[2];
   o.divopt = io[3]; o.buyopt = io[4]; o.gwmopt = io[5];
-  o.periodic = io[6]; o.bbc = io[7]; o.tbc = io[8]; o.fp64_solve = io[9];
+  o.periodic = io[6]; o.bbc = io[7]; o.tbc = io[8]; o.fp64_solve = io[9]; o.impopt = io[10];
   o.dx = ro[0]; o.dy = ro[1]; o.dz = ro[2];
   o.weicoe = ro[3];
   return o;
@@ -56,7 +56,7 @@ int run_small(const Opts& o, int sthopt, double dts, int nsstp, const float* con
   s.resize(ni, nj, nk);
   phy2cnt(o, sthopt, b, wf, wc);
   for (int n = 0; n < nsstp; ++n)
-    hevi<R>(o, sthopt, (R)dts, b, ufrc, vfrc, wfrc, pfrc, ptpf, uf, vf, wf, wc, ppf, s);
+    small_substep<R>(o, sthopt, (R)dts, b, ufrc, vfrc, wfrc, pfrc, ptpf, uf, vf, wf, wc, ppf, s);
   uf.store(st[0]); vf.store(st[1]); wf.store(st[2]); ppf.store(st[3]);
   return 0;
 }
@@ -65,7 +65,7 @@ int run_small(const Opts& o, int sthopt, double dts, int nsstp, const float* con
 
 extern "C" {
 
-// io: ni,nj,nk,divopt,buyopt,gwmopt,periodic,bbc,tbc,fp64_solve
+// io: ni,nj,nk,divopt,buyopt,gwmopt,periodic,bbc,tbc,fp64_solve,impopt
 // ro: dx,dy,dz,weicoe
 // base: B_N arrays (see BaseIdx); frc: ufrc,vfrc,wfrc,pfrc; st (in/out): uf,vf,wf,ppf
 int oracle_small_steps(int prec, int sthopt, const int* io, const double* ro, double dts,

@@ -46,6 +46,7 @@ struct Opts {
   int periodic = 1;   // wbc=ebc=sbc=nbc=-1 after chknlslv maps 1->-1 on one PE
   int bbc = 2, tbc = 2;
   int fp64_solve = 0; // solve the w tridiagonal in double (product behaviour)
+  int impopt = 1;     // 1 HE-VI (s_hevi), 0 HE-VE (s_heve), smalldrv.f90:370-384
 };
 
 }  // namespace oracle

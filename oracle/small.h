@@ -1,4 +1,4 @@
-// Oracle: the HE-VI acoustic small step (impopt=1), flat terrain
+// Oracle: the HE-VI (impopt=1) and HE-VE (impopt=0) acoustic small steps, flat terrain
 // (trnopt=0), no map factor (mfcopt=0), periodic lateral boundaries on one
 // process, rigid lid / rigid bottom (bbc=tbc=2).
 //
@@ -446,6 +446,95 @@ void hevi(const Opts& o, int sthopt, R dts, const Base<R>& b, const F3<R>& ufrc,
   advbspi(o, false, b, wf, pfrc, tmp3, tmp4, tmp1);
   // steppi(..., tmp1, ppf)                                     hevi.f90:426
   steppi(o, dts, b, tmp1, ppf);
+}
+
+// s_buoywse, SrcOrig/buoywse.f90:135-187 (gwmopt=0, lines 151 and 184): the explicit small-step
+// buoyancy added to wsml (which holds the vertical pressure gradient).
+template <class R>
+void buoywse(const Opts& o, const Base<R>& b, const F3<R>& pp, F3<R>& wsml, F3<R>& wb8s) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  const R g05n = R(-.5) * (R)Phys::g;
+  OMP_FOR for (int k = 2; k <= nk - 2; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i) wb8s(i, j, k) = pp(i, j, k) * b.rst(i, j, k) / b.rcsq(i, j, k) * g05n;
+  OMP_FOR for (int k = 3; k <= nk - 2; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i) wsml(i, j, k) = wsml(i, j, k) + (wb8s(i, j, k - 1) + wb8s(i, j, k));
+}
+
+// s_stepwe, SrcOrig/stepwe.f90:255-370 (update at 261): explicit w update, periodic wrap,
+// contravariant w and the vertical boundary rows.
+template <class R>
+void stepwe(const Opts& o, int sthopt, R dts, const Base<R>& b, const F3<R>& wfrc, const F3<R>& wsml,
+            F3<R>& wf, F3<R>& wc) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  OMP_FOR for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i)
+        wf(i, j, k) = wf(i, j, k) + dts * (wfrc(i, j, k) + wsml(i, j, k)) / b.rst8w(i, j, k);
+  bcycle(o, 2, 1, ni - 2, ni - 1, 2, 1, nj - 2, nj - 1, nk, wf);  // stepwe.f90:337
+  phy2cnt(o, sthopt, b, wf, wc);                                   // stepwe.f90:360
+  vbcw(o, b, wc, wf);                                              // stepwe.f90:368
+}
+
+// s_diverpe, SrcOrig/diverpe.f90:153-169: rcsq times the 3-D divergence of
+// the J-weighted new winds.
+template <class R>
+void diverpe(const Opts& o, const Base<R>& b, const F3<R>& u, const F3<R>& v, const F3<R>& wc, F3<R>& pdiv,
+             F3<R>& t1, F3<R>& t2, F3<R>& t3) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  diver3d(o, b.jcb8u, b.jcb8v, b.jcb8w, u, v, wc, pdiv, t1, t2, t3);
+  OMP_FOR for (int k = 2; k <= nk - 2; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i) pdiv(i, j, k) = b.rcsq(i, j, k) * pdiv(i, j, k);
+}
+
+// s_advbspe, SrcOrig/advbspe.f90:118-135 (127).
+template <class R>
+void advbspe(const Opts& o, const Base<R>& b, const F3<R>& w, const F3<R>& pdiv, F3<R>& psml) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  const R g05 = R(.5) * (R)Phys::g;
+  OMP_FOR for (int k = 2; k <= nk - 2; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i)
+        psml(i, j, k) = g05 * (w(i, j, k) + w(i, j, k + 1)) * b.rst(i, j, k) + pdiv(i, j, k);
+}
+
+// s_steppe, SrcOrig/steppe.f90:218-323 (update at 224).
+template <class R>
+void steppe(const Opts& o, R dts, const Base<R>& b, const F3<R>& pfrc, const F3<R>& psml, F3<R>& ppf) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  OMP_FOR for (int k = 2; k <= nk - 2; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i)
+        ppf(i, j, k) = ppf(i, j, k) + dts * (pfrc(i, j, k) + psml(i, j, k)) / b.jcb(i, j, k);
+  bcycle(o, 2, 1, ni - 2, ni - 1, 2, 1, nj - 2, nj - 1, nk, ppf);
+  vbcp(o, ppf);
+}
+
+// s_heve, SrcOrig/heve.f90:337-406, gwmopt=0 path.
+template <class R>
+void heve(const Opts& o, int sthopt, R dts, const Base<R>& b, const F3<R>& ufrc, const F3<R>& vfrc,
+          const F3<R>& wfrc, const F3<R>& pfrc, F3<R>& uf, F3<R>& vf, F3<R>& wf, F3<R>& wc, F3<R>& ppf,
+          SmallScratch<R>& s) {
+  F3<R>&tmp1 = s.t[0], &tmp2 = s.t[1], &tmp3 = s.t[2], &tmp4 = s.t[3], &tmp5 = s.t[4], &tmp6 = s.t[5];
+  pgrad(o, dts, b, uf, vf, wc, ppf, tmp1, tmp2, tmp3, tmp4, tmp5, tmp6);   // heve.f90:337
+  stepuv(o, dts, b, ufrc, vfrc, tmp1, tmp2, uf, vf);                       // heve.f90:346
+  if (o.buyopt == 1) buoywse(o, b, ppf, tmp3, tmp4);                        // heve.f90:356
+  stepwe(o, sthopt, dts, b, wfrc, tmp3, wf, wc);                            // heve.f90:386
+  diverpe(o, b, uf, vf, wc, tmp2, tmp3, tmp4, tmp5);                        // heve.f90:395
+  advbspe(o, b, wf, tmp2, tmp1);                                            // heve.f90:398
+  steppe(o, dts, b, pfrc, tmp1, ppf);                                       // heve.f90:404
+}
+
+// One substep of s_smalldrv's loop: s_heve for impopt=0, s_hevi otherwise
+// (smalldrv.f90:370-398).
+template <class R>
+void small_substep(const Opts& o, int sthopt, R dts, const Base<R>& b, const F3<R>& ufrc, const F3<R>& vfrc,
+                   const F3<R>& wfrc, const F3<R>& pfrc, const F3<R>& ptpf, F3<R>& uf, F3<R>& vf, F3<R>& wf,
+                   F3<R>& wc, F3<R>& ppf, SmallScratch<R>& s) {
+  if (o.impopt == 0) heve<R>(o, sthopt, dts, b, ufrc, vfrc, wfrc, pfrc, uf, vf, wf, wc, ppf, s);
+  else hevi<R>(o, sthopt, dts, b, ufrc, vfrc, wfrc, pfrc, ptpf, uf, vf, wf, wc, ppf, s);
 }
 
 }  // namespace oracle

@@ -170,7 +170,7 @@ void phase_small(DryRun<R>& r, int nsstp, R dts) {   // s_smalldrv (smalldrv.f90
   r.f.u = r.p.u; r.f.v = r.p.v; r.f.w = r.p.w; r.f.pp = r.p.pp;
   phy2cnt(r.o, r.sthopt, r.b, r.f.w, r.wc);
   for (int n = 0; n < nsstp; ++n)
-    hevi<R>(r.o, r.sthopt, dts, r.b, r.ufrc, r.vfrc, r.wfrc, r.pfrc, r.f.ptp, r.f.u, r.f.v, r.f.w, r.wc,
+    small_substep<R>(r.o, r.sthopt, dts, r.b, r.ufrc, r.vfrc, r.wfrc, r.pfrc, r.f.ptp, r.f.u, r.f.v, r.f.w, r.wc,
             r.f.pp, r.ss);
 }
 

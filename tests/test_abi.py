@@ -45,5 +45,5 @@ def test_bad_config_rejected_without_gpu(cress):
     h = ctypes.c_void_p()
     assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 1  # CRESS_E_ARG
     c.ni, c.nj, c.nk = 20, 20, 20
-    c.impopt, c.dx, c.dy, c.dz = 0, 1.0, 1.0, 1.0
+    c.impopt, c.dx, c.dy, c.dz = 2, 1.0, 1.0, 1.0   # pivoting Gauss elimination: not built
     assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 2  # unsupported

@@ -6,33 +6,38 @@ properties the reference's equations must satisfy:
   * a periodic shift of the inputs shifts the outputs (bcycle wrap);
   * the FP32 and FP64 builds agree to float rounding;
   * the FP32 Thomas solve and the FP64 solve agree to float rounding.
+The first three hold for both small steps, HE-VI (impopt=1) and HE-VE
+(impopt=0, with a step short enough for its explicit vertical terms).
 """
 import numpy as np
+import pytest
 
 import helpers as H
 
 
-def cfg_for(ni, nj, nk, dx=500.0, dz=300.0, sthopt=0):
+def cfg_for(ni, nj, nk, dx=500.0, dz=300.0, sthopt=0, impopt=1):
     return dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=sthopt, divopt=2, buyopt=1,
-                weicoe=0.6)
+                weicoe=0.6, impopt=impopt)
 
 
-def test_rest_state(oracle_lib):
+@pytest.mark.parametrize("impopt", [1, 0])
+def test_rest_state(oracle_lib, impopt):
     ni, nj, nk = H.dims(16, 12, 10)
     base = H.base3d(ni, nj, nk, 300.0)
     z = [np.zeros((nk, nj + 2, ni + 2), np.float32) for _ in range(4)]
     st = [a.copy() for a in z]
-    oracle_lib.small_steps(cfg_for(ni, nj, nk), base, z, st, 4, 0.25)
+    oracle_lib.small_steps(cfg_for(ni, nj, nk, impopt=impopt), base, z, st, 4, 0.25)
     for a in st:
         assert np.all(a == 0.0)
 
 
-def test_periodic_shift_equivariance(oracle_lib):
+@pytest.mark.parametrize("impopt", [1, 0])
+def test_periodic_shift_equivariance(oracle_lib, impopt):
     nx, ny, nz = 16, 12, 10
     ni, nj, nk = H.dims(nx, ny, nz)
     base = H.base3d(ni, nj, nk, 300.0)
     st, frc = H.small_state(ni, nj, nk, 3, base)
-    cfg = cfg_for(ni, nj, nk)
+    cfg = cfg_for(ni, nj, nk, impopt=impopt)
     a = [x.copy() for x in st]
     oracle_lib.small_steps(cfg, base, frc, a, 3, 0.25)
 
@@ -55,15 +60,17 @@ def test_periodic_shift_equivariance(oracle_lib):
         assert np.array_equal(xs[m], y[m])
 
 
-def test_fp32_vs_fp64_spread(oracle_lib):
+@pytest.mark.parametrize("impopt", [1, 0])
+def test_fp32_vs_fp64_spread(oracle_lib, impopt):
     ni, nj, nk = H.dims(20, 16, 12)
     base = H.base3d(ni, nj, nk, 250.0, sthopt=1)
     st, frc = H.small_state(ni, nj, nk, 4, base)
-    cfg = cfg_for(ni, nj, nk, dx=1000.0, dz=250.0, sthopt=1)
+    cfg = cfg_for(ni, nj, nk, dx=1000.0, dz=250.0, sthopt=1, impopt=impopt)
+    dts = 0.5 if impopt else 0.1
     a = [x.copy() for x in st]
     b = [x.copy() for x in st]
-    oracle_lib.small_steps(cfg, base, frc, a, 6, 0.5, prec=32, fp64_solve=0)
-    oracle_lib.small_steps(cfg, base, frc, b, 6, 0.5, prec=64)
+    oracle_lib.small_steps(cfg, base, frc, a, 6, dts, prec=32, fp64_solve=0)
+    oracle_lib.small_steps(cfg, base, frc, b, 6, dts, prec=64)
     for x, y in zip(a, b):
         scale = np.abs(y).max()
         assert np.abs(x - y).max() <= 1e-4 * scale

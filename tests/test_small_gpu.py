@@ -18,15 +18,15 @@ STAG = {"u": "u", "v": "v", "w": "s", "pp": "s"}
 
 
 def run_pair(cress, oracle_lib, nx, ny, nz, nsstp, sthopt=0, seed=1, dts=0.5, tile=0, dx=1000.0,
-             dz=250.0):
+             dz=250.0, impopt=1, divopt=2):
     ni, nj, nk = H.dims(nx, ny, nz)
     base = H.base3d(ni, nj, nk, dz, sthopt)
     st, frc = H.small_state(ni, nj, nk, seed, base)
-    cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=sthopt, divopt=2, buyopt=1,
-               weicoe=0.6)
+    cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=sthopt, divopt=divopt, buyopt=1,
+               weicoe=0.6, impopt=impopt)
     ref = [a.copy() for a in st]
     oracle_lib.small_steps(cfg, base, frc, ref, nsstp, dts, prec=32, fp64_solve=1)
-    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=sthopt, tile=tile)
+    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=sthopt, tile=tile, impopt=impopt, divopt=divopt)
     s.set_base3d(base)
     out = s.smalldrv(nsstp, dts, *st, *frc)
     s.close()
@@ -83,3 +83,19 @@ def test_nonuniform_base_rejected(cress):
         s.set_base3d(base)
     assert e.value.code == 4
     s.close()
+
+
+# HE-VE (impopt=0): the explicit small step, with a step short enough for
+# its vertical terms (dts < dz / c_s).
+@pytest.mark.parametrize("sthopt", [0, 1])
+def test_heve_substeps(cress, oracle_lib, sthopt):
+    ni, nj, nk, ref, out = run_pair(cress, oracle_lib, 64, 48, 40, 6, sthopt=sthopt, seed=3, dts=0.2,
+                                    impopt=0)
+    check(ni, nj, nk, ref, out, 6)
+
+
+@pytest.mark.parametrize("divopt", [0, 1])
+def test_heve_ragged_divopt(cress, oracle_lib, divopt):
+    ni, nj, nk, ref, out = run_pair(cress, oracle_lib, 45, 37, 21, 4, seed=9, dts=0.2, impopt=0,
+                                    divopt=divopt)
+    check(ni, nj, nk, ref, out, 4)
