@@ -366,9 +366,9 @@ int launch_cloudphy_fused(const MicroArgs& a, const float* w, Mlp* m, const Lear
   k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
   FusedMaps maps;
   int rc;
-  if ((rc = encode_bf16_map(&maps.w1, m->w.w1t, kMlpH, kMlpK1, kMlpK1, kMlpH)) ||
-      (rc = encode_bf16_map(&maps.w2, m->w.w2t, kMlpH, kMlpH, kMlpH, kMlpH)) ||
-      (rc = encode_bf16_map(&maps.w3, m->w.w3t, kMlpH, kMlpH, kMlpH, kMlpH)) ||
+  if ((rc = encode_bf16_map(&maps.w1, m->w.w1t, kMlpH, kMlpK1, kMlpK1, 128)) ||
+      (rc = encode_bf16_map(&maps.w2, m->w.w2t, kMlpH, kMlpH, kMlpH, 128)) ||
+      (rc = encode_bf16_map(&maps.w3, m->w.w3t, kMlpH, kMlpH, kMlpH, 128)) ||
       (rc = encode_bf16_map(&maps.w4, m->w.w4t, kMlpN4, kMlpH, kMlpH, kMlpN4)))
     return rc;
   if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmem) != cudaSuccess)
@@ -389,7 +389,7 @@ int launch_cloudphy_fused(const MicroArgs& a, const float* w, Mlp* m, const Lear
   p.err = L.err;
   cudaMemsetAsync(L.fb_count, 0, sizeof(int), st);
   const long long ntiles = (p.ncell + kFusedTile - 1) / kFusedTile;
-  const int grid = (int)(ntiles < nsm ? ntiles : nsm);
+  const int grid = (int)(ntiles < 2 * nsm ? ntiles : 2 * nsm);   // two blocks per SM
   k_mlp_fused<<<grid, kFusedThreads, kFusedSmem, st>>>(maps, a, p);
   k_micro_src_list<<<nsm * 4, 128, 0, st>>>(a, 0, L.fb_list, L.fb_count, L.chunk);
   launch_fall(a, st);

@@ -9,8 +9,9 @@
 // 32(w%4).. and half of the columns), apply bias + SiLU and write the next
 // layer's BF16 activations into shared memory in the K-major 128-byte
 // swizzle the MMA reads; warp 8 (one lane) streams the W1, W2, W3 column
-// blocks (256 x 64 BF16 each) through a 2-stage TMA ring, W4 stays
-// resident; warp 9 (one lane) issues the MMAs.  Per tile: x_full (features
+// blocks (128 output rows x 64 K, BF16) and W4 through a 2-stage TMA
+// ring; warp 9 (one lane) issues the MMAs (N = 128 per block into one half
+// of the 256 accumulator columns).  Two blocks share an SM.  Per tile: x_full (features
 // written), then per layer acc_full (accumulator ready) and h_full (next
 // activations written).  Every mbarrier wait is bounded; on expiry the
 // kernel records CRESS_E_TIMEOUT, stops all roles, drains its copies and
@@ -24,12 +25,15 @@ namespace {
 constexpr int kFusedThreads = 320;
 constexpr int kFusedTile = 128;
 constexpr uint32_t kHBytes = 4 * 16384;      // activations: 4 K-blocks of 128 x 64 bf16
-constexpr uint32_t kWStage = 32768;          // one W column block: 256 x 64 bf16
-constexpr uint32_t kW4Bytes = 4 * 8192;      // W4^T: 4 K-blocks of 64 x 64 bf16
-constexpr uint32_t kFusedSmem = kHBytes + 2 * kWStage + kW4Bytes + 4 * (3 * kMlpH + kMlpN4) + 1024;
+constexpr uint32_t kWStage = 16384;          // one W block: 128 output rows x 64 K of W1..W3 (or 64 x 64 of W4)
+constexpr uint32_t kW4Block = 8192;          // one 64 x 64 K-block of W4^T
+// about 100 KB, so two blocks share an SM and one's epilogue overlaps the
+// other's MMAs
+constexpr uint32_t kFusedSmem = kHBytes + 2 * kWStage + 4 * (3 * kMlpH + kMlpN4) + 1024;
 
 struct FusedMaps {
-  CUtensorMap w1, w2, w3, w4;   // W1^T [256][64], W2^T, W3^T [256][256], W4^T [64][256]
+  // W1^T [256][64], W2^T, W3^T [256][256] (boxes of 128 rows), W4^T [64][256] (box 64 rows)
+  CUtensorMap w1, w2, w3, w4;
 };
 
 struct FusedArgs {
@@ -179,16 +183,15 @@ __device__ __forceinline__ void fused_epilogue(const MicroArgs& a, const FusedAr
   }
 }
 
-__global__ void __launch_bounds__(kFusedThreads, 1)
+__global__ void __launch_bounds__(kFusedThreads, 2)
     k_mlp_fused(const __grid_constant__ FusedMaps maps, const MicroArgs a, const FusedArgs p) {
   extern __shared__ unsigned char fsm_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(fsm_raw) + 1023) &
                                                        ~static_cast<uintptr_t>(1023));
   unsigned char* H = sm;                          // 4 K-blocks of activations (X in K-block 0)
   unsigned char* WS = sm + kHBytes;               // 2-stage W ring
-  unsigned char* W4 = WS + 2 * kWStage;           // resident W4^T
-  float* bias = reinterpret_cast<float*>(W4 + kW4Bytes);   // b1, b2, b3 (256 each), b4 (64)
-  __shared__ __align__(8) uint64_t x_full, h_full, acc_full, w4_full, w_full[2], w_empty[2], mma_done;
+  float* bias = reinterpret_cast<float*>(WS + 2 * kWStage);   // b1, b2, b3 (256 each), b4 (64)
+  __shared__ __align__(8) uint64_t x_full, h_full, acc_full, w_full[2], w_empty[2], mma_done;
   __shared__ uint32_t tmem_slot;
   __shared__ int fail;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -204,7 +207,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     mbar_init(&x_full, 256);
     mbar_init(&h_full, 256);
     mbar_init(&acc_full, 1);
-    mbar_init(&w4_full, 1);
     mbar_init(&mma_done, 1);
     for (int s = 0; s < 2; ++s) {
       mbar_init(&w_full[s], 1);
@@ -219,64 +221,57 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
 
+  // Per tile the W blocks stream in one order: layer 1 (K-block 0, output
+  // rows 0-127 then 128-255), layers 2 and 3 (K-blocks 0-3, each in the
+  // two row halves), layer 4 (K-blocks 0-3 of W4^T, 64 rows each).
   if (warp == 8) {
     // ---------------------------------------------------------- producer
     if (lane == 0) {
-      mbar_arrive_expect_tx(&w4_full, kW4Bytes);
-      for (int kb = 0; kb < 4; ++kb) tma_load_2d(W4 + kb * 8192, &maps.w4, kb * 64, 0, &w4_full);
       int cnt = 0;
       for (long long t = blockIdx.x; t < ntiles && !*vfail; t += gridDim.x)
-        for (int l = 0; l < 3 && !*vfail; ++l)
-          for (int kb = 0; kb < (l == 0 ? 1 : 4); ++kb, ++cnt) {
-            const int s = cnt & 1, r = cnt >> 1;
-            if (*vfail || !mbar_wait(&w_empty[s], (r & 1) ^ 1)) { *vfail = 1; break; }
-            mbar_arrive_expect_tx(&w_full[s], kWStage);
-            const CUtensorMap* mp = l == 0 ? &maps.w1 : (l == 1 ? &maps.w2 : &maps.w3);
-            tma_load_2d(WS + s * kWStage, mp, kb * 64, 0, &w_full[s]);
-          }
+        for (int l = 0; l < 4 && !*vfail; ++l)
+          for (int kb = 0; kb < (l == 0 ? 1 : 4) && !*vfail; ++kb)
+            for (int h = 0; h < (l == 3 ? 1 : 2); ++h, ++cnt) {
+              const int s = cnt & 1, r = cnt >> 1;
+              if (*vfail || !mbar_wait(&w_empty[s], (r & 1) ^ 1)) { *vfail = 1; break; }
+              mbar_arrive_expect_tx(&w_full[s], l == 3 ? kW4Block : kWStage);
+              const CUtensorMap* mp = l == 0 ? &maps.w1 : l == 1 ? &maps.w2 : l == 2 ? &maps.w3 : &maps.w4;
+              tma_load_2d(WS + s * kWStage, mp, kb * 64, h * 128, &w_full[s]);
+            }
       // every copy issued lands before the block may leave: the last use of
-      // each stage is waited for (bounded), and W4 once
+      // each stage is waited for (bounded)
       for (int c = cnt - 1; c >= 0 && c >= cnt - 2; --c) mbar_wait(&w_full[c & 1], (c >> 1) & 1);
-      mbar_wait(&w4_full, 0);
     }
   } else if (warp == 9) {
     // --------------------------------------------------------------- MMA
     if (lane == 0) {
-      const uint32_t id256 = idesc_bf16_f32(128, 256), id64 = idesc_bf16_f32(128, 64);
-      const uint32_t hs = smem_u32(H), ws = smem_u32(WS), w4s = smem_u32(W4);
+      const uint32_t id128 = idesc_bf16_f32(128, 128), id64 = idesc_bf16_f32(128, 64);
+      const uint32_t hs = smem_u32(H), ws = smem_u32(WS);
       int cnt = 0, phx = 0, phh = 0;
-      bool ok = mbar_wait(&w4_full, 0);
+      bool ok = true;
       for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x) {
         if (*vfail || !mbar_wait(&x_full, phx)) { ok = false; break; }
         phx ^= 1;
-        for (int l = 0; l < 3 && ok; ++l) {
+        for (int l = 0; l < 4 && ok; ++l) {
           if (l > 0) {
             if (*vfail || !mbar_wait(&h_full, phh)) { ok = false; break; }
             phh ^= 1;
           }
           tc_fence_after();
-          for (int kb = 0; kb < (l == 0 ? 1 : 4); ++kb, ++cnt) {
-            const int s = cnt & 1, r = cnt >> 1;
-            if (*vfail || !mbar_wait(&w_full[s], r & 1)) { ok = false; break; }
-            tc_fence_after();
+          for (int kb = 0; kb < (l == 0 ? 1 : 4) && ok; ++kb)
+            for (int h = 0; h < (l == 3 ? 1 : 2); ++h, ++cnt) {
+              const int s = cnt & 1, r = cnt >> 1;
+              if (*vfail || !mbar_wait(&w_full[s], r & 1)) { ok = false; break; }
+              tc_fence_after();
+              // layers 1-3: N = 128 into accumulator columns 128h..; layer 4: N = 64
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-              umma_bf16(tmem, sw128_desc(hs + kb * 16384 + k * 32), sw128_desc(ws + s * kWStage + k * 32), id256,
-                        (kb | k) != 0 ? 1u : 0u);
-            umma_commit(&w_empty[s]);
-          }
+              for (int k = 0; k < 4; ++k)
+                umma_bf16(tmem + (uint32_t)(h * 128), sw128_desc(hs + kb * 16384 + k * 32),
+                          sw128_desc(ws + s * kWStage + k * 32), l == 3 ? id64 : id128, (kb | k) != 0 ? 1u : 0u);
+              umma_commit(&w_empty[s]);
+            }
           if (ok) umma_commit(&acc_full);
         }
-        if (!ok) break;
-        if (*vfail || !mbar_wait(&h_full, phh)) { ok = false; break; }
-        phh ^= 1;
-        tc_fence_after();
-        for (int kb = 0; kb < 4; ++kb)
-#pragma unroll
-          for (int k = 0; k < 4; ++k)
-            umma_bf16(tmem, sw128_desc(hs + kb * 16384 + k * 32), sw128_desc(w4s + kb * 8192 + k * 32), id64,
-                      (kb | k) != 0 ? 1u : 0u);
-        umma_commit(&acc_full);
       }
       if (!ok) *vfail = 1;
       umma_commit(&mma_done);   // arrives once every MMA issued above has completed
