@@ -60,4 +60,22 @@ int gemm_bf16(const bf16* A, int lda, const bf16* B, int ldb, const GemmArgs& g,
 // with boxes of box_rows x 64 and the 128-byte swizzle.
 int encode_bf16_map(CUtensorMap* m, const bf16* base, int rows, int cols, int ld, int box_rows);
 
+// SiLU of the network and its derivative through the logistic function
+// sigma(x) = (1 + tanh(x/2)) / 2 on the hardware tanh (tanh.approx.f32,
+// one special-function instruction, relative error about 2^-11): the
+// activations are stored in BF16 (relative rounding 2^-9), so the
+// approximation stays below the storage rounding, and training and
+// inference use the same function.
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sigmoid_hw(float x) { return .5f + .5f * tanh_hw(.5f * x); }
+__device__ __forceinline__ float silu(float v) { return v * sigmoid_hw(v); }
+__device__ __forceinline__ float dsilu(float z) {
+  const float s = sigmoid_hw(z);
+  return s * (1.f + z * (1.f - s));
+}
+
 }  // namespace cress

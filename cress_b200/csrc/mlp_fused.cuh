@@ -62,7 +62,6 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-__device__ __forceinline__ float silu_fast(float v) { return __fdividef(v, 1.f + __expf(-v)); }
 
 // The eight epilogue warps.  Warps 0-3 own one cell each per tile (row =
 // tensor-memory lane): features, fall speeds and the CFL limit, and at the
@@ -146,8 +145,8 @@ __device__ __forceinline__ void fused_epilogue(const MicroArgs& a, const FusedAr
         uint32_t w[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const float v0 = silu_fast(__uint_as_float(r[2 * q]) + bias[l * kMlpH + c0 + 2 * q]);
-          const float v1 = silu_fast(__uint_as_float(r[2 * q + 1]) + bias[l * kMlpH + c0 + 2 * q + 1]);
+          const float v0 = silu(__uint_as_float(r[2 * q]) + bias[l * kMlpH + c0 + 2 * q]);
+          const float v1 = silu(__uint_as_float(r[2 * q + 1]) + bias[l * kMlpH + c0 + 2 * q + 1]);
           const __nv_bfloat162 hv = __floats2bfloat162_rn(v0, v1);
           w[q] = *reinterpret_cast<const uint32_t*>(&hv);
         }

@@ -39,14 +39,6 @@ struct GemmCfg {
   static constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
 };
 
-// SiLU and its derivative with the fast exponential and division
-// intrinsics (relative error ~1e-6, far below the BF16 rounding of the
-// stored activations).
-__device__ __forceinline__ float silu(float v) { return __fdividef(v, 1.f + __expf(-v)); }
-__device__ __forceinline__ float dsilu(float z) {
-  const float s = __fdividef(1.f, 1.f + __expf(-z));
-  return s * (1.f + z * (1.f - s));
-}
 
 template <int BN>
 __global__ void __launch_bounds__(kThreads, 2)
