@@ -110,6 +110,10 @@ def lib():
     L.cress_set_tuple_sampling.argtypes = [vp, vp, i, f, ull]
     L.cress_set_graphs.argtypes = [vp, i]
     L.cress_diagnostics.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double)]
+    L.cress_ensemble_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
+    L.cress_ensemble_destroy.argtypes = [vp]
+    L.cress_ensemble_destroy.restype = None
+    L.cress_ensemble_large_step.argtypes = [vp, ll, f, i, f]
     L.cress_autotune.argtypes = [vp, i, f, i, ctypes.POINTER(i), ctypes.POINTER(f)]
     _lib = L
     return L
@@ -271,6 +275,29 @@ class Solver:
     def put_precip(self, a):
         a = np.ascontiguousarray(a, dtype=np.float32)
         _check(lib().cress_put_precip(self._h, fptr(a)))
+
+
+class Ensemble:
+    """Independent domains (Solver objects, any sizes) stepped together: each
+    large step runs every member as Solver.large_step would, with the
+    acoustic substeps of all members in one launch per substep (see the
+    ensemble section of include/cress_b200.h).  The members move to the
+    first member's stream; close the ensemble before the members."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m._h for m in self.members])
+        h = ctypes.c_void_p()
+        _check(lib().cress_ensemble_create(arr, len(self.members), ctypes.byref(h)))
+        self._h = h
+
+    def large_step(self, ctime, dtb, nsstp, dts):
+        _check(lib().cress_ensemble_large_step(self._h, int(ctime), float(dtb), int(nsstp), float(dts)))
+
+    def close(self):
+        if self._h:
+            lib().cress_ensemble_destroy(self._h)
+            self._h = None
 
 
 class Mlp:

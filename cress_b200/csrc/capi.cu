@@ -2,6 +2,7 @@
 // small-step driver.  Declarations and the reference interface each entry
 // point replaces are in include/cress_b200.h.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -288,8 +289,12 @@ int Ctx::level_table(float dtb2, const float** out) {
   return CRESS_OK;
 }
 
-int Ctx::small_steps(int nsstp, float dts) {
+int Ctx::small_steps(int nsstp, float dts) { return small_steps(nsstp, dts, nullptr); }
+
+int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
   if (!base_set) return set_error(CRESS_E_STATE, "cress_small_steps: base state not set");
+  if (jobs && (cfg.impopt != 1 || cfg.tile != 0))
+    return set_error(CRESS_E_UNSUPPORTED, "ensemble small steps need impopt=1 and tile 0");
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_small_steps: nsstp=%d", nsstp);
   const bool heve = cfg.impopt == 0;
   const ThomasSet* th = nullptr;
@@ -335,17 +340,25 @@ int Ctx::small_steps(int nsstp, float dts) {
     if ((rc = tmap(olds[0], TY + 2, &maps.u)) || (rc = tmap(olds[1], TY + 3, &maps.v)) ||
         (rc = tmap(olds[2], TY + 2, &maps.w)) || (rc = tmap(olds[3], TY + 2, &maps.p)))
       return rc;
-    if (heve) {
+    if (jobs) {
+      HeviJob jb;
+      std::memset(&jb, 0, sizeof jb);
+      jb.maps = maps;
+      jb.args = a;
+      jobs->push_back(jb);
+      rc = CRESS_OK;
+    } else if (heve) {
       // the first substep forms the contravariant w of levels 2 and nk-1
       // from the past w (phy2cnt before the loop, smalldrv.f90:358)
       a.wc_from_w = s == 0;
       a.wc_old = wcside[s & 1];
       a.wc_new = wcside[(s + 1) & 1];
       rc = launch_heve_substep(a, maps, stream);
+      ++launches;
     } else {
       rc = launch_hevi_substep(a, maps, cfg.tile, stream);
+      ++launches;
     }
-    ++launches;
     if (rc) return set_error(rc, "small-step launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     for (int n = 0; n < 4; ++n) {
       float* t = news[n];
@@ -368,7 +381,7 @@ int Ctx::small_steps(int nsstp, float dts) {
 // small steps, the theta' step (inside k_force), the moist scalar steps,
 // s_cloudphy, s_timeflt (not at ctime=0), s_satadjst on t and t+dt,
 // periodic ghost planes, swp2nxt.
-int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
+int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
   if (!base_set || !large_set)
     return set_error(CRESS_E_STATE, "cress_large_step: base state (set_base3d, set_base_large) not set");
   if (cfg.advopt != 2 || !(cfg.tubopt == 0 || cfg.tubopt == 1) || !(cfg.cphopt == 0 || cfg.cphopt == 3) ||
@@ -405,6 +418,10 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
   }
   const float cpriv = 3.f;   // min(1/prnum, 3) with prnum = 0.33 (eddyvis.f90:219-222)
   if (cfg.tubopt == 1) {
+    f.rkv = rkv_d;
+    f.cpriv = cpriv;
+  }
+  if (cfg.tubopt == 1 && phase != 2) {
     // s_turbdrv up to s_eddyvis on the past level (forceuvw.f90:423-431)
     TurbArgs t{};
     t.g = g;
@@ -423,11 +440,9 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
     t.thresq = cfg.thresq;
     if ((rc = launch_turb_visc(t, stream))) return set_error(rc, "eddy viscosity launch failed");
     ++launches;
-    f.rkv = rkv_d;
-    f.cpriv = cpriv;
   }
   f.err = err_d;
-  {
+  if (phase != 2) {
     const float* bufs[FB_NONE] = {lev[CRESS_U][N], lev[CRESS_V][N], lev[CRESS_W][N], lev[CRESS_PP][N],
                                   lev[CRESS_PTP][N], lev[CRESS_U][P], lev[CRESS_V][P], lev[CRESS_W][P],
                                   lev[CRESS_PP][P], lev[CRESS_PTP][P], f.rkv};
@@ -436,10 +451,11 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts) {
       for (int q = 0; q < force_nslots(sg, f.rkv != nullptr); ++q)
         if ((rc = tmap(bufs[force_slot_buf(sg, q)], force_slot_rows(sg, q), &fm.m[sg][q]))) return rc;
     rc = launch_force(f, fm, stream);
+    launches += 2;
+    if (rc) return set_error(rc, "forcing launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
-  launches += 2;
-  if (rc) return set_error(rc, "forcing launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-  if ((rc = small_steps(nsstp, dts))) return rc;
+  if (phase == 1) return CRESS_OK;   // an ensemble runs the small steps of all members next
+  if (phase == 0 && (rc = small_steps(nsstp, dts))) return rc;
   if (moist) {
     MoistScalarArgs m{};
     m.g = g;
@@ -683,6 +699,82 @@ int Ctx::autotune(int nsstp, float dts, int reps, int* best, float* ms) {
   cfg.tile = best_tile;
   free_graphs();
   if (best) *best = best_tile;
+  return CRESS_OK;
+}
+
+// An ensemble of independent domains on one device and one stream: every
+// member runs its own large step, except that the acoustic substeps of all
+// members run as one launch per substep (k_hevi2_batch over every
+// member's tiles), so small domains fill the GPU together.
+struct Ensemble {
+  std::vector<Ctx*> members;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  HeviJob* jobs_d = nullptr;   // nsstp x members jobs of the current step
+  HeviJob* jobs_h = nullptr;   // pinned staging
+  size_t cap = 0;
+  cudaEvent_t staged = nullptr;   // the last copy out of jobs_h has completed
+  long long launches = 0;
+  ~Ensemble() {
+    cudaSetDevice(device);
+    if (staged) { cudaEventSynchronize(staged); cudaEventDestroy(staged); }
+    if (jobs_d) cudaFree(jobs_d);
+    if (jobs_h) cudaFreeHost(jobs_h);
+  }
+  int large_step(long long ctime, float dtb, int nsstp, float dts);
+};
+
+int Ensemble::large_step(long long ctime, float dtb, int nsstp, float dts) {
+  const bool filter = ctime != 0;
+  const int n = (int)members.size();
+  int rc;
+  for (Ctx* c : members)
+    if ((rc = c->large_step(filter, dtb, nsstp, dts, 1))) return rc;
+  std::vector<std::vector<HeviJob>> per(n);
+  int nk_max = 0;
+  for (int m = 0; m < n; ++m) {
+    if ((rc = members[m]->small_steps(nsstp, dts, &per[m]))) return rc;
+    nk_max = std::max(nk_max, members[m]->g.nk);
+  }
+  const size_t need = (size_t)nsstp * n;
+  if (need > cap) {
+    if (staged) cudaEventSynchronize(staged);
+    if (jobs_d) cudaFree(jobs_d);
+    if (jobs_h) cudaFreeHost(jobs_h);
+    jobs_d = nullptr;
+    jobs_h = nullptr;
+    if ((rc = cuda_check(cudaMalloc(&jobs_d, sizeof(HeviJob) * need), "cudaMalloc ensemble jobs")) ||
+        (rc = cuda_check(cudaMallocHost(&jobs_h, sizeof(HeviJob) * need), "cudaMallocHost ensemble jobs")))
+      return rc;
+    cap = need;
+  } else if (staged) {
+    cudaEventSynchronize(staged);   // the previous step's copy has left the staging buffer
+  }
+  int nblocks = 0;
+  for (int m = 0; m < n; ++m) {
+    int tx, ty;
+    hevi_job_tiles(members[m]->g, &tx, &ty);
+    for (int st = 0; st < nsstp; ++st) {
+      HeviJob& j = jobs_h[(size_t)st * n + m];
+      j = per[m][st];
+      j.first_block = nblocks;
+      j.tiles_x = tx;
+    }
+    nblocks += tx * ty;
+  }
+  if ((rc = cuda_check(cudaMemcpyAsync(jobs_d, jobs_h, sizeof(HeviJob) * need, cudaMemcpyHostToDevice, stream),
+                       "copy ensemble jobs")))
+    return rc;
+  cudaEventRecord(staged, stream);
+  const cress_cfg& c0 = members[0]->cfg;
+  for (int st = 0; st < nsstp; ++st) {
+    if ((rc = launch_hevi_batch(jobs_d + (size_t)st * n, n, nblocks, nk_max, c0.divopt, c0.sthopt != 0,
+                                c0.buyopt == 1, stream)))
+      return set_error(rc, "ensemble small-step launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    ++launches;
+  }
+  for (Ctx* c : members)
+    if ((rc = c->large_step(filter, dtb, nsstp, dts, 2))) return rc;
   return CRESS_OK;
 }
 
@@ -1158,4 +1250,48 @@ int cress_autotune(cress_ctx* ctx, int nsstp, float dts, int reps, int* best_til
   return c->autotune(nsstp, dts, reps, best_tile, ms_per_substep);
 }
 
+int cress_ensemble_create(cress_ctx* const* members, int n, cress_ensemble** out) {
+  if (!members || n < 1 || !out) return set_error(CRESS_E_ARG, "cress_ensemble_create: bad arguments");
+  *out = nullptr;
+  Ctx* c0 = reinterpret_cast<Ctx*>(members[0]);
+  for (int m = 0; m < n; ++m) {
+    Ctx* c = reinterpret_cast<Ctx*>(members[m]);
+    if (!c) return set_error(CRESS_E_ARG, "cress_ensemble_create: null member %d", m);
+    if (c->device != c0->device) return set_error(CRESS_E_ARG, "ensemble members live on different devices");
+    if (!c->base_set || !c->large_set) return set_error(CRESS_E_STATE, "member %d: base state not set", m);
+    if (c->cfg.impopt != 1 || c->cfg.divopt != c0->cfg.divopt || (c->cfg.sthopt != 0) != (c0->cfg.sthopt != 0) ||
+        c->cfg.buyopt != c0->cfg.buyopt)
+      return set_error(CRESS_E_UNSUPPORTED, "ensemble members need impopt=1 and the same divopt, sthopt, buyopt");
+  }
+  cudaSetDevice(c0->device);
+  Ensemble* e = new Ensemble;
+  e->device = c0->device;
+  e->stream = c0->stream;
+  if (cudaEventCreateWithFlags(&e->staged, cudaEventDisableTiming) != cudaSuccess) {
+    delete e;
+    return set_error(CRESS_E_CUDA, "cudaEventCreate failed");
+  }
+  for (int m = 0; m < n; ++m) {
+    Ctx* c = reinterpret_cast<Ctx*>(members[m]);
+    cudaStreamSynchronize(c->stream);
+    c->free_graphs();
+    c->cfg.tile = 0;        // the ensemble launch runs tile 0's kernel
+    c->stream = e->stream;  // one stream orders the members' work and the shared launches
+    e->members.push_back(c);
+  }
+  *out = reinterpret_cast<cress_ensemble*>(e);
+  return CRESS_OK;
+}
+
+void cress_ensemble_destroy(cress_ensemble* e) { delete reinterpret_cast<Ensemble*>(e); }
+
+int cress_ensemble_large_step(cress_ensemble* eh, long long ctime, float dtb, int nsstp, float dts) {
+  Ensemble* e = reinterpret_cast<Ensemble*>(eh);
+  if (!e) return set_error(CRESS_E_ARG, "null ensemble");
+  if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_ensemble_large_step: nsstp=%d", nsstp);
+  cudaSetDevice(e->device);
+  return e->large_step(ctime, dtb, nsstp, dts);
+}
+
 }  // extern "C"
+

@@ -8,6 +8,7 @@
 #include <vector>
 #include "../../include/cress_b200.h"
 #include "common.cuh"
+#include "hevi.cuh"
 #include "micro.cuh"
 
 namespace cress {
@@ -51,7 +52,13 @@ struct Ctx {
   std::map<uint32_t, float*> level_tables;   // level table per 2*dtb (bits)
   int level_table(float dtb2, const float** out);
   int small_steps(int nsstp, float dts);
-  int large_step(bool filter, float dtb, int nsstp, float dts);
+  // phase 0: the whole step; 1: up to the forcing; 2: from the moist
+  // scalars on (an ensemble runs every member's small steps in between)
+  int large_step(bool filter, float dtb, int nsstp, float dts, int phase = 0);
+  // jobs != null: instead of launching, append every substep's arguments
+  // and maps (HE-VI, tile 0) for an ensemble launch; the pointer swaps that
+  // make the result the future level are done either way
+  int small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs);
   int ksp0 = 2;            // first Rayleigh-damped level
   bool large_set = false;  // cress_set_base_large was called
   bool moist_set = false;  // cress_set_base_moist was called

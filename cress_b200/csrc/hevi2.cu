@@ -24,6 +24,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 #include "common.cuh"
 #include "f2.cuh"
 #include "hevi.cuh"
@@ -71,16 +72,17 @@ struct H2Layout {
 // on them.  GT: the per-level columns and the elimination factors are read
 // from global memory (the level table, a.lvl) instead of being copied into
 // shared memory, which leaves room for more resident blocks.
+// One tile (bx, by) of one substep; m and a stay in the memory they came
+// from (kernel parameters, or an ensemble's job array in global memory).
 template <int S, int DIV, bool STH, bool BUY, bool GT>
-__global__ void __launch_bounds__(kHeviTX * kH2Rows, GT ? 5 : 4)
-k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
+__device__ __forceinline__ void hevi2_tile(const HeviMaps& m, const HeviArgs& a, int bx, int by) {
   using L = H2Layout<S>;
   constexpr int TX = kHeviTX, TY = kH2TY, BX = kHeviBoxX, NT = TX * kH2Rows;
   const unsigned full = 0xffffffffu;
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int i0 = 2 + blockIdx.x * TX, j0 = 2 + blockIdx.y * TY;
+  const int i0 = 2 + bx * TX, j0 = 2 + by * TY;
   const int xb = i0 - 2;  // box x origin (multiple of 32)
   const int ilast = min(i0 + TX - 1, ni - 2), jlast = min(j0 + TY - 1, nj - 2);
   const int i = i0 + tx, jA = j0 + 2 * ty, jB = jA + 1;
@@ -397,6 +399,37 @@ k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
   finish(cB, ownB, edgeB, ylastB, jB);
 }
 
+template <int S, int DIV, bool STH, bool BUY, bool GT>
+__global__ void __launch_bounds__(kHeviTX * kH2Rows, GT ? 5 : 4)
+k_hevi2(const __grid_constant__ HeviMaps m, const HeviArgs a) {
+  hevi2_tile<S, DIV, STH, BUY, GT>(m, a, blockIdx.x, blockIdx.y);
+}
+
+// Every member of an ensemble in one launch: block b belongs to the member
+// whose first_block is the largest not above b (the jobs are in block
+// order), which runs its tile b - first_block.
+template <int S, int DIV, bool STH, bool BUY>
+__global__ void __launch_bounds__(kHeviTX * kH2Rows, 4)
+k_hevi2_batch(const HeviJob* __restrict__ jobs, int njobs) {
+  int lo = 0, hi = njobs - 1;
+  const int b = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].first_block <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const HeviJob& job = jobs[lo];
+  const int t = b - job.first_block;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    // the maps were copied into global memory by the host: make that copy
+    // visible to the tensor-map proxy before the first TMA load reads them
+    const CUtensorMap* mp = &job.maps.u;
+    for (int q = 0; q < 8; ++q)
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mp + q) : "memory");
+  }
+  hevi2_tile<S, DIV, STH, BUY, false>(job.maps, job.args, t % job.tiles_x, t / job.tiles_x);
+}
+
 template <int S, bool GT, int DIV, bool STH, bool BUY>
 int launch_h2(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
   using L = H2Layout<S>;
@@ -437,6 +470,41 @@ int launch_hevi2(const HeviArgs& a, const HeviMaps& maps, int variant, cudaStrea
   if (a.g.count() >= (1LL << 31) || a.g.nk < 6) return CRESS_E_UNSUPPORTED;   // 32-bit indices; levels 2..nk-2 >= 3
   if (variant == 1) return a.lvl ? launch_h2_opts<3, true>(a, maps, st) : CRESS_E_UNSUPPORTED;
   return launch_h2_opts<4, false>(a, maps, st);
+}
+
+// Tiles of tile 0 (32 x 8 columns) of a member's grid.
+void hevi_job_tiles(const Grid& g, int* tx, int* ty) {
+  *tx = (g.ni - 3 + kHeviTX - 1) / kHeviTX;
+  *ty = (g.nj - 3 + kH2TY - 1) / kH2TY;
+}
+
+template <int DIV, bool STH, bool BUY>
+static int launch_batch_t(const HeviJob* jobs_d, int njobs, int nblocks, int nk_max, cudaStream_t st) {
+  constexpr int S = 4;
+  using L = H2Layout<S>;
+  const size_t bytes = L::bytes(nk_max, false);
+  if (bytes > 227 * 1024) return CRESS_E_UNSUPPORTED;
+  auto kern = k_hevi2_batch<S, DIV, STH, BUY>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+    return CRESS_E_CUDA;
+  kern<<<nblocks, dim3(kHeviTX, kH2Rows), bytes, st>>>(jobs_d, njobs);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+int launch_hevi_batch(const HeviJob* jobs_d, int njobs, int nblocks, int nk_max, int divopt, bool sth, bool buy,
+                      cudaStream_t st) {
+  auto pick = [&](auto div) -> int {
+    constexpr int D = decltype(div)::value;
+    if (sth) return buy ? launch_batch_t<D, true, true>(jobs_d, njobs, nblocks, nk_max, st)
+                        : launch_batch_t<D, true, false>(jobs_d, njobs, nblocks, nk_max, st);
+    return buy ? launch_batch_t<D, false, true>(jobs_d, njobs, nblocks, nk_max, st)
+               : launch_batch_t<D, false, false>(jobs_d, njobs, nblocks, nk_max, st);
+  };
+  switch (divopt) {
+    case 2: return pick(std::integral_constant<int, 2>{});
+    case 1: return pick(std::integral_constant<int, 1>{});
+    default: return pick(std::integral_constant<int, 0>{});
+  }
 }
 
 }  // namespace cress

@@ -173,6 +173,20 @@ int cress_diagnostics(cress_ctx* ctx, int level, double* out);
  * this grid cannot use) may be null. */
 int cress_autotune(cress_ctx* ctx, int nsstp, float dts, int reps, int* best_tile, float* ms_per_substep);
 
+/* Ensembles.  An ensemble groups contexts of independent domains (any
+ * sizes) on one device: cress_ensemble_large_step runs one large step of
+ * every member, each as cress_large_step would, except that the acoustic
+ * substeps of all members run as one kernel launch per substep over every
+ * member's tiles (small domains fill the GPU together).  Members need
+ * impopt=1 and the same divopt, sthopt (zero or not) and buyopt; creating
+ * the ensemble switches every member to the first member's stream and to
+ * tile 0.  Members stay valid contexts (sync calls, cress_large_step);
+ * destroy the ensemble before its members. */
+typedef struct cress_ensemble cress_ensemble;
+int cress_ensemble_create(cress_ctx* const* members, int n, cress_ensemble** out);
+void cress_ensemble_destroy(cress_ensemble* e);
+int cress_ensemble_large_step(cress_ensemble* e, long long ctime, float dtb, int nsstp, float dts);
+
 /* Replay whole large steps from CUDA graphs (on != 0) instead of launching
  * every kernel from the host: the second step with a given time-level
  * state and parameters is captured, later ones launch the graph.  Results
