@@ -114,6 +114,7 @@ def lib():
     L.cress_ensemble_destroy.argtypes = [vp]
     L.cress_ensemble_destroy.restype = None
     L.cress_ensemble_large_step.argtypes = [vp, ll, f, i, f]
+    L.cress_ensemble_set_graphs.argtypes = [vp, i]
     L.cress_autotune.argtypes = [vp, i, f, i, ctypes.POINTER(i), ctypes.POINTER(f)]
     _lib = L
     return L
@@ -281,15 +282,22 @@ class Ensemble:
     """Independent domains (Solver objects, any sizes) stepped together: each
     large step runs every member as Solver.large_step would, with the
     acoustic substeps of all members in one launch per substep (see the
-    ensemble section of include/cress_b200.h).  The members move to the
-    first member's stream; close the ensemble before the members."""
+    ensemble section of include/cress_b200.h).  Each member keeps its own
+    stream; repeated steps replay one CUDA graph of the whole ensemble step
+    unless graphs=False.  Close the ensemble before the members."""
 
-    def __init__(self, members):
+    def __init__(self, members, graphs=True):
         self.members = list(members)
         arr = (ctypes.c_void_p * len(self.members))(*[m._h for m in self.members])
         h = ctypes.c_void_p()
         _check(lib().cress_ensemble_create(arr, len(self.members), ctypes.byref(h)))
         self._h = h
+        if not graphs:
+            _check(lib().cress_ensemble_set_graphs(self._h, 0))
+
+    def sync(self):
+        for m in self.members:
+            m.sync()
 
     def large_step(self, ctime, dtb, nsstp, dts):
         _check(lib().cress_ensemble_large_step(self._h, int(ctime), float(dtb), int(nsstp), float(dts)))

@@ -706,30 +706,72 @@ int Ctx::autotune(int nsstp, float dts, int reps, int* best, float* ms) {
 // member runs its own large step, except that the acoustic substeps of all
 // members run as one launch per substep (k_hevi2_batch over every
 // member's tiles), so small domains fill the GPU together.
+// An ensemble step runs each member's work before and after the acoustic
+// substeps on the member's own stream (members overlap), and the substeps of
+// all members as one launch per substep on the ensemble's stream, joined to
+// the members' streams by events.  With graphs on, a step whose pointer
+// states and parameters were seen before replays one CUDA graph that holds
+// all of it (member streams forked from and joined back to the ensemble's).
 struct Ensemble {
   std::vector<Ctx*> members;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // the ensemble's own stream
   int device = 0;
-  HeviJob* jobs_d = nullptr;   // nsstp x members jobs of the current step
-  HeviJob* jobs_h = nullptr;   // pinned staging
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> ev;        // one per member
+  HeviJob* jobs_d = nullptr;          // eager steps: nsstp x members jobs
+  HeviJob* jobs_h = nullptr;          // pinned staging
   size_t cap = 0;
-  cudaEvent_t staged = nullptr;   // the last copy out of jobs_h has completed
+  cudaEvent_t staged = nullptr;       // the last copy out of jobs_h has completed
   long long launches = 0;
+  bool graphs = true;
+  struct Rec {
+    cudaGraphExec_t exec = nullptr;
+    HeviJob* jobs_d = nullptr;        // this graph's job table and its pinned source
+    HeviJob* jobs_h = nullptr;
+    long long nlaunch = 0;
+    std::vector<long long> member_launches;
+    std::vector<std::vector<float*>> post;
+  };
+  std::map<std::string, Rec> grec;
+  std::map<std::string, int> gseen;
+  void free_graphs() {
+    for (auto& kv : grec) {
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+      if (kv.second.jobs_d) cudaFree(kv.second.jobs_d);
+      if (kv.second.jobs_h) cudaFreeHost(kv.second.jobs_h);
+    }
+    grec.clear();
+    gseen.clear();
+  }
   ~Ensemble() {
     cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    free_graphs();
     if (staged) { cudaEventSynchronize(staged); cudaEventDestroy(staged); }
+    for (cudaEvent_t x : ev) cudaEventDestroy(x);
+    if (fork) cudaEventDestroy(fork);
+    if (done) cudaEventDestroy(done);
     if (jobs_d) cudaFree(jobs_d);
     if (jobs_h) cudaFreeHost(jobs_h);
+    if (stream) cudaStreamDestroy(stream);
   }
-  int large_step(long long ctime, float dtb, int nsstp, float dts);
+  int large_step(long long ctime, float dtb, int nsstp, float dts, HeviJob* jd, HeviJob* jh, bool eager);
+  int step(long long ctime, float dtb, int nsstp, float dts);
 };
 
-int Ensemble::large_step(long long ctime, float dtb, int nsstp, float dts) {
+// One ensemble step issued on the streams (eager, or inside a capture that
+// began on `stream`).  jd/jh: job table on the device and its pinned source.
+int Ensemble::large_step(long long ctime, float dtb, int nsstp, float dts, HeviJob* jd, HeviJob* jh,
+                         bool eager) {
   const bool filter = ctime != 0;
   const int n = (int)members.size();
   int rc;
-  for (Ctx* c : members)
+  cudaEventRecord(fork, stream);
+  for (int m = 0; m < n; ++m) {
+    Ctx* c = members[m];
+    cudaStreamWaitEvent(c->stream, fork, 0);
     if ((rc = c->large_step(filter, dtb, nsstp, dts, 1))) return rc;
+  }
   std::vector<std::vector<HeviJob>> per(n);
   int nk_max = 0;
   for (int m = 0; m < n; ++m) {
@@ -737,44 +779,135 @@ int Ensemble::large_step(long long ctime, float dtb, int nsstp, float dts) {
     nk_max = std::max(nk_max, members[m]->g.nk);
   }
   const size_t need = (size_t)nsstp * n;
-  if (need > cap) {
-    if (staged) cudaEventSynchronize(staged);
-    if (jobs_d) cudaFree(jobs_d);
-    if (jobs_h) cudaFreeHost(jobs_h);
-    jobs_d = nullptr;
-    jobs_h = nullptr;
-    if ((rc = cuda_check(cudaMalloc(&jobs_d, sizeof(HeviJob) * need), "cudaMalloc ensemble jobs")) ||
-        (rc = cuda_check(cudaMallocHost(&jobs_h, sizeof(HeviJob) * need), "cudaMallocHost ensemble jobs")))
-      return rc;
-    cap = need;
-  } else if (staged) {
-    cudaEventSynchronize(staged);   // the previous step's copy has left the staging buffer
-  }
+  if (eager) cudaEventSynchronize(staged);   // the previous step's copy has left the staging buffer
   int nblocks = 0;
   for (int m = 0; m < n; ++m) {
     int tx, ty;
     hevi_job_tiles(members[m]->g, &tx, &ty);
     for (int st = 0; st < nsstp; ++st) {
-      HeviJob& j = jobs_h[(size_t)st * n + m];
+      HeviJob& j = jh[(size_t)st * n + m];
       j = per[m][st];
       j.first_block = nblocks;
       j.tiles_x = tx;
     }
     nblocks += tx * ty;
   }
-  if ((rc = cuda_check(cudaMemcpyAsync(jobs_d, jobs_h, sizeof(HeviJob) * need, cudaMemcpyHostToDevice, stream),
+  for (int m = 0; m < n; ++m) {
+    cudaEventRecord(ev[m], members[m]->stream);
+    cudaStreamWaitEvent(stream, ev[m], 0);
+  }
+  if ((rc = cuda_check(cudaMemcpyAsync(jd, jh, sizeof(HeviJob) * need, cudaMemcpyHostToDevice, stream),
                        "copy ensemble jobs")))
     return rc;
-  cudaEventRecord(staged, stream);
+  if (eager) cudaEventRecord(staged, stream);
   const cress_cfg& c0 = members[0]->cfg;
   for (int st = 0; st < nsstp; ++st) {
-    if ((rc = launch_hevi_batch(jobs_d + (size_t)st * n, n, nblocks, nk_max, c0.divopt, c0.sthopt != 0,
+    if ((rc = launch_hevi_batch(jd + (size_t)st * n, n, nblocks, nk_max, c0.divopt, c0.sthopt != 0,
                                 c0.buyopt == 1, stream)))
       return set_error(rc, "ensemble small-step launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     ++launches;
   }
-  for (Ctx* c : members)
+  cudaEventRecord(done, stream);
+  for (int m = 0; m < n; ++m) {
+    Ctx* c = members[m];
+    cudaStreamWaitEvent(c->stream, done, 0);
     if ((rc = c->large_step(filter, dtb, nsstp, dts, 2))) return rc;
+  }
+  for (int m = 0; m < n; ++m) {   // join: the ensemble's stream follows every member
+    cudaEventRecord(ev[m], members[m]->stream);
+    cudaStreamWaitEvent(stream, ev[m], 0);
+  }
+  return CRESS_OK;
+}
+
+int Ensemble::step(long long ctime, float dtb, int nsstp, float dts) {
+  const int n = (int)members.size();
+  const size_t need = (size_t)nsstp * n;
+  auto eager = [&]() -> int {
+    if (need > cap) {
+      cudaEventSynchronize(staged);
+      if (jobs_d) cudaFree(jobs_d);
+      if (jobs_h) cudaFreeHost(jobs_h);
+      jobs_d = nullptr;
+      jobs_h = nullptr;
+      cap = 0;
+      int rc;
+      if ((rc = cuda_check(cudaMalloc(&jobs_d, sizeof(HeviJob) * need), "cudaMalloc ensemble jobs")) ||
+          (rc = cuda_check(cudaMallocHost(&jobs_h, sizeof(HeviJob) * need), "cudaMallocHost ensemble jobs")))
+        return rc;
+      cap = need;
+    }
+    return large_step(ctime, dtb, nsstp, dts, jobs_d, jobs_h, true);
+  };
+  bool sampling = false;
+  for (Ctx* c : members) sampling |= c->sampler != nullptr;
+  if (!graphs || sampling) return eager();
+  std::string key;
+  for (Ctx* c : members) {
+    const std::vector<float*> ps = c->pointer_state();
+    key.append(reinterpret_cast<const char*>(ps.data()), ps.size() * sizeof(float*));
+    const struct { float resid; const void* mlp; int chunk; } q{c->resid_tol, c->mlp, c->lb.chunk};
+    key.append(reinterpret_cast<const char*>(&q), sizeof q);
+  }
+  const struct { long long filter; int nsstp; float dtb, dts; } p{ctime != 0 ? 1 : 0, nsstp, dtb, dts};
+  key.append(reinterpret_cast<const char*>(&p), sizeof p);
+  auto it = grec.find(key);
+  if (it == grec.end()) {
+    if (gseen[key]++ == 0) return eager();
+    std::vector<std::vector<float*>> pre;
+    std::vector<long long> l0;
+    for (Ctx* c : members) { pre.push_back(c->pointer_state()); l0.push_back(c->launches); }
+    const long long e0 = launches;
+    Rec r;
+    if (cudaMalloc(&r.jobs_d, sizeof(HeviJob) * need) != cudaSuccess ||
+        cudaMallocHost(&r.jobs_h, sizeof(HeviJob) * need) != cudaSuccess) {
+      cudaGetLastError();
+      if (r.jobs_d) cudaFree(r.jobs_d);
+      graphs = false;
+      return eager();
+    }
+    cudaGraph_t graph = nullptr;
+    int rc = CRESS_E_CUDA;
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      rc = large_step(ctime, dtb, nsstp, dts, r.jobs_d, r.jobs_h, false);
+      const cudaError_t e = cudaStreamEndCapture(stream, &graph);
+      if (!rc && (e != cudaSuccess || cudaGraphInstantiate(&r.exec, graph, 0) != cudaSuccess)) rc = CRESS_E_CUDA;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    for (int m = 0; m < n; ++m) {
+      r.member_launches.push_back(members[m]->launches - l0[m]);
+      members[m]->launches = l0[m];
+      r.post.push_back(members[m]->pointer_state());
+      members[m]->set_pointer_state(pre[m]);
+    }
+    r.nlaunch = launches - e0;
+    launches = e0;
+    if (rc) {   // nothing ran: run eagerly from the same state
+      cudaGetLastError();
+      if (r.exec) cudaGraphExecDestroy(r.exec);
+      cudaFree(r.jobs_d);
+      cudaFreeHost(r.jobs_h);
+      graphs = false;
+      return eager();
+    }
+    it = grec.emplace(key, std::move(r)).first;
+  }
+  // the graph starts after each member's queued work and its end orders
+  // each member's later work
+  for (int m = 0; m < n; ++m) {
+    cudaEventRecord(ev[m], members[m]->stream);
+    cudaStreamWaitEvent(stream, ev[m], 0);
+  }
+  if (cudaGraphLaunch(it->second.exec, stream) != cudaSuccess)
+    return set_error(CRESS_E_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaEventRecord(done, stream);
+  launches += it->second.nlaunch;
+  for (int m = 0; m < n; ++m) {
+    Ctx* c = members[m];
+    cudaStreamWaitEvent(c->stream, done, 0);
+    c->launches += it->second.member_launches[m];
+    c->set_pointer_state(it->second.post[m]);
+  }
   return CRESS_OK;
 }
 
@@ -1266,17 +1399,24 @@ int cress_ensemble_create(cress_ctx* const* members, int n, cress_ensemble** out
   cudaSetDevice(c0->device);
   Ensemble* e = new Ensemble;
   e->device = c0->device;
-  e->stream = c0->stream;
-  if (cudaEventCreateWithFlags(&e->staged, cudaEventDisableTiming) != cudaSuccess) {
+  bool ok = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->staged, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) == cudaSuccess;
+  for (int m = 0; ok && m < n; ++m) {
+    cudaEvent_t x = nullptr;
+    ok = cudaEventCreateWithFlags(&x, cudaEventDisableTiming) == cudaSuccess;
+    if (ok) e->ev.push_back(x);
+  }
+  if (!ok) {
     delete e;
-    return set_error(CRESS_E_CUDA, "cudaEventCreate failed");
+    return set_error(CRESS_E_CUDA, "cress_ensemble_create: stream or event creation failed");
   }
   for (int m = 0; m < n; ++m) {
     Ctx* c = reinterpret_cast<Ctx*>(members[m]);
     cudaStreamSynchronize(c->stream);
     c->free_graphs();
     c->cfg.tile = 0;        // the ensemble launch runs tile 0's kernel
-    c->stream = e->stream;  // one stream orders the members' work and the shared launches
     e->members.push_back(c);
   }
   *out = reinterpret_cast<cress_ensemble*>(e);
@@ -1290,7 +1430,17 @@ int cress_ensemble_large_step(cress_ensemble* eh, long long ctime, float dtb, in
   if (!e) return set_error(CRESS_E_ARG, "null ensemble");
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_ensemble_large_step: nsstp=%d", nsstp);
   cudaSetDevice(e->device);
-  return e->large_step(ctime, dtb, nsstp, dts);
+  return e->step(ctime, dtb, nsstp, dts);
+}
+
+int cress_ensemble_set_graphs(cress_ensemble* eh, int on) {
+  Ensemble* e = reinterpret_cast<Ensemble*>(eh);
+  if (!e) return set_error(CRESS_E_ARG, "null ensemble");
+  cudaSetDevice(e->device);
+  cudaStreamSynchronize(e->stream);
+  e->free_graphs();
+  e->graphs = on != 0;
+  return CRESS_OK;
 }
 
 }  // extern "C"

@@ -177,14 +177,19 @@ int cress_autotune(cress_ctx* ctx, int nsstp, float dts, int reps, int* best_til
  * sizes) on one device: cress_ensemble_large_step runs one large step of
  * every member, each as cress_large_step would, except that the acoustic
  * substeps of all members run as one kernel launch per substep over every
- * member's tiles (small domains fill the GPU together).  Members need
- * impopt=1 and the same divopt, sthopt (zero or not) and buyopt; creating
- * the ensemble switches every member to the first member's stream and to
- * tile 0.  Members stay valid contexts (sync calls, cress_large_step);
- * destroy the ensemble before its members. */
+ * member's tiles (small domains fill the GPU together).  The rest of each
+ * member's step stays on the member's own stream, so members overlap; the
+ * shared launches run on the ensemble's stream, ordered against the
+ * members' streams by events.  A step whose pointer states and parameters
+ * were seen before replays one CUDA graph of the whole ensemble step
+ * (cress_ensemble_set_graphs(e, 0) turns that off).  Members need impopt=1
+ * and the same divopt, sthopt (zero or not) and buyopt; creating the
+ * ensemble sets every member to tile 0.  Members stay valid contexts (sync
+ * calls, cress_large_step); destroy the ensemble before its members. */
 typedef struct cress_ensemble cress_ensemble;
 int cress_ensemble_create(cress_ctx* const* members, int n, cress_ensemble** out);
 void cress_ensemble_destroy(cress_ensemble* e);
+int cress_ensemble_set_graphs(cress_ensemble* e, int on);
 int cress_ensemble_large_step(cress_ensemble* e, long long ctime, float dtb, int nsstp, float dts);
 
 /* Replay whole large steps from CUDA graphs (on != 0) instead of launching

@@ -1,5 +1,6 @@
 """Ensembles: members of uneven sizes stepped together (one acoustic launch
-per substep over every member's tiles) give bitwise the same states as the
+per substep over every member's tiles, the rest on each member's stream,
+eagerly or replayed from CUDA graphs) give bitwise the same states as the
 same members stepped one by one."""
 import numpy as np
 import pytest
@@ -30,9 +31,9 @@ def member(cress, oracle_lib, nx, ny, nz, seed):
 SIZES = [(40, 33, 22, 1), (29, 45, 22, 2), (64, 20, 22, 3)]
 
 
-def run(cress, oracle_lib, together, nsteps=3):
+def run(cress, oracle_lib, together, nsteps=3, graphs=False):
     sols = [member(cress, oracle_lib, *sz) for sz in SIZES]
-    ens = cress.Ensemble(sols) if together else None
+    ens = cress.Ensemble(sols, graphs=graphs) if together else None
     for step in range(nsteps):
         first = step == 0
         args = (step * 5000, 2.5 if first else 5.0, 10, 0.5 if first else 1.0)
@@ -49,9 +50,10 @@ def run(cress, oracle_lib, together, nsteps=3):
     return out
 
 
-def test_ensemble_matches_members_one_by_one(cress, oracle_lib):
-    a = run(cress, oracle_lib, False)
-    b = run(cress, oracle_lib, True)
+@pytest.mark.parametrize("graphs,nsteps", [(False, 3), (True, 9)])
+def test_ensemble_matches_members_one_by_one(cress, oracle_lib, graphs, nsteps):
+    a = run(cress, oracle_lib, False, nsteps)
+    b = run(cress, oracle_lib, True, nsteps, graphs)
     for m, (x, y) in enumerate(zip(a, b)):
         for n, p, q in zip(NAMES + ["precip"], x, y):
             assert np.isfinite(q).all(), (m, n)
