@@ -51,7 +51,7 @@ class Cfg(ctypes.Structure):
                 ("coropt", ctypes.c_int), ("tubopt", ctypes.c_int), ("cphopt", ctypes.c_int),
                 ("smhcoe", ctypes.c_float), ("smvcoe", ctypes.c_float), ("filcoe", ctypes.c_float),
                 ("fc", ctypes.c_float), ("vspvar", ctypes.c_char * 16),
-                ("thresq", ctypes.c_float), ("reserved", ctypes.c_int * 7)]
+                ("thresq", ctypes.c_float), ("gwave", ctypes.c_float), ("reserved", ctypes.c_int * 6)]
 
 
 _lib = None
@@ -136,14 +136,17 @@ class Solver:
     def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6, impopt=1,
                  tile=0, device=0, smtopt=3, smhcoe=0.001, smvcoe=0.0004, vspopt=2,
                  vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1, cphopt=0, thresq=1e-12,
-                 tubopt=0):
+                 tubopt=0, obc=0, gwave=20.0):
         L = lib()
         c = Cfg()
         c.ni, c.nj, c.nk = ni, nj, nk
         c.dx, c.dy, c.dz = dx, dy, dz
         c.sthopt, c.impopt, c.divopt, c.buyopt, c.gwmopt = sthopt, impopt, divopt, buyopt, 0
         c.weicoe = weicoe
-        c.wbc = c.ebc = c.sbc = c.nbc = -1
+        # obc 0: periodic on all sides; 4, 5, 7: open radiation x boundaries
+        c.wbc = c.ebc = obc if obc else -1
+        c.sbc = c.nbc = -1
+        c.gwave = gwave
         c.bbc = c.tbc = 2
         c.tile = tile
         c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = 2, smtopt, vspopt, coropt, tubopt, cphopt

@@ -16,6 +16,7 @@
 #include "diag.cuh"
 #include "hevi.cuh"
 #include "forcing.cuh"
+#include "openbc.cuh"
 #include "micro.cuh"
 #include "mlp_impl.cuh"
 
@@ -293,8 +294,10 @@ int Ctx::small_steps(int nsstp, float dts) { return small_steps(nsstp, dts, null
 
 int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
   if (!base_set) return set_error(CRESS_E_STATE, "cress_small_steps: base state not set");
-  if (jobs && (cfg.impopt != 1 || cfg.tile != 0))
-    return set_error(CRESS_E_UNSUPPORTED, "ensemble small steps need impopt=1 and tile 0");
+  if (jobs && (cfg.impopt != 1 || cfg.tile != 0 || g.openx))
+    return set_error(CRESS_E_UNSUPPORTED, "ensemble small steps need impopt=1, tile 0 and periodic x");
+  if (g.openx && cfg.tile != 0 && cfg.tile != 11)
+    return set_error(CRESS_E_UNSUPPORTED, "open x boundaries run the HE-VI tiles 0 and 11");
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_small_steps: nsstp=%d", nsstp);
   const bool heve = cfg.impopt == 0;
   const ThomasSet* th = nullptr;
@@ -358,6 +361,18 @@ int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
     } else {
       rc = launch_hevi_substep(a, maps, cfg.tile, stream);
       ++launches;
+      if (!rc && g.openx) {   // the boundary columns of this substep (stepuv/stepwi/steppi rbc*)
+        RbcSmallArgs r{};
+        r.g = g;
+        r.cp = rad_d;
+        r.col = col_d;
+        r.u_old = olds[0]; r.v_old = olds[1]; r.w_old = olds[2]; r.p_old = olds[3];
+        r.u_new = news[0]; r.v_new = news[1]; r.w_new = news[2]; r.p_new = news[3];
+        r.sthopt = cfg.sthopt;
+        r.bbc = cfg.bbc;
+        rc = launch_rbc_small(r, stream);
+        ++launches;
+      }
     }
     if (rc) return set_error(rc, "small-step launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     for (int n = 0; n < 4; ++n) {
@@ -483,8 +498,23 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     if (!m.rkv) mm.rkv = mm.w;
     if ((rc = launch_moist_scalars(m, mm, stream))) return set_error(rc, "moist scalar launch failed");
     ++launches;
-    if ((rc = cloudphy(dtb, cfg.thresq))) return rc;
   }
+  if (g.openx) {   // the leapfrog scalars' boundary columns (steps.f90:1024-1260)
+    RbcLeapArgs r{};
+    r.g = g;
+    r.cp = rad_d;
+    auto add = [&](int fld, int var, int kind) {
+      r.s[r.n] = lev[fld][N]; r.sp[r.n] = lev[fld][P]; r.sf[r.n] = lev[fld][F];
+      r.var[r.n] = var; r.kind[r.n] = kind;
+      ++r.n;
+    };
+    add(CRESS_PTP, RAD_PT, 0);
+    if (moist)
+      for (int n = 0; n < kMoistN; ++n) add(CRESS_QV + n, RAD_QV + n, n == 0 ? 1 : n < 6 ? 2 : 3);
+    if ((rc = launch_rbc_leapfrog(r, stream))) return set_error(rc, "open-boundary scalar launch failed");
+    ++launches;
+  }
+  if (moist && (rc = cloudphy(dtb, cfg.thresq))) return rc;
   if (filter) {
     FilterArgs t{};
     t.g = g;
@@ -527,6 +557,23 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     }
   if ((rc = launch_halo(h, stream))) return set_error(rc, "halo launch failed");
   ++launches;
+  if (g.openx) {   // s_phasev from the filtered present, past and future levels (intgdrv.f90:1023)
+    PhaseArgs ph{};
+    ph.g = g;
+    ph.cp = rad_d;
+    ph.obc = cfg.wbc;
+    ph.gwave = cfg.gwave;
+    ph.dxiv = 1.f / cfg.dx;
+    ph.dtb = dtb;
+    ph.dts = dts;
+    for (int n = 0; n < nrot; ++n) {
+      ph.s[n] = lev[F5[n]][N]; ph.sp[n] = lev[F5[n]][P]; ph.sf[n] = lev[F5[n]][F];
+      ph.var[n] = n;   // the rotation list is in RadVar order
+    }
+    ph.n = nrot;
+    if ((rc = launch_phase(ph, stream))) return set_error(rc, "phase-speed launch failed");
+    ++launches;
+  }
   // swp2nxt: past <- t, t <- t+dt (pointer rotation)
   for (int n = 0; n < nrot; ++n) {
     float* p = lev[F5[n]][P];
@@ -918,7 +965,7 @@ using namespace cress;
 extern "C" {
 
 const char* cress_last_error(void) { return g_last_error.c_str(); }
-int cress_abi_version(void) { return 2; }
+int cress_abi_version(void) { return 3; }
 
 int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   if (!cfg || !out) return set_error(CRESS_E_ARG, "cress_create: null argument");
@@ -927,8 +974,14 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
     return set_error(CRESS_E_ARG, "cress_create: dims too small (%d,%d,%d)", cfg->ni, cfg->nj, cfg->nk);
   if ((cfg->impopt != 0 && cfg->impopt != 1) || cfg->gwmopt != 0)
     return set_error(CRESS_E_UNSUPPORTED, "only impopt=0 (HE-VE) or 1 (HE-VI), gwmopt=0 run on the GPU");
-  if (!(cfg->wbc == -1 && cfg->ebc == -1 && cfg->sbc == -1 && cfg->nbc == -1))
-    return set_error(CRESS_E_UNSUPPORTED, "only periodic lateral boundaries (-1) run on the GPU");
+  const bool periodic = cfg->wbc == -1 && cfg->ebc == -1 && cfg->sbc == -1 && cfg->nbc == -1;
+  const bool openx = cfg->wbc == cfg->ebc && (cfg->wbc == 4 || cfg->wbc == 5 || cfg->wbc == 7) &&
+                     cfg->sbc == -1 && cfg->nbc == -1;
+  if (!periodic && !openx)
+    return set_error(CRESS_E_UNSUPPORTED,
+                     "lateral boundaries: periodic (-1) on all sides, or open x (wbc = ebc = 4, 5 or 7) with periodic y");
+  if (openx && (cfg->impopt != 1 || cfg->tubopt != 0 || cfg->advopt != 2))
+    return set_error(CRESS_E_UNSUPPORTED, "open x boundaries run with impopt=1, tubopt=0, advopt=2");
   if (cfg->bbc != 2 || cfg->tbc != 2)
     return set_error(CRESS_E_UNSUPPORTED, "only rigid bottom/top (bbc=tbc=2) run on the GPU");
   if (cfg->dx <= 0.f || cfg->dy <= 0.f || cfg->dz <= 0.f)
@@ -939,6 +992,7 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   c->device = device;
   c->cfg = *cfg;
   c->g = make_grid(cfg->ni, cfg->nj, cfg->nk);
+  c->g.openx = openx ? 1 : 0;
   if ((rc = cuda_check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate"))) {
     delete c;
     return rc;
@@ -1012,6 +1066,15 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   }
   c->owned.push_back(c->err_d);
   cudaMemsetAsync(c->err_d, 0, sizeof(int), c->stream);
+  if (openx) {   // phase speeds, zero until the first large step ends (a fresh start)
+    const size_t rb = sizeof(float) * rad_floats(c->g);
+    if ((rc = cuda_check(cudaMalloc(&c->rad_d, rb), "cudaMalloc phase speeds"))) {
+      delete c;
+      return rc;
+    }
+    c->owned.push_back(c->rad_d);
+    cudaMemsetAsync(c->rad_d, 0, rb, c->stream);
+  }
   if (cfg->impopt == 0) {   // HE-VE side buffers (two planes each)
     for (int b = 0; b < 2; ++b) {
       if ((rc = cuda_check(cudaMalloc(&c->wcside[b], sizeof(float) * 2 * c->g.plane), "cudaMalloc wc planes"))) {
@@ -1269,6 +1332,8 @@ int cress_set_learned_micro(cress_ctx* ctx, cress_mlp* mh, int chunk, float resi
   if (!mh) return CRESS_OK;
   Mlp* m = reinterpret_cast<Mlp*>(mh);
   if (c->cfg.cphopt != 3) return set_error(CRESS_E_STATE, "cress_set_learned_micro: context is not cphopt=3");
+  if (c->g.openx)   // the learned kernels cover the interior columns only
+    return set_error(CRESS_E_UNSUPPORTED, "cress_set_learned_micro: open x boundaries run the plain scheme");
   if (m->device != c->device) return set_error(CRESS_E_ARG, "MLP and context live on different devices");
   if (!(resid_tol > 0.f)) return set_error(CRESS_E_ARG, "resid_tol must be positive");
   // chunk 0: the fused kernel over all cells (the fallback list can hold
@@ -1393,8 +1458,9 @@ int cress_ensemble_create(cress_ctx* const* members, int n, cress_ensemble** out
     if (c->device != c0->device) return set_error(CRESS_E_ARG, "ensemble members live on different devices");
     if (!c->base_set || !c->large_set) return set_error(CRESS_E_STATE, "member %d: base state not set", m);
     if (c->cfg.impopt != 1 || c->cfg.divopt != c0->cfg.divopt || (c->cfg.sthopt != 0) != (c0->cfg.sthopt != 0) ||
-        c->cfg.buyopt != c0->cfg.buyopt)
-      return set_error(CRESS_E_UNSUPPORTED, "ensemble members need impopt=1 and the same divopt, sthopt, buyopt");
+        c->cfg.buyopt != c0->cfg.buyopt || c->g.openx)
+      return set_error(CRESS_E_UNSUPPORTED,
+                       "ensemble members need impopt=1, periodic x and the same divopt, sthopt, buyopt");
   }
   cudaSetDevice(c0->device);
   Ensemble* e = new Ensemble;

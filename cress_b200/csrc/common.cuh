@@ -17,6 +17,7 @@ struct Grid {
   int ni, nj, nk;   // reference dims (ni = nx+3, nj = ny+3, nk = nz+3)
   int px, py;       // x pitch (floats) and y extent of one plane
   long long plane;  // px*py
+  int openx;        // 1: open (radiation) west and east boundaries, 0: periodic x
   __host__ __device__ inline long long at(int i, int j, int k) const {
     return (long long)i + (long long)px * ((long long)j + (long long)py * (long long)(k - 1));
   }
@@ -29,8 +30,17 @@ inline Grid make_grid(int ni, int nj, int nk) {
   g.px = ((ni + 2) + 31) / 32 * 32;
   g.py = nj + 2;
   g.plane = (long long)g.px * g.py;
+  g.openx = 0;
   return g;
 }
+
+// Columns of the pointwise large-step work (microphysics, filters,
+// saturation adjustment): the interior, and with open x also the boundary
+// columns i = 1 and ni-1, which the reference's loops over i = 1..ni-1
+// update (with periodic x those are ghosts the wrap refills).
+__host__ __device__ inline int col_lo(const Grid& g) { return g.openx ? 1 : 2; }
+__host__ __device__ inline int col_hi(const Grid& g) { return g.openx ? g.ni - 1 : g.ni - 2; }
+__host__ __device__ inline int ncols(const Grid& g) { return col_hi(g) - col_lo(g) + 1; }
 
 // Staggering of a field for the periodic wrap of SrcOrig/bcycle.f90: which
 // interior index feeds which ghost.  S = scalar/w point, U = x face, V = y face.
@@ -47,8 +57,12 @@ __device__ __forceinline__ void store_periodic(float* __restrict__ f, const Grid
   int xs[2], ys[2];
   int nx = 1, ny = 1;
   xs[0] = i; ys[0] = j;
-  if (i == g.ni - 2) xs[nx++] = 1;
-  else if (stag == STAG_U ? (i == 3) : (i == 2)) xs[nx++] = (stag == STAG_U) ? g.ni : g.ni - 1;
+  if (g.openx) {   // open x: no x ghosts (the radiation boundaries set i = 1, ni-1 / ni)
+  } else if (i == g.ni - 2) {
+    xs[nx++] = 1;
+  } else if (stag == STAG_U ? (i == 3) : (i == 2)) {
+    xs[nx++] = (stag == STAG_U) ? g.ni : g.ni - 1;
+  }
   if (j == g.nj - 2) ys[ny++] = 1;
   else if (stag == STAG_V ? (j == 3) : (j == 2)) ys[ny++] = (stag == STAG_V) ? g.nj : g.nj - 1;
   for (int b = 0; b < ny; ++b)

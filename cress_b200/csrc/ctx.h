@@ -97,7 +97,8 @@ struct Ctx {
   int satadjst(int level, float thresq);
   int tmap(const float* buf, int rows, CUtensorMap* out);
   int check_device_error();
-  void* diag_d = nullptr;   // DiagAcc accumulators (allocated on first use)
+  void* diag_d = nullptr;
+  float* rad_d = nullptr;   // open x: phase speeds (openbc.cuh layout)   // DiagAcc accumulators (allocated on first use)
   int diagnostics(int level, double* out);
   int autotune(int nsstp, float dts, int reps, int* best, float* ms);
   ~Ctx();

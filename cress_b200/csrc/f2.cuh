@@ -43,6 +43,14 @@ __device__ __forceinline__ F2 operator-(F2 a, float s) { return a - f2(s); }
 __device__ __forceinline__ F2 operator-(float s, F2 b) { return f2(s) - b; }
 __device__ __forceinline__ F2 fmax2(F2 a, float s) { return f2(fmaxf(a.v.x, s), fmaxf(a.v.y, s)); }
 
+// Per-point choice: the lanes whose bit is set in mask (bit 0 the first
+// point, bit 1 the second) take a, the others b.  The float overload serves
+// one-point code (bit 0).
+__device__ __forceinline__ F2 sel2(int mask, F2 a, F2 b) {
+  return f2((mask & 1) ? a.v.x : b.v.x, (mask & 2) ? a.v.y : b.v.y);
+}
+__device__ __forceinline__ float sel2(int mask, float a, float b) { return (mask & 1) ? a : b; }
+
 // Two consecutive floats at an 8-byte aligned shared-memory address.
 __device__ __forceinline__ F2 ld2(const float* p) { return F2{*reinterpret_cast<const float2*>(p)}; }
 

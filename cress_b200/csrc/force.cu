@@ -85,10 +85,14 @@ __device__ __forceinline__ F2 gld2(const float* p) { return F2{__ldg(reinterpret
 // pair of columns, level k.  stp[d + 2] is the ring stage of level k + d,
 // rowbase the thread's own row and first column in a box, id the global
 // index of the pair's first point (even), ownB whether the second point is
-// owned too, wb_prev the w group's buoyancy term of the level below.
+// owned too, wb_prev the w group's buoyancy term of the level below,
+// edge the points (bit 0 first, bit 1 second) in an open-x boundary
+// column, where advection and smoothing keep their 2nd-order form
+// (advuvw.f90:340-430, advs.f90:312-350, advp.f90:562-600, smoo4*: the
+// 4th-order loops start at i = 2+iwest).
 template <int G, bool T>
 __device__ __forceinline__ void force_point(const ForceArgs& a, const float* const* stp,
-                                            int rowbase, long long id, int k, bool ownB, F2& wb_prev) {
+                                            int rowbase, long long id, int k, bool ownB, F2& wb_prev, int edge) {
   constexpr int SG = G <= 2 ? 0 : 1;
   using L = FLayout<SG, T>;
   constexpr int BX = kHeviBoxX;
@@ -155,7 +159,7 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
         const int kk = k + dz;
         return C(C_RST8U, kk) * (UP(dx, dy, dz) - C(C_UBR, kk)) * C(D_IJCB8U, kk);
       };
-      f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+      f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A, edge);
     }
     if (a.vspopt >= 1 && a.vsp_u && k >= a.ksp0 - 1) {
       const float r8s = .25f * (C(C_RBCT, k) + C(C_RBCT, k + 1));
@@ -179,7 +183,9 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
       return ((RXV(-1, y, 0) + RXV(0, y, 0)) + (RXV(-1, y + 1, 0) + RXV(0, y + 1, 0))) *
              (Uc(0, y + 1, 0) - Uc(0, y - 1, 0)) * dyv48;
     };
+    const F2 h2 = hadv;
     hadv = fourd3 * hadv + ((t1w(-1) + t1w(1)) + (t2w(-1) + t2w(1)));
+    if (edge) hadv = sel2(edge, h2, hadv);
     f = f + hadv + (t3(0) + t3(1));
     put(a.ufrc, id, f);
   } else if constexpr (G == 1) {
@@ -207,7 +213,7 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
         const int kk = k + dz;
         return C(C_RST8V, kk) * (VP(dx, dy, dz) - C(C_VBR, kk)) * C(D_IJCB8V, kk);
       };
-      f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+      f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A, edge);
     }
     if (a.vspopt >= 1 && a.vsp_v && k >= a.ksp0 - 1) {
       const float r8s = .25f * (C(C_RBCT, k) + C(C_RBCT, k + 1));
@@ -231,7 +237,9 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
     auto t2w = [&](int y) {
       return (RXV(0, y - 1, 0) + RXV(0, y + 1, 0)) * (Vc(0, y + 1, 0) - Vc(0, y - 1, 0)) * dyv24;
     };
+    const F2 h2 = hadv;
     hadv = fourd3 * hadv + ((t1w(-1) + t1w(1)) + (t2w(-1) + t2w(1)));
+    if (edge) hadv = sel2(edge, h2, hadv);
     f = f + hadv + (t3(0) + t3(1));
     put(a.vfrc, id, f);
   } else if constexpr (G == 2) {
@@ -260,7 +268,7 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
         const int kk = k + dz;
         return C(C_RST8W, kk) * WP(dx, dy, dz) * C(C_IJCB8W, kk);
       };
-      f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 1, A);
+      f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 1, A, edge);
     }
     if (a.vspopt >= 1 && a.vsp_w && k >= a.ksp0) f = f - C(C_RBCT, k) * C(C_RST8W, k) * WP(0, 0, 0);
     // buoywb.f90:166-172 (dry), 202-299 (moist), 307-313: the term of
@@ -292,7 +300,9 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
       return ((RXV(0, y, -1) + RXV(0, y, 0)) + (RXV(0, y + 1, -1) + RXV(0, y + 1, 0))) *
              (Wc(0, y + 1, 0) - Wc(0, y - 1, 0)) * dyv48;
     };
+    const F2 h2 = hadv;
     hadv = fourd3 * hadv + ((t1w(-1) + t1w(1)) + (t2w(-1) + t2w(1)));
+    if (edge) hadv = sel2(edge, h2, hadv);
     f = f + hadv + (t3(-1) + t3(0));
     put(a.wfrc, id, f);
   } else {
@@ -307,7 +317,9 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
       F2 sf = (t1(0) + t1(1)) + (t2(0) + t2(1));
       auto t1w = [&](int x) { return (FU(x) + FU(x + 1)) * (Sc(x + 1, 0, 0) - Sc(x - 1, 0, 0)) * dxv24; };
       auto t2w = [&](int y) { return (FV(y) + FV(y + 1)) * (Sc(0, y + 1, 0) - Sc(0, y - 1, 0)) * dyv24; };
+      const F2 s2 = sf;
       sf = fourd3 * sf + ((t1w(-1) + t1w(1)) + (t2w(-1) + t2w(1)));
+      if (edge) sf = sel2(edge, s2, sf);
       return sf + (t3(0) + t3(1));
     };
     if constexpr (G == 3) {
@@ -316,7 +328,7 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
       auto FV = [&](int y) { return C(C_JCB8V, k) * Vc(0, y, 0); };
       auto FW = [&](int z) { return C(C_JCB8W, k + z) * WC(0, 0, z); };
       F2 f = adv(FU, FV, FW);
-      if (smooth) f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, SP);
+      if (smooth) f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, SP, edge);
       if (a.vspopt >= 1 && a.vsp_p && k >= a.ksp0 - 1)
         f = f - .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1)) * C(C_JCB, k) * SP(0, 0, 0);
       put(a.pfrc, id, f);
@@ -328,7 +340,7 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
       F2 f = adv(FU, FV, FW);
       if (smooth) {
         auto A = [&](int dx, int dy, int dz) { return C(C_RBR, k + dz) * SP(dx, dy, dz); };
-        f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+        f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A, edge);
       }
       if constexpr (T) {   // forcept.f90:313-320, 383-393: mixing of the full theta at t-dt
         auto RK = [&](int dx, int dy, int dz) { return X(5, dx, dy, dz); };
@@ -371,6 +383,10 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
   const int i = i0 + 2 * tx, j = j0 + ty;
   const int imaxg = G == 0 ? ni - 1 : ni - 2, jmaxg = G == 1 ? nj - 1 : nj - 2, kmaxg = G == 2 ? nk - 1 : nk - 2;
   const bool ownA = (i <= imaxg) && (j <= jmaxg), ownB = (i + 1 <= imaxg) && (j <= jmaxg);
+  // open x: the points in the columns next to the boundaries (u: i = 2 and
+  // ni-1, the other groups: i = 2 and ni-2)
+  const int elast = G == 0 ? ni - 1 : ni - 2;
+  const int edge = g.openx ? ((i == 2 || i == elast) ? 1 : 0) | ((i + 1 == 2 || i + 1 == elast) ? 2 : 0) : 0;
   const int kmax = SG == 0 ? nk - 1 : nk - 2, lmax = SG == 0 ? nk : nk - 1;
 
   extern __shared__ __align__(1024) float fsmem[];
@@ -421,12 +437,12 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
     }
     if ((ownA || ownB) && !fail && k <= kmaxg) {
       if constexpr (SG == 0) {
-        if (gz == 0) force_point<0, T>(a, stp, rowbase, id, k, ownB, wb_prev);
-        else if (gz == 1) force_point<1, T>(a, stp, rowbase, id, k, ownB, wb_prev);
-        else force_point<2, T>(a, stp, rowbase, id, k, ownB, wb_prev);
+        if (gz == 0) force_point<0, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
+        else if (gz == 1) force_point<1, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
+        else force_point<2, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
       } else {
-        if (gz == 0) force_point<3, T>(a, stp, rowbase, id, k, ownB, wb_prev);
-        else force_point<4, T>(a, stp, rowbase, id, k, ownB, wb_prev);
+        if (gz == 0) force_point<3, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
+        else force_point<4, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
       }
     }
 #pragma unroll

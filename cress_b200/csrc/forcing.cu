@@ -10,16 +10,18 @@ namespace cress {
 namespace {
 
 // s_timeflt, SrcOrig/timeflt.f90:335-404 on the interior (ghosts are
-// refilled by k_halo afterwards).
+// refilled by k_halo afterwards); with open x also on the boundary
+// columns (u: i = 1 and ni, the rest i = 1 and ni-1), which the
+// reference's loops over i = 1..ni-1 (u: 1..ni) include.
 __global__ void __launch_bounds__(256) k_timeflt(const FilterArgs a) {
   const Grid g = a.g;
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = col_lo(g) + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
-  if (i > g.ni - 1 || j > g.nj - 1 || k > g.nk) return;
+  if (i > col_hi(g) + 1 || j > g.nj - 1 || k > g.nk) return;
   const long long id = g.at(i, j, k);
   const float fc = a.filcoe, m1fc2 = 1.f - 2.f * a.filcoe;
-  const bool si = i <= g.ni - 2, sj = j <= g.nj - 2;
+  const bool si = i <= col_hi(g), sj = j <= g.nj - 2;
   if (k <= g.nk - 1) {
     if (sj) a.u[id] = m1fc2 * a.u[id] + fc * (a.uf[id] + a.up[id]);
     if (si) a.v[id] = m1fc2 * a.v[id] + fc * (a.vf[id] + a.vp[id]);
@@ -67,7 +69,8 @@ __global__ void __launch_bounds__(128) k_halo(const HaloArgs a) {
   }
   for (int n = 0; n < a.n; ++n) {
     const int st = a.stag[n];
-    const bool gx = (st == STAG_U) ? (i <= 1 || i >= ni) : (i <= 1 || (i >= ni - 1 && i <= ni));
+    // open x: only the y wrap (over every column, boundary columns included)
+    const bool gx = !g.openx && ((st == STAG_U) ? (i <= 1 || i >= ni) : (i <= 1 || (i >= ni - 1 && i <= ni)));
     const bool gy = (st == STAG_V) ? (j <= 1 || j >= nj) : (j <= 1 || (j >= nj - 1 && j <= nj));
     const bool inx = (st == STAG_U) ? (i <= ni + 1) : (i <= ni);
     const bool iny = (st == STAG_V) ? (j <= nj + 1) : (j <= nj);
@@ -83,7 +86,7 @@ __global__ void __launch_bounds__(128) k_halo(const HaloArgs a) {
 
 int launch_timeflt(const FilterArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni - 2 + 31) / 32, (a.g.nj - 2 + 7) / 8, a.g.nk);
+  dim3 gr((ncols(a.g) + 1 + 31) / 32, (a.g.nj - 2 + 7) / 8, a.g.nk);
   k_timeflt<<<gr, b, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }

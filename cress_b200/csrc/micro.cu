@@ -55,10 +55,10 @@ __device__ __forceinline__ void store_speeds(const MicroArgs& a, long long id, c
 
 __global__ void __launch_bounds__(256, 3) k_micro_src(const MicroArgs a) {
   const Grid g = a.g;
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = col_lo(g) + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
-  const bool in = i <= g.ni - 2 && j <= g.nj - 2 && k <= g.nk - 1;
+  const bool in = i <= col_hi(g) && j <= g.nj - 2 && k <= g.nk - 1;
   float lim = 3.0e38f;
   if (in) {
     const long long id = g.at(i, j, k);
@@ -97,10 +97,10 @@ __global__ void __launch_bounds__(256, 3) k_micro_src(const MicroArgs a) {
 __global__ void __launch_bounds__(128) k_micro_fall(const MicroArgs a) {
   const Grid g = a.g;
   const int nk = g.nk;
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = col_lo(g) + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int f = blockIdx.z;
-  if (i > g.ni - 2 || j > g.nj - 2) return;
+  if (i > col_hi(g) || j > g.nj - 2) return;
   // fallblk.f90:421-449
   const float dtb = a.dtb;
   float dtp = fminf(__int_as_float(*a.dtp_bits), dtb);
@@ -164,10 +164,10 @@ __global__ void __launch_bounds__(128) k_micro_fall(const MicroArgs a) {
 // (flqcqi_opt=1), interior points, k = 1..nk-1.
 __global__ void __launch_bounds__(256) k_adjstni(const MicroArgs a) {
   const Grid g = a.g;
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = col_lo(g) + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
-  if (i > g.ni - 2 || j > g.nj - 2 || k > g.nk - 1) return;
+  if (i > col_hi(g) || j > g.nj - 2 || k > g.nk - 1) return;
   const long long id = g.at(i, j, k);
   const float rb = __ldg(a.col + C_RBR * (g.nk + 1) + k), rbv = 1.f / rb;
   float nci = a.nif[id], ncs = a.nsf[id], ncg = a.ngf[id];
@@ -180,10 +180,10 @@ __global__ void k_init_dtp(int* dtp_bits, float v) { *dtp_bits = __float_as_int(
 // s_satadjst (cphopt=3): siadjst then swadjst on one level.
 __global__ void __launch_bounds__(256) k_satadjst(const SatArgs a) {
   const Grid g = a.g;
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = col_lo(g) + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
-  if (i > g.ni - 2 || j > g.nj - 2 || k > g.nk - 1) return;
+  if (i > col_hi(g) || j > g.nj - 2 || k > g.nk - 1) return;
   const long long id = g.at(i, j, k);
   const int nc = g.nk + 1;
   const float rddvcp = 287.f / 1004.f, p0iv = 1.f / 1.e5f;
@@ -198,10 +198,10 @@ __global__ void __launch_bounds__(256) k_satadjst(const SatArgs a) {
 // t and t+dt (intgdrv.f90:985-998), interior points, k = 1..nk-1.
 __global__ void __launch_bounds__(256) k_moist_post(const MoistPostArgs a) {
   const Grid g = a.g;
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = col_lo(g) + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
-  if (i > g.ni - 2 || j > g.nj - 2 || k > g.nk - 1) return;
+  if (i > col_hi(g) || j > g.nj - 2 || k > g.nk - 1) return;
   const long long id = g.at(i, j, k);
   const int nc = g.nk + 1;
   float c[9];
@@ -261,17 +261,17 @@ int micro_init_tables() {
 // s_fallblk for the eight species, then the final adjstni (two launches).
 static void launch_fall(const MicroArgs& a, cudaStream_t st) {
   dim3 b2(32, 4, 1);
-  dim3 gr2((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 3) / 4, 8);
+  dim3 gr2((ncols(a.g) + 31) / 32, (a.g.nj - 3 + 3) / 4, 8);
   k_micro_fall<<<gr2, b2, 0, st>>>(a);
   dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
+  dim3 gr((ncols(a.g) + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
   k_adjstni<<<gr, b, 0, st>>>(a);
 }
 
 int launch_cloudphy(const MicroArgs& a, cudaStream_t st) {
   k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
   dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
+  dim3 gr((ncols(a.g) + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
   k_micro_src<<<gr, b, 0, st>>>(a);
   launch_fall(a, st);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
@@ -279,14 +279,14 @@ int launch_cloudphy(const MicroArgs& a, cudaStream_t st) {
 
 int launch_moist_post(const MoistPostArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
+  dim3 gr((ncols(a.g) + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
   k_moist_post<<<gr, b, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
 int launch_satadjst(const SatArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);
-  dim3 gr((a.g.ni - 3 + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
+  dim3 gr((ncols(a.g) + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
   k_satadjst<<<gr, b, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }

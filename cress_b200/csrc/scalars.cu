@@ -79,6 +79,8 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   const int tx = threadIdx.x, ty = threadIdx.y, tid = (q * TY + ty) * kScPairs + tx;
   const int i = i0 + 2 * tx, j = j0 + ty;
   const bool ownA = (i <= ni - 2) && (j <= nj - 2), ownB = (i + 1 <= ni - 2) && (j <= nj - 2);
+  // open x: the points in the columns next to the boundaries (i = 2, ni-2)
+  const int edge = g.openx ? ((i == 2 || i == ni - 2) ? 1 : 0) | ((i + 1 == 2 || i + 1 == ni - 2) ? 2 : 0) : 0;
 
   extern __shared__ __align__(1024) float smem[];
   float* ring = smem;
@@ -177,7 +179,9 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       const F2 w1b = (fu_p1 + fu_p2) * (ld2(S0 + 2) - s0) * dxv24;
       const F2 w2a = (fv_m1 + fv_0) * (s0 - ld2(S0 - 2 * BX)) * dyv24;
       const F2 w2b = (fv_p1 + fv_p2) * (ld2(S0 + 2 * BX) - s0) * dyv24;
+      const F2 f2nd = f;
       f = fourd3 * f + ((w1a + w1b) + (w2a + w2b));
+      if (edge) f = sel2(edge, f2nd, f);   // open x: 2nd order in the boundary columns (advs.f90:312-350)
       const F2 t3a = fw_0 * (s0 - ld2(st(-1) + L::oS + oS)) * dzv05n;
       const F2 t3b = fw_1 * (ld2(st(1) + L::oS + oS) - s0) * dzv05n;
       f = f + (t3a + t3b);
@@ -192,7 +196,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
           const F2 v = SPo(dx, dy, dz);
           return isqv ? C(C_RBR, kk) * (v - C(C_QVBR, kk)) : C(C_RBR, kk) * v;
         };
-        f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A);
+        f = smooth_tile(f, a.smtopt, a.smhcoe, a.smvcoe, k, 2, nk - 2, A, edge);
       }
       if constexpr (TURB) {
         auto R = [&](int dx, int dy, int dz) {

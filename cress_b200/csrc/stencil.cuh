@@ -4,6 +4,7 @@
 // the same terms in the same order, whatever memory its neighbours come
 // from and whether it computes one point or a pair (F2).
 #pragma once
+#include "f2.cuh"
 #include "hevi.cuh"
 
 namespace cress {
@@ -16,15 +17,19 @@ namespace cress {
 // second difference at kmin and kmax (tmp3(kmin-1) = tmp3(kmin),
 // tmp3(kmax+1) = tmp3(kmax)); here that is a selection, so every offset is
 // a compile-time constant.
-// T is float, or F2 (f2.cuh) for two points at once.
+// T is float, or F2 (f2.cuh) for two points at once.  edge: the points
+// (bit 0 first, bit 1 second) in an open-x boundary column, where only the
+// 2nd-order part applies (smoo4uvw.f90:286-330 and the other smoo4*: the
+// 4th-order loops run over i = 2+iwest .. with iwest = 1).
 template <class T, class FA>
 __device__ __forceinline__ T smooth_tile(T frc, int smtopt, float smhcoe, float smvcoe, int k, int kmin, int kmax,
-                                         const FA& A) {
+                                         const FA& A, int edge = 0) {
   auto t1 = [&](int x) { return (A(x + 1, 0, 0) + A(x - 1, 0, 0)) - 2.f * A(x, 0, 0); };
   auto t2 = [&](int y) { return (A(0, y + 1, 0) + A(0, y - 1, 0)) - 2.f * A(0, y, 0); };
   auto t3 = [&](int z) { return (A(0, 0, z + 1) + A(0, 0, z - 1)) - 2.f * A(0, 0, z); };
   const T t10 = t1(0), t20 = t2(0), t30 = t3(0);
   frc = frc + smhcoe * (t10 + t20) + smvcoe * t30;
+  const T frc2 = frc;
   if (smtopt % 10 == 2) {
     frc = frc + smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1))));
   } else {
@@ -33,7 +38,7 @@ __device__ __forceinline__ T smooth_tile(T frc, int smtopt, float smhcoe, float 
     frc = frc + (smvcoe * (t30 - (t3p + t3m)) +
                  smhcoe * ((t10 - (t1(1) + t1(-1))) + (t20 - (t2(1) + t2(-1)))));
   }
-  return frc;
+  return edge ? sel2(edge, frc2, frc) : frc;
 }
 
 // Turbulent mixing of a scalar S (the full field at t-dt) at a point of

@@ -49,7 +49,8 @@
         real(c_float) :: smhcoe, smvcoe, filcoe, fc
         character(kind=c_char) :: vspvar(16)
         real(c_float) :: thresq
-        integer(c_int) :: reserved(7)
+        real(c_float) :: gwave
+        integer(c_int) :: reserved(6)
       end type cress_cfg
 
       interface

@@ -49,7 +49,9 @@ typedef struct cress_cfg {
   int buyopt;           /* 1 = buoyancy in the small step (SrcOrig/hevi.f90:377) */
   int gwmopt;           /* 0 only */
   float weicoe;         /* implicit weight beta (SrcOrig/advbspi.f90:140) */
-  int wbc, ebc, sbc, nbc;  /* lateral BCs after chknlslv: -1 = periodic */
+  int wbc, ebc, sbc, nbc;  /* lateral BCs after chknlslv: -1 = periodic on all four sides, or
+                              wbc = ebc = 4, 5 or 7 (open radiation x boundaries: phase speed per
+                              point, its column average, or the constant gwave) with sbc = nbc = -1 */
   int bbc, tbc;         /* 2 = rigid (SrcOrig/vbcw.f90:201) */
   int tile;             /* HE-VI tile shape id (0 = default: 32x8, two rows per thread; 1-11 other shapes) */
   /* large step (SrcOrig/forcedrv.f90:548-608, SrcOrig/timeflt.f90:335) */
@@ -64,7 +66,8 @@ typedef struct cress_cfg {
   float fc;             /* 0.5*omega*sin(lat) (SrcOrig/trilat.f90:118-134) */
   char vspvar[16];      /* sponge switches u v w p pt qv q ... ('o' on / 'x' off) */
   float thresq;         /* mixing-ratio threshold of the microphysics (namelist thresq) */
-  int reserved[7];
+  float gwave;          /* phase speed of the open boundaries, wbc = 7 (namelist gwave, m/s) */
+  int reserved[6];
 } cress_cfg;
 
 typedef struct cress_ctx cress_ctx;

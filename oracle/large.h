@@ -70,6 +70,7 @@ void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw,
   const R dxv25n = R(-.25) * dxiv, dyv25n = R(-.25) * dyiv, dzv25n = R(-.25) * dziv;
   const R dxv24 = oned24 * dxiv, dyv24 = oned24 * dyiv;
   const R dxv48 = R(.5) * dxv24, dyv48 = R(.5) * dyv24;
+  const int iw = o.iw(), ie = o.ie();   // open x: 4th order away from the boundary columns
   // ---- u (advuvw.f90:231-397)
   OMP_FOR for (int k = 2; k <= nk - 2; ++k) {
     for (int j = 2; j <= nj - 2; ++j)
@@ -89,16 +90,16 @@ void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw,
         hadv(i, j, k) = (t1(i - 1, j, k) + t1(i, j, k)) + (t2(i, j, k) + t2(i, j + 1, k));
   OMP_FOR for (int k = 2; k <= nk - 2; ++k) {
     for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 1; i <= ni; ++i)
+      for (int i = 1 + iw; i <= ni - ie; ++i)
         t1(i, j, k) = (rxu(i - 1, j, k) + rxu(i + 1, j, k)) * (u(i + 1, j, k) - u(i - 1, j, k)) * dxv24;
     for (int j = 1; j <= nj - 1; ++j)
-      for (int i = 2; i <= ni - 1; ++i)
+      for (int i = 2 + iw; i <= ni - 1 - ie; ++i)
         t2(i, j, k) = ((rxv(i - 1, j, k) + rxv(i, j, k)) + (rxv(i - 1, j + 1, k) + rxv(i, j + 1, k))) *
                       (u(i, j + 1, k) - u(i, j - 1, k)) * dyv48;
   }
   OMP_FOR for (int k = 2; k <= nk - 2; ++k)
     for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 2; i <= ni - 1; ++i)
+      for (int i = 2 + iw; i <= ni - 1 - ie; ++i)
         hadv(i, j, k) = fourd3 * hadv(i, j, k) +
                         ((t1(i - 1, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j + 1, k)));
   OMP_FOR for (int k = 2; k <= nk - 2; ++k)
@@ -124,16 +125,16 @@ void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw,
         hadv(i, j, k) = (t1(i, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j, k));
   OMP_FOR for (int k = 2; k <= nk - 2; ++k) {
     for (int j = 2; j <= nj - 1; ++j)
-      for (int i = 1; i <= ni - 1; ++i)
+      for (int i = 1 + iw; i <= ni - 1 - ie; ++i)
         t1(i, j, k) = ((rxu(i, j - 1, k) + rxu(i, j, k)) + (rxu(i + 1, j - 1, k) + rxu(i + 1, j, k))) *
                       (v(i + 1, j, k) - v(i - 1, j, k)) * dxv48;
     for (int j = 1; j <= nj; ++j)
-      for (int i = 2; i <= ni - 2; ++i)
+      for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         t2(i, j, k) = (rxv(i, j - 1, k) + rxv(i, j + 1, k)) * (v(i, j + 1, k) - v(i, j - 1, k)) * dyv24;
   }
   OMP_FOR for (int k = 2; k <= nk - 2; ++k)
     for (int j = 2; j <= nj - 1; ++j)
-      for (int i = 2; i <= ni - 2; ++i)
+      for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         hadv(i, j, k) = fourd3 * hadv(i, j, k) +
                         ((t1(i - 1, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j + 1, k)));
   OMP_FOR for (int k = 2; k <= nk - 2; ++k)
@@ -159,17 +160,17 @@ void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw,
         hadv(i, j, k) = (t1(i, j, k) + t1(i + 1, j, k)) + (t2(i, j, k) + t2(i, j + 1, k));
   OMP_FOR for (int k = 2; k <= nk - 1; ++k) {
     for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 1; i <= ni - 1; ++i)
+      for (int i = 1 + iw; i <= ni - 1 - ie; ++i)
         t1(i, j, k) = ((rxu(i, j, k - 1) + rxu(i, j, k)) + (rxu(i + 1, j, k - 1) + rxu(i + 1, j, k))) *
                       (w(i + 1, j, k) - w(i - 1, j, k)) * dxv48;
     for (int j = 1; j <= nj - 1; ++j)
-      for (int i = 2; i <= ni - 2; ++i)
+      for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         t2(i, j, k) = ((rxv(i, j, k - 1) + rxv(i, j, k)) + (rxv(i, j + 1, k - 1) + rxv(i, j + 1, k))) *
                       (w(i, j + 1, k) - w(i, j - 1, k)) * dyv48;
   }
   OMP_FOR for (int k = 2; k <= nk - 1; ++k)
     for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 2; i <= ni - 2; ++i)
+      for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         hadv(i, j, k) = fourd3 * hadv(i, j, k) +
                         ((t1(i - 1, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j + 1, k)));
   OMP_FOR for (int k = 2; k <= nk - 1; ++k)
@@ -189,6 +190,7 @@ void advs(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw, c
   const R oned24 = R(1) / R(24), fourd3 = R(4) / R(3);
   const R dxv05n = R(-.5) * dxiv, dyv05n = R(-.5) * dyiv, dzv05n = R(-.5) * dziv;
   const R dxv24 = oned24 * dxiv, dyv24 = oned24 * dyiv;
+  const int iw = o.iw(), ie = o.ie();   // open x: 4th order away from the boundary columns
   OMP_FOR for (int k = 2; k <= nk - 2; ++k) {
     for (int j = 2; j <= nj - 2; ++j)
       for (int i = 2; i <= ni - 1; ++i) t1(i, j, k) = rxu(i, j, k) * (s(i, j, k) - s(i - 1, j, k)) * dxv05n;
@@ -206,15 +208,15 @@ void advs(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw, c
   F3<R>& vt = t3;
   OMP_FOR for (int k = 2; k <= nk - 2; ++k) {
     for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 1; i <= ni - 1; ++i)
+      for (int i = 1 + iw; i <= ni - 1 - ie; ++i)
         t1(i, j, k) = (rxu(i, j, k) + rxu(i + 1, j, k)) * (s(i + 1, j, k) - s(i - 1, j, k)) * dxv24;
     for (int j = 1; j <= nj - 1; ++j)
-      for (int i = 2; i <= ni - 2; ++i)
+      for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         t2(i, j, k) = (rxv(i, j, k) + rxv(i, j + 1, k)) * (s(i, j + 1, k) - s(i, j - 1, k)) * dyv24;
   }
   OMP_FOR for (int k = 2; k <= nk - 2; ++k)
     for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 2; i <= ni - 2; ++i)
+      for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         sfrc(i, j, k) = fourd3 * sfrc(i, j, k) +
                         ((t1(i - 1, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j + 1, k)));
   OMP_FOR for (int k = 2; k <= nk - 2; ++k)
@@ -234,9 +236,12 @@ void smooth4(const Opts& o, int smtopt, double smhcoe_d, double smvcoe_d, const 
              int ihi, int jlo, int jhi, int klo, int khi, bool wpoint, F3<R>& frc, F3<R>& t1, F3<R>& t2,
              F3<R>& t3) {
   const R smhcoe = R(smhcoe_d), smvcoe = R(smvcoe_d);
+  // open x: the 4th-order increments skip the boundary columns
+  // (smoo4uvw.f90:286-330 etc., i = 2+iwest .. ni-1-ieast)
+  const int i4lo = ilo + o.iw(), i4hi = ihi - o.ie();
   OMP_FOR for (int k = klo; k <= khi; ++k) {
     for (int j = jlo; j <= jhi; ++j)
-      for (int i = ilo - 1; i <= ihi + 1; ++i)
+      for (int i = ilo - 1 + o.iw(); i <= ihi + 1 - o.ie(); ++i)
         t1(i, j, k) = (a(i + 1, j, k) + a(i - 1, j, k)) - R(2) * a(i, j, k);
     for (int j = jlo - 1; j <= jhi + 1; ++j)
       for (int i = ilo; i <= ihi; ++i)
@@ -252,19 +257,19 @@ void smooth4(const Opts& o, int smtopt, double smhcoe_d, double smvcoe_d, const 
   if (smtopt % 10 == 2) {
     OMP_FOR for (int k = klo; k <= khi; ++k)
       for (int j = jlo; j <= jhi; ++j)
-        for (int i = ilo; i <= ihi; ++i)
+        for (int i = i4lo; i <= i4hi; ++i)
           frc(i, j, k) = frc(i, j, k) + smhcoe * ((t1(i, j, k) - (t1(i + 1, j, k) + t1(i - 1, j, k))) +
                                                   (t2(i, j, k) - (t2(i, j + 1, k) + t2(i, j - 1, k))));
   } else {
     for (int j = jlo; j <= jhi; ++j)
-      for (int i = ilo; i <= ihi; ++i) {
+      for (int i = i4lo; i <= i4hi; ++i) {
         t3(i, j, klo - 1) = t3(i, j, klo);
         t3(i, j, khi + 1) = t3(i, j, khi);
       }
     (void)wpoint;
     OMP_FOR for (int k = klo; k <= khi; ++k)
       for (int j = jlo; j <= jhi; ++j)
-        for (int i = ilo; i <= ihi; ++i)
+        for (int i = i4lo; i <= i4hi; ++i)
           frc(i, j, k) = frc(i, j, k) + (smvcoe * (t3(i, j, k) - (t3(i, j, k + 1) + t3(i, j, k - 1))) +
                                          smhcoe * ((t1(i, j, k) - (t1(i + 1, j, k) + t1(i - 1, j, k))) +
                                                    (t2(i, j, k) - (t2(i, j + 1, k) + t2(i, j - 1, k)))));

@@ -225,7 +225,7 @@ void moist_scalar(MoistRun<R>& m, int n, R dtb) {
           m.qfrc(i, j, k) = m.qfrc(i, j, k) - R(.5) * (r.rbct[k] + r.rbct[k + 1]) * r.b.rst(i, j, k) * d;
         }
   }
-  step_scalar(r, dtb, sp, m.qfrc, m.mf.q[n], n < M_NI);
+  step_scalar(r, dtb, sp, m.qfrc, m.mf.q[n], n < M_NI, RV_QV + n, n == M_QV ? 1 : n < M_NI ? 2 : 3, &sc);
 }
 
 // One moist large step (s_intgdrv, SrcOrig/intgdrv.f90:832-1119 with
@@ -253,7 +253,7 @@ void intgdrv_moist(MoistRun<R>& m, R dtb, int nsstp, R dts, bool filter) {
   r.dtb_cur = dtb;
   phase_forcing(r);
   phase_small(r, nsstp, dts);
-  step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false);
+  step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false, RV_PT, 0, &r.c.ptp);
   for (int n = 0; n < M_N; ++n) moist_scalar(m, n, dtb);
   m.npstp = cloudphy_fields(ni, nj, nk, o.dz, m.thresq, dtb, r.b.ptbr, r.b.rbr, r.b.pbr, r.b.jcb, r.b.rst,
                             r.p.ptp, r.p.pp, m.mp, r.f.ptp, m.mf, m.prec);
@@ -271,6 +271,11 @@ void intgdrv_moist(MoistRun<R>& m, R dtb, int nsstp, R dts, bool filter) {
   phase_halo(r);
   for (MoistLevel<R>* M : {&m.mc, &m.mf})
     for (auto& a : M->q) halo_both(o, 's', a);
+  if (o.obc) {   // phasev.f90:506-800 ('big' for qv and the species)
+    phasev_dry(r, dtb, dts);
+    for (int n = 0; n < M_N; ++n)
+      phase_var(o, RV_QV + n, false, ni - 2, nj - 1, nk - 2, dtb, dts, m.mc.q[n], m.mp.q[n], m.mf.q[n], r.rad);
+  }
   std::swap(r.p, r.c);
   std::swap(r.c, r.f);
   std::swap(m.mp, m.mc);

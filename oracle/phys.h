@@ -47,6 +47,15 @@ struct Opts {
   int bbc = 2, tbc = 2;
   int fp64_solve = 0; // solve the w tridiagonal in double (product behaviour)
   int impopt = 1;     // 1 HE-VI (s_hevi), 0 HE-VE (s_heve), smalldrv.f90:370-384
+  // Open (radiation) west and east boundaries: wbc = ebc = obc in {4, 5, 7}
+  // (0: periodic x).  y stays periodic.  The added/subtracted boundary
+  // indices iwest = ieast = 1 then narrow the 4th-order stencils
+  // (sethalo.f90:535-557); gwave is the phase speed of options 5-7.
+  int obc = 0;
+  double gwave = 20.;
+  const void* rad = nullptr;   // the run's phase speeds (openbc.h Radiation<R>)
+  int iw() const { return obc ? 1 : 0; }
+  int ie() const { return obc ? 1 : 0; }
 };
 
 }  // namespace oracle

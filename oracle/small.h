@@ -9,6 +9,7 @@
 #include <cmath>
 #include "arr.h"
 #include "phys.h"
+#include "openbc.h"
 
 // OpenMP over the outermost k (or j) loop when built for the CPU baseline;
 // iterations are independent, so results do not depend on the thread count.
@@ -35,16 +36,19 @@ struct Base {
 };
 
 // s_bcycle, SrcOrig/bcycle.f90:159-225.  Periodic wrap inside one process:
-// x first over j=0..nj+1, then y over i=0..ni+1 (so corners follow x).
+// x first over j=0..nj+1 (only when wbc = ebc = -1), then y over
+// i=0..ni+1 (so corners follow x).
 template <class R>
 void bcycle(const Opts& o, int iwsnd, int iwrcv, int iesnd, int iercv, int jssnd, int jsrcv,
             int jnsnd, int jnrcv, int kmax, F3<R>& v) {
   if (!o.periodic) return;
   const int ni = o.ni, nj = o.nj;
-  OMP_FOR for (int k = 1; k <= kmax; ++k)
-    for (int j = 0; j <= nj + 1; ++j) v(iwrcv, j, k) = v(iesnd, j, k);
-  OMP_FOR for (int k = 1; k <= kmax; ++k)
-    for (int j = 0; j <= nj + 1; ++j) v(iercv, j, k) = v(iwsnd, j, k);
+  if (!o.obc) {
+    OMP_FOR for (int k = 1; k <= kmax; ++k)
+      for (int j = 0; j <= nj + 1; ++j) v(iwrcv, j, k) = v(iesnd, j, k);
+    OMP_FOR for (int k = 1; k <= kmax; ++k)
+      for (int j = 0; j <= nj + 1; ++j) v(iercv, j, k) = v(iwsnd, j, k);
+  }
   OMP_FOR for (int k = 1; k <= kmax; ++k)
     for (int i = 0; i <= ni + 1; ++i) v(i, jsrcv, k) = v(i, jnsnd, k);
   OMP_FOR for (int k = 1; k <= kmax; ++k)
@@ -204,6 +208,8 @@ template <class R>
 void stepuv(const Opts& o, R dts, const Base<R>& b, const F3<R>& ufrc, const F3<R>& vfrc,
             const F3<R>& usml, const F3<R>& vsml, F3<R>& uf, F3<R>& vf) {
   const int ni = o.ni, nj = o.nj, nk = o.nk;
+  rbcu(o, b, uf);   // stepuv.f90:268
+  rbcv(o, b, vf);   // stepuv.f90:276
   OMP_FOR for (int k = 2; k <= nk - 2; ++k) {
     for (int j = 2; j <= nj - 2; ++j)
       for (int i = 2; i <= ni - 1; ++i)
@@ -351,6 +357,7 @@ void stepwi(const Opts& o, int sthopt, R dts, const Base<R>& b, F3<R>& fw, F3<R>
   const R g05 = R(.5) * (R)Phys::g;
   const R sbsqzi = dts * dts * weicoe * weicoe * dziv;
   const R sbsqg5 = R(.5) * (R)Phys::g * dts * dts * weicoe * weicoe;
+  rbc_point(o, RV_W, nk - 1, wf);   // stepwi.f90:296
   OMP_FOR for (int k = 3; k <= nk - 2; ++k)
     for (int j = 2; j <= nj - 2; ++j)
       for (int i = 2; i <= ni - 2; ++i) wf(i, j, k) = wf(i, j, k) + dts * fw(i, j, k) / b.rst8w(i, j, k);
@@ -401,6 +408,7 @@ void stepwi(const Opts& o, int sthopt, R dts, const Base<R>& b, F3<R>& fw, F3<R>
 template <class R>
 void steppi(const Opts& o, R dts, const Base<R>& b, const F3<R>& fp, F3<R>& ppf) {
   const int ni = o.ni, nj = o.nj, nk = o.nk;
+  rbc_point(o, RV_P, nk - 2, ppf);   // steppi.f90:199
   OMP_FOR for (int k = 2; k <= nk - 2; ++k)
     for (int j = 2; j <= nj - 2; ++j)
       for (int i = 2; i <= ni - 2; ++i) ppf(i, j, k) = ppf(i, j, k) + dts * fp(i, j, k) / b.jcb(i, j, k);

@@ -38,6 +38,7 @@ struct DryRun {
   R thresq = R(1.e-12);
   R dtb_cur = R(0);
   TurbWork<R> tw;
+  Radiation<R> rad;      // phase speeds of the open x boundaries (o.obc != 0)
   // scratch
   F3<R> ufrc, vfrc, wfrc, pfrc, ptfrc, wc, rxu, rxv, rxw, t1, t2, t3, t4, t5, jxu, jxv, jxw;
   SmallScratch<R> ss;
@@ -49,6 +50,8 @@ struct DryRun {
       a->resize(ni, nj, nk);
     ss.resize(ni, nj, nk);
     if (lo.tubopt == 1) tw.resize(ni, nj, nk);
+    rad.resize(nj, nk);   // zero until the first s_phasev (a fresh start)
+    o.rad = &rad;
   }
 };
 
@@ -175,9 +178,12 @@ void phase_small(DryRun<R>& r, int nsstp, R dts) {   // s_smalldrv (smalldrv.f90
 }
 
 // s_steps for one scalar (steps.f90:506-590): f = p + frc*2dtb/rst, clipped
-// at zero for mixing ratios, then bcycle (3979) and vbcs (4362).
+// at zero for mixing ratios, the radiation boundaries of an open x domain
+// (steps.f90:1024-1260; var, kind as in rbc_leapfrog, now = the present
+// level), then bcycle (3979) and vbcs (4362).
 template <class R>
-void step_scalar(const DryRun<R>& r, R dtb, const F3<R>& sp, const F3<R>& frc, F3<R>& sf, bool clip) {
+void step_scalar(const DryRun<R>& r, R dtb, const F3<R>& sp, const F3<R>& frc, F3<R>& sf, bool clip,
+                 int var = -1, int kind = 0, const F3<R>* now = nullptr) {
   const Opts& o = r.o;
   const int ni = o.ni, nj = o.nj, nk = o.nk;
   const R dtb2 = R(2) * dtb;
@@ -188,6 +194,7 @@ void step_scalar(const DryRun<R>& r, R dtb, const F3<R>& sp, const F3<R>& frc, F
         const R v = sp(i, j, k) + frc(i, j, k) * dtdrst;
         sf(i, j, k) = clip ? std::max(R(0), v) : v;
       }
+  if (var >= 0 && now) rbc_leapfrog(o, r.b, var, kind, *now, sp, sf);
   bcycle(o, 2, 1, ni - 2, ni - 1, 2, 1, nj - 2, nj - 1, nk, sf);
   vbcs(o, sf);
 }
@@ -220,6 +227,21 @@ void phase_halo(DryRun<R>& r) {   // shift2nd on t and t+dt (intgdrv.f90:1005,10
   }
 }
 
+// s_phasev (intgdrv.f90:1023-1056) for u, v, w, p' ('sml': scaled to the
+// small step) and theta' ('big', gwmopt=0), from the filtered present,
+// the past and the future level (phasev.f90:464-500).
+template <class R>
+void phasev_dry(DryRun<R>& r, R dtb, R dts) {
+  const Opts& o = r.o;
+  if (!o.obc) return;
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  phase_var(o, RV_U, true, ni - 1, nj - 1, nk - 2, dtb, dts, r.c.u, r.p.u, r.f.u, r.rad);
+  phase_var(o, RV_V, true, ni - 2, nj, nk - 2, dtb, dts, r.c.v, r.p.v, r.f.v, r.rad);
+  phase_var(o, RV_W, true, ni - 2, nj - 1, nk - 1, dtb, dts, r.c.w, r.p.w, r.f.w, r.rad);
+  phase_var(o, RV_P, true, ni - 2, nj - 1, nk - 2, dtb, dts, r.c.pp, r.p.pp, r.f.pp, r.rad);
+  phase_var(o, RV_PT, false, ni - 2, nj - 1, nk - 2, dtb, dts, r.c.ptp, r.p.ptp, r.f.ptp, r.rad);
+}
+
 // One dry large step (leapfrog from t-dt to t+dt with dtb, nsstp
 // substeps of dts): forcing, small steps, s_steps for theta', s_timeflt
 // (skipped on the first step, ctime=0: intgdrv.f90:968), shift2nd planes
@@ -229,9 +251,10 @@ void intgdrv_dry(DryRun<R>& r, R dtb, int nsstp, R dts, bool filter) {
   r.dtb_cur = dtb;
   phase_forcing(r);
   phase_small(r, nsstp, dts);
-  step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false);
+  step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false, RV_PT, 0, &r.c.ptp);
   if (filter) phase_timeflt(r);
   phase_halo(r);
+  phasev_dry(r, dtb, dts);
   std::swap(r.p, r.c);   // swp2nxt: past <- t, t <- t+dt
   std::swap(r.c, r.f);
 }

@@ -47,3 +47,26 @@ def test_bad_config_rejected_without_gpu(cress):
     c.ni, c.nj, c.nk = 20, 20, 20
     c.impopt, c.dx, c.dy, c.dz = 2, 1.0, 1.0, 1.0   # pivoting Gauss elimination: not built
     assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 2  # unsupported
+
+
+def test_open_boundary_configs_checked_without_gpu(cress):
+    # Lateral boundaries: periodic everywhere, or open radiation x (4, 5, 7)
+    # with periodic y; other combinations and open x with the Smagorinsky
+    # closure or the explicit small step are rejected before any CUDA call.
+    c = cress.Cfg()
+    c.ni, c.nj, c.nk = 20, 20, 20
+    c.dx, c.dy, c.dz = 1.0, 1.0, 1.0
+    c.impopt, c.advopt, c.bbc, c.tbc = 1, 2, 2, 2
+    c.sbc = c.nbc = -1
+    h = ctypes.c_void_p()
+    for wbc, ebc in ((6, 6), (4, 7), (2, 2), (-1, 4)):
+        c.wbc, c.ebc = wbc, ebc
+        assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 2, (wbc, ebc)
+    c.wbc = c.ebc = 7
+    c.sbc = c.nbc = 4
+    assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 2
+    c.sbc = c.nbc = -1
+    c.tubopt = 1
+    assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 2
+    c.tubopt, c.impopt = 0, 0
+    assert cress.lib().cress_create(ctypes.byref(c), 0, ctypes.byref(h)) == 2
