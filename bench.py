@@ -221,6 +221,58 @@ def learned_leg(args, s, stream, nsstp, cells, plain_ms, barrier, max_over_ranks
             "eval_steps": args.eval_steps, "plain_ms_per_step_timed": plain_ms}
 
 
+def squall_leg(args, rank):
+    """The squall-line configuration at full size: 1024 x 512 x 80, dx =
+    500 m, line thermal +2 K with seeded 0.1 K noise, 20 m/s low-level
+    shear, cold rain, open radiation x boundaries with per-point phase
+    speeds (wbc = ebc = 4), periodic y; dtbig 3 s, dtsml 0.5 s.  Steps
+    replayed from CUDA graphs, CUDA-event time on the library's stream."""
+    import torch
+    import cress_b200
+    from cress_b200 import cases
+    nx, ny, nz, dx, dtbig, dtsml = args.squall_nx, args.squall_ny, 80, 500.0, 3.0, 0.5
+    case = cases.squall_case(nx, ny, nz, dx, seed=21 + rank)
+    ni, nj, nk = case["dims"]
+    rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, 0.6 * case["zph"][nk - 1])
+    s = cress_b200.Solver(ni, nj, nk, dx, dx, case["dz"], sthopt=1, cphopt=3, obc=4, gwave=20.0,
+                          device=torch.cuda.current_device())
+    s.set_base3d(case["base"])
+    s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
+    s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
+    init = list(case["level"]) + [case["moist"][n] for n in MOIST]
+    for n, a in zip(NAMES, init):
+        s.put_field(n, cress_b200.PAST, a)
+        s.put_field(n, cress_b200.NOW, a)
+    del case, init
+    nsstp = nsstp_of(dtbig, dtsml)
+    s.set_graphs(True)
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    s.large_step(0, 0.5 * dtbig, nsstp, 0.5 * dtsml)
+    step = 1
+    for _ in range(13):   # an eager step and a capture per pointer state, then replays
+        s.large_step(round(step * dtbig * 1000), dtbig, nsstp, dtsml)
+        step += 1
+    s.sync()
+    k = args.steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        s.large_step(round(step * dtbig * 1000), dtbig, nsstp, dtsml)
+        step += 1
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    diag = s.diagnostics(cress_b200.NOW, check=True)
+    s.set_stream(0)
+    s.close()
+    cells = nx * ny * nz
+    return {"grid": [nx, ny, nz], "dx_m": dx, "boundaries": "open x (wbc=ebc=4), periodic y",
+            "dtbig_s": dtbig, "nsstp": nsstp, "steps": k, "ms_per_step": ms,
+            "cell_updates_per_s": cells / (ms * 1e-3), "simulated_s_per_s": dtbig / (ms * 1e-3),
+            "max_w_after": diag["max_w"], "timing": "CUDA events on the library stream, graph replay"}
+
+
 def ensemble_leg(args, rank):
     """Batched ensemble: `members` supercell domains of uneven size (nx, ny
     drawn from 96-192, nz = 48, dx = 1 km) with seeded bubble amplitude
@@ -330,6 +382,9 @@ def main():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-squall", action="store_true")
+    ap.add_argument("--squall-nx", type=int, default=1024)
+    ap.add_argument("--squall-ny", type=int, default=512)
     ap.add_argument("--members", type=int, default=32)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--eval-steps", type=int, default=6)
@@ -463,6 +518,7 @@ def main():
     learned = None if args.no_learned else learned_leg(args, s, stream, nsstp, cells, ms / args.steps,
                                                         barrier, max_over_ranks)
     ensemble = None if args.no_ensemble else ensemble_leg(args, rank)
+    squall = None if args.no_squall else squall_leg(args, rank)
 
     # End to end through the public API with host buffers: every step the
     # past and present levels (14 fields each) go host->device from pinned
@@ -521,7 +577,7 @@ def main():
                          "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
-            "cpu_baseline": cpu, "learned": learned, "ensemble": ensemble,
+            "cpu_baseline": cpu, "learned": learned, "ensemble": ensemble, "squall_line": squall,
             "budget": budget, "autotune": tune}))
     if world > 1:
         dist.destroy_process_group()

@@ -342,6 +342,45 @@ def supercell_case(nx, ny, nz, dx, ztop=18000.0, dzmin=100.0, dzmax=500.0, seed=
                 level=level, moist=moist)
 
 
+def squall_case(nx, ny, nz, dx=500.0, ztop=18000.0, dzmin=100.0, dzmax=500.0, seed=0, ptp0=2.0,
+                shear=20.0, zshear=2500.0, xrad=5000.0, zrad=1400.0, zc=1400.0, noise=0.1,
+                x0=0.0):
+    """Squall-line state (cold-rain microphysics, open x, periodic y).
+
+    Base state: the analytic sounding of moist_columns; unidirectional
+    low-level shear, u = shear * min(z / zshear, 1), v = 0.  Perturbation:
+    a line thermal along y of +ptp0 K, cos^2 in x (half width xrad, centred
+    x0 m from mid-domain) and z (half depth zrad at height zc), plus seeded
+    uniform +-noise K inside it.  Moisture: qv at the base value, no
+    hydrometeors.  Same dict layout as supercell_case."""
+    ni, nj, nk = dims(nx, ny, nz)
+    cols = moist_columns(nk, ztop, dzmin, dzmax)
+    base = {n: expand(cols[n], ni, nj, nk) for n in BASE_NAMES + ["pbr", "qvbr"]}
+    zs = cols["zs"]
+    u = shear * np.clip(zs / zshear, 0.0, 1.0)
+    base["ubr"] = expand(u.astype(np.float32), ni, nj, nk)
+    base["vbr"] = expand(np.zeros_like(u, dtype=np.float32), ni, nj, nk)
+    rng = np.random.default_rng(seed)
+    shp = (nk, nj + 2, ni + 2)
+    x = (np.arange(ni + 2, dtype=np.float64) - 0.5 * (ni + 1)) * dx - x0
+    z = zs[1:nk + 1]
+    r = np.sqrt((x[None, :] / xrad) ** 2 + ((z[:, None] - zc) / zrad) ** 2)   # (nk, ni+2)
+    line = np.where(r < 1.0, ptp0 * np.cos(0.5 * np.pi * r) ** 2, 0.0).astype(np.float32)
+    ptp = np.broadcast_to(line[:, None, :], shp).copy()
+    if noise:
+        inside = np.broadcast_to((r < 1.0)[:, None, :], shp)
+        ptp += np.where(inside, rng.uniform(-noise, noise, shp).astype(np.float32), np.float32(0))
+    level = [base["ubr"].copy(), base["vbr"].copy(), np.zeros(shp, np.float32),
+             np.zeros(shp, np.float32), ptp]
+    moist = {n: np.zeros(shp, np.float32) for n in MOIST_NAMES}
+    moist["qv"] = base["qvbr"].copy()
+    stag = ["u", "v", "s", "s", "s"]
+    level = [periodic_fill(np.asarray(a, np.float32), s) for a, s in zip(level, stag)]
+    moist = {n: periodic_fill(np.asarray(a, np.float32), "s") for n, a in moist.items()}
+    return dict(dims=(ni, nj, nk), base=base, cols=cols, zph=cols["zph"], dz=cols["dz"],
+                level=level, moist=moist)
+
+
 def qvs_water(t, p):
     """Saturation mixing ratio over water, Tetens form of SrcOrig/setblk.f90:333,338."""
     esw = 610.78 * np.exp(17.269 * (t - 273.16) / (t - 35.86))
