@@ -1,6 +1,7 @@
 """Large steps replayed from CUDA graphs give bitwise the same state as the
 eager path (same kernels, same arguments), for the dry and the moist step,
-and count the same kernel launches."""
+with periodic and with open radiation x boundaries, and count the same
+kernel launches."""
 import numpy as np
 import pytest
 
@@ -9,14 +10,14 @@ pytestmark = pytest.mark.gpu
 NAMES = ["u", "v", "w", "pp", "ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
 
 
-def make(cress, oracle_lib, graphs, cphopt):
+def make(cress, oracle_lib, graphs, cphopt, obc=0):
     from cress_b200 import cases
     case = cases.supercell_case(36, 28, 20, 1000.0, ztop=7000.0, seed=6, cloud=True,
                                 rad=(5000.0, 5000.0, 1200.0))
     ni, nj, nk = case["dims"]
     zph = case["zph"]
     rbct, ksp0 = oracle_lib.vspdmp(nk, zph, 0.005, 0.6 * zph[nk - 1])
-    s = cress.Solver(ni, nj, nk, 1000.0, 1000.0, case["dz"], sthopt=1, cphopt=cphopt)
+    s = cress.Solver(ni, nj, nk, 1000.0, 1000.0, case["dz"], sthopt=1, cphopt=cphopt, obc=obc)
     s.set_base3d(case["base"])
     s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
     names = NAMES if cphopt else NAMES[:5]
@@ -30,11 +31,11 @@ def make(cress, oracle_lib, graphs, cphopt):
     return s, names
 
 
-@pytest.mark.parametrize("cphopt", [0, 3])
-def test_graph_replay_is_bitwise_identical(cress, oracle_lib, cphopt):
+@pytest.mark.parametrize("cphopt,obc", [(0, 0), (3, 0), (3, 4)])
+def test_graph_replay_is_bitwise_identical(cress, oracle_lib, cphopt, obc):
     out = []
     for graphs in (False, True):
-        s, names = make(cress, oracle_lib, graphs, cphopt)
+        s, names = make(cress, oracle_lib, graphs, cphopt, obc)
         s.large_step(0, 2.5, 10, 0.5)
         for n in range(1, 8):
             s.large_step(n * 5000, 5.0, 10, 1.0)
