@@ -89,6 +89,8 @@ def lib():
     L.cress_satadjst.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]
     L.cress_get_precip.argtypes = [ctypes.c_void_p, _FP]
     L.cress_put_precip.argtypes = [ctypes.c_void_p, _FP]
+    L.cress_get_phase.argtypes = [ctypes.c_void_p, ctypes.c_int, _FP]
+    L.cress_put_phase.argtypes = [ctypes.c_void_p, ctypes.c_int, _FP]
     vp, i, ll, ull, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_float
     L.cress_mlp_param_count.restype = i
     L.cress_mlp_create.argtypes = [i, ull, ctypes.POINTER(vp)]
@@ -279,6 +281,18 @@ class Solver:
     def put_precip(self, a):
         a = np.ascontiguousarray(a, dtype=np.float32)
         _check(lib().cress_put_precip(self._h, fptr(a)))
+
+    def get_phase(self, name):
+        """Open x: phase speeds of one field as ucpx(1:nj,1:nk,1:2), returned
+        in C order with shape (2, nk, nj) (side, k, j)."""
+        nk, nj = self.shape[0], self.shape[1] - 2
+        a = np.empty((2, nk, nj), np.float32)
+        _check(lib().cress_get_phase(self._h, FIELD_ID[name], fptr(a)))
+        return a
+
+    def put_phase(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        _check(lib().cress_put_phase(self._h, FIELD_ID[name], fptr(a)))
 
 
 class Ensemble:

@@ -1309,6 +1309,40 @@ int cress_put_precip(cress_ctx* ctx, const float* host) {
   return cuda_check(cudaStreamSynchronize(c->stream), "precip sync");
 }
 
+// The phase speeds of one variable: device rows (nj+2 floats, j = 0..nj+1)
+// of levels k = 0..nk per side, host ucpx(1:nj,1:nk,1:2).
+static int phase_copy(Ctx* c, int field, float* host, const float* src_host, bool get) {
+  if (!c->rad_d) return set_error(CRESS_E_STATE, "phase speeds: the context has periodic x boundaries");
+  if (field < 0 || field >= CRESS_NFIELD) return set_error(CRESS_E_ARG, "phase speeds: field %d", field);
+  const Grid& g = c->g;
+  const size_t hw = sizeof(float) * (size_t)g.nj, dp = sizeof(float) * (size_t)(g.nj + 2);
+  int rc = CRESS_OK;
+  for (int side = 0; side < 2 && !rc; ++side) {
+    float* dev = c->rad_d + rad_at(g, field, side, 1, 1);
+    const size_t hoff = (size_t)side * g.nj * g.nk;
+    rc = get ? cuda_check(cudaMemcpy2DAsync(host + hoff, hw, dev, dp, hw, (size_t)g.nk, cudaMemcpyDeviceToHost,
+                                            c->stream), "phase copy")
+             : cuda_check(cudaMemcpy2DAsync(dev, dp, src_host + hoff, hw, hw, (size_t)g.nk, cudaMemcpyHostToDevice,
+                                            c->stream), "phase copy");
+  }
+  if (rc) return rc;
+  return cuda_check(cudaStreamSynchronize(c->stream), "phase sync");
+}
+
+int cress_get_phase(cress_ctx* ctx, int field, float* host) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !host) return set_error(CRESS_E_ARG, "cress_get_phase: null argument");
+  cudaSetDevice(c->device);
+  return phase_copy(c, field, host, nullptr, true);
+}
+
+int cress_put_phase(cress_ctx* ctx, int field, const float* host) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !host) return set_error(CRESS_E_ARG, "cress_put_phase: null argument");
+  cudaSetDevice(c->device);
+  return phase_copy(c, field, nullptr, host, false);
+}
+
 int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, float dts) {
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (!c) return set_error(CRESS_E_ARG, "null context");

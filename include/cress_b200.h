@@ -225,6 +225,14 @@ int cress_satadjst(cress_ctx* ctx, int level, float thresq);
 int cress_get_precip(cress_ctx* ctx, float* host);
 int cress_put_precip(cress_ctx* ctx, const float* host);
 
+/* Open x boundaries: the phase speeds of one variable (a cress_field),
+ * host layout of the reference's ucpx(1:nj,1:nk,1:2) (west, east), as
+ * s_phasev left them for the next large step (SrcOrig/phasev.f90; the
+ * restart files carry them, SrcOrig/outrst.f90).  CRESS_E_STATE on a
+ * periodic context. */
+int cress_get_phase(cress_ctx* ctx, int field, float* host);
+int cress_put_phase(cress_ctx* ctx, int field, const float* host);
+
 /* Number of kernel launches the library issued since the context was
  * created (instrumentation for benchmarks). */
 long long cress_launch_count(const cress_ctx* ctx);

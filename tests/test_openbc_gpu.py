@@ -116,3 +116,40 @@ def test_open_x_differs_from_periodic(cress, oracle_lib):
     ni = dims[0]
     d = np.abs(open_[1][0][:, :, 1:ni] - per[1][0][:, :, 1:ni]).max()
     assert d > 1e-3
+
+
+def test_phase_speeds_option7_and_restart_round_trip(cress, oracle_lib):
+    """With wbc = ebc = 7 the phase speeds after a step are the constant
+    gwave*dtb/dx, clipped at 1, scaled by dts/dtb for u, v, w, p' (phvuvw /
+    phvs), float for float; cress_put_phase / cress_get_phase round-trip the
+    reference's ucpx(1:nj,1:nk,1:2) layout."""
+    from cress_b200 import cases
+    case = cases.squall_case(40, 16, 20, 500.0, ztop=8000.0, seed=3)
+    ni, nj, nk = case["dims"]
+    zph = case["zph"]
+    rbct, ksp0 = oracle_lib.vspdmp(nk, zph, 0.005, 0.6 * zph[nk - 1])
+    s = cress.Solver(ni, nj, nk, 500.0, 500.0, case["dz"], sthopt=1, cphopt=3, obc=7, gwave=30.0)
+    s.set_base3d(case["base"])
+    s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
+    s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
+    for n, a in zip(NAMES, list(case["level"]) + [case["moist"][m] for m in NAMES[5:]]):
+        s.put_field(n, cress.PAST, a)
+        s.put_field(n, cress.NOW, a)
+    assert not s.get_phase("u").any()   # zero on a fresh start
+    dtb, dts = np.float32(3.0), np.float32(0.5)
+    s.large_step(0, 1.5, 12, 0.25)
+    s.large_step(3000, float(dtb), 12, float(dts))
+    gw = np.float32(30.0) * dtb * (np.float32(1.0) / np.float32(500.0))
+    west, east = np.maximum(-gw, np.float32(-1.0)), np.minimum(gw, np.float32(1.0))
+    for name, sml, kend in (("u", True, nk - 2), ("w", True, nk - 1), ("pp", True, nk - 2), ("ptp", False, nk - 2),
+                            ("qr", False, nk - 2)):
+        c = s.get_phase(name)   # (side, k-1, j-1)
+        scale = dts / dtb if sml else np.float32(1.0)
+        wv, ev = (west * scale, east * scale) if sml else (west, east)
+        assert np.all(c[0, 1:kend, 0:nj - 1] == wv), name
+        assert np.all(c[1, 1:kend, 0:nj - 1] == ev), name
+    rng = np.random.default_rng(0)
+    x = rng.uniform(-0.3, 0.3, (2, nk, nj)).astype(np.float32)
+    s.put_phase("v", x)
+    assert np.array_equal(s.get_phase("v"), x)
+    s.close()
