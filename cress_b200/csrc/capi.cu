@@ -136,20 +136,38 @@ Ctx::~Ctx() {
   if (own_stream) cudaStreamDestroy(own_stream);
 }
 
+// Host fields are contiguous (pitch ni+2); device fields have pitch px.
+// A strided copy of ~2 KB rows runs far below the link's bandwidth, so a
+// field crosses as one contiguous copy into (or out of) a staging buffer
+// and a kernel moves it between the two pitches.  Stream order keeps the
+// staging buffer's uses apart.
+int Ctx::stage() {
+  if (stage_d) return CRESS_OK;
+  const size_t n = (size_t)(g.ni + 2) * (size_t)(g.nj + 2) * (size_t)g.nk;
+  int rc = cuda_check(cudaMalloc(&stage_d, sizeof(float) * n), "cudaMalloc staging buffer");
+  if (!rc) owned.push_back(stage_d);
+  return rc;
+}
+
 int Ctx::put_host(float* dst, const float* host) {
-  const size_t wbytes = sizeof(float) * (size_t)(g.ni + 2);
-  const size_t rows = (size_t)(g.nj + 2) * (size_t)g.nk;
-  return cuda_check(cudaMemcpy2DAsync(dst, sizeof(float) * g.px, host, wbytes, wbytes, rows,
-                                      cudaMemcpyHostToDevice, stream),
-                    "host->device copy");
+  const long long rows = (long long)(g.nj + 2) * g.nk;
+  const size_t bytes = sizeof(float) * (size_t)(g.ni + 2) * (size_t)rows;
+  int rc;
+  if ((rc = stage())) return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(stage_d, host, bytes, cudaMemcpyHostToDevice, stream), "host->device copy")))
+    return rc;
+  ++launches;
+  return launch_repitch(stage_d, g.ni + 2, dst, g.px, g.ni + 2, rows, stream);
 }
 
 int Ctx::get_host(float* host, const float* src) {
-  const size_t wbytes = sizeof(float) * (size_t)(g.ni + 2);
-  const size_t rows = (size_t)(g.nj + 2) * (size_t)g.nk;
-  return cuda_check(cudaMemcpy2DAsync(host, wbytes, src, sizeof(float) * g.px, wbytes, rows,
-                                      cudaMemcpyDeviceToHost, stream),
-                    "device->host copy");
+  const long long rows = (long long)(g.nj + 2) * g.nk;
+  const size_t bytes = sizeof(float) * (size_t)(g.ni + 2) * (size_t)rows;
+  int rc;
+  if ((rc = stage())) return rc;
+  if ((rc = launch_repitch(src, g.px, stage_d, g.ni + 2, g.ni + 2, rows, stream))) return rc;
+  ++launches;
+  return cuda_check(cudaMemcpyAsync(host, stage_d, bytes, cudaMemcpyDeviceToHost, stream), "device->host copy");
 }
 
 // Coefficients of the w tridiagonal system of s_stepwi for buyopt=0/1

@@ -46,6 +46,8 @@ struct Ctx {
   long long launches = 0;
 
   float* alloc_field();
+  float* stage_d = nullptr;   // one field in host layout (host<->device transfers)
+  int stage();
   int put_host(float* dst, const float* host);
   int get_host(float* host, const float* src);
   int thomas_for(float dts, const ThomasSet** out);

@@ -82,7 +82,25 @@ __global__ void __launch_bounds__(128) k_halo(const HaloArgs a) {
   }
 }
 
+// One thread per element, 4 elements per thread along x; rows in blockIdx.y
+// (grid-strided).
+__global__ void __launch_bounds__(256) k_repitch(const float* __restrict__ src, int sp, float* __restrict__ dst,
+                                                 int dp, int w, long long rows) {
+  for (long long r = blockIdx.y; r < rows; r += gridDim.y) {
+    const float* s = src + r * sp;
+    float* d = dst + r * dp;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < w; x += gridDim.x * blockDim.x) d[x] = __ldg(s + x);
+  }
+}
+
 }  // namespace
+
+int launch_repitch(const float* src, int src_pitch, float* dst, int dst_pitch, int w, long long rows,
+                   cudaStream_t st) {
+  dim3 gr((w + 255) / 256, (unsigned)(rows < 65535 ? rows : 65535), 1);
+  k_repitch<<<gr, 256, 0, st>>>(src, src_pitch, dst, dst_pitch, w, rows);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
 
 int launch_timeflt(const FilterArgs& a, cudaStream_t st) {
   dim3 b(32, 8, 1);

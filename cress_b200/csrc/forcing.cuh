@@ -169,5 +169,9 @@ struct HaloArgs {
   int n;
 };
 int launch_halo(const HaloArgs& a, cudaStream_t st);
+// Copy `rows` rows of `w` floats between pitches (floats): the host
+// layout (pitch ni+2, contiguous) and the device layout (pitch px).
+int launch_repitch(const float* src, int src_pitch, float* dst, int dst_pitch, int w, long long rows,
+                   cudaStream_t st);
 
 }  // namespace cress
