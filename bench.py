@@ -63,16 +63,30 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self._p = None
+        self._t = None
+        self._first = threading.Event()
+
+    def _read(self):
+        for line in self._p.stdout:
+            if line.strip():
+                self.rows.append([x.strip() for x in line.split(",")])
+                self._first.set()
 
     def __enter__(self):
         # one nvidia-smi in its own sampling loop (every 50 ms) for the
-        # whole timed region
+        # whole timed region; its start-up (NVML initialisation) can hold
+        # up CUDA calls for a second or more, so the timed region starts
+        # only once it has delivered its first sample
         try:
             self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                         "--format=csv,noheader,nounits", "-lms", "50"],
                                        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self._p = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+        self._first.wait(timeout=20)
         return self
 
     def __exit__(self, *a):
@@ -80,13 +94,12 @@ class ClockSampler:
             return
         self._p.terminate()
         try:
-            out, _ = self._p.communicate(timeout=10)
+            self._p.wait(timeout=10)
         except Exception:
             self._p.kill()
-            out, _ = self._p.communicate()
-        for line in (out or "").splitlines():
-            if line.strip():
-                self.rows.append([x.strip() for x in line.split(",")])
+            self._p.wait()
+        if self._t is not None:
+            self._t.join(timeout=10)
 
     def summary(self):
         if not self.rows:
