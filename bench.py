@@ -433,8 +433,11 @@ def main():
         cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} supercell domain, one moist large "
                          f"step of the C++ oracle (OpenMP, {threads} threads) per timed step"}
-        print(json.dumps({"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": 0,
+        # n_gpus echoes the launch's N so the line pairs with our arm's; the
+        # work runs on the host cores (cpu_baseline.cores) of rank 0 alone
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": world,
                           "steps": args.steps, "warmup": args.warmup, "impl": "reference",
+                          "hardware": f"host CPU, {threads} threads",
                           "higher_is_better": True, "dtype": "f32", "data": "synthetic",
                           "config": cfg_json, "cpu_baseline": cpu,
                           "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
