@@ -29,7 +29,8 @@ def region(name, ni, nj, nk):
     return m
 
 
-def run_case(cress, oracle_lib, obc, nx=40, ny=24, nz=22, nsteps=5, seed=5, dtbig=5.0, dtsml=1.0, dry=False):
+def run_case(cress, oracle_lib, obc, nx=40, ny=24, nz=22, nsteps=5, seed=5, dtbig=5.0, dtsml=1.0, dry=False,
+             tile=0):
     from cress_b200 import cases
     dx = 1000.0
     case = cases.supercell_case(nx, ny, nz, dx, ztop=8000.0, seed=seed, cloud=not dry,
@@ -51,7 +52,7 @@ def run_case(cress, oracle_lib, obc, nx=40, ny=24, nz=22, nsteps=5, seed=5, dtbi
         oracle_lib.moist_steps(cfg, case["base"], zph, past, now, prec_ref, nsteps, dtbig, dtsml, start=True)
 
     s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, cphopt=0 if dry else 3, thresq=1e-12, obc=obc,
-                     gwave=20.0)
+                     gwave=20.0, tile=tile)
     s.set_base3d(case["base"])
     s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
     if not dry:
@@ -96,9 +97,10 @@ def check(dims, names, ref, got):
         assert float(np.abs(pg - pr).max()) <= 1e-3 * float(np.abs(pr).max()) + 1e-9
 
 
-@pytest.mark.parametrize("obc", [7, 4, 5])
-def test_open_x_moist_steps(cress, oracle_lib, obc):
-    dims, names, ref, got = run_case(cress, oracle_lib, obc)
+@pytest.mark.parametrize("obc,tile", [(7, 0), (4, 0), (5, 0), (4, 11)])
+def test_open_x_moist_steps(cress, oracle_lib, obc, tile):
+    # tile 11: the HE-VI variant with the level table in global memory
+    dims, names, ref, got = run_case(cress, oracle_lib, obc, tile=tile)
     check(dims, names, ref, got)
 
 
@@ -152,4 +154,16 @@ def test_phase_speeds_option7_and_restart_round_trip(cress, oracle_lib):
     x = rng.uniform(-0.3, 0.3, (2, nk, nj)).astype(np.float32)
     s.put_phase("v", x)
     assert np.array_equal(s.get_phase("v"), x)
+    s.close()
+
+
+def test_open_x_rejects_other_tiles(cress):
+    from cress_b200 import cases
+    case = cases.dry_case(40, 30, 20, 1000.0, 300.0, sthopt=1, seed=1)
+    ni, nj, nk = case["dims"]
+    s = cress.Solver(ni, nj, nk, 1000.0, 1000.0, 300.0, sthopt=1, obc=7, tile=3)
+    s.set_base3d(case["base"])
+    with pytest.raises(cress.CressError) as e:
+        s.small_steps(2, 0.5)
+    assert e.value.code == 2 and "tiles 0 and 11" in str(e.value)
     s.close()
