@@ -136,6 +136,22 @@
           real(c_float), intent(out) :: prec(*)
         end function cress_get_precip
 
+        integer(c_int) function cress_get_phase(ctx, field, cpx)       &
+     &    bind(c, name='cress_get_phase')
+          import :: c_int, c_ptr, c_float
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: field
+          real(c_float), intent(out) :: cpx(*)
+        end function cress_get_phase
+
+        integer(c_int) function cress_put_phase(ctx, field, cpx)       &
+     &    bind(c, name='cress_put_phase')
+          import :: c_int, c_ptr, c_float
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: field
+          real(c_float), intent(in) :: cpx(*)
+        end function cress_put_phase
+
         type(c_ptr) function cress_last_error()                         &
      &    bind(c, name='cress_last_error')
           import :: c_ptr
