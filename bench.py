@@ -32,9 +32,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 HEVI_BYTES_PER_CELL = 48  # u,v,w,p' read + write and 4 forcings read, float32
-# DRAM bytes per cell of one k_hevi2 launch from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum = 632.6 MB over 384*384*63 cells at 384x384x64,
-# profiles/hevi_substep_384x384x64.md); the traffic grows with the cells
+# DRAM bytes per cell of one k_hevi2 launch measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum = 632.6 MB over 384*384*63
+# cells of a 384x384x64 domain); the traffic grows with the cells
 HEVI2_TRAFFIC_PER_CELL = 632.6e6 / (384 * 384 * 63)
 METRIC = "cell-updates/s on 1 B200: plain vs learned-microphysics form at stated error"
 MOIST = ["qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
@@ -145,25 +145,33 @@ def nsstp_of(dtbig, dtsml):
     return 20 * int(1.e2 * (dtbig + .001)) // int(1.e3 * (dtsml + .0001))
 
 
-def cpu_moist(args, threads, nx, ny, nsteps):
-    """Oracle (C++ restatement, OpenMP) on a bounded sample: nx x ny x nz,
-    nsteps moist large steps.  Returns (cell-updates/s, seconds)."""
-    import oracle
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    oracle.build()
-    case = make_case(nx, ny, args.nz, args.dx, 3)
-    ni, nj, nk = case["dims"]
-    cfg = dict(ni=ni, nj=nj, nk=nk, dx=args.dx, dy=args.dx, dz=case["dz"], sthopt=1, smtopt=3,
-               vspopt=2, coropt=0, vspbar=VSPBAR, botbar=case["botbar"])
-    init = list(case["level"]) + [case["moist"][n] for n in MOIST]
-    past = [a.copy() for a in init]
-    now = [a.copy() for a in init]
-    prec = np.zeros((5, 2, nj + 2, ni + 2), np.float32)
-    t0 = time.perf_counter()
-    oracle.moist_steps(cfg, case["base"], case["zph"], past, now, prec, nsteps, args.dtbig,
-                       args.dtsml, start=False, omp=True)
-    dt = time.perf_counter() - t0
-    return nx * ny * args.nz * nsteps / dt, dt
+class CpuMoist:
+    """The oracle (C++ restatement, OpenMP on `threads` host threads) on an
+    nx x ny x nz moist supercell domain, built once; step(n) runs n moist
+    large steps and returns the seconds they took."""
+
+    def __init__(self, args, threads, nx, ny):
+        import oracle
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        oracle.build()
+        self.oracle = oracle
+        self.args = args
+        self.cells = nx * ny * args.nz
+        case = make_case(nx, ny, args.nz, args.dx, 3)
+        ni, nj, nk = case["dims"]
+        self.cfg = dict(ni=ni, nj=nj, nk=nk, dx=args.dx, dy=args.dx, dz=case["dz"], sthopt=1, smtopt=3,
+                        vspopt=2, coropt=0, vspbar=VSPBAR, botbar=case["botbar"])
+        init = list(case["level"]) + [case["moist"][n] for n in MOIST]
+        self.past = [a.copy() for a in init]
+        self.now = [a.copy() for a in init]
+        self.base, self.zph = case["base"], case["zph"]
+        self.prec = np.zeros((5, 2, nj + 2, ni + 2), np.float32)
+
+    def step(self, n=1):
+        t0 = time.perf_counter()
+        self.oracle.moist_steps(self.cfg, self.base, self.zph, self.past, self.now, self.prec, n,
+                                self.args.dtbig, self.args.dtsml, start=False, omp=True)
+        return time.perf_counter() - t0
 
 
 def learned_leg(args, s, stream, nsstp, cells, plain_ms, barrier, max_over_ranks):
@@ -388,9 +396,8 @@ def main():
                     help="small step: 1 HE-VI (the configuration's), 0 HE-VE (needs --dtsml short enough)")
     ap.add_argument("--tile", type=int, default=-1,
                     help="HE-VI tile shape; -1 (default): chosen by the autotuner on the live state")
-    ap.add_argument("--cpu-nx", type=int, default=256)
-    ap.add_argument("--cpu-ny", type=int, default=256)
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=2,
+                    help="moist large steps of the oracle timed for cpu_baseline (same domain)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
@@ -404,10 +411,15 @@ def main():
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "ours":
+        # one process per GPU: start the ranks (torchrun on this node)
+        from cress_b200.replicas import relaunch_under_torchrun
+        sys.exit(relaunch_under_torchrun(args.gpus, os.path.abspath(__file__), sys.argv[1:]))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     nsstp = nsstp_of(args.dtbig, args.dtsml)
+    # the workload: identical in both arms' lines
     cfg_json = {"workload": f"moist supercell large step (cold-rain bulk cphopt=3; forcing + "
                             f"{nsstp} HE-VI substeps + 10 scalar steps + cloud physics + Asselin "
                             f"filter + saturation adjustment + periodic halos), "
@@ -416,43 +428,43 @@ def main():
                             f"sounding, quarter-circle hodograph, +3 K bubble, seeded cloud field",
                 "nx": args.nx, "ny": args.ny, "nz": args.nz, "nsstp": nsstp,
                 "microphysics": "plain (cold-rain bulk)",
-                "launch": "CUDA-graph replay per large step" if not args.no_graphs else "eager launches",
                 "l2": "inputs larger than L2 (each field 72 MB at 512x512x64)",
-                "parallelism": f"replicas{world}"}
+                "parallelism": f"replicas{max(world, args.gpus)}"}
     cells = args.nx * args.ny * args.nz
 
     if args.impl == "reference":
+        # the reference's CPU path (the oracle port) on the same domain, one
+        # moist large step per timed step, on rank 0's host cores
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        vals = []
-        for _ in range(args.warmup + args.steps):
-            v, _dt = cpu_moist(args, threads, args.cpu_nx, args.cpu_ny, 1)
-            vals.append(v)
-        v = float(np.median(vals[args.warmup:]))
+        cpu_run = CpuMoist(args, threads, args.nx, args.ny)
+        secs = [cpu_run.step(1) for _ in range(args.warmup + args.steps)]
+        t = float(np.median(secs[args.warmup:]))
+        v = cells / t
         cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} supercell domain, one moist large "
-                         f"step of the C++ oracle (OpenMP, {threads} threads) per timed step"}
+               "sample": f"{args.nx}x{args.ny}x{args.nz} supercell domain (the workload itself), one moist "
+                         f"large step of the C++ oracle (OpenMP, {threads} threads) per timed step, "
+                         f"median of {args.steps} after {args.warmup} warm-up steps"}
         # n_gpus echoes the launch's N so the line pairs with our arm's; the
         # work runs on the host cores (cpu_baseline.cores) of rank 0 alone
-        print(json.dumps({"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": world,
-                          "steps": args.steps, "warmup": args.warmup, "impl": "reference",
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "cell-updates/s",
+                          "n_gpus": max(world, args.gpus), "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": t * 1e3, "impl": "reference",
                           "hardware": f"host CPU, {threads} threads",
-                          "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+                          "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
                           "config": cfg_json, "cpu_baseline": cpu,
                           "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}))
         return
 
     import torch
-    import torch.distributed as dist
     import cress_b200
     from cress_b200 import cases
+    from cress_b200.replicas import CudaEventTimer, Replicas, timed_steps
 
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rep = Replicas("nccl")
     case = make_case(args.nx, args.ny, args.nz, args.dx, 100 + rank)
     ni, nj, nk = case["dims"]
     rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, case["botbar"])
@@ -471,24 +483,18 @@ def main():
     s.sync()
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        torch.cuda.synchronize()
+        rep.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = rep.max
 
     s.large_step(0, 0.5 * args.dtbig, nsstp, 0.5 * args.dtsml)   # the first (half) step, ctime=0
     tune = None
     if args.tile < 0 and args.impopt == 1:
         best, tms = s.autotune(nsstp=nsstp, dts=args.dtsml, reps=2)
         tune = {"tile": best, "ms_per_substep": [round(t, 4) for t in tms]}
-    cfg_json["hevi_tile"] = tune["tile"] if tune else max(args.tile, 0)
-    cfg_json["small_step"] = "HE-VI (impopt=1)" if args.impopt == 1 else "HE-VE (impopt=0)"
+    hevi_tile = tune["tile"] if tune else max(args.tile, 0)
     if not args.no_graphs:
         # capture the CUDA graphs of the time-level rotation's 6 pointer
         # states (an eager step and a capture each) before the warm-up
@@ -500,13 +506,9 @@ def main():
     barrier()
     d0 = s.diagnostics(cress_b200.NOW)
     l0 = s.launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
-        e1.record(stream)
-        barrier()
+    clk = ClockSampler(local)
+    secs = timed_steps(rep, lambda: s.large_step(CTIME, args.dtbig, nsstp, args.dtsml), args.steps, 0,
+                       CudaEventTimer(stream), sync=torch.cuda.synchronize, inside=clk)
     launches = s.launch_count() - l0
     d1 = s.diagnostics(cress_b200.NOW)
     budget = {"water_kg": [d0["water"], d1["water"]], "precip_kg": [d0["precip"], d1["precip"]],
@@ -514,8 +516,8 @@ def main():
               "water_drift_rel": ((d1["water"] + d1["precip"]) - (d0["water"] + d0["precip"])) / d0["water"],
               "mass_drift_rel": (d1["mass"] - d0["mass"]) / d0["mass"], "max_w": d1["max_w"],
               "nonfinite": int(d1["nonfinite"]), "over": f"{args.steps} timed steps (FP64 sums on the device)"}
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    value = world * cells * args.steps / (ms * 1e-3)
+    ms = secs * 1e3
+    value = world * cells * args.steps / secs
 
     # Dominant kernel (HE-VI substep): timed alone on the same state.
     h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -569,11 +571,13 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, dt = cpu_moist(args, threads, args.cpu_nx, args.cpu_ny, args.cpu_steps)
-        cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_nx}x{args.cpu_ny}x{args.nz} supercell domain, {args.cpu_steps} "
-                         f"moist large steps of the C++ oracle (OpenMP, {threads} threads), "
-                         f"{dt:.2f} s"}
+        cpu_run = CpuMoist(args, threads, args.nx, args.ny)
+        dt = cpu_run.step(args.cpu_steps)
+        cpu = {"value": cells * args.cpu_steps / dt, "unit": "cell-updates/s", "cores": threads,
+               "kind": "port",
+               "sample": f"{args.nx}x{args.ny}x{args.nz} supercell domain (the workload's), {args.cpu_steps} "
+                         f"moist large steps of the C++ oracle (OpenMP, {threads} threads), {dt:.2f} s"}
+        del cpu_run
 
     if rank == 0:
         print(json.dumps({
@@ -581,22 +585,24 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": cfg_json,
+            "launch": "CUDA-graph replay per large step" if not args.no_graphs else "eager launches",
+            "small_step": "HE-VI (impopt=1)" if args.impopt == 1 else "HE-VE (impopt=0)",
+            "hevi_tile": hevi_tile,
             "sim_s_per_wall_s": args.dtbig / (ms / args.steps * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": (HEVI2_TRAFFIC_PER_CELL * cells
-                                     if cfg_json["hevi_tile"] == 0 and args.impopt == 1 else None),
+                                     if hevi_tile == 0 and args.impopt == 1 else None),
                          "traffic_source": "ncu dram bytes per cell at 384x384x64 scaled to this grid",
                          "peak_source": peak_kind,
                          "kernel": ("k_heve" if args.impopt == 0 else
-                                    "k_hevi2" if cfg_json["hevi_tile"] == 0 else "k_hevi_substep"),
+                                    "k_hevi2" if hevi_tile == 0 else "k_hevi_substep"),
                          "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
             "cpu_baseline": cpu, "learned": learned, "ensemble": ensemble, "squall_line": squall,
             "budget": budget, "autotune": tune}))
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":

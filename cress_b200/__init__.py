@@ -118,6 +118,7 @@ def lib():
     L.cress_ensemble_large_step.argtypes = [vp, ll, f, i, f]
     L.cress_ensemble_set_graphs.argtypes = [vp, i]
     L.cress_autotune.argtypes = [vp, i, f, i, ctypes.POINTER(i), ctypes.POINTER(f)]
+    L.cress_set_spin_limit.argtypes = [vp, i]
     _lib = L
     return L
 
@@ -173,6 +174,11 @@ class Solver:
 
     def sync(self):
         _check(lib().cress_sync(self._h))
+
+    def set_spin_limit(self, probes):
+        """Failure-path test hook: probes per HE-VI ring wait before it gives
+        up (0: at once; negative: the default)."""
+        _check(lib().cress_set_spin_limit(self._h, int(probes)))
 
     def set_base3d(self, base):
         arrs = [np.ascontiguousarray(base[n], dtype=np.float32) for n in BASE_NAMES]

@@ -19,6 +19,7 @@
 #include "openbc.cuh"
 #include "micro.cuh"
 #include "mlp_impl.cuh"
+#include "wsystem.h"
 
 namespace cress {
 
@@ -38,9 +39,6 @@ int cuda_check(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return CRESS_OK;
   return set_error(CRESS_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
-
-// Physical constants used on the host side (SrcOrig/comphy.f90:49,459).
-static const float kG = 9.8f, kDivndc = 0.05f;
 
 float* Ctx::alloc_field() {
   float* p = nullptr;
@@ -170,58 +168,19 @@ int Ctx::get_host(float* host, const float* src) {
   return cuda_check(cudaMemcpyAsync(host, stage_d, bytes, cudaMemcpyDeviceToHost, stream), "device->host copy");
 }
 
-// Coefficients of the w tridiagonal system of s_stepwi for buyopt=0/1
-// (SrcOrig/stepwi.f90:308-416), formed in float exactly as the reference
-// does for a horizontally uniform base state, followed by the
-// elimination factors of s_gaussel impopt=1 (SrcOrig/gaussel.f90:189-240)
-// in double.  They depend on dts only through sbsqzi/sbsqg5.
+// Elimination factors of the w system for one dts (w_system_factors,
+// wsystem.h: s_stepwi's coefficients and s_gaussel's factors), uploaded
+// once per distinct dts.
 int Ctx::thomas_for(float dts, const ThomasSet** out) {
   uint32_t key;
   std::memcpy(&key, &dts, 4);
   auto it = thomas.find(key);
   if (it != thomas.end()) { *out = &it->second; return CRESS_OK; }
   const int nk = g.nk;
-  auto C = [&](int f, int k) { return col_h[(size_t)f * (nk + 1) + k]; };
-  const float dziv = 1.f / cfg.dz, weicoe = cfg.weicoe;
-  const float g05 = .5f * kG;
-  const float sbsqzi = dts * dts * weicoe * weicoe * dziv;
-  const float sbsqg5 = .5f * kG * dts * dts * weicoe * weicoe;
-  std::vector<float> fwc(nk + 2, 0.f), wcc(nk + 2, 0.f), rr(nk + 2, 0.f), ss(nk + 2, 0.f),
-      tt(nk + 2, 0.f);
-  for (int k = 2; k <= nk - 2; ++k) {
-    float t1 = g05 * C(C_RBR, k) / C(C_RCSQ, k);
-    float t2 = dziv / C(C_JCB, k);
-    fwc[k] = t1 + t2;
-    wcc[k] = t1 - t2;
-  }
-  for (int k = 3; k <= nk - 2; ++k) {
-    if (cfg.buyopt == 0) {
-      float a = sbsqzi / C(C_RST8W, k);
-      float mm = a * C(C_RCSQ, k - 1);
-      float nn = a * C(C_RCSQ, k);
-      rr[k] = -mm * fwc[k - 1];
-      ss[k] = 1.f + (nn * fwc[k] - mm * wcc[k - 1]);
-      tt[k] = nn * wcc[k];
-    } else {
-      float rstiv = 1.f / C(C_RST8W, k);
-      float a = rstiv * sbsqzi;
-      float b = rstiv * sbsqg5;
-      float mm = b * C(C_RST, k - 1) - a * C(C_RCSQ, k - 1);
-      float nn = b * C(C_RST, k) + a * C(C_RCSQ, k);
-      rr[k] = mm * fwc[k - 1];
-      ss[k] = 1.f + (mm * wcc[k - 1] + nn * fwc[k]);
-      tt[k] = nn * wcc[k];
-    }
-  }
-  const int ks = 3, ke = nk - 2;
-  std::vector<double> cp(nk + 2, 0.0), aa(nk + 2, 0.0);
-  aa[ks] = 1.0 / (double)ss[ks];
-  cp[ks] = (double)tt[ks] * aa[ks];
-  for (int k = ks + 1; k <= ke - 1; ++k) {
-    aa[k] = 1.0 / ((double)ss[k] - (double)rr[k] * cp[k - 1]);
-    cp[k] = (double)tt[k] * aa[k];
-  }
-  aa[ke] = 1.0 / ((double)ss[ke] - (double)rr[ke] * cp[ke - 1]);
+  std::vector<float> rr(nk + 2), work(4 * (nk + 2));
+  std::vector<double> cp(nk + 2), aa(nk + 2);
+  w_system_factors(col_h.data(), nk, cfg.dz, cfg.weicoe, cfg.buyopt, dts, rr.data(), aa.data(), cp.data(),
+                   work.data());
   ThomasSet t;
   if (cudaMalloc(&t.rr, sizeof(float) * (nk + 2)) != cudaSuccess ||
       cudaMalloc(&t.aa, sizeof(double) * (nk + 2)) != cudaSuccess ||
@@ -341,6 +300,7 @@ int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
   a.g05 = .5f * kG;
   a.g05n = -.5f * kG;
   a.divopt = cfg.divopt; a.buyopt = cfg.buyopt; a.sthopt = cfg.sthopt; a.bbc = cfg.bbc;
+  a.spin = spin_limit;
   const int TY = hevi_tile_rows(heve ? 0 : cfg.tile);
   HeviMaps maps;
   if ((rc = tmap(lev[CRESS_U][CRESS_FORCING], TY, &maps.uf)) ||
@@ -1117,6 +1077,14 @@ int cress_set_stream(cress_ctx* ctx, void* stream) {
   return CRESS_OK;
 }
 
+int cress_set_spin_limit(cress_ctx* ctx, int probes) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  c->spin_limit = probes < 0 ? kSpinLimit : (uint32_t)probes;
+  c->free_graphs();   // captured steps carry the old limit
+  return CRESS_OK;
+}
+
 int cress_sync(cress_ctx* ctx) {
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (!c) return set_error(CRESS_E_ARG, "null context");
@@ -1132,38 +1100,12 @@ int cress_set_base3d(cress_ctx* ctx, const float* const* b3) {
     if (!b3[n]) return set_error(CRESS_E_ARG, "cress_set_base3d: array %d is null", n);
   cudaSetDevice(c->device);
   const int ni = c->cfg.ni, nj = c->cfg.nj, nk = c->cfg.nk;
-  auto at = [&](const float* a, int i, int j, int k) {
-    return a[(size_t)i + (size_t)(ni + 2) * ((size_t)j + (size_t)(nj + 2) * (size_t)(k - 1))];
-  };
-  // Map from the C-ABI list to the kernels' column ids.
-  const int map[CRESS_B_N] = {C_JCB, C_JCB8U, C_JCB8V, C_JCB8W, C_RBR, C_PTBR,
-                              C_RST, C_RST8U, C_RST8V, C_RST8W, C_RCSQ};
   // The columns are taken at the domain centre; every point the small step
   // reads (i in 1..ni, j in 1..nj) must carry the same value.
-  const int ic = ni / 2, jc = nj / 2;
-  for (int n = 0; n < CRESS_B_N; ++n) {
-    const float* a = b3[n];
-    for (int k = 1; k <= nk; ++k) {
-      const float v = at(a, ic, jc, k);
-      c->col_h[(size_t)map[n] * (nk + 1) + k] = v;
-      for (int j = 1; j <= nj; ++j)
-        for (int i = 1; i <= ni; ++i) {
-          const float x = at(a, i, j, k);
-          if (x != v && !(std::isnan(x) && std::isnan(v)))
-            return set_error(CRESS_E_NONUNIFORM,
-                             "base array %d varies horizontally at (%d,%d,%d): %g vs %g", n, i, j, k,
-                             (double)x, (double)v);
-        }
-    }
-  }
-  // Reciprocals of the per-level divisors (the kernels multiply by them).
-  const int inv_src[6] = {C_RST8U, C_RST8V, C_JCB, C_RCSQ, C_RST8W, C_JCB8W};
-  const int inv_dst[6] = {C_IRST8U, C_IRST8V, C_IJCB, C_IRCSQ, C_IRST8W, C_IJCB8W};
-  for (int n = 0; n < 6; ++n)
-    for (int k = 1; k <= nk; ++k) {
-      const float v = c->col_h[(size_t)inv_src[n] * (nk + 1) + k];
-      c->col_h[(size_t)inv_dst[n] * (nk + 1) + k] = (v != 0.f) ? 1.f / v : 0.f;
-    }
+  const NonUniform bad = base_columns(b3, ni, nj, nk, c->col_h.data());
+  if (bad.n >= 0)
+    return set_error(CRESS_E_NONUNIFORM, "base array %d varies horizontally at (%d,%d,%d): %g vs %g", bad.n,
+                     bad.i, bad.j, bad.k, (double)bad.x, (double)bad.v);
   int rc = cuda_check(cudaMemcpyAsync(c->col_d, c->col_h.data(), sizeof(float) * c->col_h.size(),
                                       cudaMemcpyHostToDevice, c->stream),
                       "copy base columns");

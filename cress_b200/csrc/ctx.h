@@ -100,7 +100,8 @@ struct Ctx {
   int tmap(const float* buf, int rows, CUtensorMap* out);
   int check_device_error();
   void* diag_d = nullptr;
-  float* rad_d = nullptr;   // open x: phase speeds (openbc.cuh layout)   // DiagAcc accumulators (allocated on first use)
+  float* rad_d = nullptr;   // open x: phase speeds (openbc.cuh layout)
+  uint32_t spin_limit = kSpinLimit;   // probes per HE-VI ring wait (cress_set_spin_limit)
   int diagnostics(int level, double* out);
   int autotune(int nsstp, float dts, int reps, int* best, float* ms);
   ~Ctx();

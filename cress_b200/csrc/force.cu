@@ -399,7 +399,9 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
   __syncthreads();
 
   // Levels 1..lmax are staged; level lv lives in slot (lv-1) % S.
+  int issued = 0;   // highest level thread 0 has issued
   auto issue = [&](int lv) {
+    issued = lv;
     const int s = (lv - 1) % S;
     float* st = ring + s * L::stage;
     uint64_t* bar = &bars[s];
@@ -431,7 +433,7 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
     // Every thread has finished level k-1, so the slot of level k-3 (last
     // read as k'-2 at k' = k-1) may be refilled with level k+S-3.
     __syncthreads();
-    if (tid == 0 && k >= 4 && k + S - 3 <= lmax) {
+    if (tid == 0 && !fail && k >= 4 && k + S - 3 <= lmax) {   // refill only after its copy was seen to land
       fence_proxy_async_smem();
       issue(k + S - 3);
     }
@@ -457,7 +459,7 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
       if (a.err) atomicExch(a.err, 1);
       for (int s = 0; s < S; ++s) {
         int kl = -1;
-        for (int lv = 1; lv <= lmax; ++lv)
+        for (int lv = 1; lv <= issued; ++lv)
           if ((lv - 1) % S == s) kl = lv;
         if (kl >= 0) mbar_wait(&bars[s], ((kl - 1) / S) & 1);
       }

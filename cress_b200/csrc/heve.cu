@@ -91,7 +91,9 @@ k_heve(const __grid_constant__ HeviMaps m, const HeviArgs a) {
 
   // Levels 1..nk-1 are staged; level lv lives in slot (lv-1) % S.
   const int lmax = nk - 1;
+  int issued = 0;   // highest level thread 0 has issued
   auto issue = [&](int lv) {
+    issued = lv;
     const int s = (lv - 1) % S;
     float* st = ring + s * L::stage;
     uint64_t* bar = &bars[s];
@@ -209,7 +211,7 @@ k_heve(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     // Every thread has finished level k-1 and written this level's t3h,
     // so the slot of level k-1 may be refilled with level k+S-1.
     __syncthreads();
-    if (tid == 0 && k >= 2 && k + S - 1 <= lmax) {
+    if (tid == 0 && !fail && k >= 2 && k + S - 1 <= lmax) {   // refill only after its copy was seen to land
       fence_proxy_async_smem();
       issue(k + S - 1);
     }
@@ -305,7 +307,7 @@ k_heve(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       atomicExch(a.err, 1);
       for (int s = 0; s < S; ++s) {
         int kl = -1;
-        for (int lv = 1; lv <= lmax; ++lv)
+        for (int lv = 1; lv <= issued; ++lv)
           if ((lv - 1) % S == s) kl = lv;
         if (kl >= 0) mbar_wait(&bars[s], ((kl - 1) / S) & 1);
       }

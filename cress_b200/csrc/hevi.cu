@@ -118,7 +118,9 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
 
   // Levels 2..nk-1 are staged (w is needed one level above the top update).
   const int klast = nk - 1;
+  int issued = 1;   // highest level thread 0 has issued
   auto issue = [&](int k) {
+    issued = k;
     const int s = (k - 2) % S;
     float* st = ring + s * L::stage;
     uint64_t* bar = &bars[s];
@@ -202,7 +204,7 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
       t3h[hy * BX + hx] = t3h_of(div3d_at(hx, hy), P[hy * BX + hx]);
     }
     __syncthreads();
-    if (tid == 0 && k + S - 1 <= klast) {
+    if (tid == 0 && !fail && k + S - 1 <= klast) {   // refill only after its copy was seen to land
       fence_proxy_async_smem();
       issue(k + S - 1);
     }
@@ -271,10 +273,9 @@ k_hevi_substep(const __grid_constant__ HeviMaps m, const HeviArgs a) {
     // land (bounded again) so no TMA write outlives the block, and leave.
     if (tid == 0) {
       atomicExch(a.err, 1);
-      const int kmax = min(nk - 2 + S - 1, klast);
       for (int s = 0; s < S; ++s) {
         int kl = -1;
-        for (int k = 2; k <= kmax; ++k)
+        for (int k = 2; k <= issued; ++k)
           if ((k - 2) % S == s) kl = k;
         if (kl >= 0) mbar_wait(&bars[s], ((kl - 2) / S) & 1);
       }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "status.h"
+#include "tma.cuh"
 
 namespace cress {
 
@@ -57,6 +58,9 @@ struct HeviArgs {
   int wc_from_w;
   float dts, dxiv, dyiv, dziv, divch, divcv, weicoe, dtdzw, dtw, g05, g05n;
   int divopt, buyopt, sthopt, bbc;
+  // probes of each ring wait of the k_hevi2 level loop before it gives up
+  // (a test of the failure path sets it to 0; the drain keeps kSpinLimit)
+  uint32_t spin = kSpinLimit;
 };
 
 // Tile heights the kernel is instantiated for.

@@ -125,8 +125,11 @@ __device__ __forceinline__ void hevi2_tile(const HeviMaps& m, const HeviArgs& a,
   __syncthreads();
 
   // Levels 2..nk-1 are staged (w is needed one level above the top update).
+  // Thread 0 issues them in order; `issued` is the highest level issued.
   const int klast = nk - 1;
+  int issued = 1;
   auto issue = [&](int k) {
+    issued = k;
     const int s = (k - 2) % S;
     float* st = ring + s * L::stage;
     uint64_t* bar = &bars[s];
@@ -174,8 +177,8 @@ __device__ __forceinline__ void hevi2_tile(const HeviMaps& m, const HeviArgs& a,
     // stage of level k-1 is refilled only after this level's barrier.
     float* t3h = t3hb + (k & 1) * L::t3h_floats;
     const int s0 = (k - 2) % S, s1 = (k - 1) % S;
-    if (!fail && k == 2) fail = !mbar_wait(&bars[s0], 0);
-    if (!fail) fail = !mbar_wait(&bars[s1], ((k - 1) / S) & 1);
+    if (!fail && k == 2) fail = !mbar_wait(&bars[s0], 0, a.spin);
+    if (!fail) fail = !mbar_wait(&bars[s1], ((k - 1) / S) & 1, a.spin);
     const float* st0 = ring + s0 * L::stage;
     const float* U = st0 + L::oU;
     const float* V = st0 + L::oV;
@@ -227,7 +230,8 @@ __device__ __forceinline__ void hevi2_tile(const HeviMaps& m, const HeviArgs& a,
     const F2 t3v = (DIV >= 1) ? pp + a.divcv * jcbk * div : pp;                    // pgrad.f90:300
     if (has_halo) t3h[hy * BX + hx] = t3h_of(div3d_at(hx, hy), P[hy * BX + hx]);
     __syncthreads();
-    if (tid == 0 && k + S - 1 <= klast) {
+    // a stage is refilled only by a thread 0 that saw its previous copy land
+    if (tid == 0 && !fail && k + S - 1 <= klast) {
       fence_proxy_async_smem();
       issue(k + S - 1);
     }
@@ -304,10 +308,9 @@ __device__ __forceinline__ void hevi2_tile(const HeviMaps& m, const HeviArgs& a,
     // land (bounded again) so no TMA write outlives the block, and leave.
     if (tid == 0) {
       atomicExch(a.err, 1);
-      const int kmax = min(nk - 2 + S - 1, klast);
       for (int s = 0; s < S; ++s) {
         int kl = -1;
-        for (int k = 2; k <= kmax; ++k)
+        for (int k = 2; k <= issued; ++k)
           if ((k - 2) % S == s) kl = k;
         if (kl >= 0) mbar_wait(&bars[s], ((kl - 2) / S) & 1);
       }

@@ -7,15 +7,24 @@
 // the substep additionally needs is small per-column data (1-D base-state
 // columns, their reciprocals, the elimination factors of the w system and
 // an error word).  Here that data lives in one file-scope __device__ array
-// of fixed size, so the call allocates nothing; the kernel is the same
-// k_hevi_substep the context API launches.
+// of fixed size, so the call allocates nothing.  The kernel is the one the
+// context API launches for the same HE-VI tile (cfg->tile 0..10; tile 0,
+// the default, is k_hevi2); tile 11 reads a level table this entry point
+// does not hold and is rejected.
 //
 // Limits and sharing:
 //   * nk <= kNoAllocMaxNk (256 levels); larger grids are rejected.
 //   * The array is one per device and holds its contents between calls.
-//     Each call rewrites all of it (the error word is cleared), so no state
-//     carries over, but two calls whose kernels overlap on the GPU (e.g. on
+//     A call rewrites it whenever its parameters differ from the previous
+//     call's on that device and always clears the error word, so no state
+//     carries over; but two calls whose kernels overlap on the GPU (e.g. on
 //     different streams) race on it: serialize them.
+//   * The horizontal-uniformity scan of the 11 base arrays (every point,
+//     as cress_set_base3d does) and the column and factor set-up run only
+//     when the call's parameters change: dims, spacing, dts, weicoe, buyopt,
+//     the base-array pointers, or any value of the base arrays' centre
+//     column.  A caller that changes base values off the centre column in
+//     place, behind the same pointers, is not re-scanned.
 //   * The first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
 //     before any stream capture begins.
@@ -28,6 +37,7 @@
 #include "common.cuh"
 #include "ctx.h"
 #include "hevi.cuh"
+#include "wsystem.h"
 
 namespace cress {
 namespace {
@@ -50,6 +60,30 @@ static __device__ __align__(256) unsigned char g_hevi_scratch[sizeof(NoAllocScra
 std::mutex g_mu;
 void* g_scratch_dev[kMaxDevices];  // device address of g_hevi_scratch per device
 bool g_ready[kMaxDevices];
+
+// What the device array of one GPU was last filled from: the parameters the
+// set-up depends on, the base arrays' centre columns and the host image.
+struct SetupKey {
+  int ni = 0, nj = 0, nk = 0, buyopt = -1;
+  float dx = 0.f, dy = 0.f, dz = 0.f, dts = 0.f, weicoe = 0.f;
+  const float* base[CRESS_B_N] = {};
+  bool operator==(const SetupKey& o) const {
+    auto same = [](float x, float y) { return std::memcmp(&x, &y, sizeof x) == 0; };
+    if (ni != o.ni || nj != o.nj || nk != o.nk || buyopt != o.buyopt || !same(dx, o.dx) || !same(dy, o.dy) ||
+        !same(dz, o.dz) || !same(dts, o.dts) || !same(weicoe, o.weicoe))
+      return false;
+    for (int n = 0; n < CRESS_B_N; ++n)
+      if (base[n] != o.base[n]) return false;
+    return true;
+  }
+};
+struct DeviceSetup {
+  bool valid = false;
+  SetupKey key;
+  float centre[CRESS_B_N * (kNoAllocMaxNk + 1)];
+  NoAllocScratch image;
+};
+DeviceSetup* g_setup[kMaxDevices];   // host memory, made on a device's first call
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -79,9 +113,9 @@ int encode(EncodeTiledFn fn, const Grid& g, const float* buf, int rows, CUtensor
   return r == CUDA_SUCCESS ? CRESS_OK : set_error(CRESS_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
 
-// Device address of the scratch on the current device (set up once).
+// Device address of the scratch on the current device (set up once; the
+// caller holds g_mu).
 int scratch_address(int dev, NoAllocScratch** out) {
-  std::lock_guard<std::mutex> lk(g_mu);
   if (!g_ready[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_hevi_scratch);
@@ -132,84 +166,55 @@ extern "C" int cress_hevi_substep_noalloc(const cress_cfg* cfg, float dts,
   int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   if (rc) return rc;
   if (dev < 0 || dev >= kMaxDevices) return set_error(CRESS_E_ARG, "device index %d out of range", dev);
-  NoAllocScratch* sd = nullptr;
-  if ((rc = scratch_address(dev, &sd))) return rc;
+  if (cfg->tile < 0 || cfg->tile > 10)
+    return set_error(CRESS_E_UNSUPPORTED,
+                     "cress_hevi_substep_noalloc: tile %d (tiles 0-10; tile 11 needs a level table)", cfg->tile);
   EncodeTiledFn fn = encoder();
   if (!fn) return set_error(CRESS_E_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 
-  // Host image of the scratch, built in a static per-thread buffer.
-  static thread_local NoAllocScratch h;
-  std::memset(&h, 0, sizeof h);
-  const int ncol = nk + 1;
-  auto at = [&](const float* a, int i, int j, int k) {
-    return a[(size_t)i + (size_t)(ni + 2) * ((size_t)j + (size_t)(nj + 2) * (size_t)(k - 1))];
-  };
-  const int map[CRESS_B_N] = {C_JCB, C_JCB8U, C_JCB8V, C_JCB8W, C_RBR, C_PTBR,
-                              C_RST, C_RST8U, C_RST8V, C_RST8W, C_RCSQ};
+  std::lock_guard<std::mutex> lk(g_mu);
+  NoAllocScratch* sd = nullptr;
+  if ((rc = scratch_address(dev, &sd))) return rc;
+  if (!g_setup[dev]) g_setup[dev] = new DeviceSetup();
+  DeviceSetup& ds = *g_setup[dev];
+  SetupKey key;
+  key.ni = ni; key.nj = nj; key.nk = nk; key.buyopt = cfg->buyopt;
+  key.dx = cfg->dx; key.dy = cfg->dy; key.dz = cfg->dz; key.dts = dts; key.weicoe = cfg->weicoe;
+  for (int n = 0; n < CRESS_B_N; ++n) key.base[n] = base3d[n];
+  // the centre column of every base array (a cheap check for values
+  // changed in place behind the same pointers)
   const int ic = ni / 2, jc = nj / 2;
+  bool same = ds.valid && ds.key == key;
   for (int n = 0; n < CRESS_B_N; ++n)
     for (int k = 1; k <= nk; ++k) {
-      const float v = at(base3d[n], ic, jc, k);
-      h.col[map[n] * ncol + k] = v;
-      for (int j = 1; j <= nj; ++j)
-        for (int i = 1; i <= ni; ++i) {
-          const float x = at(base3d[n], i, j, k);
-          if (x != v && !(std::isnan(x) && std::isnan(v)))
-            return set_error(CRESS_E_NONUNIFORM, "base array %d varies horizontally at (%d,%d,%d)", n, i, j, k);
-        }
+      const float v = base3d[n][(size_t)ic + (size_t)(ni + 2) * ((size_t)jc + (size_t)(nj + 2) * (size_t)(k - 1))];
+      float& c = ds.centre[n * (kNoAllocMaxNk + 1) + k];
+      if (same && std::memcmp(&c, &v, sizeof v) != 0) same = false;
+      c = v;
     }
-  const int inv_src[6] = {C_RST8U, C_RST8V, C_JCB, C_RCSQ, C_RST8W, C_JCB8W};
-  const int inv_dst[6] = {C_IRST8U, C_IRST8V, C_IJCB, C_IRCSQ, C_IRST8W, C_IJCB8W};
-  for (int n = 0; n < 6; ++n)
-    for (int k = 1; k <= nk; ++k) {
-      const float v = h.col[inv_src[n] * ncol + k];
-      h.col[inv_dst[n] * ncol + k] = (v != 0.f) ? 1.f / v : 0.f;
-    }
-  // w-system coefficients (stepwi.f90:308-416) and Thomas factors
-  // (gaussel.f90:189-240), as the context API forms them.
-  const float g = 9.8f;
-  const float dziv = 1.f / cfg->dz, weicoe = cfg->weicoe, g05 = .5f * g;
-  const float sbsqzi = dts * dts * weicoe * weicoe * dziv;
-  const float sbsqg5 = .5f * g * dts * dts * weicoe * weicoe;
-  float fwc[kNoAllocMaxNk + 2] = {0}, wcc[kNoAllocMaxNk + 2] = {0}, ss[kNoAllocMaxNk + 2] = {0},
-        tt[kNoAllocMaxNk + 2] = {0};
-  auto C = [&](int f, int k) { return h.col[f * ncol + k]; };
-  for (int k = 2; k <= nk - 2; ++k) {
-    const float t1 = g05 * C(C_RBR, k) / C(C_RCSQ, k), t2 = dziv / C(C_JCB, k);
-    fwc[k] = t1 + t2;
-    wcc[k] = t1 - t2;
+  if (same) {
+    // the device array already holds this set-up: clear the error word only
+    if ((rc = cuda_check(cudaMemsetAsync(&sd->err, 0, sizeof(int), st), "clear error word"))) return rc;
+  } else {
+    ds.valid = false;
+    NoAllocScratch& h = ds.image;
+    std::memset(&h, 0, sizeof h);
+    const NonUniform bad = base_columns(base3d, ni, nj, nk, h.col);
+    if (bad.n >= 0)
+      return set_error(CRESS_E_NONUNIFORM, "base array %d varies horizontally at (%d,%d,%d)", bad.n, bad.i,
+                       bad.j, bad.k);
+    float work[4 * (kNoAllocMaxNk + 2)];
+    w_system_factors(h.col, nk, cfg->dz, cfg->weicoe, cfg->buyopt, dts, h.rr, h.aa, h.cp, work);
+    h.err = 0;
+    if ((rc = cuda_check(cudaMemcpyAsync(sd, &h, sizeof h, cudaMemcpyHostToDevice, st), "copy to hevi scratch")))
+      return rc;
+    ds.key = key;
+    ds.valid = true;
   }
-  for (int k = 3; k <= nk - 2; ++k) {
-    if (cfg->buyopt == 0) {
-      const float a = sbsqzi / C(C_RST8W, k), mm = a * C(C_RCSQ, k - 1), nn = a * C(C_RCSQ, k);
-      h.rr[k] = -mm * fwc[k - 1];
-      ss[k] = 1.f + (nn * fwc[k] - mm * wcc[k - 1]);
-      tt[k] = nn * wcc[k];
-    } else {
-      const float rstiv = 1.f / C(C_RST8W, k), a = rstiv * sbsqzi, b = rstiv * sbsqg5;
-      const float mm = b * C(C_RST, k - 1) - a * C(C_RCSQ, k - 1);
-      const float nn = b * C(C_RST, k) + a * C(C_RCSQ, k);
-      h.rr[k] = mm * fwc[k - 1];
-      ss[k] = 1.f + (mm * wcc[k - 1] + nn * fwc[k]);
-      tt[k] = nn * wcc[k];
-    }
-  }
-  const int ks = 3, ke = nk - 2;
-  h.aa[ks] = 1.0 / (double)ss[ks];
-  h.cp[ks] = (double)tt[ks] * h.aa[ks];
-  for (int k = ks + 1; k <= ke - 1; ++k) {
-    h.aa[k] = 1.0 / ((double)ss[k] - (double)h.rr[k] * h.cp[k - 1]);
-    h.cp[k] = (double)tt[k] * h.aa[k];
-  }
-  h.aa[ke] = 1.0 / ((double)ss[ke] - (double)h.rr[ke] * h.cp[ke - 1]);
-  h.err = 0;
-
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  if ((rc = cuda_check(cudaMemcpyAsync(sd, &h, sizeof h, cudaMemcpyHostToDevice, st), "copy to hevi scratch")))
-    return rc;
 
   const Grid gr = make_grid(ni, nj, nk);
-  const int tile = 0;
+  const int tile = cfg->tile;
   const int TY = hevi_tile_rows(tile);
   HeviMaps maps;
   if ((rc = encode(fn, gr, u_old, TY + 2, &maps.u)) || (rc = encode(fn, gr, v_old, TY + 3, &maps.v)) ||
@@ -225,14 +230,15 @@ extern "C" int cress_hevi_substep_noalloc(const cress_cfg* cfg, float dts,
   a.thom_rr = sd->rr; a.thom_aa = sd->aa; a.thom_cp = sd->cp;
   a.err = &sd->err;
   a.dts = dts;
+  const float dziv = 1.f / cfg->dz, weicoe = cfg->weicoe;
   a.dxiv = 1.f / cfg->dx; a.dyiv = 1.f / cfg->dy; a.dziv = dziv;
-  a.divch = 0.05f / dts * cfg->dx * cfg->dy;   // pgrad.f90:253 (divndc = 0.05)
-  a.divcv = 0.05f / dts * cfg->dz * cfg->dz;   // pgrad.f90:254
+  a.divch = kDivndc / dts * cfg->dx * cfg->dy;   // pgrad.f90:253
+  a.divcv = kDivndc / dts * cfg->dz * cfg->dz;   // pgrad.f90:254
   a.weicoe = weicoe;
   a.dtdzw = dts * dziv * weicoe;
   a.dtw = dts * weicoe;
-  a.g05 = g05;
-  a.g05n = -.5f * g;
+  a.g05 = .5f * kG;
+  a.g05n = -.5f * kG;
   a.divopt = cfg->divopt; a.buyopt = cfg->buyopt; a.sthopt = cfg->sthopt; a.bbc = cfg->bbc;
   if ((rc = launch_hevi_substep(a, maps, tile, st)))
     return set_error(rc, "cress_hevi_substep_noalloc: launch failed: %s", cudaGetErrorString(cudaGetLastError()));

@@ -93,7 +93,9 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
 
   // Levels 1..nk-1 are staged; level lv lives in slot (lv-1) % S.
   const int lmax = nk - 1;
+  int issued = 0;   // highest level thread 0 has issued
   auto issue = [&](int lv) {
+    issued = lv;
     const int s = (lv - 1) % S;
     float* st = ring + s * L::stage;
     uint64_t* bar = &bars[s];
@@ -142,7 +144,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
     // Every thread has finished level k-1, so the slot of level k-3 (last
     // read as k'-2 at k' = k-1) may be refilled with level k+S-3.
     __syncthreads();
-    if (tid == 0 && k >= 4 && k + S - 3 <= lmax) {
+    if (tid == 0 && !fail && k >= 4 && k + S - 3 <= lmax) {   // refill only after its copy was seen to land
       fence_proxy_async_smem();
       issue(k + S - 3);
     }
@@ -227,10 +229,9 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
     // land (bounded again) so no TMA write outlives the block.
     if (tid == 0) {
       if (a.err) atomicExch(a.err, 1);
-      const int last = min(nk - 2 + S - 3, lmax);   // highest level issued
       for (int s = 0; s < S; ++s) {
         int kl = -1;
-        for (int lv = 1; lv <= last; ++lv)
+        for (int lv = 1; lv <= issued; ++lv)
           if ((lv - 1) % S == s) kl = lv;
         if (kl >= 0) mbar_wait(&bars[s], ((kl - 1) / S) & 1);
       }

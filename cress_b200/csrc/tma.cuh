@@ -44,9 +44,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t n = 0; n < kSpinLimit; ++n)
+// Bounded wait for the phase with the given parity to complete: at most
+// `limit` probes (limit 0 gives up at once, which a test of the failure
+// path uses).  A kernel whose wait gave up must stop issuing copies into
+// its stages and, before it exits, wait (with the full limit) for every
+// copy it issued.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kSpinLimit) {
+  for (uint32_t n = 0; n < limit; ++n)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

@@ -102,6 +102,14 @@ void cress_destroy(cress_ctx* ctx);
 int cress_set_stream(cress_ctx* ctx, void* stream);
 int cress_sync(cress_ctx* ctx);
 
+/* Failure-path test hook, no counterpart in the reference: the number of
+ * probes each ring wait of the HE-VI level loop (tile 0) makes before it
+ * gives up (default 4194304; 0 gives up at once).  A wait that gives up
+ * makes the kernel stop issuing copies, wait for the ones in flight and
+ * return, and the next synchronizing call reports CRESS_E_TIMEOUT; the
+ * context stays usable.  A negative value restores the default. */
+int cress_set_spin_limit(cress_ctx* ctx, int probes);
+
 /* Base state and metrics, as the reference holds them after s_inivar
  * (SrcOrig/inivar.f90:674-850: setbase, baserho, sndwave): CRESS_B_N host
  * arrays in reference layout.  They must be horizontally uniform (flat
@@ -110,7 +118,13 @@ int cress_set_base3d(cress_ctx* ctx, const float* const* base3d);
 
 /* Host <-> device copy of one prognostic field at one time level
  * (reference layout).  Used at restart read / dump / restart write times
- * (SrcOrig/outres.f90:868-900 reads the same arrays). */
+ * (SrcOrig/outres.f90:868-900 reads the same arrays).
+ * cress_put_field is asynchronous on the context's stream: from pageable
+ * host memory the data is taken before the call returns, but from
+ * page-locked (pinned) memory the copy may still be running, so keep such a
+ * buffer unchanged until the next synchronizing call (cress_sync,
+ * cress_get_field, cress_diagnostics).  cress_get_field returns with the
+ * data in `host`. */
 int cress_put_field(cress_ctx* ctx, int field, int level, const float* host);
 int cress_get_field(cress_ctx* ctx, int field, int level, float* host);
 
@@ -310,9 +324,14 @@ int cress_set_tuple_sampling(cress_ctx* ctx, cress_mlp* m, int stride, float kee
  * cress_set_base3d.  The small per-column data the kernel needs (base-state
  * columns, the w-system elimination factors, an error word) goes into one
  * fixed __device__ array of about 28 KB per GPU, resident until the process
- * exits; hence nk <= 256 (larger grids return CRESS_E_ARG).  Every call
- * rewrites that array, so calls whose kernels overlap on the GPU race on
- * it and must be serialized.  The first call on a device looks up the
+ * exits; hence nk <= 256 (larger grids return CRESS_E_ARG).  A call
+ * rewrites that array when its parameters (dims, spacing, dts, weicoe,
+ * buyopt, base pointers, base centre columns) differ from the previous
+ * call's on the device, and always clears its error word; calls whose
+ * kernels overlap on the GPU race on it and must be serialized.  The
+ * horizontal-uniformity scan of base3d runs only on such a change.  The
+ * kernel is the context API's for cfg->tile (0-10; 11 is rejected).
+ * The first call on a device looks up the
  * array's address with that device current; make it before any stream
  * capture begins.  The call is synchronous on `stream` (NULL = the default
  * stream) and returns CRESS_E_TIMEOUT if a bounded device-side wait gave up. */
