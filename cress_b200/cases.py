@@ -344,11 +344,13 @@ def supercell_case(nx, ny, nz, dx, ztop=18000.0, dzmin=100.0, dzmax=500.0, seed=
 
 def squall_case(nx, ny, nz, dx=500.0, ztop=18000.0, dzmin=100.0, dzmax=500.0, seed=0, ptp0=2.0,
                 shear=20.0, zshear=2500.0, xrad=5000.0, zrad=1400.0, zc=1400.0, noise=0.1,
-                x0=0.0):
+                x0=0.0, umove=0.0):
     """Squall-line state (cold-rain microphysics, open x, periodic y).
 
     Base state: the analytic sounding of moist_columns; unidirectional
-    low-level shear, u = shear * min(z / zshear, 1), v = 0.  Perturbation:
+    low-level shear, u = shear * min(z / zshear, 1) - umove, v = 0 (umove,
+    a domain translation, keeps the line inside a reduced domain without
+    changing the shear).  Perturbation:
     a line thermal along y of +ptp0 K, cos^2 in x (half width xrad, centred
     x0 m from mid-domain) and z (half depth zrad at height zc), plus seeded
     uniform +-noise K inside it.  Moisture: qv at the base value, no
@@ -357,7 +359,7 @@ def squall_case(nx, ny, nz, dx=500.0, ztop=18000.0, dzmin=100.0, dzmax=500.0, se
     cols = moist_columns(nk, ztop, dzmin, dzmax)
     base = {n: expand(cols[n], ni, nj, nk) for n in BASE_NAMES + ["pbr", "qvbr"]}
     zs = cols["zs"]
-    u = shear * np.clip(zs / zshear, 0.0, 1.0)
+    u = shear * np.clip(zs / zshear, 0.0, 1.0) - umove
     base["ubr"] = expand(u.astype(np.float32), ni, nj, nk)
     base["vbr"] = expand(np.zeros_like(u, dtype=np.float32), ni, nj, nk)
     rng = np.random.default_rng(seed)

@@ -21,6 +21,7 @@ struct ThomasSet {
   float* rr = nullptr;
   double* aa = nullptr;
   double* cp = nullptr;
+  HeviLevel* lvl3 = nullptr;   // level table of the on-chip kernel (rows 0..nk)
 };
 
 struct Ctx {

@@ -39,6 +39,25 @@ struct HeviMaps {
   CUtensorMap u, v, w, p, uf, vf, wf, pf;
 };
 
+// One row per level k of the level table of the on-chip HE-VI kernel
+// (tile 12): the base-state columns and reciprocals a substep reads, the
+// sub-diagonal a_k of the w system (float, as stepwi forms it) and the
+// FP64 elimination factors aa_k = 1/(b_k - a_k c'_{k-1}), cp_k = c'_k.
+// Five 16-byte vectors per level.
+struct alignas(16) HeviLevel {
+  float rst8u, rst8v, rst8w, ij8w;
+  float jcb, ijcb, irst8u, irst8v;
+  float jcb8u, jcb8v, rcsq, rst;
+  float rbr, ircsq, irst8w, rr;
+  double aa, cp;
+};
+static_assert(sizeof(HeviLevel) == 80, "HeviLevel is five 16-byte vectors");
+
+// Largest nk the on-chip kernel holds: the eliminated right-hand sides of
+// levels 3..nk-2 of two columns in FP64 fill 4 (nk - 4) <= 256 tensor-memory
+// columns per thread.
+constexpr int kHevi3MaxNk = 68;
+
 struct HeviArgs {
   Grid g;
   const float* u_old; const float* v_old; const float* p_old;
@@ -48,6 +67,7 @@ struct HeviArgs {
   const float* thom_rr;   // [k] sub-diagonal a_k of the w system (float, as formed by stepwi)
   const double* thom_aa;  // [k] 1/(b_k - a_k c'_{k-1})
   const double* thom_cp;  // [k] c'_k
+  const HeviLevel* lvl3;  // level table of tile 12 (rows k = 0..nk), or null
   int* err;               // device error word (nonzero: a bounded wait gave up)
   // HE-VE only: the contravariant w of levels 2 and nk-1 (two planes of
   // px*py each), which the reference keeps from the explicit update while
@@ -65,6 +85,8 @@ struct HeviArgs {
 
 // Tile heights the kernel is instantiated for.
 int hevi_tile_rows(int tile);
+// The on-chip kernel (tile 12); needs a.lvl3 and nk <= kHevi3MaxNk.
+int launch_hevi3(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st);
 // Launch one substep; `maps` must describe the buffers in `a` with the
 // box rows of HeviRows<hevi_tile_rows(tile)>.
 int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st);

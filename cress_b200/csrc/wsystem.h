@@ -113,4 +113,22 @@ inline void w_system_factors(const float* col, int nk, float dz, float weicoe, i
   aa[ke] = 1.0 / ((double)ss[ke] - (double)rr[ke] * cp[ke - 1]);
 }
 
+// Rows k = 0..nk of the level table of the on-chip HE-VI kernel (tile
+// 12) from the base columns and the w-system factors above.
+inline void hevi_level_rows(const float* col, int nk, const float* rr, const double* aa, const double* cp,
+                            HeviLevel* out) {
+  auto C = [&](int f, int k) { return col[(size_t)f * (nk + 1) + k]; };
+  for (int k = 0; k <= nk; ++k) {
+    HeviLevel r{};
+    if (k >= 1) {
+      r.rst8u = C(C_RST8U, k); r.rst8v = C(C_RST8V, k); r.rst8w = C(C_RST8W, k); r.ij8w = C(C_IJCB8W, k);
+      r.jcb = C(C_JCB, k); r.ijcb = C(C_IJCB, k); r.irst8u = C(C_IRST8U, k); r.irst8v = C(C_IRST8V, k);
+      r.jcb8u = C(C_JCB8U, k); r.jcb8v = C(C_JCB8V, k); r.rcsq = C(C_RCSQ, k); r.rst = C(C_RST, k);
+      r.rbr = C(C_RBR, k); r.ircsq = C(C_IRCSQ, k); r.irst8w = C(C_IRST8W, k);
+    }
+    r.rr = rr[k]; r.aa = aa[k]; r.cp = cp[k];
+    out[k] = r;
+  }
+}
+
 }  // namespace cress
