@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libcress_b200.so")
 FIELDS = ["u", "v", "w", "pp", "ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 PAST, NOW, FUTURE, FORCING = 0, 1, 2, 3
-NTILES = 13   # HE-VI tile shapes (cress_cfg.tile)
+NTILES = 14   # HE-VI tile shapes (cress_cfg.tile)
 # enum cress_base order
 BASE_NAMES = ["jcb", "jcb8u", "jcb8v", "jcb8w", "rbr", "ptbr", "rst", "rst8u", "rst8v",
               "rst8w", "rcsq"]

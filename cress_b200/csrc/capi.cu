@@ -183,19 +183,25 @@ int Ctx::thomas_for(float dts, const ThomasSet** out) {
                    work.data());
   std::vector<HeviLevel> rows(nk + 1);
   hevi_level_rows(col_h.data(), nk, rr.data(), aa.data(), cp.data(), rows.data());
+  std::vector<HeviLevel1> rows1(nk + 1);
+  hevi_level_rows1(col_h.data(), nk, rr.data(), aa.data(), cp.data(), rows1.data());
   ThomasSet t;
   if (cudaMalloc(&t.rr, sizeof(float) * (nk + 2)) != cudaSuccess ||
       cudaMalloc(&t.aa, sizeof(double) * (nk + 2)) != cudaSuccess ||
       cudaMalloc(&t.cp, sizeof(double) * (nk + 2)) != cudaSuccess ||
-      cudaMalloc(&t.lvl3, sizeof(HeviLevel) * (nk + 1)) != cudaSuccess)
+      cudaMalloc(&t.lvl3, sizeof(HeviLevel) * (nk + 1)) != cudaSuccess ||
+      cudaMalloc(&t.lvl4, sizeof(HeviLevel1) * (nk + 1)) != cudaSuccess)
     return set_error(CRESS_E_CUDA, "cudaMalloc (tridiagonal factors) failed");
   owned.push_back(t.rr); owned.push_back(t.aa); owned.push_back(t.cp); owned.push_back(t.lvl3);
+  owned.push_back(t.lvl4);
   int rc;
   if ((rc = cuda_check(cudaMemcpyAsync(t.rr, rr.data(), sizeof(float) * (nk + 2), cudaMemcpyHostToDevice, stream), "copy rr")) ||
       (rc = cuda_check(cudaMemcpyAsync(t.aa, aa.data(), sizeof(double) * (nk + 2), cudaMemcpyHostToDevice, stream), "copy aa")) ||
       (rc = cuda_check(cudaMemcpyAsync(t.cp, cp.data(), sizeof(double) * (nk + 2), cudaMemcpyHostToDevice, stream), "copy cp")) ||
       (rc = cuda_check(cudaMemcpyAsync(t.lvl3, rows.data(), sizeof(HeviLevel) * (nk + 1), cudaMemcpyHostToDevice,
-                                       stream), "copy level table")))
+                                       stream), "copy level table")) ||
+      (rc = cuda_check(cudaMemcpyAsync(t.lvl4, rows1.data(), sizeof(HeviLevel1) * (nk + 1),
+                                       cudaMemcpyHostToDevice, stream), "copy level table")))
     return rc;
   // The host vectors above are freed on return; make the copies complete.
   if ((rc = cuda_check(cudaStreamSynchronize(stream), "sync after factor upload"))) return rc;
@@ -278,8 +284,8 @@ int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
   if (!base_set) return set_error(CRESS_E_STATE, "cress_small_steps: base state not set");
   if (jobs && (cfg.impopt != 1 || cfg.tile != 0 || g.openx))
     return set_error(CRESS_E_UNSUPPORTED, "ensemble small steps need impopt=1, tile 0 and periodic x");
-  if (g.openx && cfg.tile != 0 && cfg.tile != 11 && cfg.tile != 12)
-    return set_error(CRESS_E_UNSUPPORTED, "open x boundaries run the HE-VI tiles 0, 11 and 12");
+  if (g.openx && cfg.tile != 0 && cfg.tile != 11 && cfg.tile != 12 && cfg.tile != 13)
+    return set_error(CRESS_E_UNSUPPORTED, "open x boundaries run the HE-VI tiles 0, 11, 12 and 13");
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_small_steps: nsstp=%d", nsstp);
   const bool heve = cfg.impopt == 0;
   const ThomasSet* th = nullptr;
@@ -293,7 +299,7 @@ int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
     if ((rc = level_table(0.f, &t))) return rc;
   }
   a.lvl = level_tables.begin()->second;
-  if (th) { a.thom_rr = th->rr; a.thom_aa = th->aa; a.thom_cp = th->cp; a.lvl3 = th->lvl3; }
+  if (th) { a.thom_rr = th->rr; a.thom_aa = th->aa; a.thom_cp = th->cp; a.lvl3 = th->lvl3; a.lvl4 = th->lvl4; }
   a.err = err_d;
   a.dts = dts;
   a.dxiv = 1.f / cfg.dx; a.dyiv = 1.f / cfg.dy; a.dziv = 1.f / cfg.dz;

@@ -22,6 +22,7 @@ struct ThomasSet {
   double* aa = nullptr;
   double* cp = nullptr;
   HeviLevel* lvl3 = nullptr;   // level table of the on-chip kernel (rows 0..nk)
+  HeviLevel1* lvl4 = nullptr;  // the same once per value (one-column-per-thread kernel)
 };
 
 struct Ctx {

@@ -372,7 +372,7 @@ int launch_t(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
 // (both recurrences always run in double).
 int hevi_tile_rows(int tile) {
   switch (tile) {
-    case 0: case 11: case 12: return 8;
+    case 0: case 11: case 12: case 13: return 8;
     case 1: case 4: case 8: return 2;
     case 2: case 5: case 7: return 8;
     default: return 4;
@@ -386,6 +386,7 @@ int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaS
     case 0: return launch_hevi2(a, maps, 0, st);
     case 11: return launch_hevi2(a, maps, 1, st);
     case 12: return launch_hevi3(a, maps, st);
+    case 13: return launch_hevi4(a, maps, st);
     case 1: return launch_t<2, 5, float>(a, maps, st);
     case 2: return launch_t<8, 4, float>(a, maps, st);
     case 3: return launch_t<4, 5, double>(a, maps, st);

@@ -43,17 +43,34 @@ struct HeviMaps {
 // (tile 12): the base-state columns and reciprocals a substep reads, the
 // sub-diagonal a_k of the w system (float, as stepwi forms it) and the
 // FP64 elimination factors aa_k = 1/(b_k - a_k c'_{k-1}), cp_k = c'_k.
-// Five 16-byte vectors per level.
+// Every float is stored twice, so a 16-byte load yields two ready operand
+// pairs of the packed FP32x2 arithmetic (f2.cuh); nine 16-byte vectors per
+// level.
 struct alignas(16) HeviLevel {
+  float rst8u[2], rst8v[2];     // vector 0
+  float rst8w[2], ij8w[2];      // vector 1
+  float jcb[2], ijcb[2];        // vector 2
+  float irst8u[2], irst8v[2];   // vector 3
+  float jcb8u[2], jcb8v[2];     // vector 4
+  float rcsq[2], rst[2];        // vector 5
+  float rbr[2], ircsq[2];       // vector 6
+  float irst8w[2], rr[2];       // vector 7
+  double aa, cp;                // vector 8
+};
+static_assert(sizeof(HeviLevel) == 144, "HeviLevel is nine 16-byte vectors");
+
+// The same values once each (five 16-byte vectors per level), for the
+// one-column-per-thread on-chip kernel (tile 13).
+struct alignas(16) HeviLevel1 {
   float rst8u, rst8v, rst8w, ij8w;
   float jcb, ijcb, irst8u, irst8v;
   float jcb8u, jcb8v, rcsq, rst;
   float rbr, ircsq, irst8w, rr;
   double aa, cp;
 };
-static_assert(sizeof(HeviLevel) == 80, "HeviLevel is five 16-byte vectors");
+static_assert(sizeof(HeviLevel1) == 80, "HeviLevel1 is five 16-byte vectors");
 
-// Largest nk the on-chip kernel holds: the eliminated right-hand sides of
+// Largest nk the on-chip kernels hold: the eliminated right-hand sides of
 // levels 3..nk-2 of two columns in FP64 fill 4 (nk - 4) <= 256 tensor-memory
 // columns per thread.
 constexpr int kHevi3MaxNk = 68;
@@ -68,6 +85,7 @@ struct HeviArgs {
   const double* thom_aa;  // [k] 1/(b_k - a_k c'_{k-1})
   const double* thom_cp;  // [k] c'_k
   const HeviLevel* lvl3;  // level table of tile 12 (rows k = 0..nk), or null
+  const HeviLevel1* lvl4; // level table of tile 13 (rows k = 0..nk), or null
   int* err;               // device error word (nonzero: a bounded wait gave up)
   // HE-VE only: the contravariant w of levels 2 and nk-1 (two planes of
   // px*py each), which the reference keeps from the explicit update while
@@ -87,6 +105,8 @@ struct HeviArgs {
 int hevi_tile_rows(int tile);
 // The on-chip kernel (tile 12); needs a.lvl3 and nk <= kHevi3MaxNk.
 int launch_hevi3(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st);
+// The on-chip kernel with one column per thread (tile 13); needs a.lvl4.
+int launch_hevi4(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st);
 // Launch one substep; `maps` must describe the buffers in `a` with the
 // box rows of HeviRows<hevi_tile_rows(tile)>.
 int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st);

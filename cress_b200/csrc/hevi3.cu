@@ -20,7 +20,9 @@
 // the two differ by FP32 rounding only.
 //
 // Per-level constants and the elimination factors come from a level table
-// in global memory (five 16-byte loads per level, L1-resident).  Blocks
+// in global memory (nine 16-byte loads per level, L1-resident, issued one
+// level ahead), each float stored twice so the loads yield ready operand
+// pairs for the packed FP32x2 arithmetic.  Blocks
 // that touch the domain's edges take a path with the ownership checks and
 // the periodic ghost stores; every other block stores plainly.
 //
@@ -106,7 +108,7 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
   float* t3hb = ring + S * L::stage;                                       // 2 x [(TY+2)][BX]
   float2* qs = reinterpret_cast<float2*>(t3hb + 2 * L::t3h_floats);        // [(k-2) * NT + tid]
   uint64_t* bars = reinterpret_cast<uint64_t*>(qs + (size_t)(nk - 3) * NT);
-  const float4* rows = reinterpret_cast<const float4*>(a.lvl3);           // 5 vectors per level
+  const float4* rows = reinterpret_cast<const float4*>(a.lvl3);           // 9 vectors per level
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -148,11 +150,11 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
     else { n -= TY; hx = TX + 2; hy = n + 1; }
   }
   const bool has_halo = tid < NH;
-  const int ox = tx + 2;
-  const int oyA = 2 * ty + 1, oyB = oyA + 1;   // own rows in the boxes that start at j0-1
-  const int fyA = 2 * ty, fyB = fyA + 1;       // own rows in the forcing boxes (from j0)
-  const float dts = a.dts, dxiv = a.dxiv, dyiv = a.dyiv, dziv = a.dziv;
-  const float weic1m = 1.f - a.weicoe;
+  const F2 dts = f2(a.dts), dxiv = f2(a.dxiv), dyiv = f2(a.dyiv), dziv = f2(a.dziv);
+  const F2 weic1m = f2(1.f - a.weicoe), g05 = f2(a.g05), g05n = f2(a.g05n), dtw = f2(a.dtw),
+           dtdzw = f2(a.dtdzw);
+  const float divch = a.divch, divcv = a.divcv;
+  const F2 divch2 = f2(divch), divcv2 = f2(divcv);
   F2 t3v_prev = f2(0.f), fpdvj_prev = f2(0.f), wb8s_prev = f2(0.f);   // rows A, B
   double fA_prev = 0.0, fB_prev = 0.0;
   bool fail = false;
@@ -160,9 +162,30 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
   const int id2 = (int)g.at(i, jA, 2);
   float* uA = a.u_new + id2;
   float* vA = a.v_new + id2;
-  float4 c0 = __ldg(rows + 2 * 5);   // level k's first vector (carried from level k-1's load)
+  // this thread's cell in the boxes that start at j0-1 (row oyA = 2ty+1,
+  // column tx+2); the forcing boxes start at j0, one row lower
+  const int tofs = (2 * ty + 1) * BX + tx + 2;
+  // the level table: nine vectors per level; row k's vectors 0, 2-8 and
+  // row k+1's vector 1 (rst8w, ij8w one level up) are loaded one level ahead
+  struct Row {
+    float4 v0, v2, v3, v4, v5, v6, v7, n1;
+    double aa;
+  };
+  auto load_row = [&](int k, Row& r) {
+    const float4* p = rows + 9 * k;
+    r.v0 = __ldg(p + 0); r.v2 = __ldg(p + 2); r.v3 = __ldg(p + 3); r.v4 = __ldg(p + 4);
+    r.v5 = __ldg(p + 5); r.v6 = __ldg(p + 6); r.v7 = __ldg(p + 7);
+    r.aa = __ldg(reinterpret_cast<const double*>(p + 8));
+    r.n1 = __ldg(p + 9 + 1);
+  };
+  auto lo2 = [](float4 v) { return F2{make_float2(v.x, v.y)}; };   // first pair of a vector
+  auto hi2 = [](float4 v) { return F2{make_float2(v.z, v.w)}; };   // second pair
+  Row cur, nxt;
+  load_row(2, cur);
+  float4 v1k = __ldg(rows + 9 * 2 + 1);   // row k's vector 1
 
   for (int k = 2; k <= nk - 2; ++k, uA += plane, vA += plane) {
+    if (k + 1 <= nk - 2) load_row(k + 1, nxt);
     // one barrier per level: t3h alternates between two buffers, and the
     // stage of level k-1 is refilled only after this level's barrier
     float* t3h = t3hb + (k & 1) * L::t3h_floats;
@@ -170,59 +193,58 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
     if (!fail && k == 2) fail = !mbar_wait(&bars[s0], 0, a.spin);
     if (!fail) fail = !mbar_wait(&bars[s1], ((k - 1) / S) & 1, a.spin);
     const float* st0 = ring + s0 * L::stage;
+    const float* W1s = ring + s1 * L::stage + L::oW;
+    const float* tb = st0 + tofs;         // own cell (row A) in every box of level k
+    const float* tw1 = W1s + tofs;        // own cell in level k+1's w box
+    float* th0 = t3h + tofs;              // own cell in the damped-pressure plane
+    const F2 rst8u = lo2(cur.v0), rst8v = hi2(cur.v0);
+    const F2 rst8wk = lo2(v1k), ij8wk = hi2(v1k), rst8wk1 = lo2(cur.n1), ij8wk1 = hi2(cur.n1);
+    const F2 jcbk = lo2(cur.v2), ijcbk = hi2(cur.v2), irst8u = lo2(cur.v3), irst8v = hi2(cur.v3);
+
+    // diver3d.f90:318 (with phy2cnt.f90:219 for the contravariant w) at a halo point
     const float* U = st0 + L::oU;
     const float* V = st0 + L::oV;
     const float* W0 = st0 + L::oW;
-    const float* W1 = ring + s1 * L::stage + L::oW;
     const float* P = st0 + L::oP;
-    const float* UF = st0 + L::oUF;
-    const float* VF = st0 + L::oVF;
-    const float* WF = st0 + L::oWF;
-    const float* PF = st0 + L::oPF;
-    const float4 c1 = __ldg(rows + k * 5 + 1), c2 = __ldg(rows + k * 5 + 2), c3 = __ldg(rows + k * 5 + 3);
-    const float4 n0 = __ldg(rows + (k + 1) * 5);
-    const float rst8u = c0.x, rst8v = c0.y, rst8wk = c0.z, ij8wk = c0.w;
-    const float rst8wk1 = n0.z, ij8wk1 = n0.w;
-    const float jcbk = c1.x, ijcbk = c1.y, irst8u = c1.z, irst8v = c1.w;
-
-    // diver3d.f90:318 (with phy2cnt.f90:219 for the contravariant w)
     auto div3d_at = [&](int x, int y) {
-      float wck = W0[y * BX + x], wck1 = W1[y * BX + x];
-      if constexpr (STH) { wck = wck * ij8wk; wck1 = wck1 * ij8wk1; }
-      return (rst8wk * wck - rst8wk1 * wck1) * dziv +
-             ((rst8u * U[y * BX + x] - rst8u * U[y * BX + x + 1]) * dxiv +
-              (rst8v * V[y * BX + x] - rst8v * V[(y + 1) * BX + x]) * dyiv);
+      float wck = W0[y * BX + x], wck1 = W1s[y * BX + x];
+      if constexpr (STH) { wck = wck * ij8wk.v.x; wck1 = wck1 * ij8wk1.v.x; }
+      return (rst8wk.v.x * wck - rst8wk1.v.x * wck1) * dziv.v.x +
+             ((rst8u.v.x * U[y * BX + x] - rst8u.v.x * U[y * BX + x + 1]) * dxiv.v.x +
+              (rst8v.v.x * V[y * BX + x] - rst8v.v.x * V[(y + 1) * BX + x]) * dyiv.v.x);
     };
     // pgrad.f90:300,341,363
     auto t3h_of = [&](float div, float pp) {
       float th;
-      if constexpr (DIV == 2) th = pp + a.divch * div * ijcbk;
-      else if constexpr (DIV == 1) th = pp + a.divcv * jcbk * div;
+      if constexpr (DIV == 2) th = pp + divch * div * ijcbk.v.x;
+      else if constexpr (DIV == 1) th = pp + divcv * jcbk.v.x * div;
       else th = pp;
-      return jcbk * th;
+      return jcbk.v.x * th;
     };
     // rows A and B of the thread in the two lanes of F2: one packed
-    // instruction for both rows
-    auto col2 = [&](const float* base, int oy) { return f2(base[oy * BX + ox], base[(oy + 1) * BX + ox]); };
-    F2 wc0 = col2(W0, oyA), wc1 = col2(W1, oyA);
+    // instruction for both rows (offsets relative to the own cell)
+    auto at2 = [&](const float* base, int off) { return f2(base[off], base[off + BX]); };
+    F2 wc0 = at2(tb, L::oW), wc1 = at2(tw1, 0);
     if constexpr (STH) { wc0 = wc0 * ij8wk; wc1 = wc1 * ij8wk1; }
-    const F2 uo = col2(U, oyA), vo = col2(V, oyA);
+    const F2 uo = at2(tb, L::oU), vo = at2(tb, L::oV);
     const F2 div = (rst8wk * wc0 - rst8wk1 * wc1) * dziv +
-                   ((rst8u * uo - rst8u * col2(U + 1, oyA)) * dxiv +
-                    (rst8v * vo - rst8v * col2(V + BX, oyA)) * dyiv);      // diver3d.f90:318
-    const F2 pp = col2(P, oyA);
+                   ((rst8u * uo - rst8u * at2(tb, L::oU + 1)) * dxiv +
+                    (rst8v * vo - rst8v * at2(tb, L::oV + BX)) * dyiv);      // diver3d.f90:318
+    const F2 pp = at2(tb, L::oP);
     F2 th;                                                                   // pgrad.f90:341,363
-    if constexpr (DIV == 2) th = pp + a.divch * div * ijcbk;
-    else if constexpr (DIV == 1) th = pp + a.divcv * jcbk * div;
+    if constexpr (DIV == 2) th = pp + divch2 * div * ijcbk;
+    else if constexpr (DIV == 1) th = pp + divcv2 * jcbk * div;
     else th = pp;
     const F2 tc = jcbk * th;
-    t3h[oyA * BX + ox] = tc.v.x;
-    t3h[oyB * BX + ox] = tc.v.y;
-    const F2 t3v = (DIV >= 1) ? pp + a.divcv * jcbk * div : pp;              // pgrad.f90:300
+    th0[0] = tc.v.x;
+    th0[BX] = tc.v.y;
+    const F2 t3v = (DIV >= 1) ? pp + divcv2 * jcbk * div : pp;               // pgrad.f90:300
     if (has_halo) t3h[hy * BX + hx] = t3h_of(div3d_at(hx, hy), P[hy * BX + hx]);
-    // the rest of this level's inputs, read before the barrier
-    const F2 uf = col2(UF, fyA), vf = col2(VF, fyA), wf = col2(WF, fyA), pf = col2(PF, fyA);
-    const float vo2 = V[(oyB + 1) * BX + ox], vf2f = VF[(fyB + 1) * BX + ox];
+    // the rest of this level's own inputs, read before the barrier
+    const F2 uf = at2(tb, L::oUF - BX), vf = at2(tb, L::oVF - BX), wf = at2(tb, L::oWF - BX),
+             pf = at2(tb, L::oPF - BX);
+    const float vo2 = tb[L::oV + 2 * BX], vf2f = tb[L::oVF + BX];
+    const F2 wk = at2(tb, L::oW), wk1 = at2(tw1, 0);
     __syncthreads();
     if (tid == 0 && !fail && k + S - 1 <= klast) {   // refill only after its copy was seen to land
       fence_proxy_async_smem();
@@ -231,18 +253,18 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
 
     // stepuv.f90:294,304 with pgrad.f90:379,389: west u faces, the east
     // face from the next lane (lane 31 forms its own)
-    const F2 un0 = uo + dts * (uf + (col2(t3h - 1, oyA) - tc) * dxiv) * irst8u;
+    const F2 un0 = uo + dts * (uf + (at2(th0, -1) - tc) * dxiv) * irst8u;
     F2 un1 = f2(__shfl_down_sync(full, un0.v.x, 1), __shfl_down_sync(full, un0.v.y, 1));
     if (tx == TX - 1)
-      un1 = col2(U + 1, oyA) + dts * (col2(UF + 1, fyA) + (tc - col2(t3h + 1, oyA)) * dxiv) * irst8u;
+      un1 = at2(tb, L::oU + 1) + dts * (at2(tb, L::oUF - BX + 1) + (tc - at2(th0, 1)) * dxiv) * irst8u;
     // v faces south of rows A and B (the one between the rows serves both),
     // and north of row B
-    const F2 vs = vo + dts * (vf + (f2(t3h[(oyA - 1) * BX + ox], tc.v.x) - tc) * dyiv) * irst8v;
-    const float vn2 = vo2 + dts * (vf2f + (tc.v.y - t3h[(oyB + 1) * BX + ox]) * dyiv) * irst8v;
+    const F2 vs = vo + dts * (vf + (f2(th0[-BX], tc.v.x) - tc) * dyiv) * irst8v;
+    const float vn2 = vo2 + a.dts * (vf2f + (tc.v.y - th0[2 * BX]) * a.dyiv) * irst8v.v.x;
     const F2 vn = f2(vs.v.y, vn2);
 
-    const float jcb8u = c2.x, jcb8v = c2.y, rcsq = c2.z, rst = c2.w;
-    const float rbr = c3.x, ircsq = c3.y, irst8w = c3.z;
+    const F2 jcb8u = lo2(cur.v4), jcb8v = hi2(cur.v4), rcsq = lo2(cur.v5), rst = hi2(cur.v5);
+    const F2 rbr = lo2(cur.v6), ircsq = hi2(cur.v6), irst8w = lo2(cur.v7);
     const bool kend = (k == 2) || (k == nk - 2);
     if constexpr (!EDGE) {
       uA[0] = un0.v.x; uA[px] = un0.v.y;
@@ -277,20 +299,19 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
 
     F2 phd = (jcb8u * un0 - jcb8u * un1) * dxiv + (jcb8v * vs - jcb8v * vn) * dyiv;    // diver2d.f90:288
     phd = rcsq * phd;                                                                   // diverpih.f90:208
-    const F2 wk = col2(W0, oyA), wk1 = col2(W1, oyA);
     const F2 pvd = rcsq * (wk - wk1) * dziv;                                            // diverpiv.f90:124
-    const F2 fp = pf + phd + weic1m * (a.g05 * (wk + wk1) * rst + pvd);                 // advbspi.f90:158
+    const F2 fp = pf + phd + weic1m * (g05 * (wk + wk1) * rst + pvd);                   // advbspi.f90:158
     const F2 q = pp + dts * fp * ijcbk;           // steppi.f90:217, explicit part of the new p'
     qs[(k - 2) * NT + tid] = q.v;
     const F2 fpdvj = fp * ijcbk;                                                        // pgradiv.f90:149
-    const F2 wb8s = (pp * rst + fp * rbr * a.dtw) * ircsq * a.g05n;                     // buoywsi.f90:171
+    const F2 wb8s = (pp * rst + fp * rbr * dtw) * ircsq * g05n;                         // buoywsi.f90:171
     if (k >= 3) {
       const F2 wpg = (t3v_prev - t3v) * dziv;                                           // pgrad.f90:320
-      F2 fw = wf + wpg + (fpdvj_prev - fpdvj) * a.dtdzw;                                // pgradiv.f90:163
+      F2 fw = wf + wpg + (fpdvj_prev - fpdvj) * dtdzw;                                  // pgradiv.f90:163
       if constexpr (BUY) fw = fw + (wb8s_prev + wb8s);                                  // buoywsi.f90:205
       const F2 wrhs = wk + dts * fw * irst8w;                                           // stepwi.f90:325
       // gaussel.f90:189-240 in double with the 1-D factors, one recurrence per row
-      const double rr = (double)c3.w, aa = __ldg(reinterpret_cast<const double*>(rows + k * 5 + 4));
+      const double rr = (double)cur.v7.z, aa = cur.aa;
       const double fA = (k == 3) ? (double)wrhs.v.x * aa : ((double)wrhs.v.x - rr * fA_prev) * aa;
       const double fB = (k == 3) ? (double)wrhs.v.y * aa : ((double)wrhs.v.y - rr * fB_prev) * aa;
       tmem_st4(tmem + 4u * (uint32_t)(k - 3), lo32(fA), hi32(fA), lo32(fB), hi32(fB));
@@ -300,7 +321,8 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
     t3v_prev = t3v;
     fpdvj_prev = fpdvj;
     wb8s_prev = wb8s;
-    c0 = n0;
+    v1k = cur.n1;
+    cur = nxt;
   }
 
   if (__syncthreads_or(fail)) {
@@ -327,7 +349,7 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
   const int ktop = nk - 2;
   double wdA = 0.0, wdB = 0.0;            // w(k+1) in double; w(nk-1) = 0 (vbcw.f90:481)
   F2 wup = f2(0.f), wkend = f2(0.f), pkend = f2(0.f), p3 = f2(0.f);
-  const float weicoe = a.weicoe, g05 = a.g05;
+  const F2 weicoe = f2(a.weicoe);
   float* wT = a.w_new + (int)g.at(i, jA, ktop);
   float* pT = a.p_new + (int)g.at(i, jA, ktop);
   for (int c = (ktop - 3) / 8; c >= 0; --c) {
@@ -338,16 +360,17 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
     for (int e = 7; e >= 0; --e) {
       const int k = 3 + 8 * c + e;
       if (k > ktop) continue;
-      const float4 d1 = __ldg(rows + k * 5 + 1), d2 = __ldg(rows + k * 5 + 2);
-      const double cpk = __ldg(reinterpret_cast<const double*>(rows + k * 5 + 4) + 1);
+      const float4* rp = rows + 9 * k;
+      const float4 d2 = __ldg(rp + 2), d5 = __ldg(rp + 5);
+      const double cpk = __ldg(reinterpret_cast<const double*>(rp + 8) + 1);
       wdA = mk64(r[4 * e], r[4 * e + 1]) - cpk * wdA;    // gaussel.f90:254
       wdB = mk64(r[4 * e + 2], r[4 * e + 3]) - cpk * wdB;
       const F2 wk = f2((float)wdA, (float)wdB);
       const F2 q = F2{qs[(k - 2) * NT + tid]};
       // steppi.f90:217 with diverpiv.f90:124 and advbspi.f90:175 (the implicit part)
-      const F2 pvd = d2.z * (wk - wup) * dziv;
-      const F2 fpw = weicoe * (g05 * (wk + wup) * d2.w + pvd);
-      const F2 pn = q + dts * fpw * d1.y;
+      const F2 pvd = lo2(d5) * (wk - wup) * dziv;
+      const F2 fpw = weicoe * (g05 * (wk + wup) * hi2(d5) + pvd);
+      const F2 pn = q + dts * fpw * hi2(d2);
       const int off = (k - ktop) * plane;
       if constexpr (!EDGE) {
         wT[off] = wk.v.x; wT[off + px] = wk.v.y;
@@ -381,12 +404,12 @@ __device__ __forceinline__ void hevi3_tile(const HeviMaps& m, const HeviArgs& a,
   // boundary rows of vbcw.f90:285,317,471,481 (wc = w / jcb8w when
   // stretched) and vbcp.f90:126-160, and level nk of u, v, p' carried over
   {
-    const float4 d1 = __ldg(rows + 2 * 5 + 1), d2 = __ldg(rows + 2 * 5 + 2);
+    const float4 d2 = __ldg(rows + 9 * 2 + 2), d5 = __ldg(rows + 9 * 2 + 5);
     const F2 q = F2{qs[tid]};
     const F2 w0 = f2(0.f);
-    const F2 pvd = d2.z * (w0 - wup) * dziv;
-    const F2 fpw = weicoe * (g05 * (w0 + wup) * d2.w + pvd);
-    const F2 p2 = q + dts * fpw * d1.y;
+    const F2 pvd = lo2(d5) * (w0 - wup) * dziv;
+    const F2 fpw = weicoe * (g05 * (w0 + wup) * hi2(d5) + pvd);
+    const F2 p2 = q + dts * fpw * hi2(d2);
     const float jw3 = __ldg(a.col + C_JCB8W * (nk + 1) + 3), jwt = __ldg(a.col + C_JCB8W * (nk + 1) + nk - 2);
     auto finish = [&](bool own, bool edge, bool ylast, int j, float p2v, float p3v, float w3, float wke,
                       float pke) {

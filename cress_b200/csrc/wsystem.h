@@ -120,13 +120,35 @@ inline void hevi_level_rows(const float* col, int nk, const float* rr, const dou
   auto C = [&](int f, int k) { return col[(size_t)f * (nk + 1) + k]; };
   for (int k = 0; k <= nk; ++k) {
     HeviLevel r{};
+    auto set = [](float* d, float v) { d[0] = d[1] = v; };
+    if (k >= 1) {
+      set(r.rst8u, C(C_RST8U, k)); set(r.rst8v, C(C_RST8V, k)); set(r.rst8w, C(C_RST8W, k));
+      set(r.ij8w, C(C_IJCB8W, k)); set(r.jcb, C(C_JCB, k)); set(r.ijcb, C(C_IJCB, k));
+      set(r.irst8u, C(C_IRST8U, k)); set(r.irst8v, C(C_IRST8V, k)); set(r.jcb8u, C(C_JCB8U, k));
+      set(r.jcb8v, C(C_JCB8V, k)); set(r.rcsq, C(C_RCSQ, k)); set(r.rst, C(C_RST, k)); set(r.rbr, C(C_RBR, k));
+      set(r.ircsq, C(C_IRCSQ, k)); set(r.irst8w, C(C_IRST8W, k));
+    }
+    set(r.rr, rr[k]);
+    r.aa = aa[k];
+    r.cp = cp[k];
+    out[k] = r;
+  }
+}
+
+inline void hevi_level_rows1(const float* col, int nk, const float* rr, const double* aa, const double* cp,
+                             HeviLevel1* out) {
+  auto C = [&](int f, int k) { return col[(size_t)f * (nk + 1) + k]; };
+  for (int k = 0; k <= nk; ++k) {
+    HeviLevel1 r{};
     if (k >= 1) {
       r.rst8u = C(C_RST8U, k); r.rst8v = C(C_RST8V, k); r.rst8w = C(C_RST8W, k); r.ij8w = C(C_IJCB8W, k);
       r.jcb = C(C_JCB, k); r.ijcb = C(C_IJCB, k); r.irst8u = C(C_IRST8U, k); r.irst8v = C(C_IRST8V, k);
       r.jcb8u = C(C_JCB8U, k); r.jcb8v = C(C_JCB8V, k); r.rcsq = C(C_RCSQ, k); r.rst = C(C_RST, k);
       r.rbr = C(C_RBR, k); r.ircsq = C(C_IRCSQ, k); r.irst8w = C(C_IRST8W, k);
     }
-    r.rr = rr[k]; r.aa = aa[k]; r.cp = cp[k];
+    r.rr = rr[k];
+    r.aa = aa[k];
+    r.cp = cp[k];
     out[k] = r;
   }
 }

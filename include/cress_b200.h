@@ -54,7 +54,8 @@ typedef struct cress_cfg {
                               point, its column average, or the constant gwave) with sbc = nbc = -1 */
   int bbc, tbc;         /* 2 = rigid (SrcOrig/vbcw.f90:201) */
   int tile;             /* HE-VI tile shape id (0 = default: 32x8, two rows per thread; 1-11 other shapes;
-                           12: 32x8 with the column kept on chip, FP64 throughout the solve, nk <= 68) */
+                           12, 13: 32x8 with the column kept on chip, FP64 throughout the solve, nk <= 68;
+                           12 two rows per thread, 13 one) */
   /* large step (SrcOrig/forcedrv.f90:548-608, SrcOrig/timeflt.f90:335) */
   int advopt;           /* 2 only: 4th-order horizontal advection */
   int smtopt;           /* 0 none, 2 horizontal, 3 horizontal + vertical 4th-order smoothing */
@@ -181,7 +182,7 @@ int cress_large_step(cress_ctx* ctx, long long ctime, float dtb, int nsstp, floa
 int cress_diagnostics(cress_ctx* ctx, int level, double* out);
 
 /* Number of HE-VI tile shapes (cress_cfg.tile = 0 .. CRESS_NTILES-1). */
-#define CRESS_NTILES 13
+#define CRESS_NTILES 14
 
 /* Autotuner: times every HE-VI tile shape (xy tile, ring depth, column
  * store) over `reps` small-step loops of nsstp substeps of length dts on

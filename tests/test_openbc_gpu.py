@@ -97,7 +97,7 @@ def check(dims, names, ref, got):
         assert float(np.abs(pg - pr).max()) <= 1e-3 * float(np.abs(pr).max()) + 1e-9
 
 
-@pytest.mark.parametrize("obc,tile", [(7, 0), (4, 0), (5, 0), (4, 11), (4, 12)])
+@pytest.mark.parametrize("obc,tile", [(7, 0), (4, 0), (5, 0), (4, 11), (4, 12), (4, 13)])
 def test_open_x_moist_steps(cress, oracle_lib, obc, tile):
     # tile 11: the HE-VI variant with the level table in global memory;
     # tile 12: the column kept on chip
@@ -166,5 +166,5 @@ def test_open_x_rejects_other_tiles(cress):
     s.set_base3d(case["base"])
     with pytest.raises(cress.CressError) as e:
         s.small_steps(2, 0.5)
-    assert e.value.code == 2 and "tiles 0, 11 and 12" in str(e.value)
+    assert e.value.code == 2 and "tiles 0, 11, 12 and 13" in str(e.value)
     s.close()

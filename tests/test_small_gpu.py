@@ -48,18 +48,19 @@ def test_one_substep(cress, oracle_lib, sthopt):
     check(ni, nj, nk, ref, out, 1)
 
 
-@pytest.mark.parametrize("tile", list(range(13)))
+@pytest.mark.parametrize("tile", list(range(14)))
 def test_ragged_domain_tiles(cress, oracle_lib, tile):
     # nx, ny not multiples of the tile: partial edge tiles on both axes
     ni, nj, nk, ref, out = run_pair(cress, oracle_lib, 45, 37, 21, 3, tile=tile, seed=5)
     check(ni, nj, nk, ref, out, 3)
 
 
+@pytest.mark.parametrize("tile", [12, 13])
 @pytest.mark.parametrize("divopt,sthopt", [(2, 1), (1, 1), (0, 0)])
-def test_onchip_tile_interior_blocks(cress, oracle_lib, divopt, sthopt):
+def test_onchip_tile_interior_blocks(cress, oracle_lib, divopt, sthopt, tile):
     # tile 12 (the column kept on chip): 4 x 5 tiles, so interior blocks
     # (plain stores) and edge blocks (periodic images, partial tiles) both run
-    ni, nj, nk, ref, out = run_pair(cress, oracle_lib, 100, 37, 30, 4, sthopt=sthopt, tile=12, seed=9,
+    ni, nj, nk, ref, out = run_pair(cress, oracle_lib, 100, 37, 30, 4, sthopt=sthopt, tile=tile, seed=9,
                                     divopt=divopt)
     check(ni, nj, nk, ref, out, 4)
 
