@@ -32,10 +32,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 HEVI_BYTES_PER_CELL = 48  # u,v,w,p' read + write and 4 forcings read, float32
-# DRAM bytes per cell of one k_hevi2 launch measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 632.6 MB over 384*384*63
-# cells of a 384x384x64 domain); the traffic grows with the cells
-HEVI2_TRAFFIC_PER_CELL = 632.6e6 / (384 * 384 * 63)
+# DRAM bytes per cell of one HE-VI launch measured by ncu on a 384x384x64
+# domain (dram__bytes_read.sum + dram__bytes_write.sum over 384*384*63
+# cells); the traffic grows with the cells.  Tile 0 (k_hevi2) parks the
+# eliminated right-hand sides in HBM: 632.6 MB; tile 13 (k_hevi4) keeps
+# them on chip: 349.7 + 121.0 MB.
+HEVI_TRAFFIC_PER_CELL = {0: 632.6e6 / (384 * 384 * 63), 13: (349.68e6 + 120.99e6) / (384 * 384 * 63)}
+HEVI_KERNEL = {0: "k_hevi2", 11: "k_hevi2", 12: "k_hevi3", 13: "k_hevi4"}
 METRIC = "cell-updates/s on 1 B200: plain vs learned-microphysics form at stated error"
 MOIST = ["qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
 NAMES = ["u", "v", "w", "pp", "ptp"] + MOIST
@@ -591,12 +594,12 @@ def main():
             "sim_s_per_wall_s": args.dtbig / (ms / args.steps * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": (HEVI2_TRAFFIC_PER_CELL * cells
-                                     if hevi_tile == 0 and args.impopt == 1 else None),
+                         "traffic": (HEVI_TRAFFIC_PER_CELL[hevi_tile] * cells
+                                     if hevi_tile in HEVI_TRAFFIC_PER_CELL and args.impopt == 1 else None),
                          "traffic_source": "ncu dram bytes per cell at 384x384x64 scaled to this grid",
                          "peak_source": peak_kind,
                          "kernel": ("k_heve" if args.impopt == 0 else
-                                    "k_hevi2" if hevi_tile == 0 else "k_hevi_substep"),
+                                    HEVI_KERNEL.get(hevi_tile, "k_hevi_substep")),
                          "bytes_per_launch": HEVI_BYTES_PER_CELL * cells,
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
