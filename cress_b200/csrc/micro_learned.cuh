@@ -249,15 +249,28 @@ __global__ void __launch_bounds__(128) k_mlp_apply(const MicroArgs a, const Appl
   const Grid g = a.g;
   const long long ncell = (long long)(g.ni - 3) * (g.nj - 3) * (g.nk - 1);
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= p.cnt || p.n0 + r >= ncell) return;
   const long long n = p.n0 + r;
-  if (mlp_apply_cell(a, n, p.y + (size_t)r * kMlpN4, p.env[r] != 0, p.norm, p.resid_tol)) {
-    atomicAdd(p.stats, 1ull);
-    return;
+  bool used = false, fb = false;
+  if (r < p.cnt && n < ncell) {
+    used = mlp_apply_cell(a, n, p.y + (size_t)r * kMlpN4, p.env[r] != 0, p.norm, p.resid_tol);
+    fb = !used;
   }
-  const int slot = atomicAdd(p.fb_count, 1);
-  if (slot < p.fb_cap) p.fb_list[slot] = (int)(n - p.n0);   // relative to the chunk
-  atomicAdd(p.stats + 1, 1ull);
+  // one set of atomics per warp (counts, and the fallback cells' slots)
+  const unsigned full = 0xffffffffu, lane = threadIdx.x & 31u;
+  const unsigned mu = __ballot_sync(full, used), mf = __ballot_sync(full, fb);
+  int base = 0;
+  if (lane == 0) {
+    if (mu) atomicAdd(p.stats, (unsigned long long)__popc(mu));
+    if (mf) {
+      atomicAdd(p.stats + 1, (unsigned long long)__popc(mf));
+      base = atomicAdd(p.fb_count, __popc(mf));
+    }
+  }
+  base = __shfl_sync(full, base, 0);
+  if (fb) {
+    const int slot = base + __popc(mf & ((1u << lane) - 1u));
+    if (slot < p.fb_cap) p.fb_list[slot] = (int)(n - p.n0);   // relative to the chunk
+  }
 }
 
 // The plain process-rate part on the listed cells of one chunk.

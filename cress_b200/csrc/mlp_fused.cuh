@@ -133,7 +133,7 @@ __device__ __forceinline__ void fused_epilogue(const MicroArgs& a, const FusedAr
     mbar_arrive(x_full);
     bool ok = true;
     for (int l = 0; l < 3; ++l) {
-      ok = __all_sync(full, mbar_wait(acc_full, pha));
+      ok = __all_sync(full, mbar_wait_sleep(acc_full, pha));
       pha ^= 1;
       if (!ok) break;
       tc_fence_after();
@@ -157,7 +157,7 @@ __device__ __forceinline__ void fused_epilogue(const MicroArgs& a, const FusedAr
       mbar_arrive(h_full);
     }
     if (!ok) { *vfail = 1; break; }
-    ok = __all_sync(full, mbar_wait(acc_full, pha));
+    ok = __all_sync(full, mbar_wait_sleep(acc_full, pha));
     pha ^= 1;
     if (!ok) { *vfail = 1; break; }
     tc_fence_after();
@@ -165,17 +165,29 @@ __device__ __forceinline__ void fused_epilogue(const MicroArgs& a, const FusedAr
       uint32_t r[16];
       tmem_ld16(tmem + lane_base, r);
       tmem_wait_ld();
+      bool used = false, fb = false;
       if (n < p.ncell) {
         float ys[kMlpOut];
 #pragma unroll
         for (int m = 0; m < kMlpOut; ++m) ys[m] = __uint_as_float(r[m]) + bias[3 * kMlpH + m];
-        if (mlp_apply_cell(a, n, ys, env, p.norm, p.resid_tol)) {
-          atomicAdd(p.stats, 1ull);
-        } else {
-          const int slot = atomicAdd(p.fb_count, 1);
-          if (slot < p.fb_cap) p.fb_list[slot] = (int)n;
-          atomicAdd(p.stats + 1, 1ull);
+        used = mlp_apply_cell(a, n, ys, env, p.norm, p.resid_tol);
+        fb = !used;
+      }
+      // one set of atomics per warp: the counts of network and fallback
+      // cells, and the fallback cells' slots in the list
+      const unsigned mu = __ballot_sync(full, used), mf = __ballot_sync(full, fb);
+      int base = 0;
+      if (lane == 0) {
+        if (mu) atomicAdd(p.stats, (unsigned long long)__popc(mu));
+        if (mf) {
+          atomicAdd(p.stats + 1, (unsigned long long)__popc(mf));
+          base = atomicAdd(p.fb_count, __popc(mf));
         }
+      }
+      base = __shfl_sync(full, base, 0);
+      if (fb) {
+        const int slot = base + __popc(mf & ((1u << lane) - 1u));
+        if (slot < p.fb_cap) p.fb_list[slot] = (int)n;
       }
     }
     tc_fence_before();
@@ -232,7 +244,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
           for (int kb = 0; kb < (l == 0 ? 1 : 4) && !*vfail; ++kb)
             for (int h = 0; h < (l == 3 ? 1 : 2); ++h, ++cnt) {
               const int s = cnt & 1, r = cnt >> 1;
-              if (*vfail || !mbar_wait(&w_empty[s], (r & 1) ^ 1)) { *vfail = 1; break; }
+              if (*vfail || !mbar_wait_sleep(&w_empty[s], (r & 1) ^ 1)) { *vfail = 1; break; }
               mbar_arrive_expect_tx(&w_full[s], l == 3 ? kW4Block : kWStage);
               const CUtensorMap* mp = l == 0 ? &maps.w1 : l == 1 ? &maps.w2 : l == 2 ? &maps.w3 : &maps.w4;
               tma_load_2d(WS + s * kWStage, mp, kb * 64, h * 128, &w_full[s]);
@@ -249,18 +261,18 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       int cnt = 0, phx = 0, phh = 0;
       bool ok = true;
       for (long long t = blockIdx.x; ok && t < ntiles; t += gridDim.x) {
-        if (*vfail || !mbar_wait(&x_full, phx)) { ok = false; break; }
+        if (*vfail || !mbar_wait_sleep(&x_full, phx)) { ok = false; break; }
         phx ^= 1;
         for (int l = 0; l < 4 && ok; ++l) {
           if (l > 0) {
-            if (*vfail || !mbar_wait(&h_full, phh)) { ok = false; break; }
+            if (*vfail || !mbar_wait_sleep(&h_full, phh)) { ok = false; break; }
             phh ^= 1;
           }
           tc_fence_after();
           for (int kb = 0; kb < (l == 0 ? 1 : 4) && ok; ++kb)
             for (int h = 0; h < (l == 3 ? 1 : 2); ++h, ++cnt) {
               const int s = cnt & 1, r = cnt >> 1;
-              if (*vfail || !mbar_wait(&w_full[s], r & 1)) { ok = false; break; }
+              if (*vfail || !mbar_wait_sleep(&w_full[s], r & 1)) { ok = false; break; }
               tc_fence_after();
               // layers 1-3: N = 128 into accumulator columns 128h..; layer 4: N = 64
 #pragma unroll

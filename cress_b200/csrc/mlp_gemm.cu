@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     int issued = 0;
     for (int kb = 0; kb < KB; ++kb) {
       const int s = kb % kStages, r = kb / kStages;
-      if (*vfail || !mbar_wait(&empty[s], (r & 1) ^ 1)) {
+      if (*vfail || !mbar_wait_sleep(&empty[s], (r & 1) ^ 1)) {
         *vfail = 1;
         break;
       }
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const uint32_t idesc = idesc_bf16_f32(kBM, BN);
     for (int kb = 0; kb < KB; ++kb) {
       const int s = kb % kStages, r = kb / kStages;
-      if (*vfail || !mbar_wait(&full[s], r & 1)) {
+      if (*vfail || !mbar_wait_sleep(&full[s], r & 1)) {
         *vfail = 1;
         break;
       }
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     umma_commit(&done);   // arrives once every MMA issued above has completed
   }
-  const bool waited = mbar_wait(&done, 0);
+  const bool waited = mbar_wait_sleep(&done, 0);
   tc_fence_after();
   const int good = __syncthreads_and(waited && !*vfail);
   if (!good) {

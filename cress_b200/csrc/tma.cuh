@@ -55,6 +55,29 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
   return false;
 }
 
+// As mbar_try_wait, but the thread may be suspended (taking no issue slots)
+// for up to `ns` nanoseconds while the phase is incomplete.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for a phase expected to take a while (a tensor-core GEMM, a
+// producer refilling a stage): at most kSleepProbes probes of up to 1 us
+// suspension each, about 2 s in all, so waiting warps leave the issue
+// slots to the warps that compute.
+constexpr uint32_t kSleepProbes = 1u << 21;
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity) {
+  for (uint32_t n = 0; n < kSleepProbes; ++n)
+    if (mbar_try_wait_sleep(bar, parity, 1000u)) return true;
+  return false;
+}
+
 // 3-D tiled TMA load of one box into shared memory, completing on `bar`.
 // The caller guarantees x*4 bytes is a multiple of 16 (x multiple of 4).
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
