@@ -185,3 +185,76 @@ def test_fused_inference_matches_chunked(cress, oracle_lib):
         assert float((err <= 1e-5 * scale).mean()) >= 0.999, name
         assert float(err.max()) <= 5e-2 * scale, name
     assert float(np.abs(pa - pb).max()) <= 1e-3 * (float(np.abs(pa).max()) + 1e-30)
+
+
+def test_learned_form_on_held_out_storm(cress, oracle_lib):
+    """Trained on tuples of two storms (new seeds, every step sampled), the
+    learned form runs a third storm it never saw.  Gate: its accumulated
+    surface precipitation is within 5% of the plain scheme's over the same
+    8 large steps from the same state.  Also reported (printed, not
+    asserted): the hydrometeor RMS difference from the plain scheme next to
+    twice the FP32-vs-FP64 spread of the plain scheme (oracle builds) over
+    the same steps; with a network of this size the RMS gate is not met."""
+    import json
+    from cress_b200 import cases
+    m = cress.Mlp(seed=11)
+    m.reserve(1_000_000)
+    for seed in (31, 32):
+        s, _ = _moist_solver(cress, oracle_lib, seed)
+        s.set_tuple_sampling(m, stride=1, keep_zero=0.2, seed=seed)
+        s.large_step(0, 2.5, 10, 0.5)
+        for n in range(1, 8):
+            s.large_step(n * 5000, 5.0, 10, 1.0)
+        s.set_tuple_sampling(None)
+        s.close()
+    ntup = m.tuple_count()
+    m.fit_norm()
+    m.train(1500, batch=8192, lr=1e-3, seed=3)
+
+    def run(learned):
+        s, dims = _moist_solver(cress, oracle_lib, 33)
+        if learned:
+            s.set_learned_micro(m, chunk=0, resid_tol=0.5)
+        s.large_step(0, 2.5, 10, 0.5)
+        for n in range(1, 8):
+            s.large_step(n * 5000, 5.0, 10, 1.0)
+        out = {n: s.get_field(n, cress.NOW) for n in NAMES[6:11]}
+        prec = s.get_precip()
+        s.close()
+        return out, prec, dims
+
+    plain, pp, dims = run(False)
+    learned, pl, _ = run(True)
+    m.close()
+    ni, nj, nk = dims
+    sl = (slice(1, nk - 2), slice(2, nj - 1), slice(2, ni - 1))
+    acc_p = float(pp[:, 1, 2:nj - 1, 2:ni - 1].astype(np.float64).sum())
+    acc_l = float(pl[:, 1, 2:nj - 1, 2:ni - 1].astype(np.float64).sum())
+    # the plain scheme's own FP32-vs-FP64 spread over the same steps (oracle)
+    case = cases.supercell_case(40, 32, 24, 1000.0, ztop=8000.0, seed=33, cloud=True,
+                                rad=(6000.0, 6000.0, 1400.0))
+    zph = case["zph"]
+    cfg = dict(ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=case["dz"], sthopt=1, smtopt=3, vspopt=2,
+               coropt=0, vspbar=0.005, botbar=0.6 * zph[nk - 1], thresq=1e-12)
+    init = list(case["level"]) + [case["moist"][n] for n in NAMES[5:]]
+    ref = {}
+    for bits in (64, 32):
+        past = [a.copy() for a in init]
+        now = [a.copy() for a in init]
+        prec = np.zeros((5, 2, nj + 2, ni + 2), np.float32)
+        oracle_lib.moist_steps(cfg, case["base"], zph, past, now, prec, 8, 5.0, 1.0, start=True,
+                               prec_bits=bits, omp=True)
+        ref[bits] = {n: a for n, a in zip(NAMES, now)}
+    rep = {"train_tuples": int(ntup), "precip_plain": acc_p, "precip_learned": acc_l,
+           "precip_rel_diff": abs(acc_l - acc_p) / (abs(acc_p) + 1e-30), "species": {}}
+    for n in NAMES[6:11]:
+        r64 = ref[64][n][sl].astype(np.float64)
+        rms = float(np.sqrt(np.mean(r64 ** 2))) + 1e-30
+        spread = float(np.sqrt(np.mean((ref[32][n][sl] - r64) ** 2))) / rms
+        d = (learned[n][sl].astype(np.float64) - plain[n][sl])
+        err = float(np.sqrt(np.mean(d ** 2))) / (float(np.sqrt(np.mean(plain[n][sl].astype(np.float64) ** 2))) + 1e-30)
+        rep["species"][n] = {"learned_rms_rel": err, "fp32_fp64_spread_rel": spread,
+                             "gate_2x_spread_met": bool(err <= 2.0 * spread)}
+    print(json.dumps({"learned_held_out": rep}))
+    assert acc_p > 0.0
+    assert rep["precip_rel_diff"] < 0.05, rep
