@@ -119,6 +119,8 @@ def lib():
     L.cress_ensemble_set_graphs.argtypes = [vp, i]
     L.cress_autotune.argtypes = [vp, i, f, i, ctypes.POINTER(i), ctypes.POINTER(f)]
     L.cress_set_spin_limit.argtypes = [vp, i]
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.cress_base_state.argtypes = [i, dp, dp, i, dp, i, i, ctypes.c_double, ctypes.c_double, dp, i]
     _lib = L
     return L
 
@@ -131,6 +133,26 @@ def _check(code):
 def fptr(a):
     assert a.dtype == np.float32 and a.flags.c_contiguous
     return a.ctypes.data_as(_FP)
+
+
+BASE_COLUMNS = ["ubr", "vbr", "pbr", "ptbr", "qvbr", "rbr", "ptvbr", "pibr", "rst", "rst8w", "rcsq"]
+
+
+def base_state(nk, zph, jcb, z, u, v, pt, qv, psnd0, thresq=1e-12, tvar="p", hvar="r", device=0):
+    """The base state from a height-level sounding, computed on the device
+    in FP64 (cress_base_state): a dict of BASE_COLUMNS, each an array of
+    nk+1 doubles by level index k.  zph, jcb: the column's w-level heights
+    and Jacobian by index k; the sounding arrays are its levels 1..nlev."""
+    dp = ctypes.POINTER(ctypes.c_double)
+    zph = np.ascontiguousarray(zph, np.float64)
+    jcb = np.ascontiguousarray(jcb, np.float64)
+    assert zph.size == nk + 1 and jcb.size == nk + 1
+    snd = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float64) for a in (z, u, v, pt, qv)]))
+    out = np.zeros((len(BASE_COLUMNS), nk + 1))
+    _check(lib().cress_base_state(int(nk), zph.ctypes.data_as(dp), jcb.ctypes.data_as(dp), len(z),
+                                  snd.ctypes.data_as(dp), ord(tvar), ord(hvar), float(psnd0), float(thresq),
+                                  out.ctypes.data_as(dp), int(device)))
+    return dict(zip(BASE_COLUMNS, out))
 
 
 class Solver:

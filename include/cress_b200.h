@@ -118,6 +118,34 @@ int cress_set_spin_limit(cress_ctx* ctx, int probes);
  * terrain, no map factors); otherwise CRESS_E_NONUNIFORM. */
 int cress_set_base3d(cress_ctx* ctx, const float* const* base3d);
 
+/* The base state from a height-level sounding, computed on the device in
+ * FP64: the hydrostatic integration of the sounding with its humidity
+ * iteration (SrcOrig/set1d.f90:278-452, 536-540; vextlow.f90:150-220),
+ * the interpolation to the scalar levels (intrpsnd.f90:190-230,
+ * vint13.f90:120-170), base density and Exner function with the boundary
+ * levels (setbase.f90:153-189, bcbase.f90:150-210), rho*J and its w-point
+ * average (baserho.f90:150-160, var8uvw.f90:190-196, bc8w.f90:136,166) and
+ * rho c^2 (sndwave.f90:119); replaces those routines for a horizontally
+ * uniform grid.
+ *   zph, jcb: nk+1 entries each (index k = 1..nk): w-level heights and
+ *     the Jacobian of the column;
+ *   sounding: 5 x nlev values, levels 1..nlev (heights increasing): z,
+ *     u, v, theta (tvar = 'p') or temperature ('t'), and relative
+ *     humidity in percent (hvar = 'r') or the mixing ratio (any other);
+ *   psnd0: pressure at the lowest sounding level (Pa); thresq: mixing
+ *     ratios at or below it become 0;
+ *   columns (out): CRESS_BS_N columns of nk+1 doubles, in the order of
+ *     enum cress_base_col; levels 1..nk-1 as the reference forms them,
+ *     level nk repeating level nk-1 (rst8w: level nk-2, as bc8w).
+ * CRESS_E_ARG when the integration reaches p <= 0 or the humidity does not
+ * converge. */
+enum cress_base_col {
+  CRESS_BS_UBR = 0, CRESS_BS_VBR, CRESS_BS_PBR, CRESS_BS_PTBR, CRESS_BS_QVBR, CRESS_BS_RBR,
+  CRESS_BS_PTVBR, CRESS_BS_PIBR, CRESS_BS_RST, CRESS_BS_RST8W, CRESS_BS_RCSQ, CRESS_BS_N
+};
+int cress_base_state(int nk, const double* zph, const double* jcb, int nlev, const double* sounding,
+                     int tvar, int hvar, double psnd0, double thresq, double* columns, int device);
+
 /* Host <-> device copy of one prognostic field at one time level
  * (reference layout).  Used at restart read / dump / restart write times
  * (SrcOrig/outres.f90:868-900 reads the same arrays).

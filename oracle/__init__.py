@@ -150,6 +150,33 @@ def moist_steps(cfg, base, zph, past, now, prec, nsteps, dtbig, dtsml, start=Tru
     return rc
 
 
+BASE_STATE_FIELDS = ["ubr", "vbr", "pbr", "ptbr", "qvbr", "rbr", "ptvbr", "pibr", "rst", "rst8w", "rcsq"]
+
+
+def base_state(nk, zph, jcb, z, u, v, pt, qv, psnd0, thresq=1e-12, tvar="p", hvar="r", prec=64):
+    """Base-state columns (index k = 0..nk) from a height-level sounding
+    (set1d, vextlow, intrpsnd, setbase/bcbase, baserho, sndwave; base.h):
+    dict of BASE_STATE_FIELDS.  zph, jcb: w-level heights and Jacobian by
+    index k; the sounding arrays are levels 1..nlev."""
+    L = lib()
+    L.oracle_base_state.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    dp = ctypes.POINTER(ctypes.c_double)
+    zph = np.ascontiguousarray(zph, np.float64)
+    jcb = np.ascontiguousarray(jcb, np.float64)
+    snd = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float64) for a in (z, u, v, pt, qv)]))
+    nlev = len(z)
+    out = np.zeros((11, nk + 1))
+    rc = L.oracle_base_state(int(prec), int(nk), zph.ctypes.data_as(dp), jcb.ctypes.data_as(dp), nlev,
+                             snd.ctypes.data_as(dp), ord(tvar), ord(hvar), float(psnd0), float(thresq),
+                             out.ctypes.data_as(dp))
+    if rc != 0:
+        raise RuntimeError(f"oracle_base_state failed ({rc})")
+    return dict(zip(BASE_STATE_FIELDS, out))
+
+
 def _fp(a):
     assert a.dtype == np.float32 and a.flags.c_contiguous
     return a.ctypes.data_as(_FP)

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <vector>
 #include "small.h"
+#include "base.h"
 
 using namespace oracle;
 
@@ -75,6 +76,42 @@ int oracle_small_steps(int prec, int sthopt, const int* io, const double* ro, do
   if (o.ni < 5 || o.nj < 5 || o.nk < 6) return 1;
   if (prec == 64) return run_small<double>(o, sthopt, dts, nsstp, base, frc, st);
   return run_small<float>(o, sthopt, dts, nsstp, base, frc, st);
+}
+
+// The base state from a height-level sounding (set1d, vextlow, intrpsnd,
+// setbase/bcbase, baserho, sndwave; base.h) on one column.  snd: nlev
+// levels each of z, u, v, pt (theta, or T when tvar == 't'), qv (RH in
+// percent when hvar == 'r'); zph, jcb: nk+1 entries (index k).  out: 11
+// columns of nk+1 entries (ubr, vbr, pbr, ptbr, qvbr, rbr, ptvbr, pibr,
+// rst, rst8w, rcsq).  Returns 0, or 1 when the integration fails.
+int oracle_base_state(int prec, int nk, const double* zph, const double* jcb, int nlev, const double* snd,
+                      int tvar, int hvar, double psnd0, double thresq, double* out) {
+  auto run = [&](auto one) -> int {
+    using R = decltype(one);
+    Sounding<R> s;
+    s.nlev = nlev;
+    for (auto* v : {&s.z, &s.u, &s.v, &s.p, &s.pt, &s.qv, &s.t}) v->assign(nlev + 1, R(0));
+    for (int kl = 1; kl <= nlev; ++kl) {
+      s.z[kl] = (R)snd[kl - 1];
+      s.u[kl] = (R)snd[nlev + kl - 1];
+      s.v[kl] = (R)snd[2 * nlev + kl - 1];
+      s.pt[kl] = (R)snd[3 * nlev + kl - 1];
+      s.qv[kl] = (R)snd[4 * nlev + kl - 1];
+    }
+    if (set1d_z<R>((char)tvar, (char)hvar, (R)psnd0, (R)thresq, s)) return 1;
+    vextlow(s);
+    std::vector<R> z(nk + 1), j(nk + 1);
+    for (int k = 0; k <= nk; ++k) { z[k] = (R)zph[k]; j[k] = (R)jcb[k]; }
+    BaseColumn<R> c;
+    base_column(nk, z.data(), j.data(), s, c);
+    const std::vector<R>* cols[11] = {&c.ubr, &c.vbr, &c.pbr, &c.ptbr, &c.qvbr, &c.rbr, &c.ptvbr, &c.pibr,
+                                      &c.rst, &c.rst8w, &c.rcsq};
+    for (int f = 0; f < 11; ++f)
+      for (int k = 0; k <= nk; ++k) out[(size_t)f * (nk + 1) + k] = (double)(*cols[f])[k];
+    return 0;
+  };
+  if (nlev < 3 || nk < 6) return 2;
+  return prec == 64 ? run(0.0) : run(0.0f);
 }
 
 int oracle_abi_version(void) { return 1; }

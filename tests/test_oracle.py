@@ -167,3 +167,29 @@ def test_smagorinsky_fp32_vs_fp64_and_active(oracle_lib):
         assert float(np.abs(a - b).max()) <= 1e-3 * scale
         changed = max(changed, float(np.abs(a - c).max()) / scale)
     assert changed > 1e-3
+
+
+def test_base_state_restatement_is_hydrostatic(oracle_lib):
+    """The base state from the supercell sounding (set1d ... sndwave): the
+    Exner function falls with height at the rate -g / (cp theta_v) to the
+    accuracy of the sounding's interpolation, and the FP32 build stays
+    within 1e-5 of the FP64 build."""
+    from cress_b200 import cases
+    nk = 67
+    c = cases.moist_columns(nk)
+    z = np.linspace(0.0, 20000.0, 121)
+    th = np.where(z <= 12000.0, 300.0 + 43.0 * (z / 12000.0) ** 1.25,
+                  343.0 * np.exp(9.8 * (z - 12000.0) / (1004.0 * 213.0)))
+    rh = 100.0 * np.where(z <= 12000.0, 1.0 - 0.75 * (z / 12000.0) ** 1.25, 0.25)
+    b = oracle_lib.base_state(nk, c["zph"], c["jcb"].astype(np.float64), z, 0 * z, 0 * z, th, rh, 1e5)
+    b32 = oracle_lib.base_state(nk, c["zph"], c["jcb"].astype(np.float64), z, 0 * z, 0 * z, th, rh, 1e5,
+                                prec=32)
+    zph = c["zph"]
+    zs = 0.5 * (zph[1:nk] + zph[2:nk + 1])           # scalar levels k = 1..nk-1
+    pi, ptv = b["pibr"][1:nk], b["ptvbr"][1:nk]
+    slope = np.diff(pi) / np.diff(zs)
+    expect = -9.8 / (1004.0 * 0.5 * (ptv[1:] + ptv[:-1]))
+    assert np.allclose(slope[1:-1], expect[1:-1], rtol=2e-3)
+    for name in ("pbr", "ptbr", "rbr", "rcsq"):
+        r = b[name][1:]
+        assert np.abs(b32[name][1:] - r).max() <= 1e-5 * np.abs(r).max(), name
