@@ -119,6 +119,8 @@ def lib():
     L.cress_ensemble_set_graphs.argtypes = [vp, i]
     L.cress_autotune.argtypes = [vp, i, f, i, ctypes.POINTER(i), ctypes.POINTER(f)]
     L.cress_set_spin_limit.argtypes = [vp, i]
+    L.cress_get_fields_async.argtypes = [vp, i, i, ctypes.POINTER(i), ctypes.POINTER(_FP)]
+    L.cress_wait_fields.argtypes = [vp]
     dp = ctypes.POINTER(ctypes.c_double)
     L.cress_base_state.argtypes = [i, dp, dp, i, dp, i, i, ctypes.c_double, ctypes.c_double, dp, i]
     _lib = L
@@ -219,6 +221,20 @@ class Solver:
         assert a.shape == self.shape and a.dtype == np.float32 and a.flags.c_contiguous
         _check(lib().cress_get_field(self._h, FIELD_ID[name], level, fptr(a)))
         return a
+
+    def get_fields_async(self, level, names, outs):
+        """Start copying fields of one level into host arrays (see
+        cress_get_fields_async); they are filled after wait_fields().  The
+        arrays must stay alive (and preferably be page-locked) until then."""
+        for a in outs:
+            assert a.shape == self.shape and a.dtype == np.float32 and a.flags.c_contiguous
+        ids = (ctypes.c_int * len(names))(*[FIELD_ID[n] for n in names])
+        ptrs = (_FP * len(outs))(*[fptr(a) for a in outs])
+        self._async_keep = (ids, ptrs, list(outs))
+        _check(lib().cress_get_fields_async(self._h, int(level), len(names), ids, ptrs))
+
+    def wait_fields(self):
+        _check(lib().cress_wait_fields(self._h))
 
     def small_steps(self, nsstp, dts):
         _check(lib().cress_small_steps(self._h, int(nsstp), float(dts)))

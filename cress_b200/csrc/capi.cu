@@ -128,6 +128,12 @@ int Ctx::step(bool filter, float dtb, int nsstp, float dts) {
 
 Ctx::~Ctx() {
   cudaSetDevice(device);
+  if (copy_stream) {
+    cudaStreamSynchronize(copy_stream);
+    cudaStreamDestroy(copy_stream);
+  }
+  if (ev_out) cudaEventDestroy(ev_out);
+  if (ev_done) cudaEventDestroy(ev_done);
   free_graphs();
   free_learned();
   for (void* p : owned) cudaFree(p);
@@ -166,6 +172,51 @@ int Ctx::get_host(float* host, const float* src) {
   if ((rc = launch_repitch(src, g.px, stage_d, g.ni + 2, g.ni + 2, rows, stream))) return rc;
   ++launches;
   return cuda_check(cudaMemcpyAsync(host, stage_d, bytes, cudaMemcpyDeviceToHost, stream), "device->host copy");
+}
+
+// Asynchronous read-back of whole fields of one time level: the fields
+// are repitched on the context's stream into one host-layout buffer each
+// (kept until the next read-back), then copied to the host on a second
+// stream.  A later read-back waits for the previous copies before it
+// reuses the buffers; cress_wait_fields waits for them on the host.
+int Ctx::get_async(int level, int n, const int* fields, float* const* host) {
+  int rc;
+  if (!copy_stream) {
+    if ((rc = cuda_check(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "copy stream")) ||
+        (rc = cuda_check(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming), "event")) ||
+        (rc = cuda_check(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming), "event")))
+      return rc;
+  }
+  const long long rows = (long long)(g.nj + 2) * g.nk;
+  const size_t bytes = sizeof(float) * (size_t)(g.ni + 2) * (size_t)rows;
+  if (out_pending && (rc = cuda_check(cudaStreamWaitEvent(stream, ev_done, 0), "wait previous read-back")))
+    return rc;
+  for (int q = 0; q < n; ++q) {
+    const int f = fields[q];
+    if (!stage_out[f]) {
+      if ((rc = cuda_check(cudaMalloc(&stage_out[f], bytes), "cudaMalloc read-back buffer"))) return rc;
+      owned.push_back(stage_out[f]);
+    }
+    if ((rc = launch_repitch(lev[f][level], g.px, stage_out[f], g.ni + 2, g.ni + 2, rows, stream))) return rc;
+    ++launches;
+  }
+  if ((rc = cuda_check(cudaEventRecord(ev_out, stream), "record read-back")) ||
+      (rc = cuda_check(cudaStreamWaitEvent(copy_stream, ev_out, 0), "order read-back")))
+    return rc;
+  for (int q = 0; q < n; ++q)
+    if ((rc = cuda_check(cudaMemcpyAsync(host[q], stage_out[fields[q]], bytes, cudaMemcpyDeviceToHost, copy_stream),
+                         "device->host copy")))
+      return rc;
+  if ((rc = cuda_check(cudaEventRecord(ev_done, copy_stream), "record read-back done"))) return rc;
+  out_pending = true;
+  return CRESS_OK;
+}
+
+int Ctx::wait_async() {
+  if (!out_pending) return CRESS_OK;
+  int rc = cuda_check(cudaEventSynchronize(ev_done), "wait read-back");
+  if (!rc) out_pending = false;
+  return rc;
 }
 
 // Elimination factors of the w system for one dts (w_system_factors,
@@ -1146,6 +1197,26 @@ int cress_get_field(cress_ctx* ctx, int field, int level, float* host) {
   int rc = c->get_host(host, c->lev[field][level]);
   if (rc) return rc;
   rc = cuda_check(cudaStreamSynchronize(c->stream), "sync after device->host copy");
+  return rc ? rc : c->check_device_error();
+}
+
+int cress_get_fields_async(cress_ctx* ctx, int level, int nfield, const int* fields, float* const* host) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !fields || !host || nfield < 1 || nfield > CRESS_NFIELD)
+    return set_error(CRESS_E_ARG, "cress_get_fields_async: bad argument");
+  if (level < 0 || level > 3) return set_error(CRESS_E_ARG, "cress_get_fields_async: level %d", level);
+  for (int q = 0; q < nfield; ++q)
+    if (fields[q] < 0 || fields[q] >= CRESS_NFIELD || !c->lev[fields[q]][level] || !host[q])
+      return set_error(CRESS_E_ARG, "cress_get_fields_async: field %d not held or null buffer", fields[q]);
+  cudaSetDevice(c->device);
+  return c->get_async(level, nfield, fields, host);
+}
+
+int cress_wait_fields(cress_ctx* ctx) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c) return set_error(CRESS_E_ARG, "null context");
+  cudaSetDevice(c->device);
+  int rc = c->wait_async();
   return rc ? rc : c->check_device_error();
 }
 

@@ -52,6 +52,15 @@ struct Ctx {
   int stage();
   int put_host(float* dst, const float* host);
   int get_host(float* host, const float* src);
+  // asynchronous read-back (cress_get_fields_async): each field is
+  // repitched on `stream` into its own host-layout buffer, then copied to
+  // the host on copy_stream, so the copy overlaps later work on `stream`
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_out = nullptr, ev_done = nullptr;
+  float* stage_out[CRESS_NFIELD] = {};
+  bool out_pending = false;
+  int get_async(int level, int n, const int* fields, float* const* host);
+  int wait_async();
   int thomas_for(float dts, const ThomasSet** out);
   std::map<uint32_t, float*> level_tables;   // level table per 2*dtb (bits)
   int level_table(float dtb2, const float** out);

@@ -158,6 +158,18 @@ int cress_base_state(int nk, const double* zph, const double* jcb, int nlev, con
 int cress_put_field(cress_ctx* ctx, int field, int level, const float* host);
 int cress_get_field(cress_ctx* ctx, int field, int level, float* host);
 
+/* Asynchronous read-back of nfield fields of one time level into host
+ * arrays (reference layout; page-locked memory for the copies to overlap):
+ * the values are captured on the context's stream at this point of its
+ * work, and the device->host copies run on a second stream, so they
+ * overlap what the context does next (the next step's host->device copies
+ * and compute).  The host arrays are filled once cress_wait_fields returns;
+ * a later read-back first waits on the device for the previous one.  No
+ * counterpart in the reference (the dump writer reads the same arrays,
+ * SrcOrig/outdmp3d.f90:159-169). */
+int cress_get_fields_async(cress_ctx* ctx, int level, int nfield, const int* fields, float* const* host);
+int cress_wait_fields(cress_ctx* ctx);
+
 /* Acoustic small-step loop on the device-resident state: replaces the body
  * of s_smalldrv (SrcOrig/smalldrv.f90:343-398): future u, v, w, p' start
  * from the past level, then nsstp substeps of dts run with the forcing
