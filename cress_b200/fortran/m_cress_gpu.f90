@@ -152,6 +152,40 @@
           real(c_float), intent(in) :: cpx(*)
         end function cress_put_phase
 
+! The 1-D base state from a sounding, FP64 on the device (set1d, setbase,
+! baserho, sndwave).  sounding(nlev,5): height, u, v, theta or T, and
+! relative humidity or mixing ratio; columns(0:nk,11) in the order of the
+! C enum cress_base_col (ubr, vbr, pbr, ptbr, qvbr, rbr, ptvbr, pibr, rst,
+! rst8w, rcsq).  tvar and hvar are the characters of the reference's
+! sndtyp ('p'/'t', 'r'/'q') as c_int codes (ichar).
+        integer(c_int) function cress_base_state(nk, zph, jcb, nlev,    &
+     &    sounding, tvar, hvar, psnd0, thresq, columns, device)          &
+     &    bind(c, name='cress_base_state')
+          import :: c_int, c_double
+          integer(c_int), value :: nk, nlev, tvar, hvar, device
+          real(c_double), intent(in) :: zph(*), jcb(*), sounding(*)
+          real(c_double), value :: psnd0, thresq
+          real(c_double), intent(out) :: columns(*)
+        end function cress_base_state
+
+! Read-back of several fields of one level on a second stream; the host
+! arrays (fields(i) -> the i-th address in host) are filled once
+! cress_wait_fields returns.  Before a dump (SrcOrig/outdmp3d.f90:159-169).
+        integer(c_int) function cress_get_fields_async(ctx, level,      &
+     &    nfield, fields, host) bind(c, name='cress_get_fields_async')
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: level, nfield
+          integer(c_int), intent(in) :: fields(*)
+          type(c_ptr), intent(in) :: host(*)
+        end function cress_get_fields_async
+
+        integer(c_int) function cress_wait_fields(ctx)                  &
+     &    bind(c, name='cress_wait_fields')
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+        end function cress_wait_fields
+
         type(c_ptr) function cress_last_error()                         &
      &    bind(c, name='cress_last_error')
           import :: c_ptr
