@@ -83,7 +83,8 @@ def vspdmp(nk, zph, vspbar, botbar):
 def dry_steps(cfg, base, zph, past, now, nsteps, dtbig, dtsml, start=True, prec=32, fp64_solve=1,
               omp=False):
     """Run nsteps dry large steps (s_intgdrv) on the CPU; past/now are lists of
-    u, v, w, pp, ptp arrays, updated in place.  omp=True uses the OpenMP build."""
+    u, v, w, pp, ptp arrays (and tke last with tubopt=2), updated in place.
+    omp=True uses the OpenMP build."""
     L = lib(omp)
     L.oracle_dry_steps.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
@@ -99,7 +100,8 @@ def dry_steps(cfg, base, zph, past, now, nsteps, dtbig, dtsml, start=True, prec=
                                 cfg.get("botbar", 1e9), cfg.get("fc", 0.0), cfg.get("gwave", 20.0))
     z = np.ascontiguousarray(zph, np.float64)
     b = [np.ascontiguousarray(base[n], np.float32) for n in DRY_BASE_NAMES]
-    st = past + now
+    st = list(past) + list(now)
+    assert len(st) == (12 if cfg.get("tubopt", 0) == 2 else 10)
     for s in st:
         assert s.dtype == np.float32 and s.flags.c_contiguous
     rc = L.oracle_dry_steps(prec, io, ro, z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
@@ -117,7 +119,8 @@ MOIST_STATE_NAMES = STATE_NAMES + ["qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns
 def moist_steps(cfg, base, zph, past, now, prec, nsteps, dtbig, dtsml, start=True, prec_bits=32,
                 fp64_solve=1, omp=False):
     """Run nsteps moist (cphopt=3) large steps on the CPU.  past/now: lists of
-    14 arrays in MOIST_STATE_NAMES order, updated in place; prec: the
+    14 arrays in MOIST_STATE_NAMES order (15 with tke last when tubopt=2),
+    updated in place; prec: the
     5 x 2 x (nj+2) x (ni+2) precipitation planes (in/out).  Returns npstp
     of the last step's sedimentation."""
     L = lib(omp)
@@ -137,7 +140,7 @@ def moist_steps(cfg, base, zph, past, now, prec, nsteps, dtbig, dtsml, start=Tru
     z = np.ascontiguousarray(zph, np.float64)
     b = [np.ascontiguousarray(base[n], np.float32) for n in MOIST_BASE_NAMES]
     st = list(past) + list(now)
-    assert len(st) == 28
+    assert len(st) == (30 if cfg.get("tubopt", 0) == 2 else 28)
     for s in st:
         assert s.dtype == np.float32 and s.flags.c_contiguous
     assert prec.dtype == np.float32 and prec.flags.c_contiguous

@@ -215,7 +215,7 @@ void moist_scalar(MoistRun<R>& m, int n, R dtb) {
     smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 2, 2, nj - 2, 2, nk - 2, false, m.qfrc,
             r.t1, r.t2, r.t3);
   }
-  if (r.lo.tubopt == 1) turbs(o, r.b, sp, r.tw, m.qfrc);   // forceqv.f90:331-345, forceq.f90:438-452
+  if (r.lo.tubopt >= 1) turbs(o, r.b, sp, r.tw, m.qfrc);   // forceqv.f90:331-345, forceq.f90:438-452
   const char sw = isqv ? r.lo.vspvar[5] : r.lo.vspvar[6];
   if (r.lo.vspopt >= 1 && sw == 'o') {
     OMP_FOR for (int k = r.lo.ksp0 - 1; k <= nk - 2; ++k)
@@ -254,6 +254,7 @@ void intgdrv_moist(MoistRun<R>& m, R dtb, int nsstp, R dts, bool filter) {
   phase_forcing(r);
   phase_small(r, nsstp, dts);
   step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false, RV_PT, 0, &r.c.ptp);
+  if (r.lo.tubopt == 2) step_scalar(r, dtb, r.p.tke, r.tkefrc, r.f.tke, true);   // steps.f90:999-1014
   for (int n = 0; n < M_N; ++n) moist_scalar(m, n, dtb);
   m.npstp = cloudphy_fields(ni, nj, nk, o.dz, m.thresq, dtb, r.b.ptbr, r.b.rbr, r.b.pbr, r.b.jcb, r.b.rst,
                             r.p.ptp, r.p.pp, m.mp, r.f.ptp, m.mf, m.prec);

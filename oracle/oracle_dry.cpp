@@ -39,8 +39,19 @@ int run_dry(const int* io, const double* ro, const double* zph, const float* con
   for (int n = 0; n < 13; ++n) bl[n]->load(base[n]);
   std::vector<double> z(zph, zph + o.nk + 1);
   r.lo.ksp0 = vspdmp<R>(o, z, vspbar, botbar, r.rbct);
-  F3<R>* sl[] = {&r.p.u, &r.p.v, &r.p.w, &r.p.pp, &r.p.ptp, &r.c.u, &r.c.v, &r.c.w, &r.c.pp, &r.c.ptp};
-  for (int n = 0; n < 10; ++n) sl[n]->load(st[n]);
+  // st: past u, v, w, pp, ptp (+ tke with tubopt=2), then the present level
+  auto slots = [&]() {
+    std::vector<F3<R>*> v;
+    for (Level<R>* L : {&r.p, &r.c}) {
+      for (F3<R>* a : {&L->u, &L->v, &L->w, &L->pp, &L->ptp}) v.push_back(a);
+      if (r.lo.tubopt == 2) v.push_back(&L->tke);
+    }
+    return v;
+  };
+  {
+    const std::vector<F3<R>*> sl = slots();
+    for (size_t n = 0; n < sl.size(); ++n) sl[n]->load(st[n]);
+  }
   // slvstep.f90:176 nsstp; timeint.f90:160-190 half steps at the start
   const int nsstp = 20 * (int)(1.e2f * ((float)dtbig + .001f)) / (int)(1.e3f * ((float)dtsml + .0001f));
   for (int s = 0; s < nsteps; ++s) {
@@ -49,8 +60,8 @@ int run_dry(const int* io, const double* ro, const double* zph, const float* con
     const R dts = first ? R(.5) * R(dtsml) : R(dtsml);
     intgdrv_dry<R>(r, dtb, nsstp, dts, !first);   // no s_timeflt at ctime=0
   }
-  F3<R>* so[] = {&r.p.u, &r.p.v, &r.p.w, &r.p.pp, &r.p.ptp, &r.c.u, &r.c.v, &r.c.w, &r.c.pp, &r.c.ptp};
-  for (int n = 0; n < 10; ++n) so[n]->store(st[n]);
+  const std::vector<F3<R>*> so = slots();
+  for (size_t n = 0; n < so.size(); ++n) so[n]->store(st[n]);
   return 0;
 }
 
@@ -62,7 +73,8 @@ extern "C" {
 // ro: dx,dy,dz,weicoe,smhcoe,smvcoe,filcoe,vspbar,botbar,fc,gwave
 // zph: w-level heights, index k = 1..nk (entry 0 unused)
 // base: jcb,jcb8u,jcb8v,jcb8w,rbr,ptbr,rst,rst8u,rst8v,rst8w,rcsq,ubr,vbr
-// st (in/out): past u,v,w,pp,ptp then present u,v,w,pp,ptp
+// st (in/out): past u,v,w,pp,ptp then present u,v,w,pp,ptp; with tubopt=2
+//   each level's list ends with tke (12 arrays)
 int oracle_dry_steps(int prec, const int* io, const double* ro, const double* zph,
                      const float* const* base, float* const* st, int nsteps, double dtbig,
                      double dtsml, int start) {

@@ -77,6 +77,7 @@ int run_moist(const int* io, const double* ro, const double* zph, const float* c
   auto slots = [&](Level<R>& L, MoistLevel<R>& M, std::vector<F3<R>*>& v) {
     for (F3<R>* a : {&L.u, &L.v, &L.w, &L.pp, &L.ptp}) v.push_back(a);
     for (auto& a : M.q) v.push_back(&a);
+    if (r.lo.tubopt == 2) v.push_back(&L.tke);
   };
   std::vector<F3<R>*> sl;
   slots(r.p, m.mp, sl);
@@ -136,7 +137,8 @@ void oracle_satadjst(int ni, int nj, int nk, double thresq, const float* ptbr, c
 // io: ni,nj,nk,divopt,buyopt,fp64_solve,sthopt,smtopt,vspopt,coropt,tubopt,impopt,obc
 // ro: dx,dy,dz,weicoe,smhcoe,smvcoe,filcoe,vspbar,botbar,fc,thresq,gwave
 // base: jcb,jcb8u,jcb8v,jcb8w,rbr,ptbr,rst,rst8u,rst8v,rst8w,rcsq,ubr,vbr,pbr,qvbr
-// st (in/out): past u,v,w,pp,ptp,qv,qc,qr,qi,qs,qg,ni,ns,ng then present (28)
+// st (in/out): past u,v,w,pp,ptp,qv,qc,qr,qi,qs,qg,ni,ns,ng then present (28);
+//   with tubopt=2 each level's list ends with tke (30 arrays)
 // prec (in/out): 10 precipitation planes.  Returns the last npstp.
 int oracle_moist_steps(int prec_bits, const int* io, const double* ro, const double* zph,
                        const float* const* base, float* const* st, float* prec, int nsteps, double dtbig,

@@ -9,13 +9,14 @@
 
 namespace oracle {
 
-// Prognostic state of one time level.
+// Prognostic state of one time level (tke only with tubopt=2).
 template <class R>
 struct Level {
-  F3<R> u, v, w, pp, ptp;
-  void resize(int ni, int nj, int nk) {
+  F3<R> u, v, w, pp, ptp, tke;
+  void resize(int ni, int nj, int nk, bool with_tke) {
     u.resize(ni, nj, nk); v.resize(ni, nj, nk); w.resize(ni, nj, nk);
     pp.resize(ni, nj, nk); ptp.resize(ni, nj, nk);
+    if (with_tke) tke.resize(ni, nj, nk);
   }
 };
 
@@ -40,16 +41,18 @@ struct DryRun {
   TurbWork<R> tw;
   Radiation<R> rad;      // phase speeds of the open x boundaries (o.obc != 0)
   // scratch
-  F3<R> ufrc, vfrc, wfrc, pfrc, ptfrc, wc, rxu, rxv, rxw, t1, t2, t3, t4, t5, jxu, jxv, jxw;
+  F3<R> ufrc, vfrc, wfrc, pfrc, ptfrc, tkefrc, wc, rxu, rxv, rxw, t1, t2, t3, t4, t5, jxu, jxv, jxw;
   SmallScratch<R> ss;
   void alloc() {
     const int ni = o.ni, nj = o.nj, nk = o.nk;
-    p.resize(ni, nj, nk); c.resize(ni, nj, nk); f.resize(ni, nj, nk);
+    const bool tke = lo.tubopt == 2;
+    p.resize(ni, nj, nk, tke); c.resize(ni, nj, nk, tke); f.resize(ni, nj, nk, tke);
     for (F3<R>* a : {&ufrc, &vfrc, &wfrc, &pfrc, &ptfrc, &wc, &rxu, &rxv, &rxw, &t1, &t2, &t3, &t4,
                      &t5, &jxu, &jxv, &jxw})
       a->resize(ni, nj, nk);
+    if (tke) tkefrc.resize(ni, nj, nk);
     ss.resize(ni, nj, nk);
-    if (lo.tubopt == 1) tw.resize(ni, nj, nk);
+    if (lo.tubopt >= 1) tw.resize(ni, nj, nk);
     rad.resize(nj, nk);   // zero until the first s_phasev (a fresh start)
     o.rad = &rad;
   }
@@ -63,10 +66,13 @@ void forceuvw(DryRun<R>& r) {
   const Opts& o = r.o;
   const int ni = o.ni, nj = o.nj, nk = o.nk;
   r.ufrc.fill(R(0)); r.vfrc.fill(R(0)); r.wfrc.fill(R(0));
-  if (r.lo.tubopt == 1) {                                               // forceuvw.f90:423-431, turbdrv.f90:245-287
+  if (r.lo.tubopt >= 1) {                                               // forceuvw.f90:423-431, turbdrv.f90:245-287
     bruntv(o, r.tqv != nullptr, r.thresq, r.b, r.p.pp, r.p.ptp, r.tqv, r.tqall, r.tw);
     defomten(o, r.b, r.p.u, r.p.v, r.p.w, r.tw);
-    eddyvis(o, r.dtb_cur, r.b, r.tw);
+    if (r.lo.tubopt == 1)
+      eddyvis(o, r.dtb_cur, r.b, r.tw);
+    else
+      eddyvis_tke(o, r.dtb_cur, r.b, r.p.tke, r.tw);
     strsten(o, r.tw);
     turbuvw(o, r.b, r.tw, r.ufrc, r.vfrc, r.wfrc);
   }
@@ -136,7 +142,7 @@ void forcept(DryRun<R>& r) {
     smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 2, 2, nj - 2, 2, nk - 2, false,
             r.ptfrc, r.t1, r.t2, r.t3);
   }
-  if (r.lo.tubopt == 1) {                                               // forcept.f90:313-320, 383-393
+  if (r.lo.tubopt >= 1) {                                               // forcept.f90:313-320, 383-393
     F3<R>& pt = r.tw.ptv;   // free after bruntv: the full potential temperature at t-dt
     for (int k = 1; k <= nk - 1; ++k)
       for (int j = 1; j <= nj - 1; ++j)
@@ -158,12 +164,44 @@ void vbcs(const Opts& o, F3<R>& sf) {
     for (int i = 1; i <= ni - 1; ++i) sf(i, j, nk - 1) = sf(i, j, nk - 2);
 }
 
+// s_forcetke (SrcOrig/forcetke.f90:269-354, smtopt 0/2/3, no lateral
+// sponge): advs of the present TKE, shear production, 4th-order smoothing
+// of rbr*tkep, dissipation, eddyvisj + tkeflx + turbtke, vsps0 when
+// vspvar(10:10)='o', eddydif (the scalar diffusivities every later s_turbs
+// uses) and the buoyancy production.
+template <class R>
+void forcetke(DryRun<R>& r) {
+  const Opts& o = r.o;
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  advs(o, r.rxu, r.rxv, r.rxw, r.c.tke, r.tkefrc, r.t1, r.t2, r.t3);
+  sheartke(o, r.b, r.tw, r.tkefrc);
+  if (r.lo.smtopt % 10 == 2 || r.lo.smtopt % 10 == 3) {
+    for (int k = 1; k <= nk - 1; ++k)                                   // smoo4s.f90:184-197
+      for (int j = 0; j <= nj; ++j)
+        for (int i = 0; i <= ni; ++i) r.t4(i, j, k) = r.b.rbr(i, j, k) * r.p.tke(i, j, k);
+    smooth4(o, r.lo.smtopt, r.lo.smhcoe, r.lo.smvcoe, r.t4, 2, ni - 2, 2, nj - 2, 2, nk - 2, false,
+            r.tkefrc, r.t1, r.t2, r.t3);
+  }
+  disptke(o, r.b, r.tw, r.p.tke, r.tkefrc);
+  eddyvisj(o, r.b, r.tw);
+  turbtke(o, r.b, r.p.tke, r.tw, r.tkefrc);
+  if (r.lo.vspopt >= 1 && r.lo.vspvar[9] == 'o')                       // vsps0.f90:114-124
+    for (int k = r.lo.ksp0 - 1; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i)
+          r.tkefrc(i, j, k) =
+              r.tkefrc(i, j, k) - R(.5) * (r.rbct[k] + r.rbct[k + 1]) * r.b.rst(i, j, k) * r.p.tke(i, j, k);
+  eddydif_tke(o, r.b, r.tw);
+  buoytke(o, r.b, r.tw, r.tkefrc);
+}
+
 // Phases of one large step (s_intgdrv, intgdrv.f90:866-1119), split so
 // the moist step can interleave its own parts.
 template <class R>
 void phase_forcing(DryRun<R>& r) {   // s_forcedrv (forcedrv.f90:548-608)
   forceuvw(r);
   if (r.lo.tubopt == 1) eddydif(r.o, r.b, r.tw);   // forcedrv.f90:565-570
+  if (r.lo.tubopt == 2) forcetke(r);               // forcedrv.f90:576-592
   forcep(r);
   forcept(r);
 }
@@ -217,6 +255,13 @@ void phase_timeflt(DryRun<R>& r) {   // s_timeflt (timeflt.f90:335-404)
   timeflt_field(o, fc, ni - 1, nj - 1, nk, r.c.w, r.f.w, r.p.w);
   timeflt_field(o, fc, ni - 1, nj - 1, nk - 1, r.c.pp, r.f.pp, r.p.pp);
   timeflt_field(o, fc, ni - 1, nj - 1, nk - 1, r.c.ptp, r.f.ptp, r.p.ptp);
+  if (r.lo.tubopt == 2) {   // timeflt.f90:866-884: twice the coefficient for the TKE
+    const R fc2 = R(2) * fc, m1fc4 = R(1) - R(4) * fc;
+    for (int k = 1; k <= nk - 1; ++k)
+      for (int j = 1; j <= nj - 1; ++j)
+        for (int i = 1; i <= ni - 1; ++i)
+          r.c.tke(i, j, k) = m1fc4 * r.c.tke(i, j, k) + fc2 * (r.f.tke(i, j, k) + r.p.tke(i, j, k));
+  }
 }
 
 template <class R>
@@ -224,6 +269,7 @@ void phase_halo(DryRun<R>& r) {   // shift2nd on t and t+dt (intgdrv.f90:1005,10
   for (Level<R>* L : {&r.c, &r.f}) {
     halo_both(r.o, 'u', L->u); halo_both(r.o, 'v', L->v); halo_both(r.o, 's', L->w);
     halo_both(r.o, 's', L->pp); halo_both(r.o, 's', L->ptp);
+    if (r.lo.tubopt == 2) halo_both(r.o, 's', L->tke);
   }
 }
 
@@ -252,6 +298,7 @@ void intgdrv_dry(DryRun<R>& r, R dtb, int nsstp, R dts, bool filter) {
   phase_forcing(r);
   phase_small(r, nsstp, dts);
   step_scalar(r, dtb, r.p.ptp, r.ptfrc, r.f.ptp, false, RV_PT, 0, &r.c.ptp);
+  if (r.lo.tubopt == 2) step_scalar(r, dtb, r.p.tke, r.tkefrc, r.f.tke, true);   // steps.f90:999-1014
   if (filter) phase_timeflt(r);
   phase_halo(r);
   phasev_dry(r, dtb, dts);

@@ -1,5 +1,6 @@
-// Oracle: Smagorinsky turbulence (tubopt=1, isoopt=1) for flat terrain
-// without map factors (trnopt=0, mfcopt=0), no surface fluxes (sfcopt=0),
+// Oracle: Smagorinsky turbulence (tubopt=1) and the 1.5-order TKE closure
+// (tubopt=2), isoopt=1, for flat terrain without map factors (trnopt=0,
+// mfcopt=0), no surface fluxes (sfcopt=0),
 // periodic lateral boundaries on one process (iwest=ieast=jsouth=jnorth=0),
 // rigid bottom and top (bbc=tbc=2).
 //
@@ -16,6 +17,8 @@ struct TurbConst {
   static constexpr double tlow = 233.16;    // comphy.f90:100
   static constexpr double lv0 = 2.50078e6, lf0 = 3.34e5, t0 = 273.16;
   static constexpr double cw = 4.218e3, ci = 2.106e3;
+  static constexpr double ckm = .1, ckmin = 1.e-6;   // comphy.f90:341-344
+  static constexpr double eps = 1.e-20;              // commath.f90:177
 };
 
 template <class R>
@@ -204,6 +207,163 @@ void eddyvis(const Opts& o, R dtb, const Base<R>& b, TurbWork<R>& tw) {
         tw.rkv(i, j, k) = kv;
         tw.rkh(i, j, k) = kv;
       }
+}
+
+// s_eddyvis tubopt>=2 (the Deardorff form), isoopt=1, mfcopt=0, sfcopt=0
+// (SrcOrig/eddyvis.f90:448-481): the length scale l = l0 = (dx dy dz
+// jcb)^(1/3) in unstable air, else max(0.1 l0, min(0.76 sqrt(e/N^2), l0));
+// 1/Pr = 1 + 2 l/l0; rkv = rkh = rbr * min(K, ckmax l0^2) with
+// K = ckm l sqrt(e), raised to ckmin l0^2 where 1/Pr N^2 < ssq.  tke is the
+// past level.
+template <class R>
+void eddyvis_tke(const Opts& o, R dtb, const Base<R>& b, const F3<R>& tke, TurbWork<R>& tw) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  const R ds3 = R(o.dx) * R(o.dy) * R(o.dz);
+  const R ckmax = R(.125) / dtb;
+  const R oned3 = R(1) / R(3);
+  const R ckm = R(TurbConst::ckm), ckmin = R(TurbConst::ckmin), eps = R(TurbConst::eps);
+  for (int k = 1; k <= nk - 1; ++k)
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) {
+        const R ln0 = std::exp(oned3 * std::log(ds3 * b.jcb(i, j, k)));
+        const R ln02 = ln0 * ln0;
+        const R nsq = tw.nsq8w(i, j, k) + tw.nsq8w(i, j, k + 1);
+        const R e = tke(i, j, k);
+        R ln;
+        if (nsq < R(0))
+          ln = ln0;
+        else
+          ln = std::max(R(.1) * ln0, std::min(R(.76) * std::sqrt(e / (nsq + eps)), ln0));
+        const R priv = R(1) + R(2) * ln / ln0;
+        tw.priv(i, j, k) = priv;
+        R kv = ckm * ln * std::sqrt(e);
+        if (priv * nsq < tw.ssq(i, j, k)) kv = std::max(kv, ckmin * ln02);
+        kv = b.rbr(i, j, k) * std::min(kv, ckmax * ln02);
+        tw.rkv(i, j, k) = kv;
+        tw.rkh(i, j, k) = kv;
+      }
+}
+
+// s_sheartke, SrcOrig/sheartke.f90:112-120: shear production jcb rkv ssq
+// (rkv as s_eddyvis left it).
+template <class R>
+void sheartke(const Opts& o, const Base<R>& b, const TurbWork<R>& tw, F3<R>& tkefrc) {
+  for (int k = 2; k <= o.nk - 2; ++k)
+    for (int j = 2; j <= o.nj - 2; ++j)
+      for (int i = 2; i <= o.ni - 2; ++i)
+        tkefrc(i, j, k) = tkefrc(i, j, k) + b.jcb(i, j, k) * tw.rkv(i, j, k) * tw.ssq(i, j, k);
+}
+
+// s_disptke isoopt=1, mfcopt=0 (SrcOrig/disptke.f90:181-195): dissipation
+// (0.37/Pr - 0.18) rst e^1.5 / l, with l = (1/Pr - 1)(dx dy dz jcb / 8)^(1/3)
+// recovered from 1/Pr; tke is the past level.
+template <class R>
+void disptke(const Opts& o, const Base<R>& b, const TurbWork<R>& tw, const F3<R>& tke, F3<R>& tkefrc) {
+  const R ds308 = R(.125) * R(o.dx) * R(o.dy) * R(o.dz);
+  const R oned3 = R(1) / R(3);
+  for (int k = 2; k <= o.nk - 2; ++k)
+    for (int j = 2; j <= o.nj - 2; ++j)
+      for (int i = 2; i <= o.ni - 2; ++i) {
+        const R priv = tw.priv(i, j, k);
+        const R ln = (priv - R(1)) * std::exp(oned3 * std::log(ds308 * b.jcb(i, j, k))) + R(TurbConst::eps);
+        const R e = tke(i, j, k);
+        tkefrc(i, j, k) = tkefrc(i, j, k) - (R(.37) * priv - R(.18)) * b.rst(i, j, k) * e * std::sqrt(e) / ln;
+      }
+}
+
+// s_eddyvisj mfcopt=0 (SrcOrig/eddyvisj.f90:121-134): rkh, rkv divided by jcb.
+template <class R>
+void eddyvisj(const Opts& o, const Base<R>& b, TurbWork<R>& tw) {
+  for (int k = 1; k <= o.nk - 1; ++k)
+    for (int j = 1; j <= o.nj - 1; ++j)
+      for (int i = 1; i <= o.ni - 1; ++i) {
+        const R jcbiv = R(1) / b.jcb(i, j, k);
+        tw.rkh(i, j, k) = jcbiv * tw.rkh(i, j, k);
+        tw.rkv(i, j, k) = jcbiv * tw.rkv(i, j, k);
+      }
+}
+
+// s_tkeflx (SrcOrig/tkeflx.f90:251-462, trnopt=0, mfcopt=0) and s_turbtke
+// (SrcOrig/turbtke.f90:203-237): turbulent transport of the past-level
+// TKE with twice the momentum diffusivity (the 2/dx of the divergence),
+// added to tkefrc.
+template <class R>
+void turbtke(const Opts& o, const Base<R>& b, const F3<R>& tke, TurbWork<R>& tw, F3<R>& tkefrc) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  const R dxiv = R(1) / R(o.dx), dyiv = R(1) / R(o.dy), dziv = R(1) / R(o.dz);
+  const R dxv5 = R(.5) * dxiv, dyv5 = R(.5) * dyiv, dzv5 = R(.5) * dziv;
+  const R dxiv2 = R(2) * dxiv, dyiv2 = R(2) * dyiv, dziv2 = R(2) * dziv;
+  F3<R>& jt = tw.jcbs;
+  for (int k = 1; k <= nk - 1; ++k)
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) jt(i, j, k) = tke(i, j, k) * b.jcb(i, j, k);
+  for (int k = 1; k <= nk - 1; ++k) {
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 1; ++i)
+        tw.h1(i, j, k) = (tw.rkh(i - 1, j, k) + tw.rkh(i, j, k)) * (jt(i, j, k) - jt(i - 1, j, k)) * dxv5;
+    for (int j = 2; j <= nj - 1; ++j)
+      for (int i = 2; i <= ni - 2; ++i)
+        tw.h2(i, j, k) = (tw.rkh(i, j - 1, k) + tw.rkh(i, j, k)) * (jt(i, j, k) - jt(i, j - 1, k)) * dyv5;
+  }
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i)
+        tw.h3(i, j, k) = (tw.rkv(i, j, k - 1) + tw.rkv(i, j, k)) * (tke(i, j, k) - tke(i, j, k - 1)) * dzv5;
+  F3<R>&a = tw.tmp1, &c = tw.tmp2;
+  for (int k = 2; k <= nk - 2; ++k) {
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 1; ++i) a(i, j, k) = b.jcb8u(i, j, k) * tw.h1(i, j, k);
+    for (int j = 2; j <= nj - 1; ++j)
+      for (int i = 2; i <= ni - 2; ++i) c(i, j, k) = b.jcb8v(i, j, k) * tw.h2(i, j, k);
+  }
+  for (int k = 2; k <= nk - 2; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i)
+        tkefrc(i, j, k) = tkefrc(i, j, k) + ((tw.h3(i, j, k + 1) - tw.h3(i, j, k)) * dziv2 +
+                                             ((a(i + 1, j, k) - a(i, j, k)) * dxiv2 + (c(i, j + 1, k) - c(i, j, k)) * dyiv2));
+}
+
+// s_eddydif tubopt>=2, isoopt=1 (SrcOrig/eddydif.f90:265-284, 333-359) after
+// s_eddyvisj, and s_kh8uv mfcopt=0 (SrcOrig/kh8uv.f90:211-230): the scalar
+// diffusivities rkh = 1/Pr rkv (rkv already divided by jcb), rkh8u, rkh8v,
+// rkv8w (into rkv), and the half value 0.5 jcb rkh at scalar points
+// (rkv8s) that the buoyancy production uses.
+template <class R>
+void eddydif_tke(const Opts& o, const Base<R>& b, TurbWork<R>& tw) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  for (int k = 1; k <= nk - 1; ++k)
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) {
+        tw.rkv8s(i, j, k) = tw.priv(i, j, k) * tw.rkv(i, j, k);
+        tw.rkh(i, j, k) = tw.rkv8s(i, j, k);
+      }
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) tw.rkv(i, j, k) = R(.5) * (tw.rkv8s(i, j, k - 1) + tw.rkv8s(i, j, k));
+  for (int k = 1; k <= nk - 1; ++k)
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) tw.rkv8s(i, j, k) = R(.5) * b.jcb(i, j, k) * tw.rkv8s(i, j, k);
+  for (int k = 1; k <= nk - 1; ++k) {
+    for (int j = 1; j <= nj - 1; ++j)
+      for (int i = 2; i <= ni - 1; ++i) tw.rkh8u(i, j, k) = tw.rkh(i - 1, j, k) + tw.rkh(i, j, k);
+    for (int j = 2; j <= nj - 1; ++j)
+      for (int i = 1; i <= ni - 1; ++i) tw.rkh8v(i, j, k) = tw.rkh(i, j - 1, k) + tw.rkh(i, j, k);
+  }
+}
+
+// s_buoytke, SrcOrig/buoytke.f90:124-151: buoyancy production
+// -(b(k) + b(k+1)) with b(k) = jcb8w N^2(k) (rkv8s(k-1) + rkv8s(k)).
+template <class R>
+void buoytke(const Opts& o, const Base<R>& b, TurbWork<R>& tw, F3<R>& tkefrc) {
+  const int ni = o.ni, nj = o.nj, nk = o.nk;
+  F3<R>& t = tw.tmp1;
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i)
+        t(i, j, k) = b.jcb8w(i, j, k) * tw.nsq8w(i, j, k) * (tw.rkv8s(i, j, k - 1) + tw.rkv8s(i, j, k));
+  for (int k = 2; k <= nk - 2; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 2; i <= ni - 2; ++i) tkefrc(i, j, k) = tkefrc(i, j, k) - (t(i, j, k) + t(i, j, k + 1));
 }
 
 // s_strsten, SrcOrig/strsten.f90:150-262 (sfcopt=0): the stresses.
