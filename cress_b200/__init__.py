@@ -19,7 +19,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libcress_b200.so")
 
 # Field and level ids (include/cress_b200.h: enum cress_field / cress_level).
-FIELDS = ["u", "v", "w", "pp", "ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng"]
+FIELDS = ["u", "v", "w", "pp", "ptp", "qv", "qc", "qr", "qi", "qs", "qg", "ni", "ns", "ng", "tke"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 PAST, NOW, FUTURE, FORCING = 0, 1, 2, 3
 NTILES = 14   # HE-VI tile shapes (cress_cfg.tile)

@@ -17,6 +17,7 @@
 #include "hevi.cuh"
 #include "forcing.cuh"
 #include "openbc.cuh"
+#include "tke.cuh"
 #include "micro.cuh"
 #include "mlp_impl.cuh"
 #include "wsystem.h"
@@ -439,11 +440,12 @@ int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
 int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
   if (!base_set || !large_set)
     return set_error(CRESS_E_STATE, "cress_large_step: base state (set_base3d, set_base_large) not set");
-  if (cfg.advopt != 2 || !(cfg.tubopt == 0 || cfg.tubopt == 1) || !(cfg.cphopt == 0 || cfg.cphopt == 3) ||
+  if (cfg.advopt != 2 || cfg.tubopt < 0 || cfg.tubopt > 2 || !(cfg.cphopt == 0 || cfg.cphopt == 3) ||
       !(cfg.smtopt == 0 || cfg.smtopt % 10 == 2 || cfg.smtopt % 10 == 3) ||
       !(cfg.vspopt == 0 || cfg.vspopt == 2) || !(cfg.coropt == 0 || cfg.coropt == 1))
     return set_error(CRESS_E_UNSUPPORTED,
-                     "cress_large_step: needs advopt=2, tubopt 0/1, cphopt 0/3, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
+                     "cress_large_step: needs advopt=2, tubopt 0/1/2, cphopt 0/3, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
+  const bool tke = cfg.tubopt == 2;
   const bool moist = cfg.cphopt == 3;
   if (moist && !moist_set) return set_error(CRESS_E_STATE, "cress_large_step: moist base state not set");
   const int N = CRESS_NOW, P = CRESS_PAST, F = CRESS_FUTURE;
@@ -472,12 +474,17 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     f.qi = lev[CRESS_QI][N]; f.qs = lev[CRESS_QS][N]; f.qg = lev[CRESS_QG][N];
   }
   const float cpriv = 3.f;   // min(1/prnum, 3) with prnum = 0.33 (eddyvis.f90:219-222)
-  if (cfg.tubopt == 1) {
+  if (cfg.tubopt >= 1) {
     f.rkv = rkv_d;
+    // the theta' mixing stages the eddy viscosity (Smagorinsky) or the
+    // scalar diffusivity the TKE closure's s_eddydif leaves
+    f.rks = tke ? rks_d : rkv_d;
+    f.kdiv = tke ? 1 : 0;
     f.cpriv = cpriv;
   }
-  if (cfg.tubopt == 1 && phase != 2) {
-    // s_turbdrv up to s_eddyvis on the past level (forceuvw.f90:423-431)
+  if (cfg.tubopt >= 1 && phase != 2) {
+    // s_turbdrv up to s_eddyvis on the past level (forceuvw.f90:423-431);
+    // with the TKE closure also the per-point terms of s_forcetke
     TurbArgs t{};
     t.g = g;
     t.col = col_d;
@@ -493,6 +500,11 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     t.ckmax = .125f / dtb;
     t.cpriv = cpriv;
     t.thresq = cfg.thresq;
+    if (tke) {
+      t.tkep = lev[CRESS_TKE][P];
+      t.rks = rks_d; t.nsq = nsq_d; t.shr = shr_d; t.dsp = dsp_d;
+      t.ds308 = .125f * cfg.dx * cfg.dy * cfg.dz;   // disptke.f90:176
+    }
     if ((rc = launch_turb_visc(t, stream))) return set_error(rc, "eddy viscosity launch failed");
     ++launches;
   }
@@ -503,14 +515,36 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
                                   lev[CRESS_PP][P], lev[CRESS_PTP][P], f.rkv};
     ForceMaps fm;
     for (int sg = 0; sg < 2; ++sg)
-      for (int q = 0; q < force_nslots(sg, f.rkv != nullptr); ++q)
-        if ((rc = tmap(bufs[force_slot_buf(sg, q)], force_slot_rows(sg, q), &fm.m[sg][q]))) return rc;
+      for (int q = 0; q < force_nslots(sg, f.rkv != nullptr); ++q) {
+        const int b = force_slot_buf(sg, q);
+        const float* buf = (sg == 1 && b == FB_RKV) ? f.rks : bufs[b];   // the theta' mixing's field
+        if ((rc = tmap(buf, force_slot_rows(sg, q), &fm.m[sg][q]))) return rc;
+      }
     rc = launch_force(f, fm, stream);
     launches += 2;
     if (rc) return set_error(rc, "forcing launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   if (phase == 1) return CRESS_OK;   // an ensemble runs the small steps of all members next
   if (phase == 0 && (rc = small_steps(nsstp, dts))) return rc;
+  if (tke) {   // s_forcetke and the TKE part of s_steps (forcetke.f90:269-354, steps.f90:999-1014)
+    TkeArgs t{};
+    t.g = g;
+    t.lvl = f.lvl;
+    t.rks = rks_d; t.nsq = nsq_d; t.shr = shr_d; t.dsp = dsp_d;
+    t.tkef = lev[CRESS_TKE][F];
+    t.dxiv = f.dxiv; t.dyiv = f.dyiv; t.dziv = f.dziv;
+    t.smhcoe = cfg.smhcoe; t.smvcoe = cfg.smvcoe;
+    t.smtopt = cfg.smtopt; t.vspopt = cfg.vspopt; t.sthopt = cfg.sthopt; t.ksp0 = ksp0;
+    t.vsp_tke = on(9);
+    t.err = err_d;
+    TkeMaps tm;
+    if ((rc = tmap(lev[CRESS_TKE][N], TkeRows::s, &tm.s)) || (rc = tmap(lev[CRESS_TKE][P], TkeRows::s, &tm.sp)) ||
+        (rc = tmap(lev[CRESS_U][N], TkeRows::u, &tm.u)) || (rc = tmap(lev[CRESS_V][N], TkeRows::v, &tm.v)) ||
+        (rc = tmap(lev[CRESS_W][N], TkeRows::w, &tm.w)) || (rc = tmap(rkv_d, TkeRows::r, &tm.rkv)))
+      return rc;
+    if ((rc = launch_tke(t, tm, stream))) return set_error(rc, "TKE launch failed");
+    ++launches;
+  }
   if (moist) {
     MoistScalarArgs m{};
     m.g = g;
@@ -525,7 +559,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     m.smhcoe = cfg.smhcoe; m.smvcoe = cfg.smvcoe; m.dtb2 = f.dtb2;
     m.smtopt = cfg.smtopt; m.vspopt = cfg.vspopt; m.sthopt = cfg.sthopt; m.ksp0 = ksp0;
     m.vsp_qv = on(5); m.vsp_q = on(6);
-    m.rkv = f.rkv; m.cpriv = cpriv;
+    m.rkv = f.rks; m.cpriv = cpriv; m.kdiv = f.kdiv;
     m.err = err_d;
     m.lvl = f.lvl;
     MoistMaps mm;
@@ -565,6 +599,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     t.up = lev[CRESS_U][P]; t.vp = lev[CRESS_V][P]; t.wp = lev[CRESS_W][P];
     t.ppp = lev[CRESS_PP][P]; t.ptpp = lev[CRESS_PTP][P];
     t.filcoe = cfg.filcoe;
+    if (tke) { t.tke = lev[CRESS_TKE][N]; t.tkef = lev[CRESS_TKE][F]; t.tkep = lev[CRESS_TKE][P]; }
     if ((rc = launch_timeflt(t, stream))) return set_error(rc, "timeflt launch failed");
     ++launches;
   }
@@ -585,10 +620,13 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
   }
   HaloArgs h{};
   h.g = g;
-  const int nrot = moist ? 5 + kMoistN : 5;
-  int F5[5 + kMoistN] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP, CRESS_PTP};
-  int S5[5 + kMoistN] = {STAG_U, STAG_V, STAG_S, STAG_S, STAG_S};
+  // the rotated fields: u, v, w, p', theta' (RadVar order), the moist
+  // species, the TKE
+  int nrot = moist ? 5 + kMoistN : 5;
+  int F5[5 + kMoistN + 1] = {CRESS_U, CRESS_V, CRESS_W, CRESS_PP, CRESS_PTP};
+  int S5[5 + kMoistN + 1] = {STAG_U, STAG_V, STAG_S, STAG_S, STAG_S};
   for (int n = 0; n < kMoistN; ++n) { F5[5 + n] = CRESS_QV + n; S5[5 + n] = STAG_S; }
+  if (tke) { F5[nrot] = CRESS_TKE; S5[nrot] = STAG_S; ++nrot; }
   for (int lvl : {N, F})
     for (int n = 0; n < nrot; ++n) {
       h.f[h.n] = lev[F5[n]][lvl];
@@ -1005,7 +1043,7 @@ using namespace cress;
 extern "C" {
 
 const char* cress_last_error(void) { return g_last_error.c_str(); }
-int cress_abi_version(void) { return 3; }
+int cress_abi_version(void) { return 4; }
 
 int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   if (!cfg || !out) return set_error(CRESS_E_ARG, "cress_create: null argument");
@@ -1087,12 +1125,24 @@ int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
     delete c;
     return set_error(CRESS_E_UNSUPPORTED, "cphopt=%d: only 0 (dry) and 3 (cold rain) run on the GPU", cfg->cphopt);
   }
-  if (cfg->tubopt == 1) {
-    c->rkv_d = c->alloc_field();   // Smagorinsky eddy viscosity
+  if (cfg->tubopt == 1 || cfg->tubopt == 2) {
+    c->rkv_d = c->alloc_field();   // eddy viscosity
     if (!c->rkv_d) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the eddy viscosity failed"); }
   } else if (cfg->tubopt != 0) {
     delete c;
-    return set_error(CRESS_E_UNSUPPORTED, "tubopt=%d: only 0 and 1 (Smagorinsky) run on the GPU", cfg->tubopt);
+    return set_error(CRESS_E_UNSUPPORTED, "tubopt=%d: 0, 1 (Smagorinsky) and 2 (TKE) run on the GPU", cfg->tubopt);
+  }
+  if (cfg->tubopt == 2) {
+    // the TKE (three time levels, its forcing goes straight into s_steps)
+    // and the per-point fields of the closure
+    for (int l = 0; l < 3; ++l) c->lev[CRESS_TKE][l] = c->alloc_field();
+    c->rks_d = c->alloc_field();
+    c->nsq_d = c->alloc_field();
+    c->shr_d = c->alloc_field();
+    c->dsp_d = c->alloc_field();
+    bool ok = c->rks_d && c->nsq_d && c->shr_d && c->dsp_d;
+    for (int l = 0; l < 3; ++l) ok = ok && c->lev[CRESS_TKE][l];
+    if (!ok) { delete c; return set_error(CRESS_E_CUDA, "cudaMalloc of the TKE fields failed"); }
   }
   c->col_h.assign((size_t)C_NFIELDS_ALL * (cfg->nk + 1), 0.f);
   if ((rc = cuda_check(cudaMalloc(&c->col_d, sizeof(float) * c->col_h.size()), "cudaMalloc cols"))) {
@@ -1355,7 +1405,7 @@ int cress_put_precip(cress_ctx* ctx, const float* host) {
 // of levels k = 0..nk per side, host ucpx(1:nj,1:nk,1:2).
 static int phase_copy(Ctx* c, int field, float* host, const float* src_host, bool get) {
   if (!c->rad_d) return set_error(CRESS_E_STATE, "phase speeds: the context has periodic x boundaries");
-  if (field < 0 || field >= CRESS_NFIELD) return set_error(CRESS_E_ARG, "phase speeds: field %d", field);
+  if (field < 0 || field >= RAD_N) return set_error(CRESS_E_ARG, "phase speeds: field %d", field);
   const Grid& g = c->g;
   const size_t hw = sizeof(float) * (size_t)g.nj, dp = sizeof(float) * (size_t)(g.nj + 2);
   int rc = CRESS_OK;

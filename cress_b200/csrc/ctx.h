@@ -77,7 +77,14 @@ struct Ctx {
   bool moist_set = false;  // cress_set_base_moist was called
   float* prec_d = nullptr; // surface precipitation planes (10 x px*py)
   float* uspd_d = nullptr; // fall speeds (8 fields)
-  float* rkv_d = nullptr;  // Smagorinsky eddy viscosity (tubopt=1)
+  float* rkv_d = nullptr;  // eddy viscosity rbr*K at scalar points (tubopt 1 and 2)
+  // TKE closure (tubopt=2), written by the eddy-viscosity kernel from the
+  // past level: the scalar diffusivity 1/Pr*rkv/jcb, N^2 at w level k, and
+  // the shear production and dissipation of the TKE at scalar points
+  float* rks_d = nullptr;
+  float* nsq_d = nullptr;
+  float* shr_d = nullptr;
+  float* dsp_d = nullptr;
   int* dtp_d = nullptr;    // sedimentation sub-step minimum (float bits)
   int cloudphy(float dtb, float thresq);
   // learned microphysics (MLP in place of the process rates) and tuple

@@ -1,6 +1,6 @@
 // Large-step forcing for sm_100a: for every grid point the complete forcing
 // of s_forceuvw, s_forcep and s_forcept (advopt=2, smtopt=2/3, vspopt=2,
-// coropt=0/1, buyopt=1, gwmopt=0, tubopt=0/1 with isoopt=1, flat terrain)
+// coropt=0/1, buyopt=1, gwmopt=0, tubopt=0/1/2 with isoopt=1, flat terrain)
 // and the theta' step of s_steps, with the terms added in the reference's
 // order:
 //   ufrc/vfrc/wfrc = turbuvw + smoo4uvw + vspuvw + coriuv + buoywb + advuvw
@@ -345,7 +345,7 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
       if constexpr (T) {   // forcept.f90:313-320, 383-393: mixing of the full theta at t-dt
         auto RK = [&](int dx, int dy, int dz) { return X(5, dx, dy, dz); };
         auto SF = [&](int dx, int dy, int dz) { return C(C_PTBR, k + dz) + SP(dx, dy, dz); };
-        f = turb_scalar_at(f, C, k, a.cpriv, dxiv, dyiv, dziv, RK, SF);
+        f = turb_scalar_at(f, C, k, a.cpriv, a.kdiv, dxiv, dyiv, dziv, RK, SF);
       }
       if (a.vspopt >= 1 && a.vsp_pt && k >= a.ksp0 - 1)
         f = f - .5f * (C(C_RBCT, k) + C(C_RBCT, k + 1)) * C(C_RST, k) * SP(0, 0, 0);

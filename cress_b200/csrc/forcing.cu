@@ -28,6 +28,8 @@ __global__ void __launch_bounds__(256) k_timeflt(const FilterArgs a) {
     if (si && sj) {
       a.pp[id] = m1fc2 * a.pp[id] + fc * (a.ppf[id] + a.ppp[id]);
       a.ptp[id] = m1fc2 * a.ptp[id] + fc * (a.ptpf[id] + a.ptpp[id]);
+      if (a.tke)   // timeflt.f90:866-884: twice the coefficient for the TKE
+        a.tke[id] = (1.f - 4.f * a.filcoe) * a.tke[id] + (2.f * a.filcoe) * (a.tkef[id] + a.tkep[id]);
     }
   }
   if (si && sj) a.w[id] = m1fc2 * a.w[id] + fc * (a.wf[id] + a.wp[id]);

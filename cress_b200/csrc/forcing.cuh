@@ -67,10 +67,14 @@ struct ForceArgs {
   // moist buoyancy (buoywb.f90:202-299, cphopt != 0): qv and the five
   // hydrometeor mixing ratios at t; null qv = dry buoyancy
   const float* qv; const float* qc; const float* qr; const float* qi; const float* qs; const float* qg;
-  // Smagorinsky turbulence (tubopt=1): eddy viscosity at scalar points from
-  // k_turb_visc (null: no turbulence) and 1/Pr (capped at 3)
+  // turbulence (tubopt 1, 2): eddy viscosity at scalar points from
+  // k_turb_visc (null: no turbulence) and 1/Pr (capped at 3); rks: the
+  // field the theta' mixing stages (rkv, or with the TKE closure the scalar
+  // diffusivity 1/Pr*rkv/jcb, kdiv = 1)
   const float* rkv;
+  const float* rks;
   float cpriv;
+  int kdiv;
   int* err;                   // device error word (a bounded wait gave up)
 };
 
@@ -105,9 +109,12 @@ struct ForceMaps {
 
 int launch_force(const ForceArgs& a, const ForceMaps& maps, cudaStream_t st);
 
-// Smagorinsky eddy viscosity (s_turbdrv up to s_eddyvis: bruntv, defomten,
-// defomssq, eddyvis for tubopt=1, isoopt=1, flat terrain) from the past
-// level into rkv at the scalar points i, j = 1..n-1, k = 1..nk-1.
+// Eddy viscosity (s_turbdrv up to s_eddyvis: bruntv, defomten, defomssq,
+// eddyvis, isoopt=1, flat terrain) from the past level into rkv at the
+// scalar points i, j = 1..n-1, k = 1..nk-1: the Smagorinsky form
+// (tubopt=1), or the Deardorff form from the past TKE (tkep non-null,
+// tubopt=2), which also writes the TKE closure's fields rks, nsq, shr, dsp
+// (Ctx::rks_d ...).
 struct TurbArgs {
   Grid g;
   const float* col;
@@ -115,6 +122,9 @@ struct TurbArgs {
   const float *qvp, *qcp, *qrp, *qip, *qsp, *qgp;          // t-dt moist species (null: dry)
   float* rkv;
   float dxiv, dyiv, dziv, ds3, ckmax, cpriv, thresq;
+  const float* tkep;                                       // TKE at t-dt (tubopt=2) or null
+  float *rks, *nsq, *shr, *dsp;
+  float ds308;                                             // dx*dy*dz/8
 };
 int launch_turb_visc(const TurbArgs& a, cudaStream_t st);
 
@@ -132,8 +142,9 @@ struct MoistScalarArgs {
   float dxiv, dyiv, dziv, smhcoe, smvcoe, dtb2;
   int smtopt, vspopt, sthopt, ksp0;
   int vsp_qv, vsp_q;          // vspvar(6:6), vspvar(7:7)
-  const float* rkv;           // eddy viscosity (tubopt=1) or null
+  const float* rkv;           // staged viscosity (tubopt 1: rkv; 2: the diffusivity rks) or null
   float cpriv;
+  int kdiv;                   // 1: the staged field is already 1/Pr*rkv/jcb (TKE closure)
   int* err;                   // device error word (a bounded wait gave up)
 };
 
@@ -157,6 +168,7 @@ struct FilterArgs {
   const float* uf; const float* vf; const float* wf; const float* ppf; const float* ptpf;
   const float* up; const float* vp; const float* wp; const float* ppp; const float* ptpp;
   float filcoe;
+  float* tke; const float* tkef; const float* tkep;   // TKE (tubopt=2) or null
 };
 int launch_timeflt(const FilterArgs& a, cudaStream_t st);
 

@@ -3,7 +3,7 @@
 //   sfrc = advs (advs.f90:205-370, 4th-order horizontal, 2nd-order vertical)
 //        + smoo4qv / smoo4s of rbr*(qvp-qvbr) or rbr*sp (smoo4s.f90:184-296)
 //        + turbs of sp with the eddy diffusivity (forceqv.f90:331-345,
-//          forceq.f90:438-452; tubopt=1 only)
+//          forceq.f90:438-452; tubopt 1 and 2)
 //        + vspqv / vsps / vsps0 (vspqv.f90:181-198, vsps.f90:181-198, vsps0.f90:114-124)
 //   sf   = sp + sfrc*2dtb/rst, clipped at 0 for the mixing ratios
 //          (steps.f90:590-764), then vbcs at k = 1, nk-1 (vbcs.f90:116-132).
@@ -204,7 +204,7 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
         auto R = [&](int dx, int dy, int dz) {
           return dz == 0 ? pair_at(st0 + L::oR + oR + dy * BX, dx) : ld2(st(dz) + L::oR + oR);
         };
-        f = turb_scalar_at(f, C, k, a.cpriv, a.dxiv, a.dyiv, a.dziv, R, SPo);
+        f = turb_scalar_at(f, C, k, a.cpriv, a.kdiv, a.dxiv, a.dyiv, a.dziv, R, SPo);
       }
       const F2 spv = ld2(SP0);
       if (vsp && k >= a.ksp0 - 1) f = f - rbct5 * rst * (isqv ? spv - C(C_QVBR, k) : spv);

@@ -1,5 +1,5 @@
 // Stencil helpers shared by the large-step kernels (internal): the
-// 4th-order numerical smoothing and the Smagorinsky mixing of a scalar,
+// 4th-order numerical smoothing and the turbulent mixing of a scalar,
 // written over accessor functors so that every kernel that uses them forms
 // the same terms in the same order, whatever memory its neighbours come
 // from and whether it computes one point or a pair (F2).
@@ -42,17 +42,22 @@ __device__ __forceinline__ T smooth_tile(T frc, int smtopt, float smhcoe, float 
 }
 
 // Turbulent mixing of a scalar S (the full field at t-dt) at a point of
-// level k: s_eddydif / s_kh8uv diffusivities from the eddy
-// viscosity (rkh = priv*rkv/jcb, rkh8u = rkh(i-1)+rkh(i), rkv8w =
-// (rkh(k-1)+rkh(k))/2; eddydif.f90:154-260, kh8uv.f90:211-230) and the
-// flux divergence of s_turbflx / s_turbs (turbflx.f90:236-352,
-// turbs.f90:189-232), added to frc.
+// level k: s_eddydif / s_kh8uv diffusivities (rkh8u = rkh(i-1)+rkh(i),
+// rkv8w = (rkh(k-1)+rkh(k))/2; eddydif.f90:154-260, 319-340,
+// kh8uv.f90:211-230) and the flux divergence of s_turbflx / s_turbs
+// (turbflx.f90:236-352, turbs.f90:189-232), added to frc.  The scalar
+// diffusivity rkh at an offset is formed from the staged field R: the
+// Smagorinsky form rkh = cpriv*rkv/jcb from the eddy viscosity (kdiv = 0),
+// or, with the TKE closure, R is already 1/Pr*rkv/jcb (kdiv = 1).
 template <class T, class FC, class FR, class FS>
-__device__ __forceinline__ T turb_scalar_at(T frc, const FC& C, int k, float cpriv, float dxiv, float dyiv,
-                                            float dziv, const FR& R, const FS& S) {
-  // R(dx, dy, dz): eddy viscosity, S(dx, dy, dz): the scalar, at an offset
-  // from the point (only dz = -1, 0, 1 on the point's own column)
-  auto RKH = [&](int dx, int dy, int dz) { return cpriv * R(dx, dy, dz) * C(C_IJCB, k + dz); };
+__device__ __forceinline__ T turb_scalar_at(T frc, const FC& C, int k, float cpriv, int kdiv, float dxiv,
+                                            float dyiv, float dziv, const FR& R, const FS& S) {
+  // R(dx, dy, dz): the staged viscosity or diffusivity, S(dx, dy, dz): the
+  // scalar, at an offset from the point (only dz = -1, 0, 1 on the point's
+  // own column)
+  auto RKH = [&](int dx, int dy, int dz) {
+    return kdiv ? R(dx, dy, dz) : cpriv * R(dx, dy, dz) * C(C_IJCB, k + dz);
+  };
   const float jc = C(C_JCB, k);
   const float dxv05 = .5f * dxiv, dyv05 = .5f * dyiv;
   auto JS = [&](int dx, int dy) { return S(dx, dy, 0) * jc; };

@@ -61,7 +61,8 @@ typedef struct cress_cfg {
   int smtopt;           /* 0 none, 2 horizontal, 3 horizontal + vertical 4th-order smoothing */
   int vspopt;           /* 0 none, 2 Rayleigh damping above botbar toward the base state */
   int coropt;           /* 0 none, 1 f-plane Coriolis on u, v */
-  int tubopt;           /* 0 none, 1 Smagorinsky (isoopt=1, flat terrain, no surface flux) */
+  int tubopt;           /* 0 none, 1 Smagorinsky, 2 the 1.5-order TKE closure (isoopt=1, flat terrain,
+                           no surface flux; SrcOrig/eddyvis.f90, SrcOrig/forcetke.f90) */
   int cphopt;           /* 0 dry, 3 cold-rain bulk (haiopt=0) */
   float smhcoe, smvcoe; /* smoothing coefficients */
   float filcoe;         /* Asselin filter coefficient */
@@ -74,11 +75,12 @@ typedef struct cress_cfg {
 
 typedef struct cress_ctx cress_ctx;
 
-/* Fields addressed by the sync calls. */
+/* Fields addressed by the sync calls (CRESS_TKE, the turbulent kinetic
+ * energy tke/tkep of the reference, exists with tubopt=2 only). */
 enum cress_field {
   CRESS_U = 0, CRESS_V, CRESS_W, CRESS_PP, CRESS_PTP, CRESS_QV,
   CRESS_QC, CRESS_QR, CRESS_QI, CRESS_QS, CRESS_QG, CRESS_NI, CRESS_NS, CRESS_NG,
-  CRESS_NFIELD
+  CRESS_TKE, CRESS_NFIELD
 };
 /* Time levels: t-dt ("p" arrays: up, vp, ...), t (u, v, ...), t+dt ("f"). */
 enum cress_level { CRESS_PAST = 0, CRESS_NOW = 1, CRESS_FUTURE = 2, CRESS_FORCING = 3 };
