@@ -330,6 +330,55 @@ def squall_leg(args, rank):
             "max_w_after": diag["max_w"], "timing": "CUDA events on the library stream, graph replay"}
 
 
+def tke_leg(args, rank, plain_ms):
+    """The supercell workload with the 1.5-order TKE closure (tubopt=2, the
+    turbulence option of the reference's shipped configurations): the same
+    512 x 512 x 64 cold-rain domain, TKE starting from zero and spun up by
+    the warm-up steps; steps replayed from CUDA graphs, CUDA-event time on
+    the library's stream.  Reported beside the plain workload's step."""
+    import torch
+    import cress_b200
+    from cress_b200 import cases
+    nsstp = nsstp_of(args.dtbig, args.dtsml)
+    case = make_case(args.nx, args.ny, args.nz, args.dx, 100 + rank)
+    ni, nj, nk = case["dims"]
+    rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, case["botbar"])
+    s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, case["dz"], sthopt=1, tile=max(args.tile, 13),
+                          device=torch.cuda.current_device(), cphopt=3, tubopt=2)
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    s.set_base3d(case["base"])
+    s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
+    s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
+    init = list(case["level"]) + [case["moist"][n] for n in MOIST]
+    for n, a in zip(NAMES, init):
+        s.put_field(n, cress_b200.PAST, a)
+        s.put_field(n, cress_b200.NOW, a)
+    del case, init
+    s.large_step(0, 0.5 * args.dtbig, nsstp, 0.5 * args.dtsml)
+    s.set_graphs(True)
+    for _ in range(12 + args.warmup):   # an eager step and a capture per pointer state, then replays
+        s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+    s.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    tke = s.get_field("tke", cress_b200.NOW)[1:nk - 1, 2:nj - 1, 2:ni - 1]
+    diag = s.diagnostics(cress_b200.NOW, check=True)
+    s.set_stream(0)
+    s.close()
+    cells = args.nx * args.ny * args.nz
+    return {"grid": [args.nx, args.ny, args.nz], "tubopt": 2, "steps": args.steps, "ms_per_step": ms,
+            "cell_updates_per_s": cells / (ms * 1e-3), "plain_ms_per_step": plain_ms,
+            "tke_cost_ms": ms - plain_ms, "tke_max_m2s2": float(tke.max()),
+            "tke_active_frac": float((tke > 0).mean()), "max_w_after": diag["max_w"],
+            "timing": "CUDA events on the library stream, graph replay"}
+
+
 def ensemble_leg(args, rank):
     """Batched ensemble: `members` supercell domains of uneven size (nx, ny
     drawn from 96-192, nz = 48, dx = 1 km) with seeded bubble amplitude
@@ -439,6 +488,7 @@ def main():
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-squall", action="store_true")
+    ap.add_argument("--no-tke", action="store_true")
     ap.add_argument("--squall-nx", type=int, default=1024)
     ap.add_argument("--squall-ny", type=int, default=512)
     ap.add_argument("--members", type=int, default=32)
@@ -578,6 +628,7 @@ def main():
                                                         barrier, max_over_ranks, rank)
     ensemble = None if args.no_ensemble else ensemble_leg(args, rank)
     squall = None if args.no_squall else squall_leg(args, rank)
+    tke = None if args.no_tke else tke_leg(args, rank, ms / args.steps)
 
     # End to end through the public API with host buffers: every step the
     # past and present levels (14 fields each) go host->device from pinned
@@ -648,6 +699,7 @@ def main():
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
             "cpu_baseline": cpu, "learned": learned, "ensemble": ensemble, "squall_line": squall,
+            "tke_closure": tke,
             "budget": budget, "autotune": tune}))
     rep.close()
 

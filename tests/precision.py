@@ -71,14 +71,13 @@ def _vsp(oracle_lib, nk, zph, vspbar, botbar):
     return oracle_lib.vspdmp(nk, zph, vspbar, botbar)
 
 
-def _run_gpu(cress, case, names, s, nsteps, dtbig, dtsml, rbct, ksp0, moist):
+def _run_gpu(cress, case, names, init, s, nsteps, dtbig, dtsml, rbct, ksp0, moist):
     from cress_b200 import cases
     ni, nj, nk = case["dims"]
     s.set_base3d(case["base"])
     s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
     if moist:
         s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
-    init = list(case["level"]) + ([case["moist"][n] for n in names[5:]] if moist else [])
     for n, a in zip(names, init):
         s.put_field(n, cress.PAST, a)
         s.put_field(n, cress.NOW, a)
@@ -94,15 +93,24 @@ def _run_gpu(cress, case, names, s, nsteps, dtbig, dtsml, rbct, ksp0, moist):
     return out, prec, diag
 
 
-def moist_study(cress, oracle_lib, case, dx, nsteps, dtbig, dtsml, obc=0, label="supercell"):
-    """Cold-rain (cphopt=3) run of `nsteps` large steps; returns the report."""
+def _tke0(case):
+    """Zero TKE (a fresh start of the TKE closure)."""
+    ni, nj, nk = case["dims"]
+    return np.zeros((nk, nj + 2, ni + 2), np.float32)
+
+
+def moist_study(cress, oracle_lib, case, dx, nsteps, dtbig, dtsml, obc=0, label="supercell", tubopt=0):
+    """Cold-rain (cphopt=3) run of `nsteps` large steps; returns the report.
+    tubopt=2 adds the TKE closure, starting from zero TKE, and the TKE to
+    the report's fields."""
     ni, nj, nk = case["dims"]
     dz, zph = case["dz"], case["zph"]
     vspbar, botbar = 0.005, 0.6 * zph[nk - 1]
     rbct, ksp0 = _vsp(oracle_lib, nk, zph, vspbar, botbar)
     cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=1, smtopt=3, vspopt=2, coropt=0,
-               vspbar=vspbar, botbar=botbar, thresq=1e-12, obc=obc, gwave=20.0)
-    init = list(case["level"]) + [case["moist"][n] for n in MOIST[5:]]
+               vspbar=vspbar, botbar=botbar, thresq=1e-12, obc=obc, gwave=20.0, tubopt=tubopt)
+    names = MOIST + (["tke"] if tubopt == 2 else [])
+    init = list(case["level"]) + [case["moist"][n] for n in MOIST[5:]] + ([_tke0(case)] if tubopt == 2 else [])
     runs = {}
     for bits in (64, 32):
         past = [a.copy() for a in init]
@@ -111,8 +119,8 @@ def moist_study(cress, oracle_lib, case, dx, nsteps, dtbig, dtsml, obc=0, label=
         oracle_lib.moist_steps(cfg, case["base"], zph, past, now, prec, nsteps, dtbig, dtsml, start=True,
                                prec_bits=bits, omp=True)
         runs[bits] = (now, prec)
-    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, cphopt=3, thresq=1e-12, obc=obc, gwave=20.0)
-    gpu, gprec, diag = _run_gpu(cress, case, MOIST, s, nsteps, dtbig, dtsml, rbct, ksp0, True)
+    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, cphopt=3, thresq=1e-12, obc=obc, gwave=20.0, tubopt=tubopt)
+    gpu, gprec, diag = _run_gpu(cress, case, names, init, s, nsteps, dtbig, dtsml, rbct, ksp0, True)
 
     i0 = 1 if obc else 2   # open x: the boundary columns are prognostic too
     sl = interior(ni, nj, nk, i0)
@@ -120,7 +128,7 @@ def moist_study(cress, oracle_lib, case, dx, nsteps, dtbig, dtsml, obc=0, label=
     o32, o32_prec = runs[32]
     rep = {"case": label, "grid": [ni - 3, nj - 3, nk - 3], "dx_m": dx, "open_x": obc, "steps": nsteps,
            "dtbig_s": dtbig, "simulated_s": nsteps * dtbig,
-           "fields": field_stats(MOIST, gpu, ref, o32, sl), "max_w_gpu": diag["max_w"]}
+           "tubopt": tubopt, "fields": field_stats(names, gpu, ref, o32, sl), "max_w_gpu": diag["max_w"]}
     acc = {k: float(v[:, 1, 2:nj - 1, i0:ni - 1].astype(np.float64).sum())
            for k, v in (("gpu", gprec), ("fp64", ref_prec), ("fp32", o32_prec))}
     rep["precip_accum_kg_m2"] = acc
@@ -136,25 +144,28 @@ def moist_study(cress, oracle_lib, case, dx, nsteps, dtbig, dtsml, obc=0, label=
 
 
 def dry_study(cress, oracle_lib, case, dx, dz, nsteps, dtbig, dtsml, tubopt=1, sthopt=0, label="dry"):
-    """Dry (cphopt=0) run of `nsteps` large steps; returns the report."""
+    """Dry (cphopt=0) run of `nsteps` large steps; returns the report.
+    tubopt=2 (the TKE closure) starts from zero TKE and reports the TKE."""
     ni, nj, nk = case["dims"]
     zph = case["zph"]
     rbct, ksp0 = _vsp(oracle_lib, nk, zph, case["vspbar"], case["botbar"])
     cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=sthopt, smtopt=3, vspopt=2, coropt=0,
                vspbar=case["vspbar"], botbar=case["botbar"], tubopt=tubopt, impopt=1)
+    names = DRY + (["tke"] if tubopt == 2 else [])
+    init = list(case["level"]) + ([_tke0(case)] if tubopt == 2 else [])
     runs = {}
     for bits in (64, 32):
-        past = [a.copy() for a in case["level"]]
-        now = [a.copy() for a in case["level"]]
+        past = [a.copy() for a in init]
+        now = [a.copy() for a in init]
         oracle_lib.dry_steps(cfg, case["base"], zph, past, now, nsteps, dtbig, dtsml, start=True, prec=bits,
                              omp=True)
         runs[bits] = now
     s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=sthopt, tubopt=tubopt)
-    gpu, _, diag = _run_gpu(cress, case, DRY, s, nsteps, dtbig, dtsml, rbct, ksp0, False)
+    gpu, _, diag = _run_gpu(cress, case, names, init, s, nsteps, dtbig, dtsml, rbct, ksp0, False)
     sl = interior(ni, nj, nk)
     rep = {"case": label, "grid": [ni - 3, nj - 3, nk - 3], "dx_m": dx, "dz_m": dz, "steps": nsteps,
            "dtbig_s": dtbig, "nsstp": nsstp_of(dtbig, dtsml), "simulated_s": nsteps * dtbig,
-           "fields": field_stats(DRY, gpu, runs[64], runs[32], sl), "max_w_gpu": diag["max_w"]}
+           "tubopt": tubopt, "fields": field_stats(names, gpu, runs[64], runs[32], sl), "max_w_gpu": diag["max_w"]}
     m0 = dry_mass(case, case["level"], dx, dz)
     for key, f in (("gpu", gpu), ("fp64", runs[64]), ("fp32", runs[32])):
         rep[f"mass_drift_{key}"] = (dry_mass(case, f, dx, dz) - m0) / m0

@@ -16,6 +16,10 @@ path against the oracle's FP64 and FP32 builds, field by field.
   (128x16x36, dx = 500 m; the frame moves at 16 m/s, umove, so the line
   stays inside the 64 km domain while its convection peaks at ~30 m/s).
 
+The reference's shipped configurations run the 1.5-order TKE closure
+(tubopt=2); C1 and C2 are also run with it, from zero TKE, with the TKE
+among the checked fields.
+
 Per-field tolerance (stated here, checked on every field): the GPU's RMS
 difference from the FP64 build, relative to the field's FP64 RMS, must be
 within K times the FP32 oracle's own spread from FP64 plus a floor:
@@ -66,6 +70,33 @@ def test_c1_dry_warm_bubble_300s(cress, oracle_lib):
     assert rep["nsstp"] == 16
     _check_fields(rep, 3.0)
     _check_budgets(rep, ("mass",))
+
+
+def test_c1_dry_warm_bubble_300s_tke(cress, oracle_lib):
+    from cress_b200 import cases
+    dx, dz = 500.0, 300.0
+    case = cases.dry_case(64, 64, 40, dx, dz, sthopt=0, seed=11, ptp0=2.0, rad=(2000.0, 2000.0, 2000.0),
+                          u0=0.0, shear=0.0, vspbar=0.005, botbar=9000.0, noise=0.01, dthdz=0.0)
+    rep = P.dry_study(cress, oracle_lib, case, dx, dz, 150, 2.0, 0.25, tubopt=2, sthopt=0,
+                      label="dry warm bubble 64x64x40, 300 s, TKE closure")
+    print(json.dumps({"named_config": rep}))
+    assert rep["fields"]["tke"]["fp64_rms"] > 0.0   # the closure is active
+    _check_fields(rep, 3.0)
+    _check_budgets(rep, ("mass",))
+
+
+def test_c2_supercell_2h_tke(cress, oracle_lib):
+    from cress_b200 import cases
+    dx = 1000.0
+    case = cases.supercell_case(40, 40, 40, dx, ztop=12000.0, seed=12, cloud=True,
+                                rad=(6000.0, 6000.0, 1400.0))
+    rep = P.moist_study(cress, oracle_lib, case, dx, 1440, 5.0, 1.0, tubopt=2,
+                        label="supercell 40x40x40, 2 h, TKE closure")
+    print(json.dumps({"named_config": rep}))
+    assert rep["fields"]["tke"]["fp64_rms"] > 0.0
+    _check_fields(rep, 4.0)
+    assert rep["precip_rel_diff_gpu"] < 0.05
+    _check_budgets(rep)
 
 
 def test_c2_supercell_2h(cress, oracle_lib):
