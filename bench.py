@@ -163,8 +163,10 @@ class CpuMoist:
         case = make_case(nx, ny, args.nz, args.dx, 3)
         ni, nj, nk = case["dims"]
         self.cfg = dict(ni=ni, nj=nj, nk=nk, dx=args.dx, dy=args.dx, dz=case["dz"], sthopt=1, smtopt=3,
-                        vspopt=2, coropt=0, vspbar=VSPBAR, botbar=case["botbar"])
+                        vspopt=2, coropt=0, vspbar=VSPBAR, botbar=case["botbar"], tubopt=args.tubopt)
         init = list(case["level"]) + [case["moist"][n] for n in MOIST]
+        if args.tubopt == 2:
+            init.append(np.zeros_like(init[0]))   # TKE from zero
         self.past = [a.copy() for a in init]
         self.now = [a.copy() for a in init]
         self.base, self.zph = case["base"], case["zph"]
@@ -489,6 +491,8 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-squall", action="store_true")
     ap.add_argument("--no-tke", action="store_true")
+    ap.add_argument("--tubopt", type=int, default=0, choices=[0, 1, 2],
+                    help="turbulence of the main workload: 0 none, 1 Smagorinsky, 2 TKE closure")
     ap.add_argument("--squall-nx", type=int, default=1024)
     ap.add_argument("--squall-ny", type=int, default=512)
     ap.add_argument("--members", type=int, default=32)
@@ -518,7 +522,7 @@ def main():
                             f"18 km, dtbig={args.dtbig:g} s, dtsml={args.dtsml:g} s; analytic "
                             f"sounding, quarter-circle hodograph, +3 K bubble, seeded cloud field",
                 "nx": args.nx, "ny": args.ny, "nz": args.nz, "nsstp": nsstp,
-                "microphysics": "plain (cold-rain bulk)",
+                "microphysics": "plain (cold-rain bulk)", "tubopt": args.tubopt,
                 "l2": "inputs larger than L2 (each field 72 MB at 512x512x64)",
                 "parallelism": f"replicas{max(world, args.gpus)}"}
     cells = args.nx * args.ny * args.nz
@@ -560,7 +564,7 @@ def main():
     ni, nj, nk = case["dims"]
     rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, case["botbar"])
     s = cress_b200.Solver(ni, nj, nk, args.dx, args.dx, case["dz"], sthopt=1, tile=max(args.tile, 0), impopt=args.impopt,
-                          device=local, cphopt=3)
+                          device=local, cphopt=3, tubopt=args.tubopt)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     s.set_stream(stream.cuda_stream)
@@ -568,7 +572,11 @@ def main():
     s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
     s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
     init = list(case["level"]) + [case["moist"][n] for n in MOIST]
-    for n, a in zip(NAMES, init):
+    names = NAMES
+    if args.tubopt == 2:   # the TKE from zero, a prognostic field like the others
+        init.append(np.zeros_like(init[0]))
+        names = NAMES + ["tke"]
+    for n, a in zip(names, init):
         s.put_field(n, cress_b200.PAST, a)
         s.put_field(n, cress_b200.NOW, a)
     s.sync()
@@ -642,13 +650,13 @@ def main():
     out_h = [[pin(np.empty_like(a)) for a in init] for _ in range(2)]
 
     def e2e_step(i):
-        for n, a, b in zip(NAMES, past_h, now_h):
+        for n, a, b in zip(names, past_h, now_h):
             s.put_field(n, cress_b200.PAST, a)
             s.put_field(n, cress_b200.NOW, b)
         s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
         if i > 0:
             s.wait_fields()   # step i-1's result is on the host
-        s.get_fields_async(cress_b200.NOW, NAMES, out_h[i % 2])
+        s.get_fields_async(cress_b200.NOW, names, out_h[i % 2])
 
     for i in range(args.warmup):
         e2e_step(i)

@@ -14,8 +14,9 @@
 //   tkef   = max(0, tkep + tkefrc 2dtb/rst)      (steps.f90:999-1014), then vbcs.
 // The shear and dissipation terms, N^2 and the scalar diffusivity come
 // per point from k_turb_visc (rks, nsq, shr, dsp); they are read on the
-// thread's own columns, N^2 and the diffusivity of levels k-1 .. k+1
-// carried in registers as the march goes up.
+// thread's own columns one level ahead of their use, N^2 and the
+// diffusivity of levels k-1 .. k+1 carried in registers as the march goes
+// up.
 //
 // Design (2.5-D), as the moist scalar kernel: a block owns a 32 x 8 tile
 // of columns and marches k upward; one elected thread issues TMA boxes of
@@ -124,12 +125,18 @@ __global__ void __launch_bounds__(kTkePairs * kScalarTY) k_tke(const __grid_cons
   const int oS = (ty + 2) * BX + ox, oR = (ty + 1) * BX + ox;
   const long long plane = g.plane;
   long long id = g.at(i, j, 2);
-  // per-point fields of levels k-1 .. k+1 on the own columns (registers)
+  // per-point fields of levels k-1 .. k+1 on the own columns (registers),
+  // each loaded one level ahead of its use
   F2 r8m = f2(0.f), r80 = f2(0.f), nq0 = f2(0.f);
+  F2 shr_n = f2(0.f), dsp_n = f2(0.f), r8p_n = f2(0.f), nq1_n = f2(0.f);
   if (ownA) {
     r8m = ldg2(a.rks + id - plane);
     r80 = ldg2(a.rks + id);
     nq0 = ldg2(a.nsq + id);
+    shr_n = ldg2(a.shr + id);
+    dsp_n = ldg2(a.dsp + id);
+    r8p_n = ldg2(a.rks + id + plane);
+    nq1_n = ldg2(a.nsq + id + plane);
   }
   auto slot_ptr = [&](int lv) { return ring + ((lv - 1 + S) % S) * L::stage; };
   const float* stp[5] = {slot_ptr(0), slot_ptr(1), slot_ptr(2), slot_ptr(3), slot_ptr(4)};
@@ -152,8 +159,13 @@ __global__ void __launch_bounds__(kTkePairs * kScalarTY) k_tke(const __grid_cons
       const float* SP0 = st0 + L::oSP + oS;
       const float* U = st0 + L::oU + oU;
       const float* V = st0 + L::oV + oV;
-      const F2 shr = ldg2(a.shr + id), dsp = ldg2(a.dsp + id);
-      const F2 r8p = ldg2(a.rks + id + plane), nq1 = ldg2(a.nsq + id + plane);
+      const F2 shr = shr_n, dsp = dsp_n, r8p = r8p_n, nq1 = nq1_n;
+      if (k + 1 <= nk - 2) {   // the next level's
+        shr_n = ldg2(a.shr + id + plane);
+        dsp_n = ldg2(a.dsp + id + plane);
+        r8p_n = ldg2(a.rks + id + 2 * plane);
+        nq1_n = ldg2(a.nsq + id + 2 * plane);
+      }
 
       // advs.f90:205-370 with the fluxes of rstuvwc.f90:172-210
       const float r8u = C(C_RST8U, k), r8v = C(C_RST8V, k);
