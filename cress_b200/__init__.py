@@ -121,6 +121,10 @@ def lib():
     L.cress_set_spin_limit.argtypes = [vp, i]
     L.cress_get_fields_async.argtypes = [vp, i, i, ctypes.POINTER(i), ctypes.POINTER(_FP)]
     L.cress_wait_fields.argtypes = [vp]
+    ll = ctypes.c_longlong
+    L.cress_dump_3d.argtypes = [vp, i, ctypes.c_char_p, vp, ll, ctypes.POINTER(ll), ctypes.c_char_p, i]
+    L.cress_restart_write.argtypes = [vp, vp, ll, ctypes.POINTER(ll)]
+    L.cress_restart_read.argtypes = [vp, vp, ll]
     dp = ctypes.POINTER(ctypes.c_double)
     L.cress_base_state.argtypes = [i, dp, dp, i, dp, i, i, ctypes.c_double, ctypes.c_double, dp, i]
     _lib = L
@@ -235,6 +239,39 @@ class Solver:
 
     def wait_fields(self):
         _check(lib().cress_wait_fields(self._h))
+
+    def dump_3d(self, dmpvar, level=NOW):
+        """The 3-D dump records of one level as s_outdmp writes them (dmplev
+        = 1, dmpfmt = 2; see cress_dump_3d): returns (records, names) with
+        records a float32 array (nvar, nz, ny, nx) whose bytes are the .bin
+        file, names the dumped variables in file order."""
+        L = lib()
+        n = ctypes.c_longlong()
+        names = ctypes.create_string_buffer(512)
+        _check(L.cress_dump_3d(self._h, int(level), dmpvar.encode(), None, 0, ctypes.byref(n), names, 512))
+        vs = [v for v in names.value.decode().split(",") if v]
+        nk, nj2, ni2 = self.shape
+        out = np.empty((len(vs), nk - 3, nj2 - 5, ni2 - 5), np.float32)
+        if vs:
+            _check(L.cress_dump_3d(self._h, int(level), dmpvar.encode(), out.ctypes.data_as(ctypes.c_void_p),
+                                   out.nbytes, ctypes.byref(n), None, 0))
+        assert n.value == out.nbytes
+        return out, vs
+
+    def restart_write(self):
+        """The device-held restart records (cress_restart_write) as bytes."""
+        L = lib()
+        n = ctypes.c_longlong()
+        _check(L.cress_restart_write(self._h, None, 0, ctypes.byref(n)))
+        out = np.empty(n.value, np.uint8)
+        _check(L.cress_restart_write(self._h, out.ctypes.data_as(ctypes.c_void_p), out.nbytes, ctypes.byref(n)))
+        return out
+
+    def restart_read(self, data):
+        """Restore the device state from restart records (cress_restart_read)."""
+        a = np.ascontiguousarray(np.frombuffer(data, np.uint8) if not isinstance(data, np.ndarray) else data,
+                                 np.uint8)
+        _check(lib().cress_restart_read(self._h, a.ctypes.data_as(ctypes.c_void_p), a.nbytes))
 
     def small_steps(self, nsstp, dts):
         _check(lib().cress_small_steps(self._h, int(nsstp), float(dts)))

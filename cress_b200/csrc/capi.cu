@@ -137,6 +137,7 @@ Ctx::~Ctx() {
   if (ev_done) cudaEventDestroy(ev_done);
   free_graphs();
   free_learned();
+  if (rec_d) cudaFree(rec_d);
   for (void* p : owned) cudaFree(p);
   if (own_stream) cudaStreamDestroy(own_stream);
 }

@@ -61,6 +61,10 @@ struct Ctx {
   bool out_pending = false;
   int get_async(int level, int n, const int* fields, float* const* host);
   int wait_async();
+  // byte stream of the dump and restart records (records.cu), kept and
+  // grown as needed
+  void* rec_d = nullptr;
+  long long rec_bytes = 0;
   int thomas_for(float dts, const ThomasSet** out);
   std::map<uint32_t, float*> level_tables;   // level table per 2*dtb (bits)
   int level_table(float dtb2, const float** out);

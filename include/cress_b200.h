@@ -172,6 +172,35 @@ int cress_get_field(cress_ctx* ctx, int field, int level, float* host);
 int cress_get_fields_async(cress_ctx* ctx, int level, int nfield, const int* fields, float* const* host);
 int cress_wait_fields(cress_ctx* ctx);
 
+/* Dump file records formed on the device: the 3-D history dump of one
+ * time level as s_outdmp / s_outdmp3d write it for dmplev = 1 and
+ * dmpfmt = 2 (SrcOrig/outdmp.f90:380-870, SrcOrig/outdmp3d.f90:159-238):
+ * for each variable dmpvar selects, in s_outdmp's order, the records
+ * k = 2..nk-2 of nx*ny native floats (i fastest), staggered variables
+ * averaged to scalar points, 'o' adding the base state before the
+ * perturbation (ubar, u, vbar, v, w, pbar, pp, ptbar, ptp, qvbar, qv), '-'
+ * giving the total or the field alone (u, v, p, pt, qv), cold rain adding
+ * qc qr qi qs qg (dmpvar(7:7)='o') and nci ncs ncg (dmpvar(8:8)='o'), the
+ * TKE closure tke (dmpvar(12:12)='o').  The bytes are the .bin file.
+ *   host null: only *nbytes and names are set (the size query);
+ *   names (optional): the dumped variables, comma-separated.
+ * pbar and p need the base pressure (cress_set_base_moist).  The maximum
+ * wind (dmpvar(12:12) '+' or '-') is rejected with CRESS_E_UNSUPPORTED. */
+int cress_dump_3d(cress_ctx* ctx, int level, const char* dmpvar, void* host, long long cap_bytes,
+                  long long* nbytes, char* names, int names_cap);
+
+/* Restart file records formed on the device: the records s_outres writes
+ * after the base state (SrcOrig/outres.f90:903-1289) -- the present and
+ * past levels of every prognostic field, the open-x phase speeds, the
+ * surface precipitation planes and the TKE, each as a Fortran sequential
+ * unformatted record (a 4-byte length before and after its payload; the
+ * framing of gfortran and ifort below 2 GiB).  host null: size query.
+ * cress_restart_read takes the same byte stream (the records s_rdres reads
+ * back, SrcOrig/rdres.f90) and restores the device state; it checks every record's length first.
+ * The y phase speeds the file carries are zero (periodic y). */
+int cress_restart_write(cress_ctx* ctx, void* host, long long cap_bytes, long long* nbytes);
+int cress_restart_read(cress_ctx* ctx, const void* host, long long nbytes);
+
 /* Acoustic small-step loop on the device-resident state: replaces the body
  * of s_smalldrv (SrcOrig/smalldrv.f90:343-398): future u, v, w, p' start
  * from the past level, then nsstp substeps of dts run with the forcing
