@@ -381,6 +381,48 @@ def tke_leg(args, rank, plain_ms):
             "timing": "CUDA events on the library stream, graph replay"}
 
 
+def records_leg(s, stream, names):
+    """Dump and restart records of the workload's state: the device writers
+    (cress_dump_3d for every variable s_outdmp dumps with dmpvar
+    'ooooooooxxxo', cress_restart_write) into page-locked host buffers,
+    against reading the 14 prognostic fields back one by one and cutting
+    their dump region on the host (the path without the device writers).
+    Wall time around each synchronous call, median of 3."""
+    import torch
+    import cress_b200
+    n = s.restart_size()
+    rst = torch.empty(n, dtype=torch.uint8).pin_memory().numpy()
+
+    def med(fn):
+        t = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            t.append(time.perf_counter() - t0)
+        return float(np.median(t))
+
+    recs, probe_names = s.dump_3d("ooooooooxxxo")
+    dmp = torch.empty(recs.shape, dtype=torch.float32).pin_memory().numpy()
+    t_dump = med(lambda: s.dump_3d("ooooooooxxxo", out=dmp))
+    t_rst = med(lambda: s.restart_write(out=rst))
+
+    def host_path():
+        # the same bytes formed on the host from fields read back one by one
+        f = {q: s.get_field(q, cress_b200.NOW) for q in names}
+        nk = f["u"].shape[0]
+        parts = [(np.float32(.5) * (f["u"][1:nk - 2, 2:-3, 2:-3] + f["u"][1:nk - 2, 2:-3, 3:-2]))]
+        for q in names[1:]:
+            parts.append(f[q][1:nk - 2, 2:-3, 2:-3])
+        return np.stack(parts)
+    t_host = med(host_path)
+    return {"dump": {"variables": probe_names, "bytes": int(dmp.nbytes), "ms": t_dump * 1e3,
+                     "gb_per_s": dmp.nbytes / t_dump / 1e9},
+            "restart": {"bytes": int(n), "ms": t_rst * 1e3, "gb_per_s": n / t_rst / 1e9},
+            "host_readback_and_pack_ms": t_host * 1e3,
+            "timing": "wall clock around each synchronous call (page-locked host buffers), median of 3"}
+
+
 def ensemble_leg(args, rank):
     """Batched ensemble: `members` supercell domains of uneven size (nx, ny
     drawn from 96-192, nz = 48, dx = 1 km) with seeded bubble amplitude
@@ -491,6 +533,7 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-squall", action="store_true")
     ap.add_argument("--no-tke", action="store_true")
+    ap.add_argument("--no-records", action="store_true")
     ap.add_argument("--tubopt", type=int, default=0, choices=[0, 1, 2],
                     help="turbulence of the main workload: 0 none, 1 Smagorinsky, 2 TKE closure")
     ap.add_argument("--squall-nx", type=int, default=1024)
@@ -672,6 +715,7 @@ def main():
            "h2d_bytes_per_step": int(sum(a.nbytes for a in past_h + now_h)),
            "d2h_bytes_per_step": int(sum(a.nbytes for a in out_h[0])),
            "overlap": "device->host read-back of step n on a second stream during step n+1's host->device copies"}
+    io = None if args.no_records else records_leg(s, stream, names)
     s.close()
 
     cpu = None
@@ -707,7 +751,7 @@ def main():
                          "ms_per_launch": hevi_ms},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(),
             "cpu_baseline": cpu, "learned": learned, "ensemble": ensemble, "squall_line": squall,
-            "tke_closure": tke,
+            "tke_closure": tke, "records": io,
             "budget": budget, "autotune": tune}))
     rep.close()
 

@@ -240,30 +240,41 @@ class Solver:
     def wait_fields(self):
         _check(lib().cress_wait_fields(self._h))
 
-    def dump_3d(self, dmpvar, level=NOW):
+    def dump_3d(self, dmpvar, level=NOW, out=None):
         """The 3-D dump records of one level as s_outdmp writes them (dmplev
         = 1, dmpfmt = 2; see cress_dump_3d): returns (records, names) with
         records a float32 array (nvar, nz, ny, nx) whose bytes are the .bin
-        file, names the dumped variables in file order."""
+        file, names the dumped variables in file order.  out: an array of
+        that shape to fill (e.g. page-locked memory)."""
         L = lib()
         n = ctypes.c_longlong()
         names = ctypes.create_string_buffer(512)
         _check(L.cress_dump_3d(self._h, int(level), dmpvar.encode(), None, 0, ctypes.byref(n), names, 512))
         vs = [v for v in names.value.decode().split(",") if v]
         nk, nj2, ni2 = self.shape
-        out = np.empty((len(vs), nk - 3, nj2 - 5, ni2 - 5), np.float32)
+        shape = (len(vs), nk - 3, nj2 - 5, ni2 - 5)
+        if out is None:
+            out = np.empty(shape, np.float32)
+        assert out.shape == shape and out.dtype == np.float32 and out.flags.c_contiguous
         if vs:
             _check(L.cress_dump_3d(self._h, int(level), dmpvar.encode(), out.ctypes.data_as(ctypes.c_void_p),
                                    out.nbytes, ctypes.byref(n), None, 0))
         assert n.value == out.nbytes
         return out, vs
 
-    def restart_write(self):
-        """The device-held restart records (cress_restart_write) as bytes."""
+    def restart_size(self):
+        n = ctypes.c_longlong()
+        _check(lib().cress_restart_write(self._h, None, 0, ctypes.byref(n)))
+        return n.value
+
+    def restart_write(self, out=None):
+        """The device-held restart records (cress_restart_write) as bytes
+        (a uint8 array; out: one of restart_size() bytes to fill)."""
         L = lib()
         n = ctypes.c_longlong()
-        _check(L.cress_restart_write(self._h, None, 0, ctypes.byref(n)))
-        out = np.empty(n.value, np.uint8)
+        if out is None:
+            out = np.empty(self.restart_size(), np.uint8)
+        assert out.dtype == np.uint8 and out.flags.c_contiguous
         _check(L.cress_restart_write(self._h, out.ctypes.data_as(ctypes.c_void_p), out.nbytes, ctypes.byref(n)))
         return out
 

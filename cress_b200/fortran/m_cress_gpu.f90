@@ -33,7 +33,7 @@
       integer(c_int), parameter :: cress_qv = 5, cress_qc = 6, cress_qr = 7
       integer(c_int), parameter :: cress_qi = 8, cress_qs = 9, cress_qg = 10
       integer(c_int), parameter :: cress_ni = 11, cress_ns = 12
-      integer(c_int), parameter :: cress_ng = 13
+      integer(c_int), parameter :: cress_ng = 13, cress_tke = 14
 
       integer(c_int), parameter :: cress_past = 0, cress_now = 1
       integer(c_int), parameter :: cress_future = 2, cress_forcing = 3
@@ -185,6 +185,39 @@
           import :: c_int, c_ptr
           type(c_ptr), value :: ctx
         end function cress_wait_fields
+
+! Dump records of one time level (dmplev = 1, dmpfmt = 2) in the .bin
+! file's byte layout; host may be c_null_ptr to query nbytes.  The bytes
+! go to the dump file as they are (access='stream', or one direct-access
+! record per nx*ny*4 bytes).
+        integer(c_int) function cress_dump_3d(ctx, level, dmpvar, host,  &
+     &    cap, nbytes, names, ncap) bind(c, name='cress_dump_3d')
+          import :: c_int, c_ptr, c_char, c_long_long
+          type(c_ptr), value :: ctx, host
+          integer(c_int), value :: level, ncap
+          character(kind=c_char), intent(in) :: dmpvar(*)
+          integer(c_long_long), value :: cap
+          integer(c_long_long), intent(out) :: nbytes
+          character(kind=c_char), intent(out) :: names(*)
+        end function cress_dump_3d
+
+! The device-held restart records, framed as sequential unformatted
+! records: written after the base-state records of s_outres (a file opened
+! with access='stream' takes them unchanged), read back before s_rdres's.
+        integer(c_int) function cress_restart_write(ctx, host, cap,      &
+     &    nbytes) bind(c, name='cress_restart_write')
+          import :: c_int, c_ptr, c_long_long
+          type(c_ptr), value :: ctx, host
+          integer(c_long_long), value :: cap
+          integer(c_long_long), intent(out) :: nbytes
+        end function cress_restart_write
+
+        integer(c_int) function cress_restart_read(ctx, host, nbytes)    &
+     &    bind(c, name='cress_restart_read')
+          import :: c_int, c_ptr, c_long_long
+          type(c_ptr), value :: ctx, host
+          integer(c_long_long), value :: nbytes
+        end function cress_restart_read
 
         type(c_ptr) function cress_last_error()                         &
      &    bind(c, name='cress_last_error')

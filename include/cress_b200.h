@@ -182,6 +182,7 @@ int cress_wait_fields(cress_ctx* ctx);
  * giving the total or the field alone (u, v, p, pt, qv), cold rain adding
  * qc qr qi qs qg (dmpvar(7:7)='o') and nci ncs ncg (dmpvar(8:8)='o'), the
  * TKE closure tke (dmpvar(12:12)='o').  The bytes are the .bin file.
+ *   dmpvar: the namelist string (its first 16 characters are read);
  *   host null: only *nbytes and names are set (the size query);
  *   names (optional): the dumped variables, comma-separated.
  * pbar and p need the base pressure (cress_set_base_moist).  The maximum
