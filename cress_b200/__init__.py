@@ -125,6 +125,14 @@ def lib():
     L.cress_dump_3d.argtypes = [vp, i, ctypes.c_char_p, vp, ll, ctypes.POINTER(ll), ctypes.c_char_p, i]
     L.cress_restart_write.argtypes = [vp, vp, ll, ctypes.POINTER(ll)]
     L.cress_restart_read.argtypes = [vp, vp, ll]
+    L.cress_slab_group_create.argtypes = [i, ctypes.POINTER(vp)]
+    L.cress_slab_group_destroy.argtypes = [vp]
+    L.cress_slab_group_destroy.restype = None
+    L.cress_slab_group_set_timeout.argtypes = [vp, i]
+    L.cress_slab_attach_local.argtypes = [vp, vp, i]
+    L.cress_slab_nccl_id.argtypes = [vp]
+    L.cress_slab_attach_nccl.argtypes = [vp, i, i, vp]
+    L.cress_slab_detach.argtypes = [vp]
     dp = ctypes.POINTER(ctypes.c_double)
     L.cress_base_state.argtypes = [i, dp, dp, i, dp, i, i, ctypes.c_double, ctypes.c_double, dp, i]
     _lib = L
@@ -159,6 +167,31 @@ def base_state(nk, zph, jcb, z, u, v, pt, qv, psnd0, thresq=1e-12, tvar="p", hva
                                   snd.ctypes.data_as(dp), ord(tvar), ord(hvar), float(psnd0), float(thresq),
                                   out.ctypes.data_as(dp), int(device)))
     return dict(zip(BASE_COLUMNS, out))
+
+
+class SlabGroup:
+    """The ranks of a y-slab decomposition that live in this process
+    (cress_slab_group): each rank's Solver attaches with slab_attach and is
+    stepped by its own thread."""
+
+    def __init__(self, nranks, timeout_ms=None):
+        h = ctypes.c_void_p()
+        _check(lib().cress_slab_group_create(int(nranks), ctypes.byref(h)))
+        self._h = h
+        if timeout_ms is not None:
+            _check(lib().cress_slab_group_set_timeout(h, int(timeout_ms)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cress_slab_group_destroy(self._h)
+            self._h = None
+
+
+def slab_nccl_id():
+    """128 bytes naming a new NCCL communicator (cress_slab_nccl_id)."""
+    b = ctypes.create_string_buffer(128)
+    _check(lib().cress_slab_nccl_id(b))
+    return b.raw
 
 
 class Solver:
@@ -283,6 +316,22 @@ class Solver:
         a = np.ascontiguousarray(np.frombuffer(data, np.uint8) if not isinstance(data, np.ndarray) else data,
                                  np.uint8)
         _check(lib().cress_restart_read(self._h, a.ctypes.data_as(ctypes.c_void_p), a.nbytes))
+
+    def slab_attach(self, group, rank):
+        """Make this context rank `rank` of a y-slab decomposition whose ranks
+        are contexts of this process (cress_slab_attach_local)."""
+        _check(lib().cress_slab_attach_local(self._h, group._h, int(rank)))
+        self._slab_group = group
+
+    def slab_attach_nccl(self, rank, nranks, uid):
+        """Rank `rank` of `nranks` processes exchanging over NCCL; uid: the
+        128 bytes of slab_nccl_id() from one rank."""
+        b = ctypes.create_string_buffer(bytes(uid), 128)
+        _check(lib().cress_slab_attach_nccl(self._h, int(rank), int(nranks), b))
+
+    def slab_detach(self):
+        _check(lib().cress_slab_detach(self._h))
+        self._slab_group = None
 
     def small_steps(self, nsstp, dts):
         _check(lib().cress_small_steps(self._h, int(nsstp), float(dts)))

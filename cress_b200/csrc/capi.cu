@@ -137,6 +137,7 @@ Ctx::~Ctx() {
   if (ev_done) cudaEventDestroy(ev_done);
   free_graphs();
   free_learned();
+  if (slab) cress_slab_detach(reinterpret_cast<cress_ctx*>(this));
   if (rec_d) cudaFree(rec_d);
   for (void* p : owned) cudaFree(p);
   if (own_stream) cudaStreamDestroy(own_stream);
@@ -417,6 +418,10 @@ int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
       }
     }
     if (rc) return set_error(rc, "small-step launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    if (slab) {   // y slab: the new level's ghost rows from the neighbours (shiftsx after each substep)
+      const int stag[4] = {STAG_U, STAG_V, STAG_S, STAG_S};
+      if ((rc = slab->exchange(this, 4, news, stag))) return rc;
+    }
     for (int n = 0; n < 4; ++n) {
       float* t = news[n];
       news[n] = (s == 0) ? spare[F[n]] : olds[n];
@@ -636,6 +641,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     }
   if ((rc = launch_halo(h, stream))) return set_error(rc, "halo launch failed");
   ++launches;
+  if (slab && (rc = slab->exchange(this, h.n, h.f, h.stag))) return rc;   // y ghosts of t and t+dt
   if (g.openx) {   // s_phasev from the filtered present, past and future levels (intgdrv.f90:1023)
     PhaseArgs ph{};
     ph.g = g;
@@ -707,7 +713,13 @@ int Ctx::cloudphy(float dtb, float thresq) {
     if (rc) return set_error(rc, "learned cloudphy failed: %s", cudaGetErrorString(cudaGetLastError()));
     return CRESS_OK;
   }
-  rc = launch_cloudphy(m, stream);
+  if (slab) {   // the sub-step minimum over all ranks between the halves (chkfall.f90:88)
+    if ((rc = launch_cloudphy_src(m, stream))) return set_error(rc, "cloudphy launch failed");
+    if ((rc = slab->min_word(this, dtp_d))) return rc;
+    rc = launch_cloudphy_fall(m, stream);
+  } else {
+    rc = launch_cloudphy(m, stream);
+  }
   launches += 4;
   if (rc) return set_error(rc, "cloudphy launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   return CRESS_OK;
@@ -792,6 +804,7 @@ int Ctx::diagnostics(int level, double* out) {
 int Ctx::autotune(int nsstp, float dts, int reps, int* best, float* ms) {
   if (nsstp < 1 || reps < 1) return set_error(CRESS_E_ARG, "cress_autotune: nsstp=%d reps=%d", nsstp, reps);
   if (cfg.impopt == 0) return set_error(CRESS_E_UNSUPPORTED, "cress_autotune: the HE-VE step has one tile shape");
+  if (slab) return set_error(CRESS_E_UNSUPPORTED, "cress_autotune: a y-slab rank steps with the other ranks");
   const int keep = cfg.tile;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
@@ -1553,6 +1566,7 @@ int cress_set_tuple_sampling(cress_ctx* ctx, cress_mlp* mh, int stride, float ke
 int cress_set_graphs(cress_ctx* ctx, int on) {
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (!c) return set_error(CRESS_E_ARG, "null context");
+  if (on && c->slab) return set_error(CRESS_E_UNSUPPORTED, "cress_set_graphs: not for a y-slab rank");
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   c->free_graphs();
@@ -1585,9 +1599,9 @@ int cress_ensemble_create(cress_ctx* const* members, int n, cress_ensemble** out
     if (c->device != c0->device) return set_error(CRESS_E_ARG, "ensemble members live on different devices");
     if (!c->base_set || !c->large_set) return set_error(CRESS_E_STATE, "member %d: base state not set", m);
     if (c->cfg.impopt != 1 || c->cfg.divopt != c0->cfg.divopt || (c->cfg.sthopt != 0) != (c0->cfg.sthopt != 0) ||
-        c->cfg.buyopt != c0->cfg.buyopt || c->g.openx)
+        c->cfg.buyopt != c0->cfg.buyopt || c->g.openx || c->slab)
       return set_error(CRESS_E_UNSUPPORTED,
-                       "ensemble members need impopt=1, periodic x and the same divopt, sthopt, buyopt");
+                       "ensemble members need impopt=1, periodic x and y and the same divopt, sthopt, buyopt");
   }
   cudaSetDevice(c0->device);
   Ensemble* e = new Ensemble;

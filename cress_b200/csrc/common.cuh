@@ -18,6 +18,7 @@ struct Grid {
   int px, py;       // x pitch (floats) and y extent of one plane
   long long plane;  // px*py
   int openx;        // 1: open (radiation) west and east boundaries, 0: periodic x
+  int slaby;        // 1: one y slab of a decomposed domain (y ghosts come from the neighbours), 0: periodic y
   __host__ __device__ inline long long at(int i, int j, int k) const {
     return (long long)i + (long long)px * ((long long)j + (long long)py * (long long)(k - 1));
   }
@@ -31,6 +32,7 @@ inline Grid make_grid(int ni, int nj, int nk) {
   g.py = nj + 2;
   g.plane = (long long)g.px * g.py;
   g.openx = 0;
+  g.slaby = 0;
   return g;
 }
 
@@ -63,8 +65,12 @@ __device__ __forceinline__ void store_periodic(float* __restrict__ f, const Grid
   } else if (stag == STAG_U ? (i == 3) : (i == 2)) {
     xs[nx++] = (stag == STAG_U) ? g.ni : g.ni - 1;
   }
-  if (j == g.nj - 2) ys[ny++] = 1;
-  else if (stag == STAG_V ? (j == 3) : (j == 2)) ys[ny++] = (stag == STAG_V) ? g.nj : g.nj - 1;
+  if (g.slaby) {   // a y slab: the neighbours' rows fill the y ghosts (slab.h)
+  } else if (j == g.nj - 2) {
+    ys[ny++] = 1;
+  } else if (stag == STAG_V ? (j == 3) : (j == 2)) {
+    ys[ny++] = (stag == STAG_V) ? g.nj : g.nj - 1;
+  }
   for (int b = 0; b < ny; ++b)
     for (int a = 0; a < nx; ++a) f[g.at(xs[a], ys[b], k)] = val;
 }

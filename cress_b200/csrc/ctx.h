@@ -10,6 +10,7 @@
 #include "common.cuh"
 #include "hevi.cuh"
 #include "micro.cuh"
+#include "slab.h"
 
 namespace cress {
 
@@ -61,6 +62,8 @@ struct Ctx {
   bool out_pending = false;
   int get_async(int level, int n, const int* fields, float* const* host);
   int wait_async();
+  // y-slab decomposition (slab.h): the link to the other ranks, or null
+  SlabLink* slab = nullptr;
   // byte stream of the dump and restart records (records.cu), kept and
   // grown as needed
   void* rec_d = nullptr;

@@ -73,7 +73,8 @@ __global__ void __launch_bounds__(128) k_halo(const HaloArgs a) {
     const int st = a.stag[n];
     // open x: only the y wrap (over every column, boundary columns included)
     const bool gx = !g.openx && ((st == STAG_U) ? (i <= 1 || i >= ni) : (i <= 1 || (i >= ni - 1 && i <= ni)));
-    const bool gy = (st == STAG_V) ? (j <= 1 || j >= nj) : (j <= 1 || (j >= nj - 1 && j <= nj));
+    // a y slab: the neighbours' rows fill the y ghosts (slab.h)
+    const bool gy = !g.slaby && ((st == STAG_V) ? (j <= 1 || j >= nj) : (j <= 1 || (j >= nj - 1 && j <= nj)));
     const bool inx = (st == STAG_U) ? (i <= ni + 1) : (i <= ni);
     const bool iny = (st == STAG_V) ? (j <= nj + 1) : (j <= nj);
     if (!(gx || gy) || !inx || !iny) continue;

@@ -268,13 +268,25 @@ static void launch_fall(const MicroArgs& a, cudaStream_t st) {
   k_adjstni<<<gr, b, 0, st>>>(a);
 }
 
-int launch_cloudphy(const MicroArgs& a, cudaStream_t st) {
+// The process rates and the sub-step minimum (two launches), then the
+// sedimentation (two launches); a y-slab rank reduces the minimum over
+// the ranks in between.
+int launch_cloudphy_src(const MicroArgs& a, cudaStream_t st) {
   k_init_dtp<<<1, 1, 0, st>>>(a.dtp_bits, a.dtb);
   dim3 b(32, 8, 1);
   dim3 gr((ncols(a.g) + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
   k_micro_src<<<gr, b, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+int launch_cloudphy_fall(const MicroArgs& a, cudaStream_t st) {
   launch_fall(a, st);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
+int launch_cloudphy(const MicroArgs& a, cudaStream_t st) {
+  int rc = launch_cloudphy_src(a, st);
+  return rc ? rc : launch_cloudphy_fall(a, st);
 }
 
 int launch_moist_post(const MoistPostArgs& a, cudaStream_t st) {

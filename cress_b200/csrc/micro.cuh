@@ -23,8 +23,11 @@ struct MicroArgs {
 
 // Koenig table upload (once per device); returns a CRESS status.
 int micro_init_tables();
-// s_cloudphy for cphopt=3: source terms and sedimentation (2 kernels).
+// s_cloudphy for cphopt=3: source terms and sedimentation; or the two
+// halves (process rates with the sub-step minimum, then sedimentation).
 int launch_cloudphy(const MicroArgs& a, cudaStream_t st);
+int launch_cloudphy_src(const MicroArgs& a, cudaStream_t st);
+int launch_cloudphy_fall(const MicroArgs& a, cudaStream_t st);
 
 struct SatArgs {
   Grid g;

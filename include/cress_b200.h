@@ -202,6 +202,36 @@ int cress_dump_3d(cress_ctx* ctx, int level, const char* dmpvar, void* host, lon
 int cress_restart_write(cress_ctx* ctx, void* host, long long cap_bytes, long long* nbytes);
 int cress_restart_read(cress_ctx* ctx, const void* host, long long nbytes);
 
+/* y-slab decomposition of one domain over ranks, in place of the
+ * reference's MPI halo exchange (SrcOrig/shiftsx.f90:139-205,
+ * SrcOrig/sethalo.f90:485-505) and its allreduce of the sedimentation
+ * sub-step (SrcOrig/chkfall.f90:88).  Each rank's context holds its slab
+ * (nj = its rows + 3, the same ni, nk and base state as the others); y is
+ * periodic over the ring of ranks (rank 0's southern neighbour is the last
+ * rank), x periodic.  Once attached, cress_large_step exchanges the ghost
+ * rows after every acoustic substep and at the end of the step, and the
+ * sub-step minimum over all ranks, as the reference's ranks do; every rank
+ * must step together.  Plain microphysics only; no CUDA graphs.
+ *   cress_slab_attach_nccl: one rank per process and GPU, rows over NCCL
+ *     (libnccl.so.2 loaded at run time); id: 128 bytes from
+ *     cress_slab_nccl_id on one rank, passed to all.
+ *   cress_slab_group_create / cress_slab_attach_local: the ranks are
+ *     contexts of this process, each stepped by its own host thread; the
+ *     rows move as device copies ordered by CUDA events and a host barrier
+ *     (bounded: a rank that waits longer than the group's timeout, 60 s
+ *     unless cress_slab_group_set_timeout says otherwise, returns
+ *     CRESS_E_TIMEOUT, and every rank of a group with a failed rank
+ *     returns CRESS_E_STATE).
+ *   cress_slab_detach: back to a periodic single domain (between steps). */
+typedef struct cress_slab_group cress_slab_group;
+int cress_slab_group_create(int nranks, cress_slab_group** out);
+void cress_slab_group_destroy(cress_slab_group* grp);
+int cress_slab_group_set_timeout(cress_slab_group* grp, int ms);
+int cress_slab_attach_local(cress_ctx* ctx, cress_slab_group* grp, int rank);
+int cress_slab_nccl_id(void* id128);
+int cress_slab_attach_nccl(cress_ctx* ctx, int rank, int nranks, const void* id128);
+int cress_slab_detach(cress_ctx* ctx);
+
 /* Acoustic small-step loop on the device-resident state: replaces the body
  * of s_smalldrv (SrcOrig/smalldrv.f90:343-398): future u, v, w, p' start
  * from the past level, then nsstp substeps of dts run with the forcing
