@@ -154,6 +154,23 @@ def test_one_rank_is_the_periodic_domain(cress, single):
     _compare(case, ref, _run_slabs(cress, case, [case["dims"][1] - 3], 4))
 
 
+def test_nccl_single_rank_is_the_periodic_domain(cress, single):
+    """The NCCL link on one GPU: a single rank is its own northern and
+    southern neighbour, so its rows go out with ncclSend and come back with
+    ncclRecv (and the sub-step word through ncclAllReduce) as the periodic
+    wrap; the result must be the single domain's."""
+    case, ref = single
+    njg = case["dims"][1]
+    s = _solver(cress, case)
+    s.slab_attach_nccl(0, 1, cress.slab_nccl_id())
+    _step(s, 4)
+    got = {(n, lvl): s.get_field(n, lvl)[:, 2:njg - 1, :] for n in NAMES for lvl in (cress.PAST, cress.NOW)}
+    precip = s.get_precip()[:, :, 2:njg - 1, :]
+    s.slab_detach()
+    s.close()
+    _compare(case, ref, (got, precip))
+
+
 def test_missing_rank_times_out(cress, single):
     case, _ = single
     ni, njg, nk = case["dims"]
