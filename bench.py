@@ -509,6 +509,68 @@ def ensemble_leg(args, rank):
                       "one CUDA graph per step"}
 
 
+def slab_main(args, rep, cfg_json, nsstp):
+    """`--decomp slab`: ONE supercell domain of nx x ny x nz split into y
+    slabs over the ranks (one per GPU), the ghost rows and the sedimentation
+    sub-step minimum exchanged over NCCL (cress_slab_attach_nccl); total
+    work fixed as N grows (strong scaling).  Eager launches (no graphs in
+    slab mode); value = all cells x steps / the slowest rank's CUDA-event
+    time."""
+    import torch
+    import cress_b200
+    from cress_b200 import cases
+    from cress_b200.replicas import CudaEventTimer, timed_steps
+    world, rank = rep.world, rep.rank
+    case = make_case(args.nx, args.ny, args.nz, args.dx, 100)    # the same domain on every rank
+    ni, njg, nk = case["dims"]
+    P = njg - 3
+    sizes = [P // world + (1 if r < P % world else 0) for r in range(world)]
+    off = sum(sizes[:rank])
+    rows = 2 + (np.arange(sizes[rank] + 5) - 2 + off) % P          # local rows 0..nj+1 -> global rows
+    cut = lambda a: np.ascontiguousarray(a[:, rows, :])
+    rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, case["botbar"])
+    s = cress_b200.Solver(ni, sizes[rank] + 3, nk, args.dx, args.dx, case["dz"], sthopt=1, tile=max(args.tile, 13),
+                          device=torch.cuda.current_device(), cphopt=3, tubopt=args.tubopt)
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    s.set_base3d({k: cut(v) for k, v in case["base"].items()})
+    s.set_base_large(cut(case["base"]["ubr"]), cut(case["base"]["vbr"]), cut(cases.expand(rbct, ni, njg, nk)), ksp0)
+    s.set_base_moist(cut(case["base"]["pbr"]), cut(case["base"]["qvbr"]))
+    init = list(case["level"]) + [case["moist"][n] for n in MOIST]
+    names = NAMES + (["tke"] if args.tubopt == 2 else [])
+    if args.tubopt == 2:
+        init.append(np.zeros_like(init[0]))
+    for n, a in zip(names, init):
+        s.put_field(n, cress_b200.PAST, cut(a))
+        s.put_field(n, cress_b200.NOW, cut(a))
+    del case, init
+    uid = [cress_b200.slab_nccl_id() if rank == 0 else None]
+    if world > 1:
+        import torch.distributed as dist
+        dist.broadcast_object_list(uid, src=0)
+    s.slab_attach_nccl(rank, world, uid[0])
+    s.large_step(0, 0.5 * args.dtbig, nsstp, 0.5 * args.dtsml)
+    for _ in range(args.warmup - 1):
+        s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+    clk = ClockSampler(torch.cuda.current_device())
+    secs = timed_steps(rep, lambda: s.large_step(CTIME, args.dtbig, nsstp, args.dtsml), args.steps, 0,
+                       CudaEventTimer(stream), sync=torch.cuda.synchronize, inside=clk)
+    diag = s.diagnostics(cress_b200.NOW)
+    water = rep.sum(diag["water"] + diag["precip"])
+    s.slab_detach()
+    s.close()
+    cells = args.nx * args.ny * args.nz
+    if rank == 0:
+        cfg = dict(cfg_json, parallelism=f"yslab{world}", slab_rows=sizes)
+        print(json.dumps({"metric": METRIC, "value": cells * args.steps / secs, "unit": "cell-updates/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "strong",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+                          "launch": "eager launches, y-slab ghost rows over NCCL after every substep",
+                          "clocks": clk.summary(), "water_plus_precip_kg": water}))
+    rep.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -534,6 +596,8 @@ def main():
     ap.add_argument("--no-squall", action="store_true")
     ap.add_argument("--no-tke", action="store_true")
     ap.add_argument("--no-records", action="store_true")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="multi-GPU mode: independent domains per GPU (weak scaling) or one domain in y slabs")
     ap.add_argument("--tubopt", type=int, default=0, choices=[0, 1, 2],
                     help="turbulence of the main workload: 0 none, 1 Smagorinsky, 2 TKE closure")
     ap.add_argument("--squall-nx", type=int, default=1024)
@@ -603,6 +667,8 @@ def main():
 
     torch.cuda.set_device(local)
     rep = Replicas("nccl")
+    if args.decomp == "slab":
+        return slab_main(args, rep, cfg_json, nsstp)
     case = make_case(args.nx, args.ny, args.nz, args.dx, 100 + rank)
     ni, nj, nk = case["dims"]
     rbct, ksp0 = vspdmp_columns(nk, case["zph"], VSPBAR, case["botbar"])
