@@ -219,6 +219,27 @@
           integer(c_long_long), value :: nbytes
         end function cress_restart_read
 
+! y-slab decomposition over NCCL (one rank per GPU): id128 from
+! cress_slab_nccl_id on one rank, broadcast to all.
+        integer(c_int) function cress_slab_nccl_id(id128)                &
+     &    bind(c, name='cress_slab_nccl_id')
+          import :: c_int, c_ptr
+          type(c_ptr), value :: id128
+        end function cress_slab_nccl_id
+
+        integer(c_int) function cress_slab_attach_nccl(ctx, rank,        &
+     &    nranks, id128) bind(c, name='cress_slab_attach_nccl')
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, id128
+          integer(c_int), value :: rank, nranks
+        end function cress_slab_attach_nccl
+
+        integer(c_int) function cress_slab_detach(ctx)                  &
+     &    bind(c, name='cress_slab_detach')
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+        end function cress_slab_detach
+
         type(c_ptr) function cress_last_error()                         &
      &    bind(c, name='cress_last_error')
           import :: c_ptr
