@@ -200,7 +200,7 @@ class Solver:
     def __init__(self, ni, nj, nk, dx, dy, dz, sthopt=0, divopt=2, buyopt=1, weicoe=0.6, impopt=1,
                  tile=0, device=0, smtopt=3, smhcoe=0.001, smvcoe=0.0004, vspopt=2,
                  vspvar="oooxoooooo", coropt=0, fc=0.0, filcoe=0.1, cphopt=0, thresq=1e-12,
-                 tubopt=0, obc=0, gwave=20.0):
+                 tubopt=0, obc=0, gwave=20.0, advopt=2):
         L = lib()
         c = Cfg()
         c.ni, c.nj, c.nk = ni, nj, nk
@@ -213,7 +213,7 @@ class Solver:
         c.gwave = gwave
         c.bbc = c.tbc = 2
         c.tile = tile
-        c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = 2, smtopt, vspopt, coropt, tubopt, cphopt
+        c.advopt, c.smtopt, c.vspopt, c.coropt, c.tubopt, c.cphopt = advopt, smtopt, vspopt, coropt, tubopt, cphopt
         c.smhcoe, c.smvcoe, c.filcoe, c.fc = smhcoe, smvcoe, filcoe, fc
         c.vspvar = vspvar.encode()[:15]
         c.thresq = thresq

@@ -446,11 +446,12 @@ int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
 int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
   if (!base_set || !large_set)
     return set_error(CRESS_E_STATE, "cress_large_step: base state (set_base3d, set_base_large) not set");
-  if (cfg.advopt != 2 || cfg.tubopt < 0 || cfg.tubopt > 2 || !(cfg.cphopt == 0 || cfg.cphopt == 3) ||
+  if (!(cfg.advopt == 2 || cfg.advopt == 3) || cfg.tubopt < 0 || cfg.tubopt > 2 ||
+      !(cfg.cphopt == 0 || cfg.cphopt == 3) ||
       !(cfg.smtopt == 0 || cfg.smtopt % 10 == 2 || cfg.smtopt % 10 == 3) ||
       !(cfg.vspopt == 0 || cfg.vspopt == 2) || !(cfg.coropt == 0 || cfg.coropt == 1))
     return set_error(CRESS_E_UNSUPPORTED,
-                     "cress_large_step: needs advopt=2, tubopt 0/1/2, cphopt 0/3, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
+                     "cress_large_step: needs advopt 2/3, tubopt 0/1/2, cphopt 0/3, smtopt 0/2/3, vspopt 0/2, coropt 0/1");
   const bool tke = cfg.tubopt == 2;
   const bool moist = cfg.cphopt == 3;
   if (moist && !moist_set) return set_error(CRESS_E_STATE, "cress_large_step: moist base state not set");
@@ -472,6 +473,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
   int rc;
   if ((rc = level_table(f.dtb2, &f.lvl))) return rc;
   f.smtopt = cfg.smtopt; f.vspopt = cfg.vspopt; f.coropt = cfg.coropt; f.sthopt = cfg.sthopt;
+  f.advopt = cfg.advopt;
   f.ksp0 = ksp0;
   auto on = [&](int n) { return cfg.vspvar[n] == 'o' ? 1 : 0; };
   f.vsp_u = on(0); f.vsp_v = on(1); f.vsp_w = on(2); f.vsp_p = on(3); f.vsp_pt = on(4);
@@ -541,6 +543,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     t.dxiv = f.dxiv; t.dyiv = f.dyiv; t.dziv = f.dziv;
     t.smhcoe = cfg.smhcoe; t.smvcoe = cfg.smvcoe;
     t.smtopt = cfg.smtopt; t.vspopt = cfg.vspopt; t.sthopt = cfg.sthopt; t.ksp0 = ksp0;
+    t.advopt = cfg.advopt;
     t.vsp_tke = on(9);
     t.err = err_d;
     TkeMaps tm;
@@ -564,6 +567,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     m.dxiv = f.dxiv; m.dyiv = f.dyiv; m.dziv = f.dziv;
     m.smhcoe = cfg.smhcoe; m.smvcoe = cfg.smvcoe; m.dtb2 = f.dtb2;
     m.smtopt = cfg.smtopt; m.vspopt = cfg.vspopt; m.sthopt = cfg.sthopt; m.ksp0 = ksp0;
+    m.advopt = cfg.advopt;
     m.vsp_qv = on(5); m.vsp_q = on(6);
     m.rkv = f.rks; m.cpriv = cpriv; m.kdiv = f.kdiv;
     m.err = err_d;

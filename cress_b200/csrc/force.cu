@@ -1,5 +1,5 @@
 // Large-step forcing for sm_100a: for every grid point the complete forcing
-// of s_forceuvw, s_forcep and s_forcept (advopt=2, smtopt=2/3, vspopt=2,
+// of s_forceuvw, s_forcep and s_forcept (advopt=2/3, smtopt=2/3, vspopt=2,
 // coropt=0/1, buyopt=1, gwmopt=0, tubopt=0/1/2 with isoopt=1, flat terrain)
 // and the theta' step of s_steps, with the terms added in the reference's
 // order:
@@ -103,8 +103,11 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
   const float dxv25n = -.25f * dxiv, dyv25n = -.25f * dyiv, dzv25n = -.25f * dziv;
   const float dxv24 = oned24 * dxiv, dyv24 = oned24 * dyiv;
   const float dxv48 = .5f * dxv24, dyv48 = .5f * dyv24;
+  const float dzv24 = oned24 * dziv, dzv48 = .5f * dzv24;
   const float dxv05n = -.5f * dxiv, dyv05n = -.5f * dyiv, dzv05n = -.5f * dziv;
   const bool smooth = (a.smtopt % 10 == 2) || (a.smtopt % 10 == 3);
+  // advopt=3: 4th-order vertical advection on the levels 3..nk-3 (w: 3..nk-2)
+  const bool adv3 = a.advopt == 3 && k >= 3 && k <= (G == 2 ? nk - 2 : nk - 3);
   const float g05 = .5f * 9.8f;
   const float* ck = a.lvl + k * kNF;
   auto C = [&](int f, int kk) { return __ldg(ck + (kk - k) * kNF + f); };
@@ -186,7 +189,15 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
     const F2 h2 = hadv;
     hadv = fourd3 * hadv + ((t1w(-1) + t1w(1)) + (t2w(-1) + t2w(1)));
     if (edge) hadv = sel2(edge, h2, hadv);
-    f = f + hadv + (t3(0) + t3(1));
+    F2 vadv = t3(0) + t3(1);
+    if (adv3) {   // advuvw.f90:399-430
+      auto t3w = [&](int z) {
+        return ((RXW(-1, 0, z) + RXW(0, 0, z)) + (RXW(-1, 0, z + 1) + RXW(0, 0, z + 1))) *
+               (Uc(0, 0, z + 1) - Uc(0, 0, z - 1)) * dzv48;
+      };
+      vadv = fourd3 * vadv + (t3w(-1) + t3w(1));
+    }
+    f = f + hadv + vadv;
     put(a.ufrc, id, f);
   } else if constexpr (G == 1) {
     // ------------------------------------------------------------ vfrc
@@ -240,7 +251,15 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
     const F2 h2 = hadv;
     hadv = fourd3 * hadv + ((t1w(-1) + t1w(1)) + (t2w(-1) + t2w(1)));
     if (edge) hadv = sel2(edge, h2, hadv);
-    f = f + hadv + (t3(0) + t3(1));
+    F2 vadv = t3(0) + t3(1);
+    if (adv3) {   // advuvw.f90:626-657
+      auto t3w = [&](int z) {
+        return ((RXW(0, -1, z) + RXW(0, 0, z)) + (RXW(0, -1, z + 1) + RXW(0, 0, z + 1))) *
+               (Vc(0, 0, z + 1) - Vc(0, 0, z - 1)) * dzv48;
+      };
+      vadv = fourd3 * vadv + (t3w(-1) + t3w(1));
+    }
+    f = f + hadv + vadv;
     put(a.vfrc, id, f);
   } else if constexpr (G == 2) {
     // ------------------------------------------------------------ wfrc
@@ -303,7 +322,14 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
     const F2 h2 = hadv;
     hadv = fourd3 * hadv + ((t1w(-1) + t1w(1)) + (t2w(-1) + t2w(1)));
     if (edge) hadv = sel2(edge, h2, hadv);
-    f = f + hadv + (t3(-1) + t3(0));
+    F2 vadv = t3(-1) + t3(0);
+    if (adv3) {   // advuvw.f90:854-884
+      auto t3w = [&](int z) {
+        return (RXW(0, 0, z - 1) + RXW(0, 0, z + 1)) * (Wc(0, 0, z + 1) - Wc(0, 0, z - 1)) * dzv24;
+      };
+      vadv = fourd3 * vadv + (t3w(-1) + t3w(1));
+    }
+    f = f + hadv + vadv;
     put(a.wfrc, id, f);
   } else {
     // --------------------------------------------- pfrc, theta' step
@@ -320,7 +346,12 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
       const F2 s2 = sf;
       sf = fourd3 * sf + ((t1w(-1) + t1w(1)) + (t2w(-1) + t2w(1)));
       if (edge) sf = sel2(edge, s2, sf);
-      return sf + (t3(0) + t3(1));
+      F2 vadv = t3(0) + t3(1);
+      if (adv3) {   // advs.f90:372-416, advp.f90:627-655
+        auto t3w = [&](int z) { return (FW(z) + FW(z + 1)) * (Sc(0, 0, z + 1) - Sc(0, 0, z - 1)) * dzv24; };
+        vadv = fourd3 * vadv + (t3w(-1) + t3w(1));
+      }
+      return sf + vadv;
     };
     if constexpr (G == 3) {
       // pressure (advp.f90:255-291 J-weighted fluxes)

@@ -63,6 +63,7 @@ struct ForceArgs {
   float fc;                   // 0.5*omega*sin(lat) when coropt=1
   float dtb2;                 // 2*dtb
   int smtopt, vspopt, coropt, sthopt, ksp0;
+  int advopt;                 // 2, or 3: 4th order in z too (advuvw.f90:309, advs.f90:284)
   int vsp_u, vsp_v, vsp_w, vsp_p, vsp_pt;  // vspvar switches
   // moist buoyancy (buoywb.f90:202-299, cphopt != 0): qv and the five
   // hydrometeor mixing ratios at t; null qv = dry buoyancy
@@ -140,7 +141,7 @@ struct MoistScalarArgs {
   const float* sp[kMoistN];   // past level t-dt
   float* sf[kMoistN];         // future level t+dt (output)
   float dxiv, dyiv, dziv, smhcoe, smvcoe, dtb2;
-  int smtopt, vspopt, sthopt, ksp0;
+  int smtopt, vspopt, sthopt, ksp0, advopt;
   int vsp_qv, vsp_q;          // vspvar(6:6), vspvar(7:7)
   const float* rkv;           // staged viscosity (tubopt 1: rkv; 2: the diffusivity rks) or null
   float cpriv;

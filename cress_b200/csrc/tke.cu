@@ -189,7 +189,16 @@ __global__ void __launch_bounds__(kTkePairs * kScalarTY) k_tke(const __grid_cons
       f = fourd3 * f + ((w1a + w1b) + (w2a + w2b));
       const F2 t3a = fw_0 * (s0 - ld2(st(-1) + L::oS + oS)) * dzv05n;
       const F2 t3b = fw_1 * (ld2(st(1) + L::oS + oS) - s0) * dzv05n;
-      f = f + (t3a + t3b);
+      F2 vadv = t3a + t3b;
+      if (a.advopt == 3 && k >= 3 && k <= nk - 3) {   // advs.f90:372-416: 4th order in z
+        const float dzv24 = oned24 * a.dziv;
+        const F2 fw_m1 = C(C_RST8W, k - 1) * WC(ld2(st(-1) + L::oW + oU), k - 1);
+        const F2 fw_2 = C(C_RST8W, k + 2) * WC(ld2(st(2) + L::oW + oU), k + 2);
+        const F2 t3w_m = (fw_m1 + fw_0) * (s0 - ld2(st(-2) + L::oS + oS)) * dzv24;
+        const F2 t3w_p = (fw_1 + fw_2) * (ld2(st(2) + L::oS + oS) - s0) * dzv24;
+        vadv = fourd3 * vadv + (t3w_m + t3w_p);
+      }
+      f = f + vadv;
 
       f = f + shr;   // sheartke
 

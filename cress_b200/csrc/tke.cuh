@@ -23,7 +23,7 @@ struct TkeArgs {
   const float *rks, *nsq, *shr, *dsp;
   float* tkef;                           // TKE at t+dt (output)
   float dxiv, dyiv, dziv, smhcoe, smvcoe;
-  int smtopt, vspopt, sthopt, ksp0;
+  int smtopt, vspopt, sthopt, ksp0, advopt;
   int vsp_tke;                           // vspvar(10:10) == 'o'
   int* err;                              // device error word (a bounded wait gave up)
 };

@@ -251,7 +251,7 @@
 
 !-----7--------------------------------------------------------------7--
 
-! The body that replaces s_intgdrv for advopt=2, tubopt=0, cphopt=0 or 3,
+! The body that replaces s_intgdrv for advopt=2 or 3, tubopt=0, 1 or 2, cphopt=0 or 3,
 ! impopt=1, periodic lateral boundaries, flat terrain: one leapfrog step
 ! on the device-resident state.  ctime, dtb, nsstp, dts are s_intgdrv's
 ! own arguments (SrcOrig/intgdrv.f90:111-116).  A nonzero status goes to

@@ -57,7 +57,7 @@ typedef struct cress_cfg {
                            12, 13: 32x8 with the column kept on chip, FP64 throughout the solve, nk <= 68;
                            12 two rows per thread, 13 one) */
   /* large step (SrcOrig/forcedrv.f90:548-608, SrcOrig/timeflt.f90:335) */
-  int advopt;           /* 2 only: 4th-order horizontal advection */
+  int advopt;           /* 2: 4th-order horizontal, 2nd-order vertical advection; 3: 4th order in z as well (periodic boundaries) */
   int smtopt;           /* 0 none, 2 horizontal, 3 horizontal + vertical 4th-order smoothing */
   int vspopt;           /* 0 none, 2 Rayleigh damping above botbar toward the base state */
   int coropt;           /* 0 none, 1 f-plane Coriolis on u, v */

@@ -90,10 +90,11 @@ def dry_steps(cfg, base, zph, past, now, nsteps, dtbig, dtsml, start=True, prec=
                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(_FP), ctypes.POINTER(_FP), ctypes.c_int,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int]
-    io = (ctypes.c_int * 13)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
+    io = (ctypes.c_int * 14)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
                              cfg.get("buyopt", 1), int(fp64_solve), cfg.get("sthopt", 0),
                              cfg.get("smtopt", 3), cfg.get("vspopt", 2), cfg.get("coropt", 0),
-                             cfg.get("tubopt", 0), cfg.get("impopt", 1), cfg.get("obc", 0))
+                             cfg.get("tubopt", 0), cfg.get("impopt", 1), cfg.get("obc", 0),
+                             cfg.get("advopt", 2))
     ro = (ctypes.c_double * 11)(cfg["dx"], cfg["dy"], cfg["dz"], cfg.get("weicoe", 0.6),
                                 cfg.get("smhcoe", 0.001), cfg.get("smvcoe", 0.0004),
                                 cfg.get("filcoe", 0.1), cfg.get("vspbar", 0.0),
@@ -128,10 +129,11 @@ def moist_steps(cfg, base, zph, past, now, prec, nsteps, dtbig, dtsml, start=Tru
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(_FP), ctypes.POINTER(_FP), _FP, ctypes.c_int,
                                      ctypes.c_double, ctypes.c_double, ctypes.c_int]
-    io = (ctypes.c_int * 13)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
+    io = (ctypes.c_int * 14)(cfg["ni"], cfg["nj"], cfg["nk"], cfg.get("divopt", 2),
                              cfg.get("buyopt", 1), int(fp64_solve), cfg.get("sthopt", 0),
                              cfg.get("smtopt", 3), cfg.get("vspopt", 2), cfg.get("coropt", 0),
-                             cfg.get("tubopt", 0), cfg.get("impopt", 1), cfg.get("obc", 0))
+                             cfg.get("tubopt", 0), cfg.get("impopt", 1), cfg.get("obc", 0),
+                             cfg.get("advopt", 2))
     ro = (ctypes.c_double * 12)(cfg["dx"], cfg["dy"], cfg["dz"], cfg.get("weicoe", 0.6),
                                 cfg.get("smhcoe", 0.001), cfg.get("smvcoe", 0.0004),
                                 cfg.get("filcoe", 0.1), cfg.get("vspbar", 0.0),

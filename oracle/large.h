@@ -59,7 +59,7 @@ void rstuvwc(const Opts& o, const Base<R>& b, const F3<R>& u, const F3<R>& v, co
       for (int i = 1; i <= ni - 1; ++i) rxw(i, j, k) = b.rst8w(i, j, k) * wc(i, j, k);
 }
 
-// s_advuvw advopt=2, SrcOrig/advuvw.f90:209-397 (u), 458-624 (v), 685-852 (w).
+// s_advuvw advopt=2 or 3, SrcOrig/advuvw.f90:209-430 (u), 458-657 (v), 685-884 (w).
 template <class R>
 void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw, const F3<R>& u,
             const F3<R>& v, const F3<R>& w, F3<R>& ufrc, F3<R>& vfrc, F3<R>& wfrc, F3<R>& t1,
@@ -70,6 +70,7 @@ void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw,
   const R dxv25n = R(-.25) * dxiv, dyv25n = R(-.25) * dyiv, dzv25n = R(-.25) * dziv;
   const R dxv24 = oned24 * dxiv, dyv24 = oned24 * dyiv;
   const R dxv48 = R(.5) * dxv24, dyv48 = R(.5) * dyv24;
+  const R dzv24 = oned24 * dziv, dzv48 = R(.5) * dzv24;
   const int iw = o.iw(), ie = o.ie();   // open x: 4th order away from the boundary columns
   // ---- u (advuvw.f90:231-397)
   OMP_FOR for (int k = 2; k <= nk - 2; ++k) {
@@ -102,10 +103,27 @@ void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw,
       for (int i = 2 + iw; i <= ni - 1 - ie; ++i)
         hadv(i, j, k) = fourd3 * hadv(i, j, k) +
                         ((t1(i - 1, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j + 1, k)));
-  OMP_FOR for (int k = 2; k <= nk - 2; ++k)
-    for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 2; i <= ni - 1; ++i)
-        ufrc(i, j, k) = ufrc(i, j, k) + hadv(i, j, k) + (t3(i, j, k) + t3(i, j, k + 1));
+  if (o.advopt == 3) {   // advuvw.f90:309-335, 399-430: 4th order in z on k = 3..nk-3
+    F3<R> va(ni, nj, nk), tz(ni, nj, nk);
+    for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 1; ++i) {
+          va(i, j, k) = t3(i, j, k) + t3(i, j, k + 1);
+          tz(i, j, k) = ((rxw(i - 1, j, k) + rxw(i, j, k)) + (rxw(i - 1, j, k + 1) + rxw(i, j, k + 1))) *
+                        (u(i, j, k + 1) - u(i, j, k - 1)) * dzv48;
+        }
+    for (int k = 3; k <= nk - 3; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 1; ++i) va(i, j, k) = fourd3 * va(i, j, k) + (tz(i, j, k - 1) + tz(i, j, k + 1));
+    for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 1; ++i) ufrc(i, j, k) = ufrc(i, j, k) + hadv(i, j, k) + va(i, j, k);
+  } else {
+    OMP_FOR for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 1; ++i)
+          ufrc(i, j, k) = ufrc(i, j, k) + hadv(i, j, k) + (t3(i, j, k) + t3(i, j, k + 1));
+  }
   // ---- v (advuvw.f90:458-624)
   OMP_FOR for (int k = 2; k <= nk - 2; ++k) {
     for (int j = 2; j <= nj - 1; ++j)
@@ -137,10 +155,27 @@ void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw,
       for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         hadv(i, j, k) = fourd3 * hadv(i, j, k) +
                         ((t1(i - 1, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j + 1, k)));
-  OMP_FOR for (int k = 2; k <= nk - 2; ++k)
-    for (int j = 2; j <= nj - 1; ++j)
-      for (int i = 2; i <= ni - 2; ++i)
-        vfrc(i, j, k) = vfrc(i, j, k) + hadv(i, j, k) + (t3(i, j, k) + t3(i, j, k + 1));
+  if (o.advopt == 3) {   // advuvw.f90:536-562, 626-657
+    F3<R> va(ni, nj, nk), tz(ni, nj, nk);
+    for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 1; ++j)
+        for (int i = 2; i <= ni - 2; ++i) {
+          va(i, j, k) = t3(i, j, k) + t3(i, j, k + 1);
+          tz(i, j, k) = ((rxw(i, j - 1, k) + rxw(i, j, k)) + (rxw(i, j - 1, k + 1) + rxw(i, j, k + 1))) *
+                        (v(i, j, k + 1) - v(i, j, k - 1)) * dzv48;
+        }
+    for (int k = 3; k <= nk - 3; ++k)
+      for (int j = 2; j <= nj - 1; ++j)
+        for (int i = 2; i <= ni - 2; ++i) va(i, j, k) = fourd3 * va(i, j, k) + (tz(i, j, k - 1) + tz(i, j, k + 1));
+    for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 1; ++j)
+        for (int i = 2; i <= ni - 2; ++i) vfrc(i, j, k) = vfrc(i, j, k) + hadv(i, j, k) + va(i, j, k);
+  } else {
+    OMP_FOR for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 1; ++j)
+        for (int i = 2; i <= ni - 2; ++i)
+          vfrc(i, j, k) = vfrc(i, j, k) + hadv(i, j, k) + (t3(i, j, k) + t3(i, j, k + 1));
+  }
   // ---- w (advuvw.f90:685-852)
   OMP_FOR for (int k = 2; k <= nk - 1; ++k) {
     for (int j = 2; j <= nj - 2; ++j)
@@ -173,13 +208,29 @@ void advuvw(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw,
       for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         hadv(i, j, k) = fourd3 * hadv(i, j, k) +
                         ((t1(i - 1, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j + 1, k)));
-  OMP_FOR for (int k = 2; k <= nk - 1; ++k)
-    for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 2; i <= ni - 2; ++i)
-        wfrc(i, j, k) = wfrc(i, j, k) + hadv(i, j, k) + (t3(i, j, k - 1) + t3(i, j, k));
+  if (o.advopt == 3) {   // advuvw.f90:763-789, 854-884
+    F3<R> va(ni, nj, nk), tz(ni, nj, nk);
+    for (int k = 2; k <= nk - 1; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i) {
+          va(i, j, k) = t3(i, j, k - 1) + t3(i, j, k);
+          tz(i, j, k) = (rxw(i, j, k - 1) + rxw(i, j, k + 1)) * (w(i, j, k + 1) - w(i, j, k - 1)) * dzv24;
+        }
+    for (int k = 3; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i) va(i, j, k) = fourd3 * va(i, j, k) + (tz(i, j, k - 1) + tz(i, j, k + 1));
+    for (int k = 2; k <= nk - 1; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i) wfrc(i, j, k) = wfrc(i, j, k) + hadv(i, j, k) + va(i, j, k);
+  } else {
+    OMP_FOR for (int k = 2; k <= nk - 1; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i)
+          wfrc(i, j, k) = wfrc(i, j, k) + hadv(i, j, k) + (t3(i, j, k - 1) + t3(i, j, k));
+  }
 }
 
-// s_advs advopt=2, SrcOrig/advs.f90:189-370: sfrc = advection of s (set,
+// s_advs advopt=2 or 3, SrcOrig/advs.f90:189-416: sfrc = advection of s (set,
 // not accumulated).  Also s_advp (advp.f90:249-620, diaopt=0) with the
 // J-weighted fluxes passed as rxu/rxv/rxw.
 template <class R>
@@ -219,9 +270,26 @@ void advs(const Opts& o, const F3<R>& rxu, const F3<R>& rxv, const F3<R>& rxw, c
       for (int i = 2 + iw; i <= ni - 2 - ie; ++i)
         sfrc(i, j, k) = fourd3 * sfrc(i, j, k) +
                         ((t1(i - 1, j, k) + t1(i + 1, j, k)) + (t2(i, j - 1, k) + t2(i, j + 1, k)));
-  OMP_FOR for (int k = 2; k <= nk - 2; ++k)
-    for (int j = 2; j <= nj - 2; ++j)
-      for (int i = 2; i <= ni - 2; ++i) sfrc(i, j, k) = sfrc(i, j, k) + (vt(i, j, k) + vt(i, j, k + 1));
+  if (o.advopt == 3) {   // advs.f90:284-300, 372-416 (advp.f90:627-655 alike)
+    const R dzv24 = oned24 * dziv;
+    F3<R> va(ni, nj, nk), tz(ni, nj, nk);
+    for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i) {
+          va(i, j, k) = vt(i, j, k) + vt(i, j, k + 1);
+          tz(i, j, k) = (rxw(i, j, k) + rxw(i, j, k + 1)) * (s(i, j, k + 1) - s(i, j, k - 1)) * dzv24;
+        }
+    for (int k = 3; k <= nk - 3; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i) va(i, j, k) = fourd3 * va(i, j, k) + (tz(i, j, k - 1) + tz(i, j, k + 1));
+    for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i) sfrc(i, j, k) = sfrc(i, j, k) + va(i, j, k);
+  } else {
+    OMP_FOR for (int k = 2; k <= nk - 2; ++k)
+      for (int j = 2; j <= nj - 2; ++j)
+        for (int i = 2; i <= ni - 2; ++i) sfrc(i, j, k) = sfrc(i, j, k) + (vt(i, j, k) + vt(i, j, k + 1));
+  }
 }
 
 // 4th-order numerical smoothing of one field, the operator shared by

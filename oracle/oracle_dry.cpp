@@ -25,6 +25,7 @@ int run_dry(const int* io, const double* ro, const double* zph, const float* con
   r.lo.tubopt = io[10];
   o.impopt = io[11];
   o.obc = io[12];          // 0 periodic x, 4/5/7 open radiation x (wbc = ebc)
+  o.advopt = io[13];       // 2 or 3 (4th-order vertical advection)
   o.gwave = ro[10];
   o.dx = ro[0]; o.dy = ro[1]; o.dz = ro[2]; o.weicoe = ro[3];
   r.lo.smhcoe = ro[4]; r.lo.smvcoe = ro[5]; r.lo.filcoe = ro[6];
@@ -69,7 +70,7 @@ int run_dry(const int* io, const double* ro, const double* zph, const float* con
 
 extern "C" {
 
-// io: ni,nj,nk,divopt,buyopt,fp64_solve,sthopt,smtopt,vspopt,coropt,tubopt,impopt,obc
+// io: ni,nj,nk,divopt,buyopt,fp64_solve,sthopt,smtopt,vspopt,coropt,tubopt,impopt,obc,advopt
 // ro: dx,dy,dz,weicoe,smhcoe,smvcoe,filcoe,vspbar,botbar,fc,gwave
 // zph: w-level heights, index k = 1..nk (entry 0 unused)
 // base: jcb,jcb8u,jcb8v,jcb8w,rbr,ptbr,rst,rst8u,rst8v,rst8w,rcsq,ubr,vbr

@@ -58,6 +58,7 @@ int run_moist(const int* io, const double* ro, const double* zph, const float* c
   r.lo.tubopt = io[10];
   o.impopt = io[11];
   o.obc = io[12];          // 0 periodic x, 4/5/7 open radiation x (wbc = ebc)
+  o.advopt = io[13];       // 2 or 3 (4th-order vertical advection)
   o.gwave = ro[11];
   o.dx = ro[0]; o.dy = ro[1]; o.dz = ro[2]; o.weicoe = ro[3];
   r.lo.smhcoe = ro[4]; r.lo.smvcoe = ro[5]; r.lo.filcoe = ro[6];
@@ -134,7 +135,7 @@ void oracle_satadjst(int ni, int nj, int nk, double thresq, const float* ptbr, c
 }
 
 // Whole moist large steps (cphopt=3).
-// io: ni,nj,nk,divopt,buyopt,fp64_solve,sthopt,smtopt,vspopt,coropt,tubopt,impopt,obc
+// io: ni,nj,nk,divopt,buyopt,fp64_solve,sthopt,smtopt,vspopt,coropt,tubopt,impopt,obc,advopt
 // ro: dx,dy,dz,weicoe,smhcoe,smvcoe,filcoe,vspbar,botbar,fc,thresq,gwave
 // base: jcb,jcb8u,jcb8v,jcb8w,rbr,ptbr,rst,rst8u,rst8v,rst8w,rcsq,ubr,vbr,pbr,qvbr
 // st (in/out): past u,v,w,pp,ptp,qv,qc,qr,qi,qs,qg,ni,ns,ng then present (28);

@@ -53,6 +53,7 @@ struct Opts {
   // (sethalo.f90:535-557); gwave is the phase speed of options 5-7.
   int obc = 0;
   double gwave = 20.;
+  int advopt = 2;     // 2: 4th-order horizontal advection; 3: 4th order in z too (advuvw.f90:309, advs.f90:284)
   const void* rad = nullptr;   // the run's phase speeds (openbc.h Radiation<R>)
   int iw() const { return obc ? 1 : 0; }
   int ie() const { return obc ? 1 : 0; }

@@ -27,7 +27,7 @@ def region(name, ni, nj, nk):
 
 
 def run_case(cress, oracle_lib, nx, ny, nz, nsteps, coropt=0, seed=3, tubopt=0, dthdz=0.003, noise=0.01,
-             impopt=1):
+             impopt=1, advopt=2):
     from cress_b200 import cases
     dx, dz, dtbig, dtsml = 500.0, 300.0, 2.0, 0.25
     case = cases.dry_case(nx, ny, nz, dx, dz, sthopt=1, seed=seed, vspbar=0.005, dthdz=dthdz, noise=noise)
@@ -37,12 +37,13 @@ def run_case(cress, oracle_lib, nx, ny, nz, nsteps, coropt=0, seed=3, tubopt=0, 
     rbct, ksp0 = oracle_lib.vspdmp(nk, zph, 0.005, botbar)
     fc = 0.5 * 7.292e-5 * np.sin(np.deg2rad(35.0)) if coropt else 0.0
     cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=1, smtopt=3, vspopt=2,
-               coropt=coropt, vspbar=0.005, botbar=botbar, fc=fc, tubopt=tubopt, impopt=impopt)
+               coropt=coropt, vspbar=0.005, botbar=botbar, fc=fc, tubopt=tubopt, impopt=impopt, advopt=advopt)
     past = [a.copy() for a in case["level"]]
     now = [a.copy() for a in case["level"]]
     oracle_lib.dry_steps(cfg, case["base"], zph, past, now, nsteps, dtbig, dtsml, start=True)
 
-    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, coropt=coropt, fc=fc, tubopt=tubopt, impopt=impopt)
+    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, coropt=coropt, fc=fc, tubopt=tubopt, impopt=impopt,
+                     advopt=advopt)
     s.set_base3d(case["base"])
     rb3 = cases.expand(rbct, ni, nj, nk)
     s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], rb3, ksp0)
@@ -84,6 +85,13 @@ def test_dry_large_steps_coriolis_ragged(cress, oracle_lib):
 def test_dry_large_steps_smagorinsky(cress, oracle_lib):
     # neutral stratification and noise so the eddy viscosity is active
     dims, ref, got = run_case(cress, oracle_lib, 40, 32, 24, 4, seed=5, tubopt=1, dthdz=0.0, noise=0.5)
+    check(dims, ref, got)
+
+
+def test_dry_large_steps_4th_order_vertical_advection(cress, oracle_lib):
+    # advopt=3: 4th-order vertical advection of u, v, w and theta' on
+    # levels 3..nk-3 (w: 3..nk-2), 2nd order next to the boundaries
+    dims, ref, got = run_case(cress, oracle_lib, 37, 29, 20, 3, seed=4, dthdz=0.0, noise=0.5, advopt=3)
     check(dims, ref, got)
 
 

@@ -39,7 +39,8 @@ def region(name, ni, nj, nk):
     return m
 
 
-def run_case(cress, oracle_lib, nx, ny, nz, nsteps, seed=3, cloud=True, dtbig=5.0, dtsml=1.0, tubopt=0):
+def run_case(cress, oracle_lib, nx, ny, nz, nsteps, seed=3, cloud=True, dtbig=5.0, dtsml=1.0, tubopt=0,
+             advopt=2):
     from cress_b200 import cases
     dx = 1000.0
     case = cases.supercell_case(nx, ny, nz, dx, ztop=8000.0, seed=seed, cloud=cloud,
@@ -49,14 +50,14 @@ def run_case(cress, oracle_lib, nx, ny, nz, nsteps, seed=3, cloud=True, dtbig=5.
     vspbar, botbar = 0.005, 0.6 * zph[nk - 1]
     rbct, ksp0 = oracle_lib.vspdmp(nk, zph, vspbar, botbar)
     cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=1, smtopt=3, vspopt=2, coropt=0,
-               vspbar=vspbar, botbar=botbar, thresq=1e-12, tubopt=tubopt)
+               vspbar=vspbar, botbar=botbar, thresq=1e-12, tubopt=tubopt, advopt=advopt)
     init = list(case["level"]) + [case["moist"][n] for n in NAMES[5:]]
     past = [a.copy() for a in init]
     now = [a.copy() for a in init]
     prec_ref = np.zeros((5, 2, nj + 2, ni + 2), np.float32)
     oracle_lib.moist_steps(cfg, case["base"], zph, past, now, prec_ref, nsteps, dtbig, dtsml, start=True)
 
-    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, cphopt=3, thresq=1e-12, tubopt=tubopt)
+    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, cphopt=3, thresq=1e-12, tubopt=tubopt, advopt=advopt)
     s.set_base3d(case["base"])
     s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
     s.set_base_moist(case["base"]["pbr"], case["base"]["qvbr"])
@@ -115,4 +116,10 @@ def test_moist_large_steps_clear_ragged(cress, oracle_lib):
 
 def test_moist_large_steps_smagorinsky(cress, oracle_lib):
     dims, ref, got = run_case(cress, oracle_lib, 36, 30, 22, 3, seed=11, tubopt=1)
+    check(dims, ref, got)
+
+
+def test_moist_large_steps_4th_order_vertical_advection(cress, oracle_lib):
+    # advopt=3 on the water species too (the moist scalar kernel)
+    dims, ref, got = run_case(cress, oracle_lib, 36, 30, 22, 3, seed=12, advopt=3)
     check(dims, ref, got)

@@ -205,6 +205,34 @@ def test_tke_closure_fp32_vs_fp64_spins_up(oracle_lib):
     assert changed > 1e-3
 
 
+def test_fourth_order_vertical_advection(oracle_lib):
+    """advopt=3 (advuvw.f90 / advs.f90 / advp.f90, the advopt.eq.3 branches):
+    float and double agree, and the result differs from advopt=2 by a
+    small amount (the vertical truncation error of the 2nd-order scheme)."""
+    from cress_b200 import cases
+    dx, dz = 500.0, 300.0
+    case = cases.dry_case(24, 20, 16, dx, dz, sthopt=1, seed=3, vspbar=0.005, dthdz=0.0, noise=0.5)
+    ni, nj, nk = case["dims"]
+    zph = case["zph"]
+    out = {}
+    for adv, prec in ((3, 32), (3, 64), (2, 32)):
+        cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=1, vspbar=0.005,
+                   botbar=0.6 * zph[nk - 1], advopt=adv)
+        past = [a.copy() for a in case["level"]]
+        now = [a.copy() for a in case["level"]]
+        oracle_lib.dry_steps(cfg, case["base"], zph, past, now, 3, 2.0, 0.25, start=True, prec=prec)
+        out[(adv, prec)] = now
+    sl = (slice(0, nk - 1), slice(2, nj - 1), slice(2, ni - 1))
+    changed = 0.0
+    for n in range(5):
+        a, b, c = out[(3, 32)][n][sl], out[(3, 64)][n][sl], out[(2, 32)][n][sl]
+        scale = float(np.abs(b).max()) + 1e-12
+        assert np.isfinite(a).all()
+        assert float(np.abs(a - b).max()) <= 1e-3 * scale
+        changed = max(changed, float(np.abs(a - c).max()) / scale)
+    assert 1e-7 < changed < 1e-2
+
+
 def test_base_state_restatement_is_hydrostatic(oracle_lib):
     """The base state from the supercell sounding (set1d ... sndwave): the
     Exner function falls with height at the rate -g / (cp theta_v) to the

@@ -36,7 +36,7 @@ def seeded_tke(shape, seed, amp=0.4):
     return H.bcycle(t, "s")
 
 
-def run_dry(cress, oracle_lib, nx, ny, nz, nsteps, seed, tke0):
+def run_dry(cress, oracle_lib, nx, ny, nz, nsteps, seed, tke0, advopt=2):
     from cress_b200 import cases
     dx, dz, dtbig, dtsml = 500.0, 300.0, 2.0, 0.25
     case = cases.dry_case(nx, ny, nz, dx, dz, sthopt=1, seed=seed, vspbar=0.005, dthdz=0.0, noise=0.5)
@@ -48,12 +48,12 @@ def run_dry(cress, oracle_lib, nx, ny, nz, nsteps, seed, tke0):
     tke = seeded_tke(shape, seed + 100) if tke0 else np.zeros(shape, np.float32)
     init = list(case["level"]) + [tke]
     cfg = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, sthopt=1, smtopt=3, vspopt=2, coropt=0,
-               vspbar=0.005, botbar=botbar, tubopt=2)
+               vspbar=0.005, botbar=botbar, tubopt=2, advopt=advopt)
     past = [a.copy() for a in init]
     now = [a.copy() for a in init]
     oracle_lib.dry_steps(cfg, case["base"], zph, past, now, nsteps, dtbig, dtsml, start=True)
 
-    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, tubopt=2)
+    s = cress.Solver(ni, nj, nk, dx, dx, dz, sthopt=1, tubopt=2, advopt=advopt)
     s.set_base3d(case["base"])
     s.set_base_large(case["base"]["ubr"], case["base"]["vbr"], cases.expand(rbct, ni, nj, nk), ksp0)
     names = LG.NAMES + ["tke"]
@@ -90,6 +90,12 @@ def test_dry_large_steps_tke_seeded(cress, oracle_lib):
 
 def test_dry_large_steps_tke_from_zero_ragged(cress, oracle_lib):
     dims, ref, got = run_dry(cress, oracle_lib, 37, 29, 20, 5, seed=9, tke0=False)
+    check_dry(dims, ref, got)
+
+
+def test_dry_large_steps_tke_4th_order_vertical_advection(cress, oracle_lib):
+    # advopt=3 in the TKE equation's advection as well
+    dims, ref, got = run_dry(cress, oracle_lib, 40, 32, 24, 4, seed=6, tke0=True, advopt=3)
     check_dry(dims, ref, got)
 
 
