@@ -59,13 +59,18 @@ struct MCell {
   R ucq, urq, uiq, usq, ugq, ucn, urn, uin, usn, ugn;
 };
 
+// sqrt(sqrt(x)); for x = +-0 it returns x, which is what the two square
+// roots give there, without taking the square root's special-operand path
+// (clear-air cells have zero hydrometeors, so most calls see a zero).
+__device__ __forceinline__ R root4(R x) { return x == R(0) ? x : sqrtf(sqrtf(x)); }
+
 // s_diagnw, SrcOrig/diagnw.f90:120-160: diagnosed cloud and rain numbers.
 __device__ inline void diagnw_cell(R rbr, R qr, R& ncc, R& ncr) {
   const R mrmiv2 = R(1.e-2) / R(MP::mrmax), mr0iv2 = R(1.e2) / R(MP::mr0);
   const R cdiaqr = R(MP::nr0) * R(MP::nr0) * R(MP::nr0) / (R(MP::cc) * R(MP::rhow));
   const R rbv = R(1) / rbr;
   ncc = R(MP::nclcst) * rbv;
-  ncr = sqrtf(sqrtf(cdiaqr * rbr * qr)) * rbv;
+  ncr = root4(cdiaqr * rbr * qr) * rbv;
   ncr = fminf(fmaxf(ncr, mrmiv2 * qr), mr0iv2 * qr);
 }
 
@@ -77,10 +82,10 @@ __device__ inline void adjstni_cell(R rbr, R rbv, R qi, R qs, R qg, R& nci, R& n
   const R cdiaqs = R(MP::ns0) * R(MP::ns0) * R(MP::ns0) / (R(MP::cc) * R(MP::rhos));
   const R cdiaqg = R(MP::ng0) * R(MP::ng0) * R(MP::ng0) / (R(MP::cc) * R(MP::rhog));
   nci = fminf(fmaxf(nci, mimiv5 * qi), mi0iv2 * qi);
-  R ndia = sqrtf(sqrtf(cdiaqs * rbr * qs)) * rbv;
+  R ndia = root4(cdiaqs * rbr * qs) * rbv;
   ncs = fmaxf(fmaxf(ncs, msmiv2 * qs), R(5.62341e-3) * ndia);
   ncs = fminf(fminf(ncs, ms0iv2 * qs), R(1.77838e2) * ndia);
-  ndia = sqrtf(sqrtf(cdiaqg * rbr * qg)) * rbv;
+  ndia = root4(cdiaqg * rbr * qg) * rbv;
   ncg = fmaxf(fmaxf(ncg, mgmiv2 * qg), R(5.62341e-3) * ndia);
   ncg = fminf(fminf(ncg, mg0iv2 * qg), R(1.77838e2) * ndia);
 }
