@@ -750,37 +750,40 @@ def main():
     # End to end through the public API with host buffers: every step the
     # past and present levels (14 fields each) go host->device from pinned
     # memory, one large step runs, the new present level (14 fields) comes
-    # back.  The read-back of step n runs on a second stream while step n+1
-    # copies its inputs in (the link is full duplex); the host has step n's
-    # result once the next step is queued (results double-buffered).
+    # back.  The inputs of step n+1 are queued on their own stream before
+    # the host waits, so they cross while step n computes; the read-back of
+    # step n runs on a third stream (the link is full duplex); the host
+    # waits for step n-1's result while step n's is in flight (results
+    # double-buffered).
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     past_h = [pin(a) for a in init]
     now_h = [pin(a) for a in init]
     out_h = [[pin(np.empty_like(a)) for a in init] for _ in range(2)]
 
-    def e2e_step(i):
-        for n, a, b in zip(names, past_h, now_h):
-            s.put_field(n, cress_b200.PAST, a)
-            s.put_field(n, cress_b200.NOW, b)
-        s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
-        if i > 0:
-            s.wait_fields()   # step i-1's result is on the host
-        s.get_fields_async(cress_b200.NOW, names, out_h[i % 2])
+    def e2e_run(nsteps):
+        s.put_fields_async(cress_b200.PAST, names, past_h)
+        s.put_fields_async(cress_b200.NOW, names, now_h)
+        for i in range(nsteps):
+            s.large_step(CTIME, args.dtbig, nsstp, args.dtsml)
+            s.get_fields_async(cress_b200.NOW, names, out_h[i % 2])
+            if i + 1 < nsteps:   # the next step's inputs
+                s.put_fields_async(cress_b200.PAST, names, past_h)
+                s.put_fields_async(cress_b200.NOW, names, now_h)
+            s.wait_fields(in_flight=1)   # step i-1's result is on the host
+        s.wait_fields()
 
-    for i in range(args.warmup):
-        e2e_step(i)
-    s.wait_fields()
+    e2e_run(args.warmup)
     barrier()
     t0 = time.perf_counter()
-    for i in range(args.steps):
-        e2e_step(i)
-    s.wait_fields()
+    e2e_run(args.steps)
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
            "h2d_bytes_per_step": int(sum(a.nbytes for a in past_h + now_h)),
            "d2h_bytes_per_step": int(sum(a.nbytes for a in out_h[0])),
-           "overlap": "device->host read-back of step n on a second stream during step n+1's host->device copies"}
+           "overlap": "host->device copies of step n+1 on their own stream during step n's compute; "
+                      "device->host read-back of step n on a third stream during step n+1's host->device copies; "
+                      "the host waits for step n-1's result while step n's is in flight"}
     io = None if args.no_records else records_leg(s, stream, names)
     s.close()
 

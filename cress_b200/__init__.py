@@ -121,6 +121,8 @@ def lib():
     L.cress_set_spin_limit.argtypes = [vp, i]
     L.cress_get_fields_async.argtypes = [vp, i, i, ctypes.POINTER(i), ctypes.POINTER(_FP)]
     L.cress_wait_fields.argtypes = [vp]
+    L.cress_wait_fields_to.argtypes = [vp, i]
+    L.cress_put_fields_async.argtypes = [vp, i, i, ctypes.POINTER(i), ctypes.POINTER(_FP)]
     ll = ctypes.c_longlong
     L.cress_dump_3d.argtypes = [vp, i, ctypes.c_char_p, vp, ll, ctypes.POINTER(ll), ctypes.c_char_p, i]
     L.cress_restart_write.argtypes = [vp, vp, ll, ctypes.POINTER(ll)]
@@ -267,11 +269,28 @@ class Solver:
             assert a.shape == self.shape and a.dtype == np.float32 and a.flags.c_contiguous
         ids = (ctypes.c_int * len(names))(*[FIELD_ID[n] for n in names])
         ptrs = (_FP * len(outs))(*[fptr(a) for a in outs])
-        self._async_keep = (ids, ptrs, list(outs))
+        # two read-backs may be in flight: keep both sets of arguments alive
+        self._async_keep = (getattr(self, "_async_keep", ()) + ((ids, ptrs, list(outs)),))[-2:]
         _check(lib().cress_get_fields_async(self._h, int(level), len(names), ids, ptrs))
 
-    def wait_fields(self):
-        _check(lib().cress_wait_fields(self._h))
+    def wait_fields(self, in_flight=0):
+        """Wait until at most `in_flight` (0 or 1) read-backs are running."""
+        _check(lib().cress_wait_fields_to(self._h, int(in_flight)))
+
+    def put_fields_async(self, level, names, arrs):
+        """Start copying host arrays into fields of one level (see
+        cress_put_fields_async): the copies overlap the work already queued
+        and the values are in the level for the calls that follow.  The
+        arrays (float32, C-contiguous, preferably page-locked) are kept
+        referenced here and must not change until a synchronizing call."""
+        for a in arrs:
+            assert a.shape == self.shape and a.dtype == np.float32 and a.flags.c_contiguous
+        ids = (ctypes.c_int * len(names))(*[FIELD_ID[n] for n in names])
+        ptrs = (_FP * len(arrs))(*[fptr(a) for a in arrs])
+        if not hasattr(self, "_put_keep"):
+            self._put_keep = {}
+        self._put_keep[int(level)] = (ids, ptrs, list(arrs))
+        _check(lib().cress_put_fields_async(self._h, int(level), len(names), ids, ptrs))
 
     def dump_3d(self, dmpvar, level=NOW, out=None):
         """The 3-D dump records of one level as s_outdmp writes them (dmplev

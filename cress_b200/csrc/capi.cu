@@ -133,8 +133,19 @@ Ctx::~Ctx() {
     cudaStreamSynchronize(copy_stream);
     cudaStreamDestroy(copy_stream);
   }
-  if (ev_out) cudaEventDestroy(ev_out);
-  if (ev_done) cudaEventDestroy(ev_done);
+  for (int b = 0; b < 2; ++b) {
+    if (ev_out[b]) cudaEventDestroy(ev_out[b]);
+    if (ev_done[b]) cudaEventDestroy(ev_done[b]);
+  }
+  if (err_h) cudaFreeHost(err_h);
+  if (in_stream) {
+    cudaStreamSynchronize(in_stream);
+    cudaStreamDestroy(in_stream);
+  }
+  for (int l = 0; l < 4; ++l) {
+    if (ev_in[l]) cudaEventDestroy(ev_in[l]);
+    if (ev_in_free[l]) cudaEventDestroy(ev_in_free[l]);
+  }
   free_graphs();
   free_learned();
   if (slab) cress_slab_detach(reinterpret_cast<cress_ctx*>(this));
@@ -179,47 +190,106 @@ int Ctx::get_host(float* host, const float* src) {
 
 // Asynchronous read-back of whole fields of one time level: the fields
 // are repitched on the context's stream into one host-layout buffer each
-// (kept until the next read-back), then copied to the host on a second
-// stream.  A later read-back waits for the previous copies before it
-// reuses the buffers; cress_wait_fields waits for them on the host.
+// (two sets, used in turn), then copied to the host on a second stream,
+// with the device error word as the work before the read-back left it.
+// A read-back's repitch waits on the device for the copies of the
+// read-back two before it, the last user of its set; cress_wait_fields
+// waits for them on the host without waiting for the context's stream.
 int Ctx::get_async(int level, int n, const int* fields, float* const* host) {
   int rc;
   if (!copy_stream) {
     if ((rc = cuda_check(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "copy stream")) ||
-        (rc = cuda_check(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming), "event")) ||
-        (rc = cuda_check(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming), "event")))
+        (rc = cuda_check(cudaHostAlloc(&err_h, 2 * sizeof(int), cudaHostAllocDefault), "cudaHostAlloc error words")))
       return rc;
+    for (int b = 0; b < 2; ++b)
+      if ((rc = cuda_check(cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming), "event")) ||
+          (rc = cuda_check(cudaEventCreateWithFlags(&ev_done[b], cudaEventDisableTiming), "event")))
+        return rc;
   }
   const long long rows = (long long)(g.nj + 2) * g.nk;
   const size_t bytes = sizeof(float) * (size_t)(g.ni + 2) * (size_t)rows;
-  if (out_pending && (rc = cuda_check(cudaStreamWaitEvent(stream, ev_done, 0), "wait previous read-back")))
+  const int b = (int)(out_issued & 1);
+  if (out_issued >= 2 && (rc = cuda_check(cudaStreamWaitEvent(stream, ev_done[b], 0), "wait earlier read-back")))
     return rc;
   for (int q = 0; q < n; ++q) {
-    const int f = fields[q];
-    if (!stage_out[f]) {
-      if ((rc = cuda_check(cudaMalloc(&stage_out[f], bytes), "cudaMalloc read-back buffer"))) return rc;
-      owned.push_back(stage_out[f]);
+    float*& st = stage_out[fields[q]][b];
+    if (!st) {
+      if ((rc = cuda_check(cudaMalloc(&st, bytes), "cudaMalloc read-back buffer"))) return rc;
+      owned.push_back(st);
     }
-    if ((rc = launch_repitch(lev[f][level], g.px, stage_out[f], g.ni + 2, g.ni + 2, rows, stream))) return rc;
+    if ((rc = launch_repitch(lev[fields[q]][level], g.px, st, g.ni + 2, g.ni + 2, rows, stream))) return rc;
     ++launches;
   }
-  if ((rc = cuda_check(cudaEventRecord(ev_out, stream), "record read-back")) ||
-      (rc = cuda_check(cudaStreamWaitEvent(copy_stream, ev_out, 0), "order read-back")))
+  if ((rc = cuda_check(cudaEventRecord(ev_out[b], stream), "record read-back")) ||
+      (rc = cuda_check(cudaStreamWaitEvent(copy_stream, ev_out[b], 0), "order read-back")) ||
+      (rc = cuda_check(cudaMemcpyAsync(&err_h[b], err_d, sizeof(int), cudaMemcpyDeviceToHost, copy_stream),
+                       "read error word")))
     return rc;
   for (int q = 0; q < n; ++q)
-    if ((rc = cuda_check(cudaMemcpyAsync(host[q], stage_out[fields[q]], bytes, cudaMemcpyDeviceToHost, copy_stream),
+    if ((rc = cuda_check(cudaMemcpyAsync(host[q], stage_out[fields[q]][b], bytes, cudaMemcpyDeviceToHost, copy_stream),
                          "device->host copy")))
       return rc;
-  if ((rc = cuda_check(cudaEventRecord(ev_done, copy_stream), "record read-back done"))) return rc;
-  out_pending = true;
+  if ((rc = cuda_check(cudaEventRecord(ev_done[b], copy_stream), "record read-back done"))) return rc;
+  ++out_issued;
   return CRESS_OK;
 }
 
-int Ctx::wait_async() {
-  if (!out_pending) return CRESS_OK;
-  int rc = cuda_check(cudaEventSynchronize(ev_done), "wait read-back");
-  if (!rc) out_pending = false;
-  return rc;
+// Asynchronous input of whole fields of one time level: contiguous
+// host->device copies on in_stream, each into its own staging buffer, then
+// the repitch kernels on the context's stream, so the copies overlap the
+// work already queued there (the previous step) and the copy engine is not
+// held up by the repitch of the field before.
+int Ctx::put_async(int level, int n, const int* fields, const float* const* host) {
+  int rc;
+  if (!in_stream && (rc = cuda_check(cudaStreamCreateWithFlags(&in_stream, cudaStreamNonBlocking), "input stream")))
+    return rc;
+  if (!ev_in[level] &&
+      ((rc = cuda_check(cudaEventCreateWithFlags(&ev_in[level], cudaEventDisableTiming), "event")) ||
+       (rc = cuda_check(cudaEventCreateWithFlags(&ev_in_free[level], cudaEventDisableTiming), "event"))))
+    return rc;
+  const long long rows = (long long)(g.nj + 2) * g.nk;
+  const size_t bytes = sizeof(float) * (size_t)(g.ni + 2) * (size_t)rows;
+  if (in_used[level] && (rc = cuda_check(cudaStreamWaitEvent(in_stream, ev_in_free[level], 0), "order input copies")))
+    return rc;
+  for (int q = 0; q < n; ++q) {
+    float*& st = stage_in[fields[q]][level];
+    if (!st) {
+      if ((rc = cuda_check(cudaMalloc(&st, bytes), "cudaMalloc input buffer"))) return rc;
+      owned.push_back(st);
+    }
+    if ((rc = cuda_check(cudaMemcpyAsync(st, host[q], bytes, cudaMemcpyHostToDevice, in_stream), "host->device copy")))
+      return rc;
+  }
+  if ((rc = cuda_check(cudaEventRecord(ev_in[level], in_stream), "record input copies")) ||
+      (rc = cuda_check(cudaStreamWaitEvent(stream, ev_in[level], 0), "wait input copies")))
+    return rc;
+  for (int q = 0; q < n; ++q) {
+    const int f = fields[q];
+    if ((rc = launch_repitch(stage_in[f][level], g.ni + 2, lev[f][level], g.px, g.ni + 2, rows, stream))) return rc;
+    ++launches;
+  }
+  if ((rc = cuda_check(cudaEventRecord(ev_in_free[level], stream), "record input repitch"))) return rc;
+  in_used[level] = true;
+  return CRESS_OK;
+}
+
+// Read-backs complete in issue order (one copy stream).  A nonzero error
+// word in a completed read-back (a bounded device-side wait gave up in the
+// work before it) is reported once and the word cleared.
+int Ctx::wait_async(int keep) {
+  bool failed = false;
+  while (out_issued - out_waited > keep) {
+    const int b = (int)(out_waited & 1);
+    const int rc = cuda_check(cudaEventSynchronize(ev_done[b]), "wait read-back");
+    if (rc) return rc;
+    failed = failed || err_h[b] != 0;
+    ++out_waited;
+  }
+  if (failed) {
+    cudaMemsetAsync(err_d, 0, sizeof(int), stream);
+    return set_error(CRESS_E_TIMEOUT, "a bounded device-side wait gave up (TMA staging did not complete)");
+  }
+  return CRESS_OK;
 }
 
 // Elimination factors of the w system for one dts (w_system_factors,
@@ -1061,7 +1131,7 @@ using namespace cress;
 extern "C" {
 
 const char* cress_last_error(void) { return g_last_error.c_str(); }
-int cress_abi_version(void) { return 4; }
+int cress_abi_version(void) { return 5; }
 
 int cress_create(const cress_cfg* cfg, int device, cress_ctx** out) {
   if (!cfg || !out) return set_error(CRESS_E_ARG, "cress_create: null argument");
@@ -1280,12 +1350,31 @@ int cress_get_fields_async(cress_ctx* ctx, int level, int nfield, const int* fie
   return c->get_async(level, nfield, fields, host);
 }
 
+int cress_put_fields_async(cress_ctx* ctx, int level, int nfield, const int* fields, const float* const* host) {
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c || !fields || !host || nfield < 1 || nfield > CRESS_NFIELD)
+    return set_error(CRESS_E_ARG, "cress_put_fields_async: bad argument");
+  if (level < 0 || level > 3) return set_error(CRESS_E_ARG, "cress_put_fields_async: level %d", level);
+  for (int q = 0; q < nfield; ++q) {
+    if (fields[q] < 0 || fields[q] >= CRESS_NFIELD || !c->lev[fields[q]][level] || !host[q])
+      return set_error(CRESS_E_ARG, "cress_put_fields_async: field %d not held or null buffer", fields[q]);
+    for (int r = 0; r < q; ++r)
+      if (fields[r] == fields[q]) return set_error(CRESS_E_ARG, "cress_put_fields_async: field %d twice", fields[q]);
+  }
+  cudaSetDevice(c->device);
+  return c->put_async(level, nfield, fields, host);
+}
+
 int cress_wait_fields(cress_ctx* ctx) {
+  return cress_wait_fields_to(ctx, 0);
+}
+
+int cress_wait_fields_to(cress_ctx* ctx, int in_flight) {
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (!c) return set_error(CRESS_E_ARG, "null context");
+  if (in_flight < 0 || in_flight > 1) return set_error(CRESS_E_ARG, "cress_wait_fields_to: in_flight %d (0 or 1)", in_flight);
   cudaSetDevice(c->device);
-  int rc = c->wait_async();
-  return rc ? rc : c->check_device_error();
+  return c->wait_async(in_flight);
 }
 
 int cress_small_steps(cress_ctx* ctx, int nsstp, float dts) {

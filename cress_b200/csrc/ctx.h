@@ -55,13 +55,26 @@ struct Ctx {
   int get_host(float* host, const float* src);
   // asynchronous read-back (cress_get_fields_async): each field is
   // repitched on `stream` into its own host-layout buffer, then copied to
-  // the host on copy_stream, so the copy overlaps later work on `stream`
+  // the host on copy_stream, so the copy overlaps later work on `stream`.
+  // Two sets of buffers: read-back n uses set n % 2, and its repitch waits
+  // (on the device) only for the copies of read-back n-2.
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t ev_out = nullptr, ev_done = nullptr;
-  float* stage_out[CRESS_NFIELD] = {};
-  bool out_pending = false;
+  cudaEvent_t ev_out[2] = {}, ev_done[2] = {};
+  float* stage_out[CRESS_NFIELD][2] = {};
+  long long out_issued = 0, out_waited = 0;   // read-backs issued / seen complete on the host
+  int* err_h = nullptr;   // page-locked: the device error word as each set's read-back saw it
   int get_async(int level, int n, const int* fields, float* const* host);
-  int wait_async();
+  int wait_async(int keep);   // until at most `keep` read-backs are in flight
+  // asynchronous input (cress_put_fields_async): the host->device copies
+  // run on in_stream into one host-layout buffer per field and level; the
+  // repitch into the level runs on `stream` once they have landed
+  // (ev_in[level]); the next copies into a level's buffers wait for the
+  // repitch that read them (ev_in_free[level])
+  cudaStream_t in_stream = nullptr;
+  cudaEvent_t ev_in[4] = {}, ev_in_free[4] = {};
+  bool in_used[4] = {};
+  float* stage_in[CRESS_NFIELD][4] = {};
+  int put_async(int level, int n, const int* fields, const float* const* host);
   // y-slab decomposition (slab.h): the link to the other ranks, or null
   SlabLink* slab = nullptr;
   // byte stream of the dump and restart records (records.cu), kept and

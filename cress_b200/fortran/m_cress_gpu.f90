@@ -186,6 +186,25 @@
           type(c_ptr), value :: ctx
         end function cress_wait_fields
 
+        integer(c_int) function cress_wait_fields_to(ctx, in_flight)    &
+     &    bind(c, name='cress_wait_fields_to')
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: in_flight
+        end function cress_wait_fields_to
+
+! Input of several fields of one level on a stream of its own, overlapping
+! the work already queued; the host arrays stay unchanged until the next
+! synchronizing call.
+        integer(c_int) function cress_put_fields_async(ctx, level,      &
+     &    nfield, fields, host) bind(c, name='cress_put_fields_async')
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: level, nfield
+          integer(c_int), intent(in) :: fields(*)
+          type(c_ptr), intent(in) :: host(*)
+        end function cress_put_fields_async
+
 ! Dump records of one time level (dmplev = 1, dmpfmt = 2) in the .bin
 ! file's byte layout; host may be c_null_ptr to query nbytes.  The bytes
 ! go to the dump file as they are (access='stream', or one direct-access

@@ -165,12 +165,29 @@ int cress_get_field(cress_ctx* ctx, int field, int level, float* host);
  * the values are captured on the context's stream at this point of its
  * work, and the device->host copies run on a second stream, so they
  * overlap what the context does next (the next step's host->device copies
- * and compute).  The host arrays are filled once cress_wait_fields returns;
- * a later read-back first waits on the device for the previous one.  No
- * counterpart in the reference (the dump writer reads the same arrays,
- * SrcOrig/outdmp3d.f90:159-169). */
+ * and compute).  Two read-backs may be in flight; a third first waits on
+ * the device for the first.  cress_wait_fields returns once every
+ * read-back issued so far has filled its host arrays, cress_wait_fields_to
+ * once at most in_flight (0 or 1) of them are still running (the older
+ * ones are filled); neither waits for the context's other work.  Both
+ * return CRESS_E_TIMEOUT if a bounded device-side wait gave up in the work
+ * before a completed read-back.  No counterpart in the reference (the dump
+ * writer reads the same arrays, SrcOrig/outdmp3d.f90:159-169). */
 int cress_get_fields_async(cress_ctx* ctx, int level, int nfield, const int* fields, float* const* host);
 int cress_wait_fields(cress_ctx* ctx);
+int cress_wait_fields_to(cress_ctx* ctx, int in_flight);
+
+/* Asynchronous input of nfield distinct fields of one time level from host
+ * arrays (reference layout; page-locked memory for the copies to overlap):
+ * the host->device copies run on a stream of their own, so they overlap
+ * the work the context already has queued (a previous step's compute and
+ * read-back), and the values enter the level at this point of the
+ * context's work, for the calls that follow.  Keep the host arrays
+ * unchanged until a synchronizing call (cress_sync, cress_get_field,
+ * cress_diagnostics) or a cress_wait_fields for a read-back issued after
+ * this call returns.  No counterpart in the reference (its host arrays are
+ * the state). */
+int cress_put_fields_async(cress_ctx* ctx, int level, int nfield, const int* fields, const float* const* host);
 
 /* Dump file records formed on the device: the 3-D history dump of one
  * time level as s_outdmp / s_outdmp3d write it for dmplev = 1 and

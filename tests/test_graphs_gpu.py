@@ -82,3 +82,50 @@ def test_async_readback_matches_sync(cress, oracle_lib):
         assert np.array_equal(g, w), (4, f)
     s.close()
     ref.close()
+
+
+def test_async_input_matches_put_field(cress, oracle_lib):
+    """cress_put_fields_async: every step's past and present levels go in
+    from host arrays on the input stream, queued behind the previous step,
+    whose compute and read-back are still in flight, and the host waits
+    for a step's result only after the next step is queued (two read-backs
+    in flight); each step's result equals the same step fed through
+    cress_put_field, bit for bit, with inputs that differ from step to step
+    (states of a third run)."""
+    import torch
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    src, names = make(cress, oracle_lib, True, 3)
+    states = []
+    src.large_step(0, 2.5, 10, 0.5)
+    for n in range(1, 5):
+        src.large_step(n * 5000, 5.0, 10, 1.0)
+        states.append(([pin(src.get_field(f, cress.PAST)) for f in names],
+                       [pin(src.get_field(f, cress.NOW)) for f in names]))
+    src.close()
+    ref, _ = make(cress, oracle_lib, True, 3)
+    want = []
+    for n, (past, now) in enumerate(states):
+        for f, a, b in zip(names, past, now):
+            ref.put_field(f, cress.PAST, a)
+            ref.put_field(f, cress.NOW, b)
+        ref.large_step(50000 + n * 5000, 5.0, 10, 1.0)
+        want.append([ref.get_field(f, cress.NOW) for f in names])
+    ref.close()
+    s, _ = make(cress, oracle_lib, True, 3)
+    bufs = [[pin(np.zeros(s.shape, np.float32)) for _ in names] for _ in range(2)]
+    s.put_fields_async(cress.PAST, names, states[0][0])
+    s.put_fields_async(cress.NOW, names, states[0][1])
+    for n in range(len(states)):
+        s.large_step(50000 + n * 5000, 5.0, 10, 1.0)
+        s.get_fields_async(cress.NOW, names, bufs[n % 2])
+        if n + 1 < len(states):   # the next inputs, queued before the host waits
+            s.put_fields_async(cress.PAST, names, states[n + 1][0])
+            s.put_fields_async(cress.NOW, names, states[n + 1][1])
+        s.wait_fields(in_flight=1)
+        if n > 0:
+            for f, g, w in zip(names, bufs[(n - 1) % 2], want[n - 1]):
+                assert np.array_equal(g, w), (n - 1, f)
+    s.wait_fields()
+    for f, g, w in zip(names, bufs[(len(states) - 1) % 2], want[-1]):
+        assert np.array_equal(g, w), (len(states) - 1, f)
+    s.close()
