@@ -117,6 +117,8 @@ def lib():
     L.cress_ensemble_destroy.restype = None
     L.cress_ensemble_large_step.argtypes = [vp, ll, f, i, f]
     L.cress_ensemble_set_graphs.argtypes = [vp, i]
+    L.cress_ensemble_set_tile.argtypes = [vp, i]
+    L.cress_ensemble_autotune.argtypes = [vp, i, f, i, ctypes.POINTER(i), ctypes.POINTER(f)]
     L.cress_autotune.argtypes = [vp, i, f, i, ctypes.POINTER(i), ctypes.POINTER(f)]
     L.cress_set_spin_limit.argtypes = [vp, i]
     L.cress_get_fields_async.argtypes = [vp, i, i, ctypes.POINTER(i), ctypes.POINTER(_FP)]
@@ -478,6 +480,18 @@ class Ensemble:
 
     def large_step(self, ctime, dtb, nsstp, dts):
         _check(lib().cress_ensemble_large_step(self._h, int(ctime), float(dtb), int(nsstp), float(dts)))
+
+    def set_tile(self, tile):
+        """The batched acoustic kernel: 0 or 13 (see cress_ensemble_set_tile)."""
+        _check(lib().cress_ensemble_set_tile(self._h, int(tile)))
+
+    def autotune(self, nsstp, dts, reps=3):
+        """Time the batched substep with tiles 0 and 13, keep the faster;
+        returns (tile, {tile: ms per substep})."""
+        best = ctypes.c_int(-1)
+        ms = (ctypes.c_float * 2)()
+        _check(lib().cress_ensemble_autotune(self._h, int(nsstp), float(dts), int(reps), ctypes.byref(best), ms))
+        return best.value, {0: ms[0], 13: ms[1]}
 
     def close(self):
         if self._h:

@@ -406,8 +406,8 @@ int Ctx::small_steps(int nsstp, float dts) { return small_steps(nsstp, dts, null
 
 int Ctx::small_steps(int nsstp, float dts, std::vector<HeviJob>* jobs) {
   if (!base_set) return set_error(CRESS_E_STATE, "cress_small_steps: base state not set");
-  if (jobs && (cfg.impopt != 1 || cfg.tile != 0 || g.openx))
-    return set_error(CRESS_E_UNSUPPORTED, "ensemble small steps need impopt=1, tile 0 and periodic x");
+  if (jobs && (cfg.impopt != 1 || (cfg.tile != 0 && cfg.tile != 13) || g.openx))
+    return set_error(CRESS_E_UNSUPPORTED, "ensemble small steps need impopt=1, tile 0 or 13 and periodic x");
   if (g.openx && cfg.tile != 0 && cfg.tile != 11 && cfg.tile != 12 && cfg.tile != 13)
     return set_error(CRESS_E_UNSUPPORTED, "open x boundaries run the HE-VI tiles 0, 11, 12 and 13");
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_small_steps: nsstp=%d", nsstp);
@@ -937,6 +937,7 @@ struct Ensemble {
   cudaEvent_t staged = nullptr;       // the last copy out of jobs_h has completed
   long long launches = 0;
   bool graphs = true;
+  int tile = 0;                       // the batched acoustic kernel: tile 0's or tile 13's
   struct Rec {
     cudaGraphExec_t exec = nullptr;
     HeviJob* jobs_d = nullptr;        // this graph's job table and its pinned source
@@ -970,6 +971,15 @@ struct Ensemble {
   }
   int large_step(long long ctime, float dtb, int nsstp, float dts, HeviJob* jd, HeviJob* jh, bool eager);
   int step(long long ctime, float dtb, int nsstp, float dts);
+  int set_tile(int t);
+  int batch(const HeviJob* jd, int nblocks, int nk_max) {
+    const cress_cfg& c0 = members[0]->cfg;
+    const int n = (int)members.size();
+    return tile == 13 ? launch_hevi4_batch(jd, n, nblocks, nk_max, c0.divopt, c0.sthopt != 0, c0.buyopt == 1, stream)
+                      : launch_hevi_batch(jd, n, nblocks, nk_max, c0.divopt, c0.sthopt != 0, c0.buyopt == 1, stream);
+  }
+  int jobs_for(int nsstp, float dts, HeviJob* jh, int* nblocks, int* nk_max);
+  int autotune(int nsstp, float dts, int reps, int* best, float* ms);
 };
 
 // One ensemble step issued on the streams (eager, or inside a capture that
@@ -985,26 +995,10 @@ int Ensemble::large_step(long long ctime, float dtb, int nsstp, float dts, HeviJ
     cudaStreamWaitEvent(c->stream, fork, 0);
     if ((rc = c->large_step(filter, dtb, nsstp, dts, 1))) return rc;
   }
-  std::vector<std::vector<HeviJob>> per(n);
-  int nk_max = 0;
-  for (int m = 0; m < n; ++m) {
-    if ((rc = members[m]->small_steps(nsstp, dts, &per[m]))) return rc;
-    nk_max = std::max(nk_max, members[m]->g.nk);
-  }
   const size_t need = (size_t)nsstp * n;
   if (eager) cudaEventSynchronize(staged);   // the previous step's copy has left the staging buffer
-  int nblocks = 0;
-  for (int m = 0; m < n; ++m) {
-    int tx, ty;
-    hevi_job_tiles(members[m]->g, &tx, &ty);
-    for (int st = 0; st < nsstp; ++st) {
-      HeviJob& j = jh[(size_t)st * n + m];
-      j = per[m][st];
-      j.first_block = nblocks;
-      j.tiles_x = tx;
-    }
-    nblocks += tx * ty;
-  }
+  int nblocks = 0, nk_max = 0;
+  if ((rc = jobs_for(nsstp, dts, jh, &nblocks, &nk_max))) return rc;
   for (int m = 0; m < n; ++m) {
     cudaEventRecord(ev[m], members[m]->stream);
     cudaStreamWaitEvent(stream, ev[m], 0);
@@ -1013,10 +1007,8 @@ int Ensemble::large_step(long long ctime, float dtb, int nsstp, float dts, HeviJ
                        "copy ensemble jobs")))
     return rc;
   if (eager) cudaEventRecord(staged, stream);
-  const cress_cfg& c0 = members[0]->cfg;
   for (int st = 0; st < nsstp; ++st) {
-    if ((rc = launch_hevi_batch(jd + (size_t)st * n, n, nblocks, nk_max, c0.divopt, c0.sthopt != 0,
-                                c0.buyopt == 1, stream)))
+    if ((rc = batch(jd + (size_t)st * n, nblocks, nk_max)))
       return set_error(rc, "ensemble small-step launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     ++launches;
   }
@@ -1031,6 +1023,104 @@ int Ensemble::large_step(long long ctime, float dtb, int nsstp, float dts, HeviJ
     cudaStreamWaitEvent(stream, ev[m], 0);
   }
   return CRESS_OK;
+}
+
+// The acoustic jobs of one large step: nsstp x members HeviJobs in jh
+// (substep-major, members in block order), the blocks of one launch and
+// the deepest member.
+int Ensemble::jobs_for(int nsstp, float dts, HeviJob* jh, int* nblocks, int* nk_max) {
+  const int n = (int)members.size();
+  int rc;
+  *nblocks = 0;
+  *nk_max = 0;
+  for (int m = 0; m < n; ++m) {
+    std::vector<HeviJob> per;
+    if ((rc = members[m]->small_steps(nsstp, dts, &per))) return rc;
+    *nk_max = std::max(*nk_max, members[m]->g.nk);
+    int tx, ty;
+    hevi_job_tiles(members[m]->g, &tx, &ty);
+    for (int st = 0; st < nsstp; ++st) {
+      HeviJob& j = jh[(size_t)st * n + m];
+      j = per[st];
+      j.first_block = *nblocks;
+      j.tiles_x = tx;
+    }
+    *nblocks += tx * ty;
+  }
+  return CRESS_OK;
+}
+
+// Tile 13 holds each column's eliminated right-hand sides on chip, so every
+// member needs nk <= kHevi3MaxNk.
+int Ensemble::set_tile(int t) {
+  if (t != 0 && t != 13) return set_error(CRESS_E_ARG, "ensemble tile %d (0 or 13)", t);
+  if (t == 13)
+    for (Ctx* c : members)
+      if (c->g.nk > kHevi3MaxNk || c->g.nk < 8)
+        return set_error(CRESS_E_UNSUPPORTED, "ensemble tile 13 needs 8 <= nk <= %d", kHevi3MaxNk);
+  cudaStreamSynchronize(stream);
+  free_graphs();
+  for (Ctx* c : members) {
+    cudaStreamSynchronize(c->stream);
+    c->free_graphs();
+    c->cfg.tile = t;
+  }
+  tile = t;
+  return CRESS_OK;
+}
+
+// Time the batched substep with each tile on the members' present forcing
+// (the future levels are overwritten, the present and past are not) and
+// keep the faster.  ms[0], ms[1]: tile 0, tile 13 (-1: not usable).
+int Ensemble::autotune(int nsstp, float dts, int reps, int* best, float* ms) {
+  if (nsstp < 1 || reps < 1) return set_error(CRESS_E_ARG, "cress_ensemble_autotune: nsstp=%d reps=%d", nsstp, reps);
+  const int n = (int)members.size(), keep = tile;
+  const size_t need = (size_t)nsstp * n;
+  HeviJob* jd = nullptr;
+  HeviJob* jh = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = CRESS_OK, best_t = -1;
+  float best_ms = 0.f;
+  if (cudaMalloc(&jd, sizeof(HeviJob) * need) != cudaSuccess ||
+      cudaMallocHost(&jh, sizeof(HeviJob) * need) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess)
+    rc = set_error(CRESS_E_CUDA, "cress_ensemble_autotune: allocation failed");
+  const int cand[2] = {0, 13};
+  for (int q = 0; q < 2 && !rc; ++q) {
+    if (ms) ms[q] = -1.f;
+    if (set_tile(cand[q]) != CRESS_OK) continue;   // tile 13 needs nk <= kHevi3MaxNk
+    int nblocks = 0, nk_max = 0;
+    if ((rc = jobs_for(nsstp, dts, jh, &nblocks, &nk_max))) break;
+    if ((rc = cuda_check(cudaMemcpyAsync(jd, jh, sizeof(HeviJob) * need, cudaMemcpyHostToDevice, stream),
+                         "copy ensemble jobs")))
+      break;
+    for (int st = 0; st < nsstp && !rc; ++st) rc = batch(jd + (size_t)st * n, nblocks, nk_max);   // warm-up
+    cudaEventRecord(e0, stream);
+    for (int r = 0; r < reps && !rc; ++r)
+      for (int st = 0; st < nsstp && !rc; ++st) rc = batch(jd + (size_t)st * n, nblocks, nk_max);
+    cudaEventRecord(e1, stream);
+    if (rc == CRESS_E_UNSUPPORTED) { rc = CRESS_OK; continue; }
+    if (rc || (rc = cuda_check(cudaEventSynchronize(e1), "ensemble autotune sync"))) break;
+    for (Ctx* c : members)
+      if ((rc = c->check_device_error())) break;
+    if (rc) break;
+    float t_ms = 0.f;
+    cudaEventElapsedTime(&t_ms, e0, e1);
+    t_ms /= (float)(reps * nsstp);
+    if (ms) ms[q] = t_ms;
+    if (best_t < 0 || t_ms < best_ms) { best_ms = t_ms; best_t = cand[q]; }
+  }
+  cudaStreamSynchronize(stream);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (jd) cudaFree(jd);
+  if (jh) cudaFreeHost(jh);
+  if (rc || best_t < 0) {
+    set_tile(keep);
+    return rc ? rc : set_error(CRESS_E_UNSUPPORTED, "cress_ensemble_autotune: no batched tile fits");
+  }
+  if (best) *best = best_t;
+  return set_tile(best_t);
 }
 
 int Ensemble::step(long long ctime, float dtb, int nsstp, float dts) {
@@ -1716,9 +1806,13 @@ int cress_ensemble_create(cress_ctx* const* members, int n, cress_ensemble** out
     Ctx* c = reinterpret_cast<Ctx*>(members[m]);
     cudaStreamSynchronize(c->stream);
     c->free_graphs();
-    c->cfg.tile = 0;        // the ensemble launch runs tile 0's kernel
     e->members.push_back(c);
   }
+  // the batched acoustic kernel: tile 13 when every member asks for it,
+  // else tile 0 (the members follow the ensemble's choice)
+  bool all13 = true;
+  for (Ctx* c : e->members) all13 = all13 && c->cfg.tile == 13;
+  if (!(all13 && e->set_tile(13) == CRESS_OK)) e->set_tile(0);
   *out = reinterpret_cast<cress_ensemble*>(e);
   return CRESS_OK;
 }
@@ -1731,6 +1825,20 @@ int cress_ensemble_large_step(cress_ensemble* eh, long long ctime, float dtb, in
   if (nsstp < 1) return set_error(CRESS_E_ARG, "cress_ensemble_large_step: nsstp=%d", nsstp);
   cudaSetDevice(e->device);
   return e->step(ctime, dtb, nsstp, dts);
+}
+
+int cress_ensemble_set_tile(cress_ensemble* eh, int tile) {
+  Ensemble* e = reinterpret_cast<Ensemble*>(eh);
+  if (!e) return set_error(CRESS_E_ARG, "null ensemble");
+  cudaSetDevice(e->device);
+  return e->set_tile(tile);
+}
+
+int cress_ensemble_autotune(cress_ensemble* eh, int nsstp, float dts, int reps, int* best, float* ms) {
+  Ensemble* e = reinterpret_cast<Ensemble*>(eh);
+  if (!e) return set_error(CRESS_E_ARG, "null ensemble");
+  cudaSetDevice(e->device);
+  return e->autotune(nsstp, dts, reps, best, ms);
 }
 
 int cress_ensemble_set_graphs(cress_ensemble* eh, int on) {

@@ -110,8 +110,9 @@ int launch_hevi4(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st);
 // Launch one substep; `maps` must describe the buffers in `a` with the
 // box rows of HeviRows<hevi_tile_rows(tile)>.
 int launch_hevi_substep(const HeviArgs& a, const HeviMaps& maps, int tile, cudaStream_t st);
-// One member's substep in an ensemble launch (tile 0's kernel over every
-// member's tiles); 64-byte aligned for the tensor maps, in block order.
+// One member's substep in an ensemble launch (tile 0's or tile 13's kernel
+// over every member's tiles); 64-byte aligned for the tensor maps, in
+// block order.
 struct alignas(64) HeviJob {
   HeviMaps maps;
   HeviArgs args;
@@ -123,6 +124,10 @@ void hevi_job_tiles(const Grid& g, int* tx, int* ty);
 // all); every member uses divopt, sthopt != 0 (sth), buyopt == 1 (buy).
 int launch_hevi_batch(const HeviJob* jobs_d, int njobs, int nblocks, int nk_max, int divopt, bool sth, bool buy,
                       cudaStream_t st);
+// The same with the one-column-per-thread on-chip kernel (tile 13: the same
+// 32 x 8 tiles; every member's args.lvl4 set, nk <= kHevi3MaxNk).
+int launch_hevi4_batch(const HeviJob* jobs_d, int njobs, int nblocks, int nk_max, int divopt, bool sth, bool buy,
+                       cudaStream_t st);
 
 // One HE-VE substep (impopt=0, s_heve); the maps are those of tile 0's
 // box rows (HeviRows<8>) and a.lvl must hold the level table.

@@ -28,6 +28,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 #include "common.cuh"
 #include "hevi.cuh"
 #include "tma.cuh"
@@ -101,6 +102,7 @@ struct H4Env {
   uint64_t* bars;
   const float4* rows;      // the level table
   uint32_t tcol;           // this warp's tensor-memory columns
+  int bx, by;              // the tile's position in the domain's tile grid
   int tid, tx, i, j, ho;
   bool has_halo, own, edge, xlast, ylast;
 };
@@ -113,7 +115,7 @@ __device__ __forceinline__ void h4_issue(const HeviMaps& m, const H4Env& e, H4Up
   const int s = (k - 2) % S;
   float* st = e.ring + s * L::stage;
   uint64_t* bar = &e.bars[s];
-  const int z = k - 1, xb = blockIdx.x * kH4TX, j0 = 2 + blockIdx.y * kH4TY;
+  const int z = k - 1, xb = e.bx * kH4TX, j0 = 2 + e.by * kH4TY;
   mbar_arrive_expect_tx(bar, L::tx_bytes);
   tma_load_3d(st + L::oU, &m.u, xb, j0 - 1, z, bar);
   tma_load_3d(st + L::oV, &m.v, xb, j0 - 1, z, bar);
@@ -277,16 +279,19 @@ __device__ __forceinline__ void h4_level(const HeviMaps& m, const HeviArgs& a, c
 }
 
 template <int S, int DIV, bool STH, bool BUY, bool EDGE>
-__device__ __forceinline__ void hevi4_tile(const HeviMaps& m, const HeviArgs& a, float* smem, uint32_t tmem) {
+__device__ __forceinline__ void hevi4_tile(const HeviMaps& m, const HeviArgs& a, float* smem, uint32_t tmem, int bx,
+                                           int by) {
   using L = H4Layout<S>;
   constexpr int TX = kH4TX, TY = kH4TY, BX = kHeviBoxX, NT = kH4NT;
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
   H4Env e;
+  e.bx = bx;
+  e.by = by;
   e.tx = threadIdx.x;
   const int ty = threadIdx.y;
   e.tid = ty * TX + e.tx;
-  const int i0 = 2 + blockIdx.x * TX, j0 = 2 + blockIdx.y * TY;
+  const int i0 = 2 + bx * TX, j0 = 2 + by * TY;
   e.i = i0 + e.tx;
   e.j = j0 + ty;
   const int tid = e.tid, i = e.i, j = e.j;
@@ -466,8 +471,12 @@ __device__ __forceinline__ void hevi4_tile(const HeviMaps& m, const HeviArgs& a,
   if (ylast) store_periodic(a.v_new, g, STAG_V, i, j + 1, nk, a.v_old[g.at(i, j + 1, nk)]);
 }
 
+// One block: allocate the block's tensor memory, run tile (bx, by) of a
+// tx_n x ty_n tile grid (the tiles on its border take the edge path), free
+// the tensor memory.
 template <int S, int DIV, bool STH, bool BUY>
-__global__ void __launch_bounds__(kH4NT, 2) k_hevi4(const __grid_constant__ HeviMaps m, const HeviArgs a) {
+__device__ __forceinline__ void hevi4_block(const HeviMaps& m, const HeviArgs& a, int bx, int by, int tx_n,
+                                            int ty_n) {
   extern __shared__ __align__(128) float smem[];
   __shared__ uint32_t tmem_slot;
   const int warp = threadIdx.y;   // blockDim = (32, 8): one warp per thread row
@@ -477,15 +486,55 @@ __global__ void __launch_bounds__(kH4NT, 2) k_hevi4(const __grid_constant__ Hevi
   tc_fence_after();
   // lanes 32(w % 4) .. 32(w % 4) + 31 belong to warp w
   const uint32_t tmem = tmem_slot + ((uint32_t)((warp & 3) * 32) << 16);
-  const bool edge = blockIdx.x == 0 || blockIdx.x == gridDim.x - 1 || blockIdx.y == 0 || blockIdx.y == gridDim.y - 1;
-  if (edge) hevi4_tile<S, DIV, STH, BUY, true>(m, a, smem, tmem);
-  else hevi4_tile<S, DIV, STH, BUY, false>(m, a, smem, tmem);
+  const bool edge = bx == 0 || bx == tx_n - 1 || by == 0 || by == ty_n - 1;
+  if (edge) hevi4_tile<S, DIV, STH, BUY, true>(m, a, smem, tmem, bx, by);
+  else hevi4_tile<S, DIV, STH, BUY, false>(m, a, smem, tmem, bx, by);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
     tmem_dealloc(tmem_slot, kH4TmemCols);
   }
+}
+
+template <int S, int DIV, bool STH, bool BUY>
+__global__ void __launch_bounds__(kH4NT, 2) k_hevi4(const __grid_constant__ HeviMaps m, const HeviArgs a) {
+  hevi4_block<S, DIV, STH, BUY>(m, a, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y);
+}
+
+// Every member of an ensemble in one launch: block b belongs to the member
+// whose first_block is the largest not above b (the jobs are in block
+// order), which runs its tile b - first_block (the same 32 x 8 tiles as
+// tile 0's batch).
+template <int S, int DIV, bool STH, bool BUY>
+__global__ void __launch_bounds__(kH4NT, 2) k_hevi4_batch(const HeviJob* __restrict__ jobs, int njobs) {
+  int lo = 0, hi = njobs - 1;
+  const int b = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].first_block <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const HeviJob& job = jobs[lo];
+  const int t = b - job.first_block;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    // the maps were copied into global memory by the host: make that copy
+    // visible to the tensor-map proxy before the first TMA load reads them
+    const CUtensorMap* mp = &job.maps.u;
+    for (int q = 0; q < 8; ++q)
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mp + q) : "memory");
+  }
+  // the member's arguments in shared memory: read every level without
+  // global loads that the kernel's stores could alias
+  __shared__ alignas(16) uint32_t sa_words[sizeof(HeviArgs) / 4];
+  static_assert(sizeof(HeviArgs) % 4 == 0, "HeviArgs is copied as words");
+  const int tid = threadIdx.y * kH4TX + threadIdx.x;
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(&job.args);
+  for (int w = tid; w < (int)(sizeof(HeviArgs) / 4); w += kH4NT) sa_words[w] = src[w];
+  __syncthreads();
+  const HeviArgs& sa = *reinterpret_cast<const HeviArgs*>(sa_words);
+  const int ty_n = (sa.g.nj - 3 + kH4TY - 1) / kH4TY;
+  hevi4_block<S, DIV, STH, BUY>(job.maps, sa, t % job.tiles_x, t / job.tiles_x, job.tiles_x, ty_n);
 }
 
 template <int S, int DIV, bool STH, bool BUY>
@@ -513,7 +562,38 @@ int launch_h4_div(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
   return buy ? launch_h4<S, DIV, false, true>(a, maps, st) : launch_h4<S, DIV, false, false>(a, maps, st);
 }
 
+template <int DIV, bool STH, bool BUY>
+int launch_h4_batch_t(const HeviJob* jobs_d, int njobs, int nblocks, int nk_max, cudaStream_t st) {
+  constexpr int S = 4;
+  using L = H4Layout<S>;
+  const size_t bytes = L::bytes(nk_max) > (size_t)kH4MinSmem ? L::bytes(nk_max) : (size_t)kH4MinSmem;
+  // two blocks per SM, each also holding its member's arguments
+  if (bytes > 113 * 1024 - 64 - sizeof(HeviArgs)) return CRESS_E_UNSUPPORTED;
+  auto kern = k_hevi4_batch<S, DIV, STH, BUY>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+    return CRESS_E_CUDA;
+  kern<<<nblocks, dim3(kH4TX, kH4TY), bytes, st>>>(jobs_d, njobs);
+  return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
+}
+
 }  // namespace
+
+int launch_hevi4_batch(const HeviJob* jobs_d, int njobs, int nblocks, int nk_max, int divopt, bool sth, bool buy,
+                       cudaStream_t st) {
+  if (nk_max > kHevi3MaxNk) return CRESS_E_UNSUPPORTED;
+  auto pick = [&](auto div) -> int {
+    constexpr int D = decltype(div)::value;
+    if (sth) return buy ? launch_h4_batch_t<D, true, true>(jobs_d, njobs, nblocks, nk_max, st)
+                        : launch_h4_batch_t<D, true, false>(jobs_d, njobs, nblocks, nk_max, st);
+    return buy ? launch_h4_batch_t<D, false, true>(jobs_d, njobs, nblocks, nk_max, st)
+               : launch_h4_batch_t<D, false, false>(jobs_d, njobs, nblocks, nk_max, st);
+  };
+  switch (divopt) {
+    case 2: return pick(std::integral_constant<int, 2>{});
+    case 1: return pick(std::integral_constant<int, 1>{});
+    default: return pick(std::integral_constant<int, 0>{});
+  }
+}
 
 int launch_hevi4(const HeviArgs& a, const HeviMaps& maps, cudaStream_t st) {
   if (!a.lvl4 || a.g.nk > kHevi3MaxNk || a.g.nk < 8 || a.g.count() >= (1LL << 31)) return CRESS_E_UNSUPPORTED;

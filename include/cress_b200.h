@@ -321,13 +321,23 @@ int cress_autotune(cress_ctx* ctx, int nsstp, float dts, int reps, int* best_til
  * members' streams by events.  A step whose pointer states and parameters
  * were seen before replays one CUDA graph of the whole ensemble step
  * (cress_ensemble_set_graphs(e, 0) turns that off).  Members need impopt=1
- * and the same divopt, sthopt (zero or not) and buyopt; creating the
- * ensemble sets every member to tile 0.  Members stay valid contexts (sync
- * calls, cress_large_step); destroy the ensemble before its members. */
+ * and the same divopt, sthopt (zero or not) and buyopt.  The shared
+ * acoustic launch runs tile 0's kernel or tile 13's (the FP64 right-hand
+ * sides on chip; every member with 8 <= nk <= 68): tile 13 when every
+ * member was created with tile 13, else tile 0, and the members are set
+ * to the ensemble's tile.  cress_ensemble_set_tile switches it (0 or 13);
+ * cress_ensemble_autotune times both over `reps` loops of nsstp batched
+ * substeps of length dts on the members' present state (only the future
+ * levels are written) and keeps the faster (best_tile, ms_per_substep[2]
+ * for tiles 0 and 13, -1 where unusable; both may be null).  Members stay
+ * valid contexts (sync calls, cress_large_step); destroy the ensemble
+ * before its members. */
 typedef struct cress_ensemble cress_ensemble;
 int cress_ensemble_create(cress_ctx* const* members, int n, cress_ensemble** out);
 void cress_ensemble_destroy(cress_ensemble* e);
 int cress_ensemble_set_graphs(cress_ensemble* e, int on);
+int cress_ensemble_set_tile(cress_ensemble* e, int tile);
+int cress_ensemble_autotune(cress_ensemble* e, int nsstp, float dts, int reps, int* best_tile, float* ms_per_substep);
 int cress_ensemble_large_step(cress_ensemble* e, long long ctime, float dtb, int nsstp, float dts);
 
 /* Replay whole large steps from CUDA graphs (on != 0) instead of launching
