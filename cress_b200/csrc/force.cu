@@ -62,9 +62,9 @@ struct FLayout {
     for (int p = 0; p < nf; ++p) b += 4u * BX * force_slot_rows(SG, p);
     return b;
   }
-  static size_t bytes(int nk) {
-    return 4 * (size_t)S * stage + 8 * (size_t)S;
-  }
+  // ring, mbarriers, then the level table (rows 0..nk, kNF floats each)
+  __host__ __device__ static size_t tab_offset() { return 4 * (size_t)S * stage + 16 * (((size_t)S + 1) / 2); }
+  static size_t bytes(int nk) { return tab_offset() + 4 * (size_t)(nk + 1) * kNF; }
 };
 
 // Slot of group G's field q.  Field numbering per group: u: u, v, w, up,
@@ -91,7 +91,7 @@ __device__ __forceinline__ F2 gld2(const float* p) { return F2{__ldg(reinterpret
 // (advuvw.f90:340-430, advs.f90:312-350, advp.f90:562-600, smoo4*: the
 // 4th-order loops start at i = 2+iwest).
 template <int G, bool T>
-__device__ __forceinline__ void force_point(const ForceArgs& a, const float* const* stp,
+__device__ __forceinline__ void force_point(const ForceArgs& a, const float* tab, const float* const* stp,
                                             int rowbase, long long id, int k, bool ownB, F2& wb_prev, int edge) {
   constexpr int SG = G <= 2 ? 0 : 1;
   using L = FLayout<SG, T>;
@@ -109,8 +109,8 @@ __device__ __forceinline__ void force_point(const ForceArgs& a, const float* con
   // advopt=3: 4th-order vertical advection on the levels 3..nk-3 (w: 3..nk-2)
   const bool adv3 = a.advopt == 3 && k >= 3 && k <= (G == 2 ? nk - 2 : nk - 3);
   const float g05 = .5f * 9.8f;
-  const float* ck = a.lvl + k * kNF;
-  auto C = [&](int f, int kk) { return __ldg(ck + (kk - k) * kNF + f); };
+  const float* ck = tab + k * kNF;   // the level table in shared memory
+  auto C = [&](int f, int kk) { return ck[(kk - k) * kNF + f]; };
   // field q of this group at the offset (dx, dy, dz), both points
   auto X = [&](int q, int dx, int dy, int dz) {
     const int s = force_slot(G, q);
@@ -423,6 +423,14 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
   extern __shared__ __align__(1024) float fsmem[];
   float* ring = fsmem;
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + S * L::stage);
+  // the level table in shared memory (one shared load per constant)
+  float* tab = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(fsmem) + L::tab_offset());
+  {
+    const float4* src = reinterpret_cast<const float4*>(a.lvl);
+    float4* dst = reinterpret_cast<float4*>(tab);
+    const int nv = (nk + 1) * kNF / 4, nt = kFPairs * TY * L::ngroups;
+    for (int v = tid; v < nv; v += nt) dst[v] = __ldg(src + v);
+  }
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -470,12 +478,12 @@ k_force(const __grid_constant__ ForceMaps m, const ForceArgs a) {
     }
     if ((ownA || ownB) && !fail && k <= kmaxg) {
       if constexpr (SG == 0) {
-        if (gz == 0) force_point<0, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
-        else if (gz == 1) force_point<1, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
-        else force_point<2, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
+        if (gz == 0) force_point<0, T>(a, tab, stp, rowbase, id, k, ownB, wb_prev, edge);
+        else if (gz == 1) force_point<1, T>(a, tab, stp, rowbase, id, k, ownB, wb_prev, edge);
+        else force_point<2, T>(a, tab, stp, rowbase, id, k, ownB, wb_prev, edge);
       } else {
-        if (gz == 0) force_point<3, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
-        else force_point<4, T>(a, stp, rowbase, id, k, ownB, wb_prev, edge);
+        if (gz == 0) force_point<3, T>(a, tab, stp, rowbase, id, k, ownB, wb_prev, edge);
+        else force_point<4, T>(a, tab, stp, rowbase, id, k, ownB, wb_prev, edge);
       }
     }
 #pragma unroll

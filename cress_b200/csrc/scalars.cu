@@ -54,7 +54,9 @@ struct ScLayout {
   static constexpr uint32_t tx_bytes =
       4u * BX * (kScGroup * 2 * R::s + R::u + R::v + R::w + (TURB ? R::r : 0));
   static constexpr int NF = kLevelStride;   // stride of the level table
-  __host__ __device__ static size_t bytes(int) { return 4 * (size_t)S * stage + 8 * (size_t)S; }
+  // ring, mbarriers, then the level table (rows 0..nk, NF floats each)
+  __host__ __device__ static size_t tab_offset() { return 4 * (size_t)S * stage + 16 * (((size_t)S + 1) / 2); }
+  __host__ __device__ static size_t bytes(int nk) { return tab_offset() + 4 * (size_t)(nk + 1) * NF; }
 };
 
 // Threads: 16 x 8 x 3; thread (tx, ty, tz) owns the pair of columns
@@ -85,6 +87,15 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
   extern __shared__ __align__(1024) float smem[];
   float* ring = smem;
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + S * L::stage);
+  // the level table in shared memory: every per-level constant below is one
+  // shared load at a fixed offset from the level's row
+  float* tab = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(smem) + L::tab_offset());
+  {
+    const float4* src = reinterpret_cast<const float4*>(a.lvl);
+    float4* dst = reinterpret_cast<float4*>(tab);
+    const int nv = (nk + 1) * L::NF / 4, nt = kScPairs * TY * kScGroup;
+    for (int v = tid; v < nv; v += nt) dst[v] = __ldg(src + v);
+  }
   if (tid == 0) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
@@ -149,8 +160,8 @@ k_scalars(const __grid_constant__ MoistMaps m, const MoistScalarArgs a) {
       issue(k + S - 3);
     }
     if ((ownA || ownB) && !fail) {
-      const float* ck = a.lvl + k * L::NF;
-      auto C = [&](int f, int kk) { return __ldg(ck + (kk - k) * L::NF + f); };
+      const float* ck = tab + k * L::NF;
+      auto C = [&](int f, int kk) { return ck[(kk - k) * L::NF + f]; };
       auto st = [&](int d) { return stp[d + 2]; };
       const float* st0 = st(0);
       const float* S0 = st0 + L::oS + oS;
