@@ -566,6 +566,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     TurbArgs t{};
     t.g = g;
     t.col = col_d;
+    t.lvl = f.lvl;
     t.up = lev[CRESS_U][P]; t.vp = lev[CRESS_V][P]; t.wp = lev[CRESS_W][P];
     t.ptpp = lev[CRESS_PTP][P]; t.ppp = lev[CRESS_PP][P];
     if (moist) {

@@ -119,6 +119,7 @@ int launch_force(const ForceArgs& a, const ForceMaps& maps, cudaStream_t st);
 struct TurbArgs {
   Grid g;
   const float* col;
+  const float* lvl;           // a level table (rows 0..nk, kLevelStride floats; its dtb is not used)
   const float *up, *vp, *wp, *ptpp, *ppp;                  // t-dt
   const float *qvp, *qcp, *qrp, *qip, *qsp, *qgp;          // t-dt moist species (null: dry)
   float* rkv;

@@ -40,19 +40,41 @@ constexpr float kLv0 = 2.50078e6f, kLf0 = 3.34e5f, kT0 = 273.16f, kCwmci = 4.218
 // saturated and virtual forms, which cost five exp/log each) is formed
 // once and serves N^2 at the w levels below and above it, and the z-x /
 // z-y deformation components at the upper faces of level k are kept for
-// the lower faces of level k+1.
+// the lower faces of level k+1.  The block first copies the level table
+// into shared memory (the columns and the reciprocals defomten and bruntv
+// divide by, one shared load each) and forms the per-level length scales
+// (ds3 jcb)^(1/3) and (ds308 jcb)^(1/3) once per level instead of once per
+// point.
+constexpr int kTurbThreads = 128;
+
 template <bool TKE>
-__global__ void __launch_bounds__(128) k_turb_visc(const TurbArgs a) {
+__global__ void __launch_bounds__(kTurbThreads) k_turb_visc(const TurbArgs a) {
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  extern __shared__ __align__(16) float tsm[];
+  float* tab = tsm;                                   // rows 0..nk of the level table
+  float* lnk = tab + (nk + 1) * kLevelStride;         // (ds3 jcb)^(1/3) per level
+  float* ldk = lnk + (nk + 1);                        // (ds308 jcb)^(1/3) per level (TKE)
+  const float oned3 = 1.f / 3.f;
+  {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const float4* src = reinterpret_cast<const float4*>(a.lvl);
+    float4* dst = reinterpret_cast<float4*>(tab);
+    const int nv = (nk + 1) * kLevelStride / 4;
+    for (int v = tid; v < nv; v += kTurbThreads) dst[v] = __ldg(src + v);
+    for (int kk = tid; kk <= nk; kk += kTurbThreads) {
+      const float jcb = __ldg(a.lvl + kk * kLevelStride + C_JCB);
+      lnk[kk] = expf(oned3 * logf(a.ds3 * jcb));
+      if constexpr (TKE) ldk[kk] = expf(oned3 * logf(a.ds308 * jcb));
+    }
+  }
+  __syncthreads();
   if (i > ni - 1 || j > nj - 1) return;
   const long long px = g.px, pl = g.plane;
   const long long id0 = g.at(i, j, 1);
-  const int nc = nk + 1;
-  auto B = [&](int f, int kk) { return __ldg(a.col + f * nc + kk); };
-  auto C = [&](int f, int kk) { return level_value(f, kk, B, 0.f); };
+  auto C = [&](int f, int kk) { return tab[kk * kLevelStride + f]; };
   const float gdzv = 9.8f * a.dziv, gdzv05 = .5f * 9.8f * a.dziv;
   const bool moist = a.qvp != nullptr;
 
@@ -88,7 +110,6 @@ __global__ void __launch_bounds__(128) k_turb_visc(const TurbArgs a) {
 
   Lev lc = lev(2);   // the upper level of the last N^2 formed
   float nq = 0.f, c31_0 = 0.f, c31_1 = 0.f, c32_0 = 0.f, c32_1 = 0.f;
-  const float oned3 = 1.f / 3.f;
   for (int k = 1; k <= nk - 1; ++k) {
     const long long id = id0 + (long long)(k - 1) * pl;
     auto U = [&](int x, int y, int z) { return __ldg(a.up + id + x + y * px + z * pl); };
@@ -126,7 +147,7 @@ __global__ void __launch_bounds__(128) k_turb_visc(const TurbArgs a) {
     const float ssq =
         .5f * (s33 * s33 + (s11 * s11 + s22 * s22)) + .0625f * (s128s * s128s + (s318s * s318s + s328s * s328s));
     if constexpr (!TKE) {
-      const float ln = expf(oned3 * logf(a.ds3 * C(C_JCB, k)));
+      const float ln = lnk[k];   // (ds3 jcb)^(1/3)
       const float ln2 = ln * ln;
       float kv = (.21f * .21f) * ln2 * sqrtf(fmaxf(ssq - (nk0 + nk1) * a.cpriv, 0.f));
       kv = C(C_RBR, k) * fminf(kv, a.ckmax * ln2);
@@ -134,7 +155,7 @@ __global__ void __launch_bounds__(128) k_turb_visc(const TurbArgs a) {
     } else {
       constexpr float ckm = .1f, ckmin = 1.e-6f, eps = 1.e-20f;   // comphy.f90:341-344, commath.f90:177
       const float jcb = C(C_JCB, k);
-      const float ln0 = expf(oned3 * logf(a.ds3 * jcb));
+      const float ln0 = lnk[k];   // (ds3 jcb)^(1/3)
       const float ln02 = ln0 * ln0;
       const float ns = nk0 + nk1;
       const float e = __ldg(a.tkep + id);
@@ -147,7 +168,7 @@ __global__ void __launch_bounds__(128) k_turb_visc(const TurbArgs a) {
       a.rks[id] = priv * (C(C_IJCB, k) * kv);
       a.nsq[id] = nk0;
       a.shr[id] = jcb * kv * ssq;
-      const float ld = (priv - 1.f) * expf(oned3 * logf(a.ds308 * jcb)) + eps;
+      const float ld = (priv - 1.f) * ldk[k] + eps;   // (ds308 jcb)^(1/3)
       a.dsp[id] = (.37f * priv - .18f) * C(C_RST, k) * e * sqrtf(e) / ld;
     }
   }
@@ -156,13 +177,15 @@ __global__ void __launch_bounds__(128) k_turb_visc(const TurbArgs a) {
 }  // namespace
 
 int launch_turb_visc(const TurbArgs& a, cudaStream_t st) {
-  if (a.g.nk < 4) return CRESS_E_UNSUPPORTED;
-  dim3 b(32, 4, 1);
-  dim3 gr((a.g.ni - 1 + 31) / 32, (a.g.nj - 1 + 3) / 4, 1);
+  if (a.g.nk < 4 || !a.lvl) return CRESS_E_UNSUPPORTED;
+  const size_t bytes = sizeof(float) * ((size_t)(a.g.nk + 1) * kLevelStride + 2 * (size_t)(a.g.nk + 1));
+  if (bytes > 48 * 1024) return CRESS_E_UNSUPPORTED;
+  dim3 b(32, kTurbThreads / 32, 1);
+  dim3 gr((a.g.ni - 1 + 31) / 32, (a.g.nj - 1 + b.y - 1) / b.y, 1);
   if (a.tkep)
-    k_turb_visc<true><<<gr, b, 0, st>>>(a);
+    k_turb_visc<true><<<gr, b, bytes, st>>>(a);
   else
-    k_turb_visc<false><<<gr, b, 0, st>>>(a);
+    k_turb_visc<false><<<gr, b, bytes, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
