@@ -669,7 +669,8 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     if ((rc = launch_rbc_leapfrog(r, stream))) return set_error(rc, "open-boundary scalar launch failed");
     ++launches;
   }
-  if (moist && (rc = cloudphy(dtb, cfg.thresq))) return rc;
+  // the final adjstni of cloudphy runs inside the moist post kernel below
+  if (moist && (rc = cloudphy(dtb, cfg.thresq, true))) return rc;
   if (filter) {
     FilterArgs t{};
     t.g = g;
@@ -696,6 +697,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
     m.ptpc = lev[CRESS_PTP][N]; m.ppc = lev[CRESS_PP][N];
     m.ptpf = lev[CRESS_PTP][F]; m.ppf = lev[CRESS_PP][F];
     m.filcoe = cfg.filcoe; m.thresq = cfg.thresq; m.filter = filter ? 1 : 0;
+    m.adjstni = 1;
     if ((rc = launch_moist_post(m, stream))) return set_error(rc, "moist filter/adjustment launch failed");
     ++launches;
   }
@@ -745,7 +747,7 @@ int Ctx::large_step(bool filter, float dtb, int nsstp, float dts, int phase) {
 }
 
 // s_cloudphy for cphopt=3 on the device-resident past and future levels.
-int Ctx::cloudphy(float dtb, float thresq) {
+int Ctx::cloudphy(float dtb, float thresq, bool defer_adjstni) {
   if (cfg.cphopt != 3 || !prec_d) return set_error(CRESS_E_STATE, "cress_cloudphy: context is not cphopt=3");
   if (!base_set || !moist_set) return set_error(CRESS_E_STATE, "cress_cloudphy: base state not set");
   MicroArgs m{};
@@ -764,6 +766,7 @@ int Ctx::cloudphy(float dtb, float thresq) {
   m.dtb = 2.f * dtb;        // cloudphy.f90:282
   m.dz = cfg.dz;
   m.thresq = thresq;
+  m.defer_adjstni = defer_adjstni ? 1 : 0;
   int rc;
   if (sampler) {
     // tuples of the plain scheme on this step's state (before it changes)
@@ -795,7 +798,7 @@ int Ctx::cloudphy(float dtb, float thresq) {
   } else {
     rc = launch_cloudphy(m, stream);
   }
-  launches += 4;
+  launches += defer_adjstni ? 3 : 4;
   if (rc) return set_error(rc, "cloudphy launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   return CRESS_OK;
 }

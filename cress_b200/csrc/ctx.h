@@ -106,7 +106,8 @@ struct Ctx {
   float* shr_d = nullptr;
   float* dsp_d = nullptr;
   int* dtp_d = nullptr;    // sedimentation sub-step minimum (float bits)
-  int cloudphy(float dtb, float thresq);
+  // defer_adjstni: leave the final adjstni to the moist post kernel (large step)
+  int cloudphy(float dtb, float thresq, bool defer_adjstni = false);
   // learned microphysics (MLP in place of the process rates) and tuple
   // sampling of the plain scheme for its training
   Mlp* mlp = nullptr;

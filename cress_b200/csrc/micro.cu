@@ -194,8 +194,10 @@ __global__ void __launch_bounds__(256) k_satadjst(const SatArgs a) {
   a.ptp[id] = ptp; a.qv[id] = qv; a.qc[id] = qc; a.qi[id] = qi; a.ni[id] = ni;
 }
 
-// s_timeflt for the moist fields (timeflt.f90:405-520) then s_satadjst on
-// t and t+dt (intgdrv.f90:985-998), interior points, k = 1..nk-1.
+// In a large step: cloudphy's final adjstni on t+dt (coldblk.f90:469; the
+// dry filter that runs in between does not touch these fields), s_timeflt
+// for the moist fields (timeflt.f90:405-520), then s_satadjst on t and
+// t+dt (intgdrv.f90:985-998), interior points, k = 1..nk-1.
 __global__ void __launch_bounds__(256) k_moist_post(const MoistPostArgs a) {
   const Grid g = a.g;
   const int i = col_lo(g) + blockIdx.x * blockDim.x + threadIdx.x;
@@ -204,6 +206,12 @@ __global__ void __launch_bounds__(256) k_moist_post(const MoistPostArgs a) {
   if (i > col_hi(g) || j > g.nj - 2 || k > g.nk - 1) return;
   const long long id = g.at(i, j, k);
   const int nc = g.nk + 1;
+  if (a.adjstni) {   // what k_adjstni does, on the future numbers
+    const float rb = __ldg(a.col + C_RBR * nc + k), rbv = 1.f / rb;
+    float nci = a.f[6][id], ncs = a.f[7][id], ncg = a.f[8][id];
+    adjstni_cell(rb, rbv, a.f[3][id], a.f[4][id], a.f[5][id], nci, ncs, ncg);
+    a.f[6][id] = nci; a.f[7][id] = ncs; a.f[8][id] = ncg;
+  }
   float c[9];
 #pragma unroll
   for (int n = 0; n < 9; ++n) c[n] = a.c[n][id];
@@ -258,11 +266,13 @@ int micro_init_tables() {
   return CRESS_OK;
 }
 
-// s_fallblk for the eight species, then the final adjstni (two launches).
+// s_fallblk for the eight species, then the final adjstni (two launches;
+// one when k_moist_post applies the adjstni).
 static void launch_fall(const MicroArgs& a, cudaStream_t st) {
   dim3 b2(32, 4, 1);
   dim3 gr2((ncols(a.g) + 31) / 32, (a.g.nj - 3 + 3) / 4, 8);
   k_micro_fall<<<gr2, b2, 0, st>>>(a);
+  if (a.defer_adjstni) return;
   dim3 b(32, 8, 1);
   dim3 gr((ncols(a.g) + 31) / 32, (a.g.nj - 3 + 7) / 8, a.g.nk - 1);
   k_adjstni<<<gr, b, 0, st>>>(a);
@@ -366,7 +376,7 @@ int launch_cloudphy_learned(const MicroArgs& a, const float* w, Mlp* m, const Le
     if (cudaGetLastError() != cudaSuccess) return CRESS_E_CUDA;
   }
   launch_fall(a, st);
-  *launches += 2;
+  *launches += a.defer_adjstni ? 1 : 2;
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 
@@ -405,7 +415,7 @@ int launch_cloudphy_fused(const MicroArgs& a, const float* w, Mlp* m, const Lear
   k_mlp_fused<<<grid, kFusedThreads, kFusedSmem, st>>>(maps, a, p);
   k_micro_src_list<<<nsm * 4, 128, 0, st>>>(a, 0, L.fb_list, L.fb_count, L.chunk);
   launch_fall(a, st);
-  *launches += 5;
+  *launches += a.defer_adjstni ? 4 : 5;
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
 

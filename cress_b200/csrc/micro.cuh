@@ -19,6 +19,7 @@ struct MicroArgs {
   int* dtp_bits;     // domain minimum of the sedimentation step (float bits, positive)
   float dtb;         // microphysics step = 2*dtb of the leapfrog (cloudphy.f90:282)
   float dz, thresq;
+  int defer_adjstni; // 1: the final adjstni is left to k_moist_post (large step)
 };
 
 // Koenig table upload (once per device); returns a CRESS status.
@@ -51,6 +52,7 @@ struct MoistPostArgs {
   float* ptpf; const float* ppf;   // theta', p' at t+dt
   float filcoe, thresq;
   int filter;
+  int adjstni;          // 1: apply cloudphy's final adjstni to t+dt first (coldblk.f90:469)
 };
 int launch_moist_post(const MoistPostArgs& a, cudaStream_t st);
 
