@@ -48,9 +48,10 @@ __device__ __forceinline__ int wrap(int x, int n) {
 
 // Threads run over the frame of possible ghost points only: the rows
 // j in {0, 1, nj-1, nj, nj+1} (all i) and the columns i in {0, 1, ni-1, ni,
-// ni+1} (j = 2..nj-2), one level per blockIdx.y; per field the staggering
-// decides which of them are ghosts.  Sources are never ghosts, so the
-// order of the copies does not matter.
+// ni+1} (j = 2..nj-2), one level per blockIdx.y and one field per
+// blockIdx.z (every copy its own thread, so none waits behind another's
+// store); the field's staggering decides which points are ghosts.
+// Sources are never ghosts, so the order of the copies does not matter.
 __global__ void __launch_bounds__(128) k_halo(const HaloArgs a) {
   const Grid g = a.g;
   const int ni = g.ni, nj = g.nj;
@@ -69,20 +70,19 @@ __global__ void __launch_bounds__(128) k_halo(const HaloArgs a) {
     j = 2 + c % (nj - 3);
     i = q < 2 ? q : ni - 1 + (q - 2);
   }
-  for (int n = 0; n < a.n; ++n) {
-    const int st = a.stag[n];
-    // open x: only the y wrap (over every column, boundary columns included)
-    const bool gx = !g.openx && ((st == STAG_U) ? (i <= 1 || i >= ni) : (i <= 1 || (i >= ni - 1 && i <= ni)));
-    // a y slab: the neighbours' rows fill the y ghosts (slab.h)
-    const bool gy = !g.slaby && ((st == STAG_V) ? (j <= 1 || j >= nj) : (j <= 1 || (j >= nj - 1 && j <= nj)));
-    const bool inx = (st == STAG_U) ? (i <= ni + 1) : (i <= ni);
-    const bool iny = (st == STAG_V) ? (j <= nj + 1) : (j <= nj);
-    if (!(gx || gy) || !inx || !iny) continue;
-    const int si = gx ? wrap(i, ni) : i;
-    const int sj = gy ? wrap(j, nj) : j;
-    float* f = a.f[n];
-    f[g.at(i, j, k)] = f[g.at(si, sj, k)];
-  }
+  const int n = blockIdx.z;
+  const int st = a.stag[n];
+  // open x: only the y wrap (over every column, boundary columns included)
+  const bool gx = !g.openx && ((st == STAG_U) ? (i <= 1 || i >= ni) : (i <= 1 || (i >= ni - 1 && i <= ni)));
+  // a y slab: the neighbours' rows fill the y ghosts (slab.h)
+  const bool gy = !g.slaby && ((st == STAG_V) ? (j <= 1 || j >= nj) : (j <= 1 || (j >= nj - 1 && j <= nj)));
+  const bool inx = (st == STAG_U) ? (i <= ni + 1) : (i <= ni);
+  const bool iny = (st == STAG_V) ? (j <= nj + 1) : (j <= nj);
+  if (!(gx || gy) || !inx || !iny) return;
+  const int si = gx ? wrap(i, ni) : i;
+  const int sj = gy ? wrap(j, nj) : j;
+  float* f = a.f[n];
+  f[g.at(i, j, k)] = f[g.at(si, sj, k)];
 }
 
 // One thread per element, 4 elements per thread along x; rows in blockIdx.y
@@ -114,7 +114,8 @@ int launch_timeflt(const FilterArgs& a, cudaStream_t st) {
 
 int launch_halo(const HaloArgs& a, cudaStream_t st) {
   const int frame = 5 * (a.g.ni + 2) + 5 * (a.g.nj - 3);
-  dim3 gr((frame + 127) / 128, a.g.nk, 1);
+  if (a.n < 1) return CRESS_OK;
+  dim3 gr((frame + 127) / 128, a.g.nk, a.n);
   k_halo<<<gr, 128, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : CRESS_E_CUDA;
 }
