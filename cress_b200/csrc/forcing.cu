@@ -22,17 +22,26 @@ __global__ void __launch_bounds__(256) k_timeflt(const FilterArgs a) {
   const long long id = g.at(i, j, k);
   const float fc = a.filcoe, m1fc2 = 1.f - 2.f * a.filcoe;
   const bool si = i <= col_hi(g), sj = j <= g.nj - 2;
-  if (k <= g.nk - 1) {
-    if (sj) a.u[id] = m1fc2 * a.u[id] + fc * (a.uf[id] + a.up[id]);
-    if (si) a.v[id] = m1fc2 * a.v[id] + fc * (a.vf[id] + a.vp[id]);
-    if (si && sj) {
-      a.pp[id] = m1fc2 * a.pp[id] + fc * (a.ppf[id] + a.ppp[id]);
-      a.ptp[id] = m1fc2 * a.ptp[id] + fc * (a.ptpf[id] + a.ptpp[id]);
-      if (a.tke)   // timeflt.f90:866-884: twice the coefficient for the TKE
-        a.tke[id] = (1.f - 4.f * a.filcoe) * a.tke[id] + (2.f * a.filcoe) * (a.tkef[id] + a.tkep[id]);
-    }
+  const bool lk = k <= g.nk - 1;
+  // every load before the first store (the compiler cannot tell the fields
+  // apart), so a thread's loads are all in flight at once
+  const bool du = lk && sj, dv = lk && si, ds = lk && si && sj, dw = si && sj, dt = ds && a.tke;
+  float u0 = 0.f, u1 = 0.f, u2 = 0.f, v0 = 0.f, v1 = 0.f, v2 = 0.f, p0 = 0.f, p1 = 0.f, p2 = 0.f;
+  float t0 = 0.f, t1 = 0.f, t2 = 0.f, w0 = 0.f, w1 = 0.f, w2 = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f;
+  if (du) { u0 = a.u[id]; u1 = a.uf[id]; u2 = a.up[id]; }
+  if (dv) { v0 = a.v[id]; v1 = a.vf[id]; v2 = a.vp[id]; }
+  if (ds) { p0 = a.pp[id]; p1 = a.ppf[id]; p2 = a.ppp[id]; t0 = a.ptp[id]; t1 = a.ptpf[id]; t2 = a.ptpp[id]; }
+  if (dt) { e0 = a.tke[id]; e1 = a.tkef[id]; e2 = a.tkep[id]; }
+  if (dw) { w0 = a.w[id]; w1 = a.wf[id]; w2 = a.wp[id]; }
+  if (du) a.u[id] = m1fc2 * u0 + fc * (u1 + u2);
+  if (dv) a.v[id] = m1fc2 * v0 + fc * (v1 + v2);
+  if (ds) {
+    a.pp[id] = m1fc2 * p0 + fc * (p1 + p2);
+    a.ptp[id] = m1fc2 * t0 + fc * (t1 + t2);
   }
-  if (si && sj) a.w[id] = m1fc2 * a.w[id] + fc * (a.wf[id] + a.wp[id]);
+  if (dt)   // timeflt.f90:866-884: twice the coefficient for the TKE
+    a.tke[id] = (1.f - 4.f * a.filcoe) * e0 + (2.f * a.filcoe) * (e1 + e2);
+  if (dw) a.w[id] = m1fc2 * w0 + fc * (w1 + w2);
 }
 
 // Both periodic ghost layers (bcycle.f90:159-225 with the stepper and the

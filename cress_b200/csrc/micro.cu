@@ -206,37 +206,43 @@ __global__ void __launch_bounds__(256) k_moist_post(const MoistPostArgs a) {
   if (i > col_hi(g) || j > g.nj - 2 || k > g.nk - 1) return;
   const long long id = g.at(i, j, k);
   const int nc = g.nk + 1;
+  // every load before the first store, so they are all in flight at once
+  // (the stores could alias them as far as the compiler knows)
+  float c[9], fv[9], pv[9];
+#pragma unroll
+  for (int n = 0; n < 9; ++n) {
+    c[n] = a.c[n][id];
+    fv[n] = a.f[n][id];
+    if (a.filter) pv[n] = __ldg(a.p[n] + id);
+  }
+  const float ppc = a.ppc[id], ptpc = a.ptpc[id], ppf = a.ppf[id], ptpf = a.ptpf[id];
   if (a.adjstni) {   // what k_adjstni does, on the future numbers
     const float rb = __ldg(a.col + C_RBR * nc + k), rbv = 1.f / rb;
-    float nci = a.f[6][id], ncs = a.f[7][id], ncg = a.f[8][id];
-    adjstni_cell(rb, rbv, a.f[3][id], a.f[4][id], a.f[5][id], nci, ncs, ncg);
-    a.f[6][id] = nci; a.f[7][id] = ncs; a.f[8][id] = ncg;
+    adjstni_cell(rb, rbv, fv[3], fv[4], fv[5], fv[6], fv[7], fv[8]);
+    a.f[6][id] = fv[6]; a.f[7][id] = fv[7]; a.f[8][id] = fv[8];
   }
-  float c[9];
-#pragma unroll
-  for (int n = 0; n < 9; ++n) c[n] = a.c[n][id];
   if (a.filter) {
     const float fc = a.filcoe, m1fc2 = 1.f - 2.f * a.filcoe;
 #pragma unroll
     for (int n = 0; n < 9; ++n) {
-      c[n] = m1fc2 * c[n] + fc * (a.f[n][id] + __ldg(a.p[n] + id));
+      c[n] = m1fc2 * c[n] + fc * (fv[n] + pv[n]);
       if (n != 0 && n != 1 && n != 3 && n != 6) a.c[n][id] = c[n];
     }
   }
   const float rddvcp = 287.f / 1004.f, p0iv = 1.f / 1.e5f;
   const float pbr = __ldg(a.col + C_PBR * nc + k), ptbr = __ldg(a.col + C_PTBR * nc + k);
   {
-    const float p = pbr + a.ppc[id];                                    // getexner.f90:129
+    const float p = pbr + ppc;                                          // getexner.f90:129
     const float pi = expf(rddvcp * logf(p0iv * p));
-    float ptp = a.ptpc[id];
+    float ptp = ptpc;
     satadjst_cell(a.thresq, ptbr, pi, p, ptp, c[0], c[1], c[3], c[6]);
     a.ptpc[id] = ptp;
     a.c[0][id] = c[0]; a.c[1][id] = c[1]; a.c[3][id] = c[3]; a.c[6][id] = c[6];
   }
   {
-    const float p = pbr + a.ppf[id];
+    const float p = pbr + ppf;
     const float pi = expf(rddvcp * logf(p0iv * p));
-    float ptp = a.ptpf[id], qv = a.f[0][id], qc = a.f[1][id], qi = a.f[3][id], ni = a.f[6][id];
+    float ptp = ptpf, qv = fv[0], qc = fv[1], qi = fv[3], ni = fv[6];
     satadjst_cell(a.thresq, ptbr, pi, p, ptp, qv, qc, qi, ni);
     a.ptpf[id] = ptp;
     a.f[0][id] = qv; a.f[1][id] = qc; a.f[3][id] = qi; a.f[6][id] = ni;
