@@ -23,12 +23,18 @@ among the checked fields.
 Per-field tolerance (stated here, checked on every field): the GPU's RMS
 difference from the FP64 build, relative to the field's FP64 RMS, must be
 within K times the FP32 oracle's own spread from FP64 plus a floor:
-    gpu_rms_rel <= K * fp32_rms_rel + FLOOR
+    gpu_rms_rel <= K * spread + FLOOR
 with K = 3 for the dry bubble (a smooth flow: both FP32 builds round
 differently but neither diverges) and K = 4 for the moist runs (moist
 convection amplifies round-off over hours, so two FP32 builds drift apart
 by amounts of the order of their distance from FP64), FLOOR = 1e-6
-(fields that stay near zero).  Budgets: the total-water and mass drifts
+(fields that stay near zero).  For the dry bubble the spread is the FP32
+oracle's distance from FP64; for the moist runs it is the larger of that
+and the distance of a second FP32 oracle run, started from theta' one ulp
+up: after hours of convection one FP32 run is a single sample of the
+chaotic growth of round-off, and in the C2 supercell the ice number of
+one FP32 run stayed at 0.19 of its RMS from FP64 while the run one ulp
+away reached 0.70 (the two FP32 runs 0.79 apart).  Budgets: the total-water and mass drifts
 over the run (relative to the initial totals) must match the FP64 build's
 within 3 times the FP32 build's own drift difference plus 1e-5, and the
 accumulated surface precipitation within 5% of the FP64 build's.  Each
@@ -54,8 +60,9 @@ def _check_fields(rep, k, floor=1e-6):
     bad = []
     for n, f in rep["fields"].items():
         assert f["finite"], n
-        if f["gpu_rms_rel"] > k * f["fp32_rms_rel"] + floor:
-            bad.append((n, f["gpu_rms_rel"], f["fp32_rms_rel"]))
+        spread = max(f["fp32_rms_rel"], f.get("fp32p_rms_rel", 0.0))
+        if f["gpu_rms_rel"] > k * spread + floor:
+            bad.append((n, f["gpu_rms_rel"], f["fp32_rms_rel"], f.get("fp32p_rms_rel")))
     assert not bad, bad
 
 
