@@ -144,11 +144,31 @@ __device__ inline void srcblk_cell(R dtb, R thresq, MCell& c) {
   const R cvntg = R(.31) * sqrtf(R(MP::aug)) * expf(oned3 * logf(R(MP::sc))) * R(MP::gf5bug);
   const R t = (c.ptbr + c.ptpp) * c.pi;
   const R tcel = t - t0;
-  const R esw = R(MP::es0) * expf(R(17.269) * tcel / (t - R(35.86)));
   const R esi = R(MP::es0) * expf(R(21.875) * tcel / (t - R(7.66)));
+  const R qvsi = R(MP::epsva) * esi / (p - esi);
+  // Clear air: no hydrometeor above thresq at t-dt and no ice nucleation
+  // from vapour (s_nuc1stv's condition below does not hold).  Every process
+  // rate that follows is then exactly zero (each is guarded by one of those
+  // conditions), and s_newblk reduces to subtracting or adding zero sinks
+  // and its clipping at zero; with no negative future mixing ratio for its
+  // sink cascade to act on, that is all that happens to the cell.
+  if (!(qc > thresq) && !(qr > thresq) && !(qi > thresq) && !(qs > thresq) && !(qg > thresq) &&
+      !(qv > thresq && qv > qvsi && t > tlow && t < t0) && c.qrf >= R(0) && c.qcf >= R(0) && c.qif >= R(0)) {
+    c.ptpf = c.ptpf + R(0);
+    c.qrf = c.qrf - R(0);
+    c.qcf = c.qcf - R(0);
+    c.qif = c.qif - R(0);
+    c.qvf = fmaxf(c.qvf - R(0), R(0));
+    c.qsf = fmaxf(c.qsf - R(0), R(0));
+    c.qgf = fmaxf(c.qgf + R(0), R(0));
+    c.ncif = c.ncif + R(0);
+    c.ncsf = c.ncsf + R(0);
+    c.ncgf = c.ncgf + R(0);
+    return;
+  }
+  const R esw = R(MP::es0) * expf(R(17.269) * tcel / (t - R(35.86)));
   const R qvsst0 = qv - epses0 / (p - R(MP::es0));
   const R qvsw = R(MP::epsva) * esw / (p - esw);
-  const R qvsi = R(MP::epsva) * esi / (p - esi);
   const R lv = R(MP::lv0) * expf((R(.167) + R(3.67e-4) * t) * logf(t0 / t));
   const R lf = R(MP::lf0) + cwmci * tcel;
   const R ls = lv + lf;
